@@ -1,0 +1,175 @@
+/*
+ * fwix_b200.h -- C ABI of the B200 (sm_100a) one-way wave-equation depth-stepping
+ * library (libfwix_b200.so).
+ *
+ * Conventions
+ *   - Every array argument is a DEVICE pointer owned by the caller, except the
+ *     host arrays that fwix_traces_create copies.  Complex values are interleaved
+ *     float pairs (complex64).  Layouts are row-major with x fastest:
+ *       wavefield  [ns][nw][NY][NX]        NX = nx + padx, NY = ny + pady
+ *       model      [nz][nw][ny][nx]        (s^2 = 1/v^2, density), strides given
+ *       labels     uint8, [nz][nw][NY][NX] with caller strides (w stride may be 0)
+ *       refs       [nz][nref][nw]          complex reference s^2
+ *       traces     [ntrace][nw]
+ *   - "add" follows the reference operators: add == 0 overwrites the output,
+ *     add != 0 accumulates into it.
+ *   - Calls are stream ordered on the cudaStream_t passed as `stream` (NULL = the
+ *     legacy default stream) and never synchronise the device.
+ *   - Errors are negative status codes; fwix_last_error() returns the message
+ *     of the last failure on the calling thread.  Nothing calls exit().
+ *   - A plan may be used by one host thread at a time.
+ *   - Wavefield-sized temporaries come from a caller-provided workspace
+ *     (fwix_plan_workspace_bytes / fwix_plan_set_workspace); only small tables
+ *     (wavenumbers, twiddles, trace lists) are allocated by the library, at
+ *     plan / trace-set creation.
+ *
+ * Reference interface each entry point replaces (paths inside pyfwix):
+ *   operator/src/CudaOperator.h:61-72          cu_forward / cu_adjoint(add, m, d)
+ *   operator/src/FFT.cpp:36-69                 cuFFT2d
+ *   propagator/src/PhaseShift.cpp:27-41        PhaseShift fwd / adj / inverse
+ *   propagator/src/Selector.h:38-45            Selector
+ *   propagator/src/Taper.h:30-37               Taper
+ *   propagator/src/PSPI.cpp:6-103              PSPI (add and in-place forms)
+ *   propagator/src/NSPS.cpp:6-45               NSPS
+ *   propagator/src/Injection.cpp:35-44         Injection fwd / adj
+ *   propagator/src/Reflect.cpp:45-62           Reflect
+ *   propagator/src/Scatter.cpp:76-133          Scatter
+ *   propagator/src/ImagingCondition.cpp:33-48  ImagingCondition
+ *   propagator/src/LinReflect.cpp:28-40        LinReflect
+ *   propagator/src/OneWay.cpp:24-79            Downward / Upward
+ *   propagator/src/Propagator.cpp:121-221      Propagator::forward
+ *   propagator/src/ExtendedBorn.cpp:80-150     ExtendedBorn::forward / adjoint
+ */
+#ifndef FWIX_B200_H
+#define FWIX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fwix_status {
+  FWIX_OK = 0,
+  FWIX_ERR_INVALID = -1,     /* bad argument or descriptor                     */
+  FWIX_ERR_UNSUPPORTED = -2, /* size or option outside what the kernels cover  */
+  FWIX_ERR_CUDA = -3,        /* CUDA runtime error                             */
+  FWIX_ERR_STATE = -4,       /* refs / model / workspace not bound yet         */
+  FWIX_ERR_WORKSPACE = -5    /* workspace smaller than required                */
+} fwix_status;
+
+/* Depth-step kinds (the reference's OneWay always uses PSPI,
+ * propagator/src/OneWay.h:24-25). */
+enum { FWIX_STEP_PSPI = 0, FWIX_STEP_NSPS = 1 };
+
+/* Directions of a depth step.
+ *   FWD      : out (+)= sum_r mask_r F^-1(P_r F(taper in))       PSPI.cpp:6-24 / :66-83
+ *   ADJ_ADD  : out (+)= F^-1(sum_r P_r^* F(mask_r in))           PSPI.cpp:26-44 (no taper)
+ *   ADJ_INPL : out (+)= taper F^-1(sum_r P_r^* F(mask_r in))     PSPI.cpp:85-103
+ * For NSPS the taper never applies (NSPS.cpp:6-45). */
+enum { FWIX_FWD = 0, FWIX_ADJ_ADD = 1, FWIX_ADJ_INPL = 2 };
+
+/* PhaseShift modes (phase_shift.cu:7-61, :125-184, :248-305). */
+enum { FWIX_PS_FWD = 0, FWIX_PS_ADJ = 1, FWIX_PS_INV = 2 };
+
+/* Workspace classes for fwix_plan_workspace_bytes. */
+enum { FWIX_WS_STEP = 0, FWIX_WS_SWEEP = 1, FWIX_WS_BORN = 2 };
+
+typedef struct fwix_desc {
+  int nx, ny;        /* model lateral size                                   */
+  int padx, pady;    /* wavefield = (nx + padx) x (ny + pady)                 */
+  int nw;            /* frequencies                                           */
+  int ns;            /* shots in the wavefield batch                          */
+  int nz;            /* depth levels                                          */
+  float ox, oy, oz;  /* origins [m]                                           */
+  float dx, dy, dz;  /* sampling [m]                                          */
+  float ow, dw;      /* first frequency and step [Hz]                         */
+  int nref;          /* reference slownesses per depth ("nref")               */
+  float eps;         /* phase-shift damping ("eps")                           */
+  int taperx, tapery;/* lateral taper widths ("taperx", "tapery")             */
+  float eps_scat;    /* Born damping ("eps_scat", default 0.04)               */
+  int taylor;        /* Born Taylor order ("taylor", default 1, max 4)        */
+  int step_kind;     /* FWIX_STEP_PSPI or FWIX_STEP_NSPS for the sweeps       */
+} fwix_desc;
+
+typedef struct fwix_plan fwix_plan;
+typedef struct fwix_traces fwix_traces;
+
+const char* fwix_last_error(void);
+int fwix_version(void);
+
+/* ---- plan ------------------------------------------------------------------ */
+fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** plan);
+fwix_status fwix_plan_destroy(fwix_plan* plan);
+size_t fwix_plan_workspace_bytes(const fwix_plan* plan, int ws_class);
+fwix_status fwix_plan_set_workspace(fwix_plan* plan, void* dev_ptr, size_t bytes);
+/* sref: [nz][nref][nw] complex; labels: uint8 label of (iz, iw, y, x) at
+ * labels[iz*z_stride + iw*w_stride + y*NX + x] (RefSampler.cpp:27-28, 126-133). */
+fwix_status fwix_plan_set_refs(fwix_plan* plan, const void* sref, const uint8_t* labels,
+                               int64_t labels_z_stride, int64_t labels_w_stride);
+/* Background s^2 and density, element (iz,iw,y,x) at
+ * p[iz*z_stride + iw*w_stride + y*nx + x] (Reflect.h:20-38, Scatter.cpp:68-74). */
+fwix_status fwix_plan_set_model(fwix_plan* plan, const void* slow, const void* den,
+                                int64_t z_stride, int64_t w_stride);
+
+/* ---- one-slice operators (device -> device) --------------------------------- */
+/* Unitary 2D FFT, forward e^{-i} or inverse e^{+i}, x 1/sqrt(NX*NY). */
+fwix_status fwix_fft2d(fwix_plan* plan, int inverse, const void* in, void* out, int add, void* stream);
+/* Phase shift in the wavenumber domain with per-frequency reference s^2 sref_w[nw]. */
+fwix_status fwix_phase_shift(fwix_plan* plan, int mode, const void* sref_w, const void* in,
+                             void* out, int add, void* stream);
+fwix_status fwix_select(fwix_plan* plan, int iz, int value, const void* in, void* out, int add,
+                        void* stream);
+fwix_status fwix_taper(fwix_plan* plan, const void* in, void* out, int add, void* stream);
+/* One depth step at level iz; in may equal out. */
+fwix_status fwix_step(fwix_plan* plan, int kind, int iz, int dir, const void* in, void* out,
+                      int add, void* stream);
+/* Born scattering at level iz (adjoint != 0 for the transpose). */
+fwix_status fwix_scatter(fwix_plan* plan, int iz, int adjoint, const void* in, void* out, int add,
+                         void* stream);
+/* Reflection at level iz: fwd up (+)= r down, adj down (+)= conj(r) up. */
+fwix_status fwix_reflect(fwix_plan* plan, int iz, int adjoint, const void* in, void* out, int add,
+                         void* stream);
+/* Imaging condition: fwd wfld (+)= bg * image; adj image (+)= sum_s conj(bg) wfld.
+ * image is [nw][ny][nx]. */
+fwix_status fwix_imaging(fwix_plan* plan, int adjoint, const void* bg, void* image, void* wfld,
+                         int add, void* stream);
+/* Linearised reflection at level iz: dmodel [4][nw][ny][nx] = (ds2(iz), ds2(iz+1),
+ * drho(iz), drho(iz+1)) <-> dr [nw][ny][nx]. */
+fwix_status fwix_lin_reflect(fwix_plan* plan, int iz, int adjoint, void* dmodel, void* dr, int add,
+                             void* stream);
+
+/* ---- acquisition ------------------------------------------------------------ */
+/* Host coordinate arrays; ids are dense shot indices in [0, ns). */
+fwix_status fwix_traces_create(fwix_plan* plan, int ntrace, const float* cx, const float* cy,
+                               const float* cz, const int32_t* ids, fwix_traces** out);
+fwix_status fwix_traces_destroy(fwix_traces* tr);
+/* adjoint == 0: wfld (+)= inject(traces) at level iz (inj_forward);
+ * adjoint != 0: traces (+)= record(wfld) (inj_adjoint). */
+fwix_status fwix_inject(fwix_plan* plan, const fwix_traces* tr, int iz, int adjoint, void* traces,
+                        void* wfld, int add, void* stream);
+
+/* ---- depth sweeps ------------------------------------------------------------ */
+/* Downward / Upward continuation in place over all nz levels. */
+fwix_status fwix_downward(fwix_plan* plan, int adjoint, void* wfld, void* stream);
+fwix_status fwix_upward(fwix_plan* plan, int adjoint, void* wfld, void* stream);
+/* Nonlinear modelling wavelet -> data.  bg_down / bg_up: [nz] wavefields (may be
+ * NULL when the Born operators are not needed). */
+fwix_status fwix_propagate(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
+                           const void* wavelet, void* data, int add, void* bg_down, void* bg_up,
+                           void* stream);
+/* Lockstep migration image[nz][ny][nx] (float) (+)= sum_w Re sum_s conj(S) R. */
+fwix_status fwix_migrate(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
+                         const void* wavelet, const void* data, float* image, int add,
+                         void* stream);
+/* Extended Born: forward (dslow, dden) -> data, adjoint data -> (dslow, dden);
+ * dslow/dden are [nz][nw][ny][nx]. */
+fwix_status fwix_born(fwix_plan* plan, int adjoint, const fwix_traces* rec, const void* bg_down,
+                      const void* bg_up, void* dslow, void* dden, void* data, int add,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FWIX_B200_H */

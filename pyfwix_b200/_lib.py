@@ -1,0 +1,106 @@
+"""ctypes binding of libfwix_b200.so (the C ABI declared in include/fwix_b200.h).
+
+The library is the product path: if it cannot be loaded the import fails with a
+clear error.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfwix_b200.so")
+
+FWIX_OK = 0
+STATUS = {0: "FWIX_OK", -1: "FWIX_ERR_INVALID", -2: "FWIX_ERR_UNSUPPORTED", -3: "FWIX_ERR_CUDA",
+          -4: "FWIX_ERR_STATE", -5: "FWIX_ERR_WORKSPACE"}
+
+STEP_PSPI, STEP_NSPS = 0, 1
+FWD, ADJ_ADD, ADJ_INPL = 0, 1, 2
+PS_FWD, PS_ADJ, PS_INV = 0, 1, 2
+WS_STEP, WS_SWEEP, WS_BORN = 0, 1, 2
+
+
+class FwixDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("padx", ctypes.c_int), ("pady", ctypes.c_int),
+        ("nw", ctypes.c_int), ("ns", ctypes.c_int), ("nz", ctypes.c_int),
+        ("ox", ctypes.c_float), ("oy", ctypes.c_float), ("oz", ctypes.c_float),
+        ("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float),
+        ("ow", ctypes.c_float), ("dw", ctypes.c_float),
+        ("nref", ctypes.c_int), ("eps", ctypes.c_float),
+        ("taperx", ctypes.c_int), ("tapery", ctypes.c_int),
+        ("eps_scat", ctypes.c_float), ("taylor", ctypes.c_int),
+        ("step_kind", ctypes.c_int),
+    ]
+
+
+P = ctypes.c_void_p
+I = ctypes.c_int
+I64 = ctypes.c_int64
+
+# name -> argtypes (all return fwix_status as int unless listed in _RET)
+SIGNATURES = {
+    "fwix_last_error": [],
+    "fwix_version": [],
+    "fwix_plan_create": [ctypes.POINTER(FwixDesc), ctypes.POINTER(P)],
+    "fwix_plan_destroy": [P],
+    "fwix_plan_workspace_bytes": [P, I],
+    "fwix_plan_set_workspace": [P, P, ctypes.c_size_t],
+    "fwix_plan_set_refs": [P, P, P, I64, I64],
+    "fwix_plan_set_model": [P, P, P, I64, I64],
+    "fwix_fft2d": [P, I, P, P, I, P],
+    "fwix_phase_shift": [P, I, P, P, P, I, P],
+    "fwix_select": [P, I, I, P, P, I, P],
+    "fwix_taper": [P, P, P, I, P],
+    "fwix_step": [P, I, I, I, P, P, I, P],
+    "fwix_scatter": [P, I, I, P, P, I, P],
+    "fwix_reflect": [P, I, I, P, P, I, P],
+    "fwix_imaging": [P, I, P, P, P, I, P],
+    "fwix_lin_reflect": [P, I, I, P, P, I, P],
+    "fwix_traces_create": [P, I, P, P, P, P, ctypes.POINTER(P)],
+    "fwix_traces_destroy": [P],
+    "fwix_inject": [P, P, I, I, P, P, I, P],
+    "fwix_downward": [P, I, P, P],
+    "fwix_upward": [P, I, P, P],
+    "fwix_propagate": [P, P, P, P, P, I, P, P, P],
+    "fwix_migrate": [P, P, P, P, P, P, I, P],
+    "fwix_born": [P, I, P, P, P, P, P, P, I, P],
+}
+_RET = {"fwix_last_error": ctypes.c_char_p, "fwix_version": I, "fwix_plan_workspace_bytes": ctypes.c_size_t}
+
+_lib = None
+
+
+def load():
+    """Load (once) and return the ctypes handle of libfwix_b200.so."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m pyfwix_b200.build` "
+            "(nvcc, sm_100a).  pyfwix_b200 has no CPU fallback.")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RET.get(name, I)
+    _lib = lib
+    return lib
+
+
+class FwixError(RuntimeError):
+    """Raised for a negative fwix_status; carries the status code."""
+
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def check(status):
+    if status != FWIX_OK:
+        msg = load().fwix_last_error()
+        raise FwixError(status, msg.decode() if msg else "")
+    return status

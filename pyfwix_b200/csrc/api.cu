@@ -1,0 +1,827 @@
+// C ABI of libfwix_b200.so: plans, tables, one-slice operators, acquisition and
+// the depth-sweep drivers (Downward / Upward, Propagator::forward, lockstep
+// migration, ExtendedBorn forward / adjoint).  Host control flow only; every
+// numerical operation is a kernel of spectral.cu / pointwise.cu enqueued on the
+// caller's stream.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "fwix_b200.h"
+#include "internal.h"
+
+using fwix::Dims;
+using fwix::SpecArgs;
+
+namespace {
+
+thread_local std::string g_err;
+
+fwix_status fail(fwix_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+#define FWIX_CU(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess)                                                                 \
+      return fail(FWIX_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));      \
+  } while (0)
+
+#define FWIX_TRY(call)              \
+  do {                              \
+    fwix_status _s = (call);        \
+    if (_s != FWIX_OK) return _s;   \
+  } while (0)
+
+bool make_fft_plan(int n, Fft1D* p) {
+  if (n < 1 || n > FWIX_MAX_N) return false;
+  p->n = n;
+  p->npass = 0;
+  int m = n;
+  const int radices[6] = {8, 4, 2, 3, 5, 7};
+  for (int R : radices) {
+    while (m % R == 0) {
+      if (p->npass >= FWIX_MAX_PASS) return false;
+      p->radix[p->npass++] = R;
+      m /= R;
+    }
+  }
+  return m == 1;
+}
+
+// Wavenumber table of propagator/src/PhaseShift.h:47-57, in the same float
+// arithmetic (dk rounded to float, then ik * dk).
+std::vector<float> k_table(int n, float d) {
+  std::vector<float> k(n);
+  const int half = n / 2;
+  const float dk = (float)(2 * M_PI / (double)(d * (float)n));
+  for (int i = 0; i <= half && i < n; ++i) k[i] = (float)i * dk;
+  for (int i = half + 1; i < n; ++i) k[i] = (float)(i - n) * dk;
+  return k;
+}
+
+// Taper weights of propagator/src/taper.cu:46-60.
+std::vector<float> taper_table(int n, int tap) {
+  std::vector<float> w(n, 1.0f);
+  for (int i = 0; i < n; ++i) {
+    if (i < tap && tap > 0)
+      w[i] = 0.5f * (1.0f - cosf((float)(M_PI * i / tap)));
+    else if (i >= n - tap && i < n)
+      w[i] = 0.5f * (1.0f + cosf((float)(M_PI * (i - n + tap) / tap)));
+  }
+  return w;
+}
+
+std::vector<float2> twiddles(int n) {
+  std::vector<float2> t(n);
+  for (int m = 0; m < n; ++m) {
+    const double a = -2.0 * M_PI * (double)m / (double)n;
+    t[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  return t;
+}
+
+template <typename T>
+cudaError_t upload(T** dst, const std::vector<T>& v) {
+  *dst = nullptr;
+  if (v.empty()) return cudaSuccess;
+  cudaError_t e = cudaMalloc((void**)dst, v.size() * sizeof(T));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+
+struct fwix_plan {
+  fwix_desc desc;
+  Dims d;
+  Fft1D px, py;
+  float2 *twx = nullptr, *twy = nullptr;
+  float *kx = nullptr, *ky = nullptr, *w2 = nullptr, *w = nullptr, *tapx = nullptr, *tapy = nullptr;
+  const float2* sref = nullptr;
+  const uint8_t* labels = nullptr;
+  long long lab_z = 0, lab_w = 0;
+  const float2* slow = nullptr;
+  const float2* den = nullptr;
+  long long m_z = 0, m_w = 0;
+  char* ws = nullptr;
+  size_t ws_bytes = 0;
+  int nterm_max = 1;
+  float coef[5] = {1.f, 1.f / 2.f, 3.f / 8.f, 5.f / 16.f, 35.f / 128.f};  // Scatter.h:526
+
+  size_t wbytes() const { return (size_t)d.wfld * sizeof(float2); }
+  size_t ws_need(int cls) const {
+    size_t b = 2 * (size_t)nterm_max * wbytes();  // t1, t2
+    if (cls >= FWIX_WS_SWEEP) b += 3 * wbytes();  // A, B, SC
+    if (cls >= FWIX_WS_BORN) b += (size_t)desc.nz * wbytes();  // per-level field store
+    return b;
+  }
+  float2* t1() const { return (float2*)ws; }
+  float2* t2() const { return (float2*)(ws + (size_t)nterm_max * wbytes()); }
+  float2* wA() const { return (float2*)(ws + 2 * (size_t)nterm_max * wbytes()); }
+  float2* wB() const { return wA() + d.wfld; }
+  float2* wSC() const { return wB() + d.wfld; }
+  float2* store(int iz) const { return wSC() + d.wfld * (long long)(1 + iz); }
+
+  SpecArgs args(const float2* in, float2* out, int add) const {
+    SpecArgs a;
+    memset(&a, 0, sizeof(a));
+    a.d = d;
+    a.px = px;
+    a.py = py;
+    a.twx = twx;
+    a.twy = twy;
+    a.kx = kx;
+    a.ky = ky;
+    a.w2 = w2;
+    a.w = w;
+    a.tapx = tapx;
+    a.tapy = tapy;
+    a.dz = desc.dz;
+    a.eps = desc.eps;
+    a.eps_scat = desc.eps_scat;
+    for (int i = 0; i < 5; ++i) a.coef[i] = coef[i];
+    a.norm = 1.0f / ((float)d.NX * (float)d.NY);
+    a.nterm = 1;
+    a.in = in;
+    a.out = out;
+    a.add = add;
+    a.t1 = t1();
+    a.t2 = t2();
+    return a;
+  }
+};
+
+struct fwix_traces {
+  int ntrace = 0;
+  int nlevel = 0;
+  std::vector<fwix::InjectLevel> level;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+fwix_status need_ws(const fwix_plan* p, int cls) {
+  if (!p->ws) return fail(FWIX_ERR_STATE, "workspace not bound (fwix_plan_set_workspace)");
+  if (p->ws_bytes < p->ws_need(cls))
+    return fail(FWIX_ERR_WORKSPACE, "workspace smaller than fwix_plan_workspace_bytes for this call");
+  return FWIX_OK;
+}
+
+fwix_status need_refs(const fwix_plan* p) {
+  if (!p->sref || !p->labels) return fail(FWIX_ERR_STATE, "reference slownesses not bound (fwix_plan_set_refs)");
+  return FWIX_OK;
+}
+
+fwix_status need_model(const fwix_plan* p) {
+  if (!p->slow || !p->den) return fail(FWIX_ERR_STATE, "background model not bound (fwix_plan_set_model)");
+  return FWIX_OK;
+}
+
+fwix_status check_iz(const fwix_plan* p, int iz) {
+  if (iz < 0 || iz >= p->desc.nz) return fail(FWIX_ERR_INVALID, "depth index out of range");
+  return FWIX_OK;
+}
+
+fwix_status cu(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return fail(FWIX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return FWIX_OK;
+}
+
+// One depth step: PSPI (PSPI.cpp:6-103) or NSPS (NSPS.cpp:6-45).
+fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, float2* out, int add,
+                    cudaStream_t s) {
+  SpecArgs a = p->args(in, out, add);
+  a.sref = p->sref + (long long)iz * p->desc.nref * p->d.nw;
+  a.lab = p->labels + iz * p->lab_z;
+  a.lab_w = p->lab_w;
+  a.nterm = p->desc.nref;
+  if (kind == FWIX_STEP_PSPI) {
+    if (dir == FWIX_FWD) {
+      FWIX_TRY(cu(fwix::row_forward(a, fwix::W_TAPER, s), "pspi row pass"));
+      FWIX_TRY(cu(fwix::col_type_a(a, fwix::Q_PS_FWD, s), "pspi column pass"));
+      FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_MASK, 0, s), "pspi inverse row pass"));
+    } else {
+      FWIX_TRY(cu(fwix::row_forward(a, fwix::W_MASK, s), "pspi adjoint row pass"));
+      FWIX_TRY(cu(fwix::col_type_b(a, fwix::Q_PS_ADJ, s), "pspi adjoint column pass"));
+      FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_ONE, dir == FWIX_ADJ_INPL, s), "pspi adjoint inverse row pass"));
+    }
+  } else {
+    if (dir == FWIX_FWD) {
+      FWIX_TRY(cu(fwix::row_forward(a, fwix::W_MASK, s), "nsps row pass"));
+      FWIX_TRY(cu(fwix::col_type_b(a, fwix::Q_PS_FWD, s), "nsps column pass"));
+      FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_ONE, 0, s), "nsps inverse row pass"));
+    } else {
+      FWIX_TRY(cu(fwix::row_forward(a, fwix::W_ONE, s), "nsps adjoint row pass"));
+      FWIX_TRY(cu(fwix::col_type_a(a, fwix::Q_PS_ADJ, s), "nsps adjoint column pass"));
+      FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_MASK, 0, s), "nsps adjoint inverse row pass"));
+    }
+  }
+  return FWIX_OK;
+}
+
+SpecArgs scatter_args(const fwix_plan* p, int iz, const float2* in, float2* out, int add) {
+  SpecArgs a = p->args(in, out, add);
+  a.slow = p->slow + iz * p->m_z;
+  a.slow_w = p->m_w;
+  a.nterm = p->desc.taylor + 1;
+  return a;
+}
+
+// Scatter::cu_forward / cu_adjoint (Scatter.cpp:76-133).  With image != NULL the
+// forward input is the imaging-condition product bg * image (ImagingCondition fwd,
+// imaging_condition.cu:9-55) formed inside the first pass.
+fwix_status do_scatter(fwix_plan* p, int iz, int adjoint, const float2* in, float2* out, int add,
+                       const float2* image, cudaStream_t s) {
+  SpecArgs a = scatter_args(p, iz, in, out, add);
+  if (!adjoint) {
+    a.image = image;
+    FWIX_TRY(cu(fwix::row_forward(a, image ? fwix::W_IC : fwix::W_ONE, s), "scatter row pass"));
+    FWIX_TRY(cu(fwix::col_type_a(a, fwix::Q_KPOW, s), "scatter column pass"));
+    FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_SCAT, 0, s), "scatter inverse row pass"));
+  } else {
+    FWIX_TRY(cu(fwix::row_forward(a, fwix::W_SCAT_CONJ, s), "scatter adjoint row pass"));
+    FWIX_TRY(cu(fwix::col_type_b(a, fwix::Q_KPOW, s), "scatter adjoint column pass"));
+    FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_ONE, 0, s), "scatter adjoint inverse row pass"));
+  }
+  return FWIX_OK;
+}
+
+int lower_iz(const fwix_plan* p, int iz) { return iz < p->desc.nz - 1 ? iz + 1 : iz; }
+
+fwix_status do_reflect(fwix_plan* p, int iz, int adjoint, const float2* in, float2* out, int add,
+                       cudaStream_t s) {
+  const int z1 = lower_iz(p, iz);
+  return cu(fwix::launch_reflect(p->d, adjoint, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                 p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, in, out, add, s),
+            "reflect");
+}
+
+const fwix::InjectLevel* level_of(const fwix_traces* tr, int iz) {
+  if (!tr || iz < 0 || iz >= tr->nlevel) return nullptr;
+  return &tr->level[iz];
+}
+
+fwix_status do_inject(fwix_plan* p, const fwix_traces* tr, int iz, const float2* traces, float2* wfld,
+                      cudaStream_t s) {
+  const fwix::InjectLevel* L = level_of(tr, iz);
+  if (!L) return FWIX_OK;
+  return cu(fwix::launch_inject(p->d, *L, traces, wfld, s), "inject");
+}
+
+fwix_status do_record(fwix_plan* p, const fwix_traces* tr, int iz, const float2* wfld, float2* traces,
+                      cudaStream_t s) {
+  const fwix::InjectLevel* L = level_of(tr, iz);
+  if (!L) return FWIX_OK;
+  return cu(fwix::launch_record(p->d, *L, wfld, traces, s), "record");
+}
+
+// ForwardScattering::cu_forward (Scattering.cpp:43-52): target += step_add(scatter(bg * image)).
+fwix_status fscat_fwd(fwix_plan* p, int iz_prop, const float2* bg, const float2* image, float2* target,
+                      cudaStream_t s) {
+  FWIX_TRY(do_scatter(p, iz_prop, 0, bg, p->wSC(), 0, image, s));
+  return do_step(p, p->desc.step_kind, iz_prop, FWIX_FWD, p->wSC(), target, 1, s);
+}
+
+// ForwardScattering::cu_adjoint (Scattering.cpp:54-61): gimage += ic_adj(scatter^T(step_adj_add(wfld))).
+fwix_status fscat_adj(fwix_plan* p, int iz_prop, const float2* bg, const float2* wfld, float2* gimage,
+                      cudaStream_t s) {
+  FWIX_TRY(do_step(p, p->desc.step_kind, iz_prop, FWIX_ADJ_ADD, wfld, p->wSC(), 0, s));
+  FWIX_TRY(do_scatter(p, iz_prop, 1, p->wSC(), p->wSC(), 0, nullptr, s));
+  return cu(fwix::launch_ic_adj(p->d, bg, p->wSC(), gimage, 1, s), "imaging adjoint");
+}
+
+long long mslice(const fwix_plan* p) { return (long long)p->d.nw * p->d.ny * p->d.nx; }
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+const char* fwix_last_error(void) { return g_err.c_str(); }
+
+int fwix_version(void) { return 100; }
+
+fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
+  if (!desc || !out) return fail(FWIX_ERR_INVALID, "null descriptor or output");
+  *out = nullptr;
+  const fwix_desc& q = *desc;
+  if (q.nx < 1 || q.ny < 1 || q.nw < 1 || q.ns < 1 || q.nz < 1 || q.padx < 0 || q.pady < 0)
+    return fail(FWIX_ERR_INVALID, "sizes must be positive and pads non-negative");
+  if (q.nref < 1 || q.nref > 255) return fail(FWIX_ERR_INVALID, "nref must be in [1, 255]");
+  if (q.taylor < 0 || q.taylor > 4) return fail(FWIX_ERR_INVALID, "taylor must be in [0, 4]");
+  if (q.taperx < 0 || q.tapery < 0) return fail(FWIX_ERR_INVALID, "taper widths must be non-negative");
+  if (!(q.dx > 0) || !(q.dy > 0) || !(q.dz > 0)) return fail(FWIX_ERR_INVALID, "sampling must be positive");
+  if (q.step_kind != FWIX_STEP_PSPI && q.step_kind != FWIX_STEP_NSPS)
+    return fail(FWIX_ERR_INVALID, "unknown step kind");
+  fwix_plan* p = new fwix_plan();
+  p->desc = q;
+  p->d.nx = q.nx;
+  p->d.ny = q.ny;
+  p->d.NX = q.nx + q.padx;
+  p->d.NY = q.ny + q.pady;
+  p->d.nw = q.nw;
+  p->d.ns = q.ns;
+  p->d.slice = (long long)p->d.NX * p->d.NY;
+  p->d.wfld = p->d.slice * q.nw * q.ns;
+  if (!make_fft_plan(p->d.NX, &p->px) || !make_fft_plan(p->d.NY, &p->py)) {
+    delete p;
+    return fail(FWIX_ERR_UNSUPPORTED, "wavefield sizes must be 2^a 3^b 5^c 7^d and at most 1024");
+  }
+  p->nterm_max = std::max(q.nref, q.taylor + 1);
+  std::vector<float> w2(q.nw), w(q.nw);
+  for (int i = 0; i < q.nw; ++i) {
+    // PhaseShift.h:59-70 and Scatter.h:544-556 (float f, then 2 pi f in double)
+    float f = q.ow + (float)i * q.dw;
+    float wf = (float)(2 * M_PI * f);
+    w2[i] = wf * wf;
+    w[i] = (float)(2 * M_PI * f);
+  }
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = upload(&p->twx, twiddles(p->d.NX));
+  if (e == cudaSuccess) e = upload(&p->twy, twiddles(p->d.NY));
+  if (e == cudaSuccess) e = upload(&p->kx, k_table(p->d.NX, q.dx));
+  if (e == cudaSuccess) e = upload(&p->ky, k_table(p->d.NY, q.dy));
+  if (e == cudaSuccess) e = upload(&p->w2, w2);
+  if (e == cudaSuccess) e = upload(&p->w, w);
+  if (e == cudaSuccess) e = upload(&p->tapx, taper_table(p->d.NX, q.taperx));
+  if (e == cudaSuccess) e = upload(&p->tapy, taper_table(p->d.NY, q.tapery));
+  if (e != cudaSuccess) {
+    fwix_plan_destroy(p);
+    return fail(FWIX_ERR_CUDA, std::string("plan tables: ") + cudaGetErrorString(e));
+  }
+  *out = p;
+  return FWIX_OK;
+}
+
+fwix_status fwix_plan_destroy(fwix_plan* p) {
+  if (!p) return FWIX_OK;
+  void* ptrs[] = {p->twx, p->twy, p->kx, p->ky, p->w2, p->w, p->tapx, p->tapy};
+  for (void* v : ptrs)
+    if (v) cudaFree(v);
+  delete p;
+  return FWIX_OK;
+}
+
+size_t fwix_plan_workspace_bytes(const fwix_plan* p, int cls) { return p ? p->ws_need(cls) : 0; }
+
+fwix_status fwix_plan_set_workspace(fwix_plan* p, void* ptr, size_t bytes) {
+  if (!p) return fail(FWIX_ERR_INVALID, "null plan");
+  if (((uintptr_t)ptr) % 16 != 0) return fail(FWIX_ERR_INVALID, "workspace must be 16-byte aligned");
+  p->ws = (char*)ptr;
+  p->ws_bytes = bytes;
+  return FWIX_OK;
+}
+
+fwix_status fwix_plan_set_refs(fwix_plan* p, const void* sref, const uint8_t* labels, int64_t z_stride,
+                               int64_t w_stride) {
+  if (!p || !sref || !labels) return fail(FWIX_ERR_INVALID, "null plan, refs or labels");
+  p->sref = (const float2*)sref;
+  p->labels = labels;
+  p->lab_z = z_stride;
+  p->lab_w = w_stride;
+  return FWIX_OK;
+}
+
+fwix_status fwix_plan_set_model(fwix_plan* p, const void* slow, const void* den, int64_t z_stride,
+                                int64_t w_stride) {
+  if (!p || !slow || !den) return fail(FWIX_ERR_INVALID, "null plan or model");
+  p->slow = (const float2*)slow;
+  p->den = (const float2*)den;
+  p->m_z = z_stride;
+  p->m_w = w_stride;
+  return FWIX_OK;
+}
+
+fwix_status fwix_fft2d(fwix_plan* p, int inverse, const void* in, void* out, int add, void* stream) {
+  if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  cudaStream_t s = (cudaStream_t)stream;
+  SpecArgs a = p->args((const float2*)in, (float2*)out, add);
+  const float sc = 1.0f / sqrtf((float)p->d.NX * (float)p->d.NY);
+  if (!inverse) {
+    FWIX_TRY(cu(fwix::row_forward(a, fwix::W_ONE, s), "fft row pass"));
+    FWIX_TRY(cu(fwix::col_fft(a, 0, p->t1(), (float2*)out, add, sc, s), "fft column pass"));
+  } else {
+    FWIX_TRY(cu(fwix::col_fft(a, 1, (const float2*)in, p->t2(), 0, sc, s), "ifft column pass"));
+    FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_ONE, 0, s), "ifft row pass"));
+  }
+  return FWIX_OK;
+}
+
+fwix_status fwix_phase_shift(fwix_plan* p, int mode, const void* sref_w, const void* in, void* out, int add,
+                             void* stream) {
+  if (!p || !sref_w || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  int q = mode == FWIX_PS_FWD ? fwix::Q_PS_FWD : mode == FWIX_PS_ADJ ? fwix::Q_PS_ADJ
+        : mode == FWIX_PS_INV ? fwix::Q_PS_INV : -1;
+  if (q < 0) return fail(FWIX_ERR_INVALID, "unknown phase-shift mode");
+  SpecArgs a = p->args((const float2*)in, (float2*)out, add);
+  return cu(fwix::launch_phase_shift(a, q, (const float2*)sref_w, (const float2*)in, (float2*)out, add,
+                                     (cudaStream_t)stream),
+            "phase shift");
+}
+
+fwix_status fwix_select(fwix_plan* p, int iz, int value, const void* in, void* out, int add, void* stream) {
+  if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(check_iz(p, iz));
+  SpecArgs a = p->args((const float2*)in, (float2*)out, add);
+  a.lab = p->labels + iz * p->lab_z;
+  a.lab_w = p->lab_w;
+  return cu(fwix::launch_select(a, value, (const float2*)in, (float2*)out, add, (cudaStream_t)stream), "select");
+}
+
+fwix_status fwix_taper(fwix_plan* p, const void* in, void* out, int add, void* stream) {
+  if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  SpecArgs a = p->args((const float2*)in, (float2*)out, add);
+  return cu(fwix::launch_taper(a, (const float2*)in, (float2*)out, add, (cudaStream_t)stream), "taper");
+}
+
+fwix_status fwix_step(fwix_plan* p, int kind, int iz, int dir, const void* in, void* out, int add,
+                      void* stream) {
+  if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  if (kind != FWIX_STEP_PSPI && kind != FWIX_STEP_NSPS) return fail(FWIX_ERR_INVALID, "unknown step kind");
+  if (dir != FWIX_FWD && dir != FWIX_ADJ_ADD && dir != FWIX_ADJ_INPL)
+    return fail(FWIX_ERR_INVALID, "unknown step direction");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  FWIX_TRY(check_iz(p, iz));
+  return do_step(p, kind, iz, dir, (const float2*)in, (float2*)out, add, (cudaStream_t)stream);
+}
+
+fwix_status fwix_scatter(fwix_plan* p, int iz, int adjoint, const void* in, void* out, int add, void* stream) {
+  if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  FWIX_TRY(check_iz(p, iz));
+  return do_scatter(p, iz, adjoint, (const float2*)in, (float2*)out, add, nullptr, (cudaStream_t)stream);
+}
+
+fwix_status fwix_reflect(fwix_plan* p, int iz, int adjoint, const void* in, void* out, int add, void* stream) {
+  if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(check_iz(p, iz));
+  return do_reflect(p, iz, adjoint, (const float2*)in, (float2*)out, add, (cudaStream_t)stream);
+}
+
+fwix_status fwix_imaging(fwix_plan* p, int adjoint, const void* bg, void* image, void* wfld, int add,
+                         void* stream) {
+  if (!p || !bg || !image || !wfld) return fail(FWIX_ERR_INVALID, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!adjoint)
+    return cu(fwix::launch_ic_fwd(p->d, (const float2*)bg, (const float2*)image, (float2*)wfld, add, s),
+              "imaging forward");
+  return cu(fwix::launch_ic_adj(p->d, (const float2*)bg, (const float2*)wfld, (float2*)image, add, s),
+            "imaging adjoint");
+}
+
+fwix_status fwix_lin_reflect(fwix_plan* p, int iz, int adjoint, void* dmodel, void* dr, int add, void* stream) {
+  if (!p || !dmodel || !dr) return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(check_iz(p, iz));
+  const int z1 = lower_iz(p, iz);
+  float2* dm = (float2*)dmodel;
+  const long long n = mslice(p);
+  return cu(fwix::launch_lin_reflect(p->d, adjoint, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                     p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, dm, dm + n,
+                                     dm + 2 * n, dm + 3 * n, (float2*)dr, add, (cudaStream_t)stream),
+            "linearised reflection");
+}
+
+// ---------------------------------------------------------------- acquisition
+
+fwix_status fwix_traces_create(fwix_plan* p, int ntrace, const float* cx, const float* cy, const float* cz,
+                               const int32_t* ids, fwix_traces** out) {
+  if (!p || !out || ntrace < 0 || (ntrace > 0 && (!cx || !cy || !cz || !ids)))
+    return fail(FWIX_ERR_INVALID, "bad trace arguments");
+  *out = nullptr;
+  const Dims& d = p->d;
+  const float OX = p->desc.ox, OY = p->desc.oy, DX = p->desc.dx, DY = p->desc.dy;
+  const float oz = p->desc.oz, dz = p->desc.dz;
+  const int nlevel = p->desc.nz;
+  // gather lists per level: cell -> (trace, weight)
+  std::vector<std::map<long long, std::vector<std::pair<int, float>>>> inj(nlevel);
+  std::vector<std::vector<int>> rtr(nlevel), rcell(nlevel);
+  std::vector<std::vector<float4>> rw(nlevel);
+  for (int t = 0; t < ntrace; ++t) {
+    if (ids[t] < 0 || ids[t] >= d.ns) return fail(FWIX_ERR_INVALID, "trace shot id outside [0, ns)");
+    // injection.cu:34-53, in float
+    const int iy = (int)floorf((cy[t] - OY) / DY);
+    const float y = OY + (float)iy * DY;
+    const float ly = 1.f - (cy[t] - y) / DY;
+    const int ix = (int)floorf((cx[t] - OX) / DX);
+    const float x = OX + (float)ix * DX;
+    const float lx = 1.f - (cx[t] - x) / DX;
+    const int izt = (int)floorf((cz[t] - oz) / dz);
+    const float z = oz + (float)izt * dz;
+    const float lz = 1.f - (cz[t] - z) / dz;
+    if (ix < 0 || ix >= d.NX - 1 || iy < 0 || iy >= d.NY - 1) continue;  // injection.cu:46-48
+    for (int lev = izt; lev <= izt + 1; ++lev) {
+      if (lev < 0 || lev >= nlevel) continue;
+      const float zz = (lev == izt) ? lz : (1 - lz);
+      const float w0 = zz * lx * ly, w1 = zz * (1 - lx) * ly, w2 = zz * lx * (1 - ly),
+                  w3 = zz * (1 - lx) * (1 - ly);
+      const long long base = (long long)ids[t] * d.slice + (long long)iy * d.NX + ix;
+      inj[lev][base].push_back({t, w0});
+      inj[lev][base + 1].push_back({t, w1});
+      inj[lev][base + d.NX].push_back({t, w2});
+      inj[lev][base + d.NX + 1].push_back({t, w3});
+      rtr[lev].push_back(t);
+      rcell[lev].push_back((int)base);
+      rw[lev].push_back(make_float4(w0, w1, w2, w3));
+    }
+  }
+  fwix_traces* tr = new fwix_traces();
+  tr->ntrace = ntrace;
+  tr->nlevel = nlevel;
+  tr->level.resize(nlevel);
+  // pack all levels into flat host arrays, upload once, then point into them
+  std::vector<int> cells, starts, trs, rtrace, rcells;
+  std::vector<float> wts;
+  std::vector<float4> rws;
+  std::vector<long long> off_cell(nlevel), off_start(nlevel), off_tr(nlevel), off_r(nlevel);
+  for (int lev = 0; lev < nlevel; ++lev) {
+    off_cell[lev] = cells.size();
+    off_start[lev] = starts.size();
+    off_tr[lev] = trs.size();
+    off_r[lev] = rtrace.size();
+    for (auto& kv : inj[lev]) {
+      if (kv.first > 0x7fffffffLL) {
+        delete tr;
+        return fail(FWIX_ERR_UNSUPPORTED, "wavefield batch too large for 32-bit cell indices");
+      }
+      cells.push_back((int)kv.first);
+      starts.push_back((int)(trs.size() - off_tr[lev]));
+      for (auto& tw : kv.second) {
+        trs.push_back(tw.first);
+        wts.push_back(tw.second);
+      }
+    }
+    starts.push_back((int)(trs.size() - off_tr[lev]));
+    for (size_t k = 0; k < rtr[lev].size(); ++k) {
+      rtrace.push_back(rtr[lev][k]);
+      rcells.push_back(rcell[lev][k]);
+      rws.push_back(rw[lev][k]);
+    }
+  }
+  int *dcells = nullptr, *dstarts = nullptr, *dtrs = nullptr, *drtrace = nullptr, *drcells = nullptr;
+  float* dwts = nullptr;
+  float4* drws = nullptr;
+  cudaError_t e = upload(&dcells, cells);
+  if (e == cudaSuccess) e = upload(&dstarts, starts);
+  if (e == cudaSuccess) e = upload(&dtrs, trs);
+  if (e == cudaSuccess) e = upload(&dwts, wts);
+  if (e == cudaSuccess) e = upload(&drtrace, rtrace);
+  if (e == cudaSuccess) e = upload(&drcells, rcells);
+  if (e == cudaSuccess) e = upload(&drws, rws);
+  void* allocs[] = {dcells, dstarts, dtrs, dwts, drtrace, drcells, drws};
+  for (void* v : allocs)
+    if (v) tr->allocs.push_back(v);
+  if (e != cudaSuccess) {
+    fwix_traces_destroy(tr);
+    return fail(FWIX_ERR_CUDA, std::string("trace tables: ") + cudaGetErrorString(e));
+  }
+  for (int lev = 0; lev < nlevel; ++lev) {
+    fwix::InjectLevel& L = tr->level[lev];
+    const long long nc = (lev + 1 < nlevel ? off_cell[lev + 1] : (long long)cells.size()) - off_cell[lev];
+    L.ncell = (int)nc;
+    L.cell = dcells ? dcells + off_cell[lev] : nullptr;
+    L.start = dstarts + off_start[lev];
+    L.trace = dtrs ? dtrs + off_tr[lev] : nullptr;
+    L.weight = dwts ? dwts + off_tr[lev] : nullptr;
+    const long long nr = (lev + 1 < nlevel ? off_r[lev + 1] : (long long)rtrace.size()) - off_r[lev];
+    L.ntr = (int)nr;
+    L.rtrace = drtrace ? drtrace + off_r[lev] : nullptr;
+    L.rcell = drcells ? drcells + off_r[lev] : nullptr;
+    L.rw = drws ? drws + off_r[lev] : nullptr;
+  }
+  *out = tr;
+  return FWIX_OK;
+}
+
+fwix_status fwix_traces_destroy(fwix_traces* tr) {
+  if (!tr) return FWIX_OK;
+  for (void* v : tr->allocs) cudaFree(v);
+  delete tr;
+  return FWIX_OK;
+}
+
+fwix_status fwix_inject(fwix_plan* p, const fwix_traces* tr, int iz, int adjoint, void* traces, void* wfld,
+                        int add, void* stream) {
+  if (!p || !tr || !traces || !wfld) return fail(FWIX_ERR_INVALID, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!adjoint) {
+    if (!add) FWIX_CU(cudaMemsetAsync(wfld, 0, p->wbytes(), s));
+    return do_inject(p, tr, iz, (const float2*)traces, (float2*)wfld, s);
+  }
+  if (!add) FWIX_CU(cudaMemsetAsync(traces, 0, (size_t)tr->ntrace * p->d.nw * sizeof(float2), s));
+  return do_record(p, tr, iz, (const float2*)wfld, (float2*)traces, s);
+}
+
+// ---------------------------------------------------------------- sweeps
+
+fwix_status fwix_downward(fwix_plan* p, int adjoint, void* wfld, void* stream) {
+  if (!p || !wfld) return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  cudaStream_t s = (cudaStream_t)stream;
+  float2* w = (float2*)wfld;
+  const int k = p->desc.step_kind;
+  if (!adjoint) {
+    for (int iz = 0; iz < p->desc.nz; ++iz) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, w, w, 0, s));
+  } else {
+    for (int iz = p->desc.nz - 1; iz >= 0; --iz) FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, w, w, 0, s));
+  }
+  return FWIX_OK;
+}
+
+fwix_status fwix_upward(fwix_plan* p, int adjoint, void* wfld, void* stream) {
+  if (!p || !wfld) return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  cudaStream_t s = (cudaStream_t)stream;
+  float2* w = (float2*)wfld;
+  const int k = p->desc.step_kind;
+  if (!adjoint) {
+    for (int iz = p->desc.nz - 1; iz >= 0; --iz) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, w, w, 0, s));
+  } else {
+    for (int iz = 0; iz < p->desc.nz; ++iz) FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, w, w, 0, s));
+  }
+  return FWIX_OK;
+}
+
+// Propagator::forward (Propagator.cpp:121-221).  The level-iz checkpoints are the
+// working buffers themselves: the step from iz writes straight into slot iz+1.
+fwix_status fwix_propagate(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec, const void* wavelet,
+                           void* data, int add, void* bg_down, void* bg_up, void* stream) {
+  if (!p || !src || !rec || !wavelet || !data) return fail(FWIX_ERR_INVALID, "null argument");
+  if (!bg_down) return fail(FWIX_ERR_INVALID, "bg_down storage ([nz] wavefields) is required");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_SWEEP));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nz = p->desc.nz, k = p->desc.step_kind;
+  const long long W = p->d.wfld;
+  float2* down = (float2*)bg_down;
+  float2* up = (float2*)bg_up;
+  float2* dat = (float2*)data;
+  const float2* wav = (const float2*)wavelet;
+  if (!add) FWIX_CU(cudaMemsetAsync(dat, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
+  FWIX_CU(cudaMemsetAsync(down, 0, p->wbytes(), s));
+  for (int iz = 0; iz < nz; ++iz) {
+    float2* cur = down + iz * W;
+    FWIX_TRY(do_inject(p, src, iz, wav, cur, s));
+    FWIX_TRY(do_record(p, rec, iz, cur, dat, s));
+    if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, cur, down + (iz + 1) * W, 0, s));
+  }
+  float2* prev = nullptr;
+  for (int iz = nz - 1; iz >= 0; --iz) {
+    float2* cur = up ? up + iz * W : ((nz - 1 - iz) % 2 ? p->wB() : p->wA());
+    if (prev)
+      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, prev, cur, 0, s));
+    else
+      FWIX_CU(cudaMemsetAsync(cur, 0, p->wbytes(), s));  // stepping the zero field gives zero
+    FWIX_TRY(do_reflect(p, iz, 0, down + iz * W, cur, 1, s));
+    FWIX_TRY(do_record(p, rec, iz, cur, dat, s));
+    prev = cur;
+  }
+  return FWIX_OK;
+}
+
+// Lockstep migration: the source field (Propagator.cpp:155-180) and the receiver
+// field of the back-scattering adjoint (ExtendedBorn.cpp:396-408) move down
+// together and image[iz] accumulates sum_w Re sum_s conj(S) R
+// (imaging_condition.cu:57-108 summed over frequency).
+fwix_status fwix_migrate(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec, const void* wavelet,
+                         const void* data, float* image, int add, void* stream) {
+  if (!p || !src || !rec || !wavelet || !data || !image) return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_SWEEP));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nz = p->desc.nz, k = p->desc.step_kind;
+  float2* S = p->wA();
+  float2* R = p->wB();
+  FWIX_CU(cudaMemsetAsync(S, 0, p->wbytes(), s));
+  FWIX_CU(cudaMemsetAsync(R, 0, p->wbytes(), s));
+  const long long plane = (long long)p->d.ny * p->d.nx;
+  for (int iz = 0; iz < nz; ++iz) {
+    FWIX_TRY(do_inject(p, src, iz, (const float2*)wavelet, S, s));
+    FWIX_TRY(do_inject(p, rec, iz, (const float2*)data, R, s));
+    FWIX_TRY(cu(fwix::launch_image_acc(p->d, S, R, image + iz * plane, add, s), "image"));
+    if (iz < nz - 1) {
+      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, S, S, 0, s));
+      FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, R, R, 0, s));
+    }
+  }
+  return FWIX_OK;
+}
+
+// ExtendedBorn::forward / adjoint (ExtendedBorn.cpp:80-453).
+fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const void* bg_down_v,
+                      const void* bg_up_v, void* dslow_v, void* dden_v, void* data_v, int add, void* stream) {
+  if (!p || !rec || !bg_down_v || !bg_up_v || !dslow_v || !dden_v || !data_v)
+    return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_BORN));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nz = p->desc.nz, k = p->desc.step_kind;
+  const long long W = p->d.wfld, M = mslice(p);
+  const float2* bgd = (const float2*)bg_down_v;
+  const float2* bgu = (const float2*)bg_up_v;
+  float2* ds = (float2*)dslow_v;
+  float2* dr = (float2*)dden_v;
+  float2* data = (float2*)data_v;
+  float2* A = p->wA();
+  float2* DR = p->wB();  // [nw][ny][nx] scratch for the linearised reflection
+  const size_t wb = p->wbytes();
+  if (!adjoint) {
+    if (!add) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
+    // 1. down scattering (ExtendedBorn.cpp:152-178); store[iz] holds the field before step iz
+    FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
+    for (int iz = 0; iz < nz; ++iz) {
+      float2* cur = p->store(iz);
+      float2* next = iz < nz - 1 ? p->store(iz + 1) : A;
+      FWIX_TRY(do_record(p, rec, iz, cur, data, s));
+      if (iz == nz - 1) break;  // the last step feeds nothing that is recorded or stored
+      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, cur, next, 0, s));
+      FWIX_TRY(fscat_fwd(p, iz, bgd + iz * W, ds + iz * M, next, s));
+    }
+    // 2. reflected up by the background (ExtendedBorn.cpp:210-238)
+    FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+    for (int iz = nz - 1; iz >= 0; --iz) {
+      if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s));
+      FWIX_TRY(do_reflect(p, iz, 0, p->store(iz), A, 1, s));
+      FWIX_TRY(do_record(p, rec, iz, A, data, s));
+    }
+    // 3. up scattering (ExtendedBorn.cpp:282-311)
+    FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+    for (int iz = nz - 1; iz >= 0; --iz) {
+      FWIX_TRY(do_record(p, rec, iz, A, data, s));
+      if (iz > 0) {
+        FWIX_TRY(do_step(p, k, iz - 1, FWIX_FWD, A, A, 0, s));
+        FWIX_TRY(fscat_fwd(p, iz - 1, bgu + iz * W, ds + iz * M, A, s));
+      }
+    }
+    // 4. back scattering (ExtendedBorn.cpp:352-389)
+    FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+    for (int iz = nz - 1; iz >= 0; --iz) {
+      const int z1 = lower_iz(p, iz);
+      if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s));
+      FWIX_TRY(cu(fwix::launch_lin_reflect(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                           p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
+                                           ds + z1 * M, dr + iz * M, dr + z1 * M, DR, 0, s),
+                  "linearised reflection"));
+      FWIX_TRY(cu(fwix::launch_ic_fwd(p->d, bgd + iz * W, DR, A, 1, s), "imaging forward"));
+      FWIX_TRY(do_record(p, rec, iz, A, data, s));
+    }
+    return FWIX_OK;
+  }
+  if (!add) {
+    FWIX_CU(cudaMemsetAsync(ds, 0, (size_t)nz * M * sizeof(float2), s));
+    FWIX_CU(cudaMemsetAsync(dr, 0, (size_t)nz * M * sizeof(float2), s));
+  }
+  // up-scattering adjoint (ExtendedBorn.cpp:313-349); store[iz] keeps the adjoint
+  // up-going field that the reflected sweep consumes
+  FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
+  for (int iz = 0; iz < nz; ++iz) {
+    float2* cur = p->store(iz);
+    if (iz > 0) {
+      float2* prev = p->store(iz - 1);
+      FWIX_TRY(fscat_adj(p, iz - 1, bgu + iz * W, prev, ds + iz * M, s));
+      FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_INPL, prev, cur, 0, s));
+    }
+    FWIX_TRY(do_inject(p, rec, iz, data, cur, s));
+  }
+  // reflected and direct down-scattering adjoints (ExtendedBorn.cpp:240-280 and
+  // :180-208) share the recursion, so their sources are summed in one sweep
+  FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+  for (int iz = nz - 1; iz >= 0; --iz) {
+    if (iz < nz - 1) {
+      FWIX_TRY(fscat_adj(p, iz, bgd + iz * W, A, ds + iz * M, s));
+      FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, A, A, 0, s));
+    }
+    FWIX_TRY(do_reflect(p, iz, 1, p->store(iz), A, 1, s));
+    FWIX_TRY(do_inject(p, rec, iz, data, A, s));
+  }
+  // back-scattering adjoint (ExtendedBorn.cpp:391-453)
+  FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+  for (int iz = 0; iz < nz; ++iz) {
+    const int z1 = lower_iz(p, iz);
+    FWIX_TRY(do_inject(p, rec, iz, data, A, s));
+    FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgd + iz * W, A, DR, 0, s), "imaging adjoint"));
+    FWIX_TRY(cu(fwix::launch_lin_reflect(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                         p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
+                                         ds + z1 * M, dr + iz * M, dr + z1 * M, DR, 1, s),
+                "linearised reflection adjoint"));
+    if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, A, A, 0, s));
+  }
+  return FWIX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// Internal declarations shared by the translation units of libfwix_b200.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "fft_device.cuh"
+
+namespace fwix {
+
+// Per-cell pre-weights of a forward row pass and post-weights of an inverse row pass.
+enum RowWeight {
+  W_ONE = 0,        // 1
+  W_TAPER = 1,      // separable taper w_x * w_y            (taper.cu:46-63)
+  W_MASK = 2,       // labels == term                        (selector.cu:29-35)
+  W_SCAT = 3,       // Born weight W_n                       (scatter.cu:61-106,155-195)
+  W_SCAT_CONJ = 4,  // conj(W_n)
+  W_IC = 5          // bg * image on the unpadded window      (imaging_condition.cu:39-52)
+};
+
+// Spectral multipliers applied between the column FFTs.
+enum ColMult {
+  Q_PS_FWD = 0,  // e^{Im dz}(cos - i sin)(Re dz)            (phase_shift.cu:36-55)
+  Q_PS_ADJ = 1,  // conjugate with the b>0 branch             (phase_shift.cu:153-178)
+  Q_PS_INV = 2,  // growing inverse                           (phase_shift.cu:274-298)
+  Q_KPOW = 3,    // (|k| / w)^(2n)                            (scatter.cu:49-55)
+  Q_ONE = 4
+};
+
+struct Dims {
+  int NX, NY;       // wavefield (padded)
+  int nx, ny;       // model window
+  int nw, ns;       // frequencies, shots
+  long long slice;  // NX * NY
+  long long wfld;   // ns * nw * NX * NY
+};
+
+// Everything a spectral kernel may read.  Passed by value (kernel parameter).
+struct SpecArgs {
+  Dims d;
+  Fft1D px, py;
+  const float2* twx;
+  const float2* twy;
+  // tables
+  const float* kx;     // [NX]
+  const float* ky;     // [NY]
+  const float* w2;     // [nw]
+  const float* w;      // [nw]
+  const float* tapx;   // [NX]
+  const float* tapy;   // [NY]
+  // depth-dependent inputs
+  const float2* sref;  // [nref][nw] at this depth
+  const uint8_t* lab;  // labels at this depth, element (iw, y, x) at lab[iw*lab_w + y*NX + x]
+  long long lab_w;
+  const float2* slow;  // s^2 at this depth (unpadded), (iw, y, x) at slow[iw*slow_w + y*nx + x]
+  long long slow_w;
+  const float2* image; // imaging-condition image [nw][ny][nx] (W_IC)
+  float dz, eps, eps_scat;
+  float coef[5];
+  float norm;          // scale folded into the column multiplier
+  int nterm;           // references (W_MASK) or Taylor terms (W_SCAT)
+  // buffers
+  const float2* in;    // row-pass input (W_IC: the background wavefield)
+  float2* out;         // row-pass output
+  int add;
+  float2* t1;          // nterm wavefield-sized buffers, stride d.wfld
+  float2* t2;
+};
+
+// Spectral passes (spectral.cu).  Each returns a CUDA error code.
+cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s);      // in -> t1[0..nterm)
+cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s);  // t2 -> out
+cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s);     // t1[0] -> t2[0..nterm)
+cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s);     // t1[0..nterm) -> t2[0]
+cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add,
+                    float scale, cudaStream_t s);
+
+// Pointwise kernels (pointwise.cu).
+cudaError_t launch_phase_shift(const SpecArgs& a, int mode, const float2* sref_w, const float2* in,
+                               float2* out, int add, cudaStream_t s);
+cudaError_t launch_select(const SpecArgs& a, int value, const float2* in, float2* out, int add,
+                          cudaStream_t s);
+cudaError_t launch_taper(const SpecArgs& a, const float2* in, float2* out, int add, cudaStream_t s);
+cudaError_t launch_reflect(const Dims& d, int adjoint, const float2* s0, const float2* s1,
+                           const float2* r0, const float2* r1, long long mw, const float2* in,
+                           float2* out, int add, cudaStream_t s);
+cudaError_t launch_ic_fwd(const Dims& d, const float2* bg, const float2* image, float2* wfld,
+                          int add, cudaStream_t s);
+cudaError_t launch_ic_adj(const Dims& d, const float2* bg, const float2* wfld, float2* image,
+                          int add, cudaStream_t s);
+cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, const float2* s1,
+                               const float2* r0, const float2* r1, long long mw, float2* dm0,
+                               float2* dm1, float2* dm2, float2* dm3, float2* dr, int add,
+                               cudaStream_t s);
+cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, float* img, int add,
+                             cudaStream_t s);
+cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s);
+
+// Acquisition kernels (pointwise.cu).  A depth level's injection is a gather
+// list: for each target cell, the (trace, weight) pairs that land on it.
+struct InjectLevel {
+  int ncell;             // target cells touched at this level
+  const int* cell;       // [ncell] flat (shot, y, x) -> shot*NY*NX + y*NX + x, no frequency
+  const int* start;      // [ncell + 1] offsets into trace/weight
+  const int* trace;      // contributing trace
+  const float* weight;   // its weight
+  int ntr;               // traces recorded at this level
+  const int* rtrace;     // [ntr] trace index
+  const int* rcell;      // [ntr] flat (shot, y, x) of the (y, x) corner
+  const float4* rw;      // [ntr] the four corner weights
+};
+cudaError_t launch_inject(const Dims& d, const InjectLevel& L, const float2* traces, float2* wfld,
+                          cudaStream_t s);
+cudaError_t launch_record(const Dims& d, const InjectLevel& L, const float2* wfld, float2* traces,
+                          cudaStream_t s);
+
+}  // namespace fwix

@@ -1,0 +1,528 @@
+// Spectral passes of one depth step.  A 2D unitary transform is split into a row
+// pass (one warp per row of NX samples, contiguous in HBM) and a column pass (one
+// CTA per tile of TX columns x NY rows, one warp per column).  The per-cell work
+// of the reference's separate elementwise kernels -- taper, reference selection,
+// Born weights, imaging-condition product, phase shift, k-filters -- is applied
+// while the data sits in shared memory, so a PSPI or NSPS step costs three
+// kernels instead of 1 + 3*nref elementwise passes plus nref+1 cuFFT calls
+// (propagator/src/PSPI.cpp:6-103, propagator/src/NSPS.cpp:6-45).
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "internal.h"
+
+namespace fwix {
+
+namespace {
+
+constexpr int kMaxSmem = 227 * 1024;
+
+// Opt a kernel in to more than 48 KB of dynamic shared memory, once per
+// (kernel, device) and size.
+template <typename K>
+cudaError_t ensure_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_pair((const void*)kernel, dev);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done[key] = bytes;
+  return e;
+}
+
+// Born weight W_n = (-i w dz / 2) c_n s~^(-1/2-n), s~ = Re s^2 + i (Im s^2 - eps Re s^2),
+// read from the unpadded slice with edge replication into the pad
+// (scatter.cu:61-106 slow_scale, :155-195 scale_by_iw, :240-277 pad_fwd).
+// s~^(-1/2-n) = (1/sqrt(s~)) (1/s~)^n with the principal root.
+__device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, int y, int x) {
+  const int xs = min(x, a.d.nx - 1), ys = min(y, a.d.ny - 1);
+  const float2 s2 = a.slow[(long long)iw * a.slow_w + (long long)ys * a.d.nx + xs];
+  const float2 st = make_float2(s2.x, s2.y - a.eps_scat * s2.x);
+  float2 p = cinv(csqrt_ref(st));
+  if (n > 0) {
+    const float2 is = cinv(st);
+    for (int k = 0; k < n; ++k) p = cmul(p, is);
+  }
+  const float f = 0.5f * a.w[iw] * a.dz * a.coef[n];
+  return rot90<false>(cscale(p, f));
+}
+
+template <int W>
+__device__ __forceinline__ float2 row_weight(const SpecArgs& a, int t, int iw, int y, int x, float2 v) {
+  if (W == W_ONE) return v;
+  if (W == W_TAPER) return cscale(v, a.tapx[x] * a.tapy[y]);
+  if (W == W_MASK) {
+    const uint8_t l = a.lab[(long long)iw * a.lab_w + (long long)y * a.d.NX + x];
+    return (int)l == t ? v : make_float2(0.f, 0.f);
+  }
+  if (W == W_SCAT) return cmul(v, scat_weight(a, t, iw, y, x));
+  if (W == W_SCAT_CONJ) return cmul_conj(v, scat_weight(a, t, iw, y, x));
+  // W_IC
+  if (y < a.d.ny && x < a.d.nx)
+    return cmul(v, a.image[(long long)iw * a.d.ny * a.d.nx + (long long)y * a.d.nx + x]);
+  return make_float2(0.f, 0.f);
+}
+
+// Column multiplier for term t at (iw, ky[y], kx[x]), scaled by a.norm.
+template <int QM>
+__device__ __forceinline__ float2 qmult(const SpecArgs& a, int t, int iw, int x, int y) {
+  if (QM == Q_ONE) return make_float2(a.norm, 0.f);
+  const float kx = a.kx[x], ky = a.ky[y];
+  if (QM == Q_KPOW) {
+    if (t == 0) return make_float2(a.norm, 0.f);
+    const float k2 = kx * kx + ky * ky;
+    return make_float2(powf(sqrtf(k2) / a.w[iw], 2.0f * t) * a.norm, 0.f);
+  }
+  const float2 sr = a.sref[t * a.d.nw + iw];
+  const float w2 = a.w2[iw];
+  const float aa = w2 * sr.x - (kx * kx + ky * ky);
+  const float bb = w2 * (sr.y - a.eps * sr.x);
+  float re, im;
+  if (bb == 0.f) {
+    // c = sqrt(a^2) = |a| exactly, so the general branch reduces to one root.
+    if (aa >= 0.f) {
+      re = sqrtf(aa);
+      im = 0.f;
+    } else {
+      re = 0.f;
+      im = -sqrtf(-aa);
+    }
+  } else {
+    // Re = sqrt((c+a)/2), Im = -sqrt((c-a)/2) as phase_shift.cu:38-41, with the
+    // smaller of the two taken from Re |Im| = |b| / 2: the same values without
+    // the cancellation of c - a (or c + a) in float.
+    const float c = sqrtf(aa * aa + bb * bb);
+    if (aa >= 0.f) {
+      re = sqrtf((c + aa) * 0.5f);
+      im = -(fabsf(bb) * 0.5f) / re;
+    } else {
+      im = -sqrtf((c - aa) * 0.5f);
+      re = (fabsf(bb) * 0.5f) / -im;
+    }
+  }
+  if (QM == Q_PS_ADJ && bb > 0.f) re = -re;
+  if (QM == Q_PS_INV) {
+    im = -im;
+    if (bb > 0.f) re = -re;
+  }
+  const float att = (im == 0.f ? 1.f : expf(im * a.dz)) * a.norm;
+  float sn = 0.f, cs = 1.f;
+  if (re != 0.f) sincosf(re * a.dz, &sn, &cs);
+  return QM == Q_PS_FWD ? make_float2(att * cs, -att * sn) : make_float2(att * cs, att * sn);
+}
+
+// ---------------------------------------------------------------- row passes
+
+template <int PRE>
+__global__ void __launch_bounds__(256) k_row_forward(const SpecArgs a, int nchunk) {
+  extern __shared__ float2 smem[];
+  const int NX = a.d.NX;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  float2* tw = smem;
+  float2* lineIn = smem + NX + warp * 3 * NX;
+  float2* lineA = lineIn + NX;
+  float2* lineB = lineA + NX;
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.twx[i];
+  __syncthreads();
+  const long long b = blockIdx.x / nchunk;
+  const int chunk = blockIdx.x - (int)(b * nchunk);
+  const int iw = (int)(b % a.d.nw);
+  const int nterm = (PRE == W_MASK || PRE == W_SCAT || PRE == W_SCAT_CONJ) ? a.nterm : 1;
+  for (int y = chunk * nwarp + warp; y < a.d.NY; y += nchunk * nwarp) {
+    const long long roff = (b * a.d.NY + y) * NX;
+    for (int x = lane; x < NX; x += 32) lineIn[x] = a.in[roff + x];
+    __syncwarp();
+    for (int t = 0; t < nterm; ++t) {
+      for (int x = lane; x < NX; x += 32) lineA[x] = row_weight<PRE>(a, t, iw, y, x, lineIn[x]);
+      __syncwarp();
+      const float2* r = warp_fft<false>(lineA, lineB, 1, a.px, tw, lane);
+      float2* o = a.t1 + (long long)t * a.d.wfld + roff;
+      for (int x = lane; x < NX; x += 32) o[x] = r[x];
+      __syncwarp();
+    }
+  }
+}
+
+template <int POST>
+__global__ void __launch_bounds__(256) k_row_inverse(const SpecArgs a, int nchunk, int post_taper) {
+  extern __shared__ float2 smem[];
+  const int NX = a.d.NX;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  float2* tw = smem;
+  float2* acc = smem + NX + warp * 3 * NX;
+  float2* lineA = acc + NX;
+  float2* lineB = lineA + NX;
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.twx[i];
+  __syncthreads();
+  const long long b = blockIdx.x / nchunk;
+  const int chunk = blockIdx.x - (int)(b * nchunk);
+  const int iw = (int)(b % a.d.nw);
+  const int nterm = (POST == W_MASK || POST == W_SCAT || POST == W_SCAT_CONJ) ? a.nterm : 1;
+  for (int y = chunk * nwarp + warp; y < a.d.NY; y += nchunk * nwarp) {
+    const long long roff = (b * a.d.NY + y) * NX;
+    for (int x = lane; x < NX; x += 32) acc[x] = make_float2(0.f, 0.f);
+    for (int t = 0; t < nterm; ++t) {
+      if (POST == W_MASK) {
+        // skip references that no cell of this row selects
+        bool hit = false;
+        const uint8_t* lrow = a.lab + (long long)iw * a.lab_w + (long long)y * NX;
+        for (int x = lane; x < NX; x += 32) hit |= ((int)lrow[x] == t);
+        if (!__any_sync(0xffffffffu, hit)) continue;
+      }
+      const float2* src = a.t2 + (long long)t * a.d.wfld + roff;
+      for (int x = lane; x < NX; x += 32) lineA[x] = src[x];
+      __syncwarp();
+      const float2* r = warp_fft<true>(lineA, lineB, 1, a.px, tw, lane);
+      for (int x = lane; x < NX; x += 32) {
+        if (POST == W_MASK) {
+          const uint8_t l = a.lab[(long long)iw * a.lab_w + (long long)y * NX + x];
+          if ((int)l == t) acc[x] = r[x];
+        } else {
+          acc[x] = cadd(acc[x], row_weight<POST>(a, t, iw, y, x, r[x]));
+        }
+      }
+      __syncwarp();
+    }
+    const float ty = post_taper ? a.tapy[y] : 1.f;
+    for (int x = lane; x < NX; x += 32) {
+      float2 v = acc[x];
+      if (post_taper) v = cscale(v, a.tapx[x] * ty);
+      if (a.add) v = cadd(a.out[roff + x], v);
+      a.out[roff + x] = v;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- column passes
+
+struct ColTiles {
+  float2 *tw, *T0, *T1, *T2;
+};
+
+__device__ __forceinline__ ColTiles col_tiles(float2* smem, int NY, int TS) {
+  ColTiles c;
+  c.tw = smem;
+  c.T0 = smem + NY;
+  c.T1 = c.T0 + NY * TS;
+  c.T2 = c.T1 + NY * TS;
+  return c;
+}
+
+__device__ __forceinline__ void tile_load(float2* T, int TS, const float2* __restrict__ src, int NX,
+                                          int NY, int x0, int TX) {
+  for (int i = threadIdx.x; i < NY * TX; i += blockDim.x) {
+    const int y = i / TX, c = i - y * TX;
+    T[y * TS + c] = src[(long long)y * NX + x0 + c];
+  }
+}
+
+__device__ __forceinline__ void tile_store(const float2* T, int TS, float2* __restrict__ dst, int NX,
+                                           int NY, int x0, int TX, int add, float scale) {
+  for (int i = threadIdx.x; i < NY * TX; i += blockDim.x) {
+    const int y = i / TX, c = i - y * TX;
+    float2 v = cscale(T[y * TS + c], scale);
+    float2* p = dst + (long long)y * NX + x0 + c;
+    if (add) v = cadd(*p, v);
+    *p = v;
+  }
+}
+
+template <int QM>
+__global__ void __launch_bounds__(256) k_col_a(const SpecArgs a, int TX, int nxt) {
+  extern __shared__ float2 smem[];
+  const int NY = a.d.NY, NX = a.d.NX, TS = TX + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  ColTiles s = col_tiles(smem, NY, TS);
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) s.tw[i] = a.twy[i];
+  const long long b = blockIdx.x / nxt;
+  const int x0 = (int)(blockIdx.x - b * nxt) * TX;
+  const int iw = (int)(b % a.d.nw);
+  tile_load(s.T0, TS, a.t1 + b * a.d.slice, NX, NY, x0, TX);
+  __syncthreads();
+  for (int c = warp; c < TX; c += nwarp) warp_fft<false>(s.T0 + c, s.T1 + c, TS, a.py, s.tw, lane);
+  const bool odd = a.py.npass & 1;
+  float2* F = odd ? s.T1 : s.T0;
+  float2* G = odd ? s.T0 : s.T1;
+  float2* H = s.T2;
+  float2* R = odd ? H : G;
+  for (int t = 0; t < a.nterm; ++t) {
+    for (int c = warp; c < TX; c += nwarp) {
+      const int x = x0 + c;
+      for (int y = lane; y < NY; y += 32) G[y * TS + c] = cmul(F[y * TS + c], qmult<QM>(a, t, iw, x, y));
+      __syncwarp();
+      warp_fft<true>(G + c, H + c, TS, a.py, s.tw, lane);
+    }
+    __syncthreads();
+    tile_store(R, TS, a.t2 + (long long)t * a.d.wfld + b * a.d.slice, NX, NY, x0, TX, 0, 1.f);
+    __syncthreads();
+  }
+}
+
+template <int QM>
+__global__ void __launch_bounds__(256) k_col_b(const SpecArgs a, int TX, int nxt) {
+  extern __shared__ float2 smem[];
+  const int NY = a.d.NY, NX = a.d.NX, TS = TX + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  ColTiles s = col_tiles(smem, NY, TS);
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) s.tw[i] = a.twy[i];
+  const long long b = blockIdx.x / nxt;
+  const int x0 = (int)(blockIdx.x - b * nxt) * TX;
+  const int iw = (int)(b % a.d.nw);
+  float2* Z = s.T2;
+  for (int i = threadIdx.x; i < NY * TS; i += blockDim.x) Z[i] = make_float2(0.f, 0.f);
+  const bool odd = a.py.npass & 1;
+  for (int t = 0; t < a.nterm; ++t) {
+    tile_load(s.T0, TS, a.t1 + (long long)t * a.d.wfld + b * a.d.slice, NX, NY, x0, TX);
+    __syncthreads();
+    float2* F = odd ? s.T1 : s.T0;
+    for (int c = warp; c < TX; c += nwarp) {
+      warp_fft<false>(s.T0 + c, s.T1 + c, TS, a.py, s.tw, lane);
+      const int x = x0 + c;
+      for (int y = lane; y < NY; y += 32)
+        Z[y * TS + c] = cadd(Z[y * TS + c], cmul(F[y * TS + c], qmult<QM>(a, t, iw, x, y)));
+    }
+    __syncthreads();
+  }
+  for (int c = warp; c < TX; c += nwarp) warp_fft<true>(Z + c, s.T0 + c, TS, a.py, s.tw, lane);
+  __syncthreads();
+  tile_store(odd ? s.T0 : Z, TS, a.t2 + b * a.d.slice, NX, NY, x0, TX, 0, 1.f);
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(256) k_col_fft(const SpecArgs a, int TX, int nxt, const float2* in,
+                                                 float2* out, int add, float scale) {
+  extern __shared__ float2 smem[];
+  const int NY = a.d.NY, NX = a.d.NX, TS = TX + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  ColTiles s = col_tiles(smem, NY, TS);
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) s.tw[i] = a.twy[i];
+  const long long b = blockIdx.x / nxt;
+  const int x0 = (int)(blockIdx.x - b * nxt) * TX;
+  tile_load(s.T0, TS, in + b * a.d.slice, NX, NY, x0, TX);
+  __syncthreads();
+  for (int c = warp; c < TX; c += nwarp) warp_fft<INV>(s.T0 + c, s.T1 + c, TS, a.py, s.tw, lane);
+  __syncthreads();
+  tile_store((a.py.npass & 1) ? s.T1 : s.T0, TS, out + b * a.d.slice, NX, NY, x0, TX, add, scale);
+}
+
+// ---------------------------------------------------------------- launch geometry
+
+struct RowGeom {
+  int nwarp, nchunk;
+  size_t smem;
+};
+
+RowGeom row_geom(const Dims& d) {
+  RowGeom g;
+  const long long per_warp = 3LL * d.NX * (long long)sizeof(float2);
+  int nw = 8;
+  while (nw > 1 && (size_t)(d.NX * sizeof(float2) + nw * per_warp) > (size_t)kMaxSmem / 2) nw >>= 1;
+  g.nwarp = nw;
+  g.nchunk = (d.NY + nw - 1) / nw;
+  g.smem = d.NX * sizeof(float2) + nw * per_warp;
+  return g;
+}
+
+struct ColGeom {
+  int TX, nxt, nwarp;
+  size_t smem;
+};
+
+ColGeom col_geom(const Dims& d) {
+  ColGeom g;
+  int tx = 16;
+  while (tx > 1 && (d.NX % tx != 0 ||
+                    (size_t)(d.NY + 3LL * d.NY * (tx + 1)) * sizeof(float2) > (size_t)kMaxSmem / 2))
+    tx >>= 1;
+  g.TX = tx;
+  g.nxt = d.NX / tx;
+  g.nwarp = std::min(tx, 8);
+  g.smem = (size_t)(d.NY + 3LL * d.NY * (tx + 1)) * sizeof(float2);
+  return g;
+}
+
+long long nblocks(long long slices, long long per) { return slices * per; }
+
+}  // namespace
+
+// ---------------------------------------------------------------- host launchers
+
+cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
+  RowGeom g = row_geom(a.d);
+  const long long blocks = nblocks((long long)a.d.ns * a.d.nw, g.nchunk);
+  dim3 grid((unsigned)blocks), block(32 * g.nwarp);
+  cudaError_t e = cudaSuccess;
+#define FWIX_ROWF(W)                                                      \
+  case W:                                                                 \
+    e = ensure_smem(k_row_forward<W>, g.smem);                            \
+    if (e == cudaSuccess) k_row_forward<W><<<grid, block, g.smem, s>>>(a, g.nchunk); \
+    break;
+  switch (pre) {
+    FWIX_ROWF(W_ONE)
+    FWIX_ROWF(W_TAPER)
+    FWIX_ROWF(W_MASK)
+    FWIX_ROWF(W_SCAT_CONJ)
+    FWIX_ROWF(W_IC)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_ROWF
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s) {
+  RowGeom g = row_geom(a.d);
+  const long long blocks = nblocks((long long)a.d.ns * a.d.nw, g.nchunk);
+  dim3 grid((unsigned)blocks), block(32 * g.nwarp);
+  cudaError_t e = cudaSuccess;
+#define FWIX_ROWI(W)                                                                  \
+  case W:                                                                             \
+    e = ensure_smem(k_row_inverse<W>, g.smem);                                        \
+    if (e == cudaSuccess) k_row_inverse<W><<<grid, block, g.smem, s>>>(a, g.nchunk, post_taper); \
+    break;
+  switch (post) {
+    FWIX_ROWI(W_ONE)
+    FWIX_ROWI(W_MASK)
+    FWIX_ROWI(W_SCAT)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_ROWI
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
+  ColGeom g = col_geom(a.d);
+  dim3 grid((unsigned)((long long)a.d.ns * a.d.nw * g.nxt)), block(32 * g.nwarp);
+  cudaError_t e = cudaSuccess;
+#define FWIX_COLA(Q)                                                              \
+  case Q:                                                                         \
+    e = ensure_smem(k_col_a<Q>, g.smem);                                          \
+    if (e == cudaSuccess) k_col_a<Q><<<grid, block, g.smem, s>>>(a, g.TX, g.nxt); \
+    break;
+  switch (qmode) {
+    FWIX_COLA(Q_PS_FWD)
+    FWIX_COLA(Q_PS_ADJ)
+    FWIX_COLA(Q_KPOW)
+    FWIX_COLA(Q_ONE)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_COLA
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s) {
+  ColGeom g = col_geom(a.d);
+  dim3 grid((unsigned)((long long)a.d.ns * a.d.nw * g.nxt)), block(32 * g.nwarp);
+  cudaError_t e = cudaSuccess;
+#define FWIX_COLB(Q)                                                              \
+  case Q:                                                                         \
+    e = ensure_smem(k_col_b<Q>, g.smem);                                          \
+    if (e == cudaSuccess) k_col_b<Q><<<grid, block, g.smem, s>>>(a, g.TX, g.nxt); \
+    break;
+  switch (qmode) {
+    FWIX_COLB(Q_PS_FWD)
+    FWIX_COLB(Q_PS_ADJ)
+    FWIX_COLB(Q_KPOW)
+    FWIX_COLB(Q_ONE)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_COLB
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add,
+                    float scale, cudaStream_t s) {
+  ColGeom g = col_geom(a.d);
+  dim3 grid((unsigned)((long long)a.d.ns * a.d.nw * g.nxt)), block(32 * g.nwarp);
+  cudaError_t e;
+  if (inverse) {
+    e = ensure_smem(k_col_fft<true>, g.smem);
+    if (e == cudaSuccess) k_col_fft<true><<<grid, block, g.smem, s>>>(a, g.TX, g.nxt, in, out, add, scale);
+  } else {
+    e = ensure_smem(k_col_fft<false>, g.smem);
+    if (e == cudaSuccess) k_col_fft<false><<<grid, block, g.smem, s>>>(a, g.TX, g.nxt, in, out, add, scale);
+  }
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+}  // namespace fwix
+
+// ---------------------------------------------------------------- single-slice operators
+// PhaseShift (phase_shift.cu:7-305), Selector (selector.cu:7-37) and Taper
+// (taper.cu:7-77) as standalone operators; inside a depth step they are fused
+// into the passes above.
+
+namespace fwix {
+namespace {
+
+template <int QM>
+__global__ void k_phase_shift(const SpecArgs a, const float2* __restrict__ in, float2* out, int add) {
+  const long long n = a.d.wfld;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % a.d.NX);
+    const long long r = i / a.d.NX;
+    const int y = (int)(r % a.d.NY);
+    const int iw = (int)((r / a.d.NY) % a.d.nw);
+    float2 v = cmul(in[i], qmult<QM>(a, 0, iw, x, y));
+    if (add) v = cadd(out[i], v);
+    out[i] = v;
+  }
+}
+
+template <int W>
+__global__ void k_weight(const SpecArgs a, int t, const float2* __restrict__ in, float2* out, int add) {
+  const long long n = a.d.wfld;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % a.d.NX);
+    const long long r = i / a.d.NX;
+    const int y = (int)(r % a.d.NY);
+    const int iw = (int)((r / a.d.NY) % a.d.nw);
+    float2 v = row_weight<W>(a, t, iw, y, x, in[i]);
+    if (add) v = cadd(out[i], v);
+    out[i] = v;
+  }
+}
+
+unsigned grid1d(long long n) {
+  long long b = (n + 255) / 256;
+  return (unsigned)std::min<long long>(b, 148LL * 32);
+}
+
+}  // namespace
+
+cudaError_t launch_phase_shift(const SpecArgs& a, int mode, const float2* sref_w, const float2* in,
+                               float2* out, int add, cudaStream_t s) {
+  SpecArgs b = a;
+  b.sref = sref_w;
+  b.norm = 1.f;
+  const unsigned g = grid1d(a.d.wfld);
+  switch (mode) {
+    case Q_PS_FWD: k_phase_shift<Q_PS_FWD><<<g, 256, 0, s>>>(b, in, out, add); break;
+    case Q_PS_ADJ: k_phase_shift<Q_PS_ADJ><<<g, 256, 0, s>>>(b, in, out, add); break;
+    case Q_PS_INV: k_phase_shift<Q_PS_INV><<<g, 256, 0, s>>>(b, in, out, add); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_select(const SpecArgs& a, int value, const float2* in, float2* out, int add,
+                          cudaStream_t s) {
+  k_weight<W_MASK><<<grid1d(a.d.wfld), 256, 0, s>>>(a, value, in, out, add);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_taper(const SpecArgs& a, const float2* in, float2* out, int add, cudaStream_t s) {
+  k_weight<W_TAPER><<<grid1d(a.d.wfld), 256, 0, s>>>(a, 0, in, out, add);
+  return cudaGetLastError();
+}
+
+}  // namespace fwix

@@ -1,0 +1,223 @@
+"""Plan object: owns a C-ABI plan, its workspace and the bound inputs.
+
+Arrays are torch CUDA tensors in the reference layouts (complex64, x fastest):
+wavefield [ns][nw][NY][NX], model [nz][nw][ny][nx], labels [nz][nw][NY][NX]
+(uint8), refs [nz][nref][nw], traces [ntrace][nw].  Every call is enqueued on
+torch's current CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+STEP_KINDS = {"pspi": L.STEP_PSPI, "nsps": L.STEP_NSPS}
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _c64(t, device):
+    t = torch.as_tensor(t)
+    if not t.is_complex():
+        t = t.to(torch.float32)
+    return t.to(device=device, dtype=torch.complex64).contiguous()
+
+
+class Plan:
+    """One wavefield geometry (NX x NY x nw x ns) over nz depth levels plus the
+    ``par`` keys of the path."""
+
+    def __init__(self, nx, ny, nw, ns, nz, dx=1.0, dy=1.0, dz=1.0, ox=0.0, oy=0.0, oz=0.0,
+                 ow=1.0, dw=1.0, padx=0, pady=0, nref=1, eps=0.0, taperx=0, tapery=0,
+                 eps_scat=0.04, taylor=1, step="pspi", device=None):
+        self.lib = L.load()
+        self.device = torch.device(device if device is not None else "cuda")
+        self.desc = L.FwixDesc(nx=nx, ny=ny, padx=padx, pady=pady, nw=nw, ns=ns, nz=nz,
+                               ox=ox, oy=oy, oz=oz, dx=dx, dy=dy, dz=dz, ow=ow, dw=dw,
+                               nref=nref, eps=eps, taperx=taperx, tapery=tapery,
+                               eps_scat=eps_scat, taylor=taylor, step_kind=STEP_KINDS[step])
+        self.nx, self.ny, self.nw, self.ns, self.nz = nx, ny, nw, ns, nz
+        self.NX, self.NY = nx + padx, ny + pady
+        self.nref, self.taylor, self.step_kind = nref, taylor, STEP_KINDS[step]
+        self._h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            L.check(self.lib.fwix_plan_create(ctypes.byref(self.desc), ctypes.byref(self._h)))
+        self._ws = None
+        self._keep = {}
+
+    # ------------------------------------------------------------------ shapes
+    @property
+    def wshape(self):
+        return (self.ns, self.nw, self.NY, self.NX)
+
+    @property
+    def mshape(self):
+        return (self.nz, self.nw, self.ny, self.nx)
+
+    def wavefield(self, zero=True):
+        f = torch.zeros if zero else torch.empty
+        return f(self.wshape, dtype=torch.complex64, device=self.device)
+
+    # ------------------------------------------------------------------ binding
+    def ensure_workspace(self, cls=L.WS_STEP):
+        need = int(self.lib.fwix_plan_workspace_bytes(self._h, cls))
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = None
+            self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+            L.check(self.lib.fwix_plan_set_workspace(self._h, _p(self._ws), need))
+        return self._ws
+
+    def set_refs(self, sref, labels):
+        """sref [nz][nref][nw] complex; labels [nz][nw or 1][NY][NX] integer."""
+        sref = _c64(sref, self.device)
+        if tuple(sref.shape) != (self.nz, self.nref, self.nw):
+            raise ValueError(f"sref shape {tuple(sref.shape)} != {(self.nz, self.nref, self.nw)}")
+        labels = torch.as_tensor(labels)
+        if labels.dim() != 4 or tuple(labels.shape[2:]) != (self.NY, self.NX) or labels.shape[0] != self.nz \
+                or labels.shape[1] not in (1, self.nw):
+            raise ValueError(f"labels shape {tuple(labels.shape)} does not match [nz][nw|1][NY][NX]")
+        if labels.numel() and (int(labels.min()) < 0 or int(labels.max()) > 255):
+            raise ValueError("labels must lie in [0, 255]")
+        labels = labels.to(device=self.device, dtype=torch.uint8).contiguous()
+        wst = 0 if labels.shape[1] == 1 else self.NY * self.NX
+        zst = labels.shape[1] * self.NY * self.NX
+        L.check(self.lib.fwix_plan_set_refs(self._h, _p(sref), _p(labels), zst, wst))
+        self._keep["sref"], self._keep["labels"] = sref, labels
+        return sref, labels
+
+    def set_model(self, slow, den):
+        """Background s^2 and density, [nz][nw or 1][ny][nx] complex."""
+        slow = _c64(slow, self.device)
+        den = _c64(den, self.device)
+        for t in (slow, den):
+            if t.dim() != 4 or tuple(t.shape[2:]) != (self.ny, self.nx) or t.shape[0] != self.nz \
+                    or t.shape[1] not in (1, self.nw):
+                raise ValueError(f"model shape {tuple(t.shape)} does not match [nz][nw|1][ny][nx]")
+        if slow.shape != den.shape:
+            raise ValueError("slowness and density shapes differ")
+        wst = 0 if slow.shape[1] == 1 else self.ny * self.nx
+        zst = slow.shape[1] * self.ny * self.nx
+        L.check(self.lib.fwix_plan_set_model(self._h, _p(slow), _p(den), zst, wst))
+        self._keep["slow"], self._keep["den"] = slow, den
+        return slow, den
+
+    # ------------------------------------------------------------------ operators
+    def fft2d(self, inp, out, inverse=False, add=False):
+        self.ensure_workspace(L.WS_STEP)
+        L.check(self.lib.fwix_fft2d(self._h, int(inverse), _p(inp), _p(out), int(add), _stream()))
+        return out
+
+    def phase_shift(self, sref_w, inp, out, mode=L.PS_FWD, add=False):
+        sref_w = _c64(sref_w, self.device)
+        L.check(self.lib.fwix_phase_shift(self._h, mode, _p(sref_w), _p(inp), _p(out), int(add), _stream()))
+        return out
+
+    def select(self, iz, value, inp, out, add=False):
+        L.check(self.lib.fwix_select(self._h, iz, value, _p(inp), _p(out), int(add), _stream()))
+        return out
+
+    def taper(self, inp, out, add=False):
+        L.check(self.lib.fwix_taper(self._h, _p(inp), _p(out), int(add), _stream()))
+        return out
+
+    def step(self, iz, inp, out, direction=L.FWD, add=False, kind=None):
+        self.ensure_workspace(L.WS_STEP)
+        k = self.step_kind if kind is None else STEP_KINDS.get(kind, kind)
+        L.check(self.lib.fwix_step(self._h, k, iz, direction, _p(inp), _p(out), int(add), _stream()))
+        return out
+
+    def scatter(self, iz, inp, out, adjoint=False, add=False):
+        self.ensure_workspace(L.WS_STEP)
+        L.check(self.lib.fwix_scatter(self._h, iz, int(adjoint), _p(inp), _p(out), int(add), _stream()))
+        return out
+
+    def reflect(self, iz, inp, out, adjoint=False, add=False):
+        L.check(self.lib.fwix_reflect(self._h, iz, int(adjoint), _p(inp), _p(out), int(add), _stream()))
+        return out
+
+    def imaging(self, bg, image, wfld, adjoint=False, add=False):
+        L.check(self.lib.fwix_imaging(self._h, int(adjoint), _p(bg), _p(image), _p(wfld), int(add), _stream()))
+
+    def lin_reflect(self, iz, dmodel, dr, adjoint=False, add=False):
+        L.check(self.lib.fwix_lin_reflect(self._h, iz, int(adjoint), _p(dmodel), _p(dr), int(add), _stream()))
+
+    def traces(self, cx, cy, cz, ids):
+        return Traces(self, cx, cy, cz, ids)
+
+    def inject(self, tr, iz, traces, wfld, adjoint=False, add=True):
+        L.check(self.lib.fwix_inject(self._h, tr._h, iz, int(adjoint), _p(traces), _p(wfld), int(add), _stream()))
+
+    # ------------------------------------------------------------------ sweeps
+    def downward(self, wfld, adjoint=False):
+        self.ensure_workspace(L.WS_STEP)
+        L.check(self.lib.fwix_downward(self._h, int(adjoint), _p(wfld), _stream()))
+        return wfld
+
+    def upward(self, wfld, adjoint=False):
+        self.ensure_workspace(L.WS_STEP)
+        L.check(self.lib.fwix_upward(self._h, int(adjoint), _p(wfld), _stream()))
+        return wfld
+
+    def propagate(self, src, rec, wavelet, data, bg_down, bg_up=None, add=False):
+        self.ensure_workspace(L.WS_SWEEP)
+        L.check(self.lib.fwix_propagate(self._h, src._h, rec._h, _p(wavelet), _p(data), int(add),
+                                        _p(bg_down), _p(bg_up), _stream()))
+        return data
+
+    def migrate(self, src, rec, wavelet, data, image, add=False):
+        self.ensure_workspace(L.WS_SWEEP)
+        L.check(self.lib.fwix_migrate(self._h, src._h, rec._h, _p(wavelet), _p(data), _p(image), int(add),
+                                      _stream()))
+        return image
+
+    def born(self, rec, bg_down, bg_up, dslow, dden, data, adjoint=False, add=False):
+        self.ensure_workspace(L.WS_BORN)
+        L.check(self.lib.fwix_born(self._h, int(adjoint), rec._h, _p(bg_down), _p(bg_up), _p(dslow), _p(dden),
+                                   _p(data), int(add), _stream()))
+
+    def __del__(self):
+        try:
+            if self._h:
+                self.lib.fwix_plan_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+
+class Traces:
+    """Trace coordinates (host) turned into per-depth gather lists on the device
+    (``propagator/src/injection.cu:33-71`` weights)."""
+
+    def __init__(self, plan, cx, cy, cz, ids):
+        self.plan = plan
+        cx = np.ascontiguousarray(cx, dtype=np.float32)
+        cy = np.ascontiguousarray(cy, dtype=np.float32)
+        cz = np.ascontiguousarray(cz, dtype=np.float32)
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        n = len(cx)
+        if not (len(cy) == len(cz) == len(ids) == n):
+            raise ValueError("coordinate and id arrays differ in length")
+        self.ntrace = n
+        self._h = ctypes.c_void_p()
+        with torch.cuda.device(plan.device):
+            L.check(plan.lib.fwix_traces_create(plan._h, n, cx.ctypes.data_as(ctypes.c_void_p),
+                                                cy.ctypes.data_as(ctypes.c_void_p),
+                                                cz.ctypes.data_as(ctypes.c_void_p),
+                                                ids.ctypes.data_as(ctypes.c_void_p), ctypes.byref(self._h)))
+
+    def __del__(self):
+        try:
+            if self._h:
+                self.plan.lib.fwix_traces_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass

@@ -1,0 +1,119 @@
+"""Parity of the depth-sweep drivers with the FP64 oracle: Downward / Upward
+(OneWay.cpp:24-79), Propagator::forward (Propagator.cpp:121-221), the lockstep
+migration image and ExtendedBorn forward / adjoint (ExtendedBorn.cpp:80-453).
+Tolerance 1e-4 relative L2 for the swept outputs (image bar of the spec)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import wem
+from tests.conftest import crandn
+from tests.gpu_helpers import make_case, make_plan, oracle_labels, rel, to_dev, to_host, wavefield
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+@pytest.mark.parametrize("kind", ["pspi", "nsps"])
+def test_down_up(kind):
+    g, rng, sref, labels, _, _ = make_case(nx=32, ny=24, nw=4, nz=6, nref=3, padx=4, pady=4)
+    lab = oracle_labels(labels, g)
+    st = wem.Stepper(g, sref, lab, kind)
+    p = make_plan(g, 2, sref, labels, step=kind)
+    x = wavefield(rng, 2, g)
+    for adj, fn in ((False, wem.downward), (True, wem.downward_adjoint)):
+        y = to_host(p.downward(to_dev(x), adjoint=adj))
+        assert rel(y, fn(st, g.nz, x)) < TOL
+    for adj, fn in ((False, wem.upward), (True, wem.upward_adjoint)):
+        y = to_host(p.upward(to_dev(x), adjoint=adj))
+        assert rel(y, fn(st, g.nz, x)) < TOL
+
+
+def _acq_case(kind="pspi", taper=3, pad=4, nz=7):
+    g, rng, sref, labels, slow, den = make_case(nx=32, ny=24, nw=4, nz=nz, nref=3, padx=pad, pady=pad,
+                                                taperx=taper, tapery=taper)
+    slow = slow.copy()
+    slow[nz - 3:] *= 1.8  # reflector
+    lab = oracle_labels(labels, g)
+    st = wem.Stepper(g, sref, lab, kind)
+    geom = dict(sx=[80.0, 200.0, 200.0], sy=[96.0, 120.0, 120.0], sz=[0.0, 5.0, 5.0], s_ids=[4, 9, 9],
+                rx=list(np.linspace(0, 300, 16)), ry=[100.0] * 16, rz=[0.0] * 8 + [12.0] * 8,
+                r_ids=[4, 9] * 8)
+    acq = wem.make_acquisition(g, geom)
+    p = make_plan(g, acq.ns, sref, labels, slow, den, step=kind)
+    src = p.traces(geom["sx"], geom["sy"], geom["sz"], acq.src.ids)
+    rec = p.traces(geom["rx"], geom["ry"], geom["rz"], acq.rec.ids)
+    wav = crandn(rng, (3, g.nw))
+    return g, rng, st, acq, p, src, rec, wav, slow, den
+
+
+@pytest.mark.parametrize("kind", ["pspi", "nsps"])
+def test_propagate(kind):
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind)
+    data, bgd, bgu = wem.propagate(g, st, acq, slow, den, wav)
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((len(acq.rec.ix), g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, to_dev(wav), d, bd, bu)
+    assert rel(to_host(d), data) < TOL
+    assert rel(to_host(bd), np.stack(bgd)) < TOL
+    assert rel(to_host(bu), np.stack(bgu)) < TOL
+    # add semantics
+    d2 = to_dev(data)
+    p.propagate(src, rec, to_dev(wav), d2, bd, bu, add=True)
+    assert rel(to_host(d2), 2 * data) < TOL
+
+
+def test_migrate():
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case()
+    data = crandn(rng, (len(acq.rec.ix), g.nw))
+    img = wem.migrate(g, st, acq, wav, data)
+    out = torch.empty((g.nz, g.ny, g.nx), dtype=torch.float32, device="cuda")
+    p.migrate(src, rec, to_dev(wav), to_dev(data), out)
+    torch.cuda.synchronize()
+    assert rel(out.cpu().numpy(), img) < TOL
+
+
+@pytest.mark.parametrize("kind,taper", [("pspi", 3), ("nsps", 0)])
+def test_born(kind, taper):
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind, taper=taper)
+    data, bgd, bgu = wem.propagate(g, st, acq, slow, den, wav)
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((len(acq.rec.ix), g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, to_dev(wav), d, bd, bu)
+    ms = crandn(rng, (g.nz, g.nw, g.ny, g.nx))
+    mr = crandn(rng, (g.nz, g.nw, g.ny, g.nx))
+    ref = wem.born_forward(g, st, acq, slow, den, bgd, bgu, ms, mr)
+    out = torch.empty_like(d)
+    p.born(rec, bd, bu, to_dev(ms), to_dev(mr), out)
+    assert rel(to_host(out), ref) < TOL
+    r = crandn(rng, d.shape)
+    gs_ref, gr_ref = wem.born_adjoint(g, st, acq, slow, den, bgd, bgu, r)
+    gs = torch.empty((g.nz, g.nw, g.ny, g.nx), dtype=torch.complex64, device="cuda")
+    gr = torch.empty_like(gs)
+    p.born(rec, bd, bu, gs, gr, to_dev(r), adjoint=True)
+    assert rel(to_host(gs), gs_ref) < TOL
+    assert rel(to_host(gr), gr_ref) < TOL
+
+
+def test_born_dot_product_device():
+    """ExtendedBorn dot test (propagator/src/ExtendedBorn.h:61-128) entirely on the
+    device, taper off as in born_unit_test.cpp:392-393."""
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case("pspi", taper=0)
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((len(acq.rec.ix), g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, to_dev(wav), d, bd, bu)
+    ms = crandn(rng, (g.nz, g.nw, g.ny, g.nx))
+    mr = crandn(rng, (g.nz, g.nw, g.ny, g.nx))
+    r = crandn(rng, d.shape)
+    out = torch.empty_like(d)
+    p.born(rec, bd, bu, to_dev(ms), to_dev(mr), out)
+    gs = torch.empty((g.nz, g.nw, g.ny, g.nx), dtype=torch.complex64, device="cuda")
+    gr = torch.empty_like(gs)
+    p.born(rec, bd, bu, gs, gr, to_dev(r), adjoint=True)
+    lhs = np.vdot(r.ravel(), to_host(out).ravel())
+    rhs = np.vdot(to_host(gs).ravel(), ms.ravel()) + np.vdot(to_host(gr).ravel(), mr.ravel())
+    assert abs((lhs / rhs).real - 1) < 1e-5
