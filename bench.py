@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark of the one-way WEM depth-stepping path on B200.
+
+Workload (default, ``--config config2``): Born forward + adjoint (migration) with
+NSPS on one shot, 256 x 256 x 200, 128 frequencies (3-40 Hz), seeded synthetic
+model (see pyfwix_b200/workloads.py).  One step = ExtendedBorn forward of the
+5-layer reflectivity (all four scattering sweeps) followed by ExtendedBorn
+adjoint of the data it produced (the FWI/migration gradient), with the
+background wavefields already computed and resident in HBM.
+
+Metric: Gcell-steps/s, one cell-step = one (x, y, w) sample advanced one depth
+level, counted once per operator application (Born forward and Born adjoint:
+2 * nx*ny*nw*nz per step).
+
+Under torchrun each rank runs its own shot (independent replicas, no collective
+on the data path): value = cell-steps of all ranks / max-over-ranks time,
+scaling "weak".
+
+``--impl reference`` times the reference path's CPU restatement (the oracle in
+complex64 with scipy.fft on all host threads) on a bounded slab of the same
+workload; the reference itself has no CPU implementation of this path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-steps/s (x*y*w*z), Born forward + adjoint"
+HBM_FALLBACK_GBS = 6650.0
+ALG_BYTES_PER_CELL_STEP = 16  # one wavefield read + written once per depth step
+
+
+def args_():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--config", default="config2")
+    ap.add_argument("--nz", type=int, default=None, help="override depth count (quick runs only)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- helpers
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def profiled_traffic(name):
+    """Per-step DRAM bytes of the depth step from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_step:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ----------------------------------------------------------------------------- B200 arm
+
+def setup_born(w, device):
+    import torch
+
+    from pyfwix_b200 import refsampler
+    from pyfwix_b200.plan import Plan
+
+    plan = Plan(ns=1, device=device, **w.plan_kwargs())
+    s2 = torch.as_tensor(w.slow2)[:, None].to(device)                    # [nz][1][ny][nx]
+    sref, labels = refsampler.sample(s2, w.nref, w.padx, w.pady)
+    plan.set_refs(refsampler.expand_refs(sref, w.nw), labels)
+    s2c = s2.to(torch.complex64)
+    plan.set_model(s2c, torch.ones_like(s2c))
+    g = w.geom
+    src = plan.traces(g["sx"], g["sy"], g["sz"], np.zeros(len(g["sx"]), np.int32))
+    rec = plan.traces(g["rx"], g["ry"], g["rz"], np.zeros(len(g["rx"]), np.int32))
+    wav = torch.as_tensor(w.wavelet).to(device)
+    bd = torch.empty((w.nz,) + plan.wshape, dtype=torch.complex64, device=device)
+    bu = torch.empty_like(bd)
+    data = torch.empty((len(g["rx"]), w.nw), dtype=torch.complex64, device=device)
+    plan.propagate(src, rec, wav, data, bd, bu)
+    dslow = torch.as_tensor(w.dslow)[:, None].to(device).to(torch.complex64)
+    dden = torch.zeros_like(dslow)
+    gs = torch.empty_like(dslow)
+    gr = torch.empty_like(dslow)
+    plan.ensure_workspace(2)
+    torch.cuda.synchronize()
+    return dict(plan=plan, rec=rec, bd=bd, bu=bu, data=data, dslow=dslow, dden=dden, gs=gs, gr=gr)
+
+
+def born_step(st):
+    p = st["plan"]
+    p.born(st["rec"], st["bd"], st["bu"], st["dslow"], st["dden"], st["data"])
+    p.born(st["rec"], st["bd"], st["bu"], st["gs"], st["gr"], st["data"], adjoint=True)
+
+
+def born_step_e2e(st, host):
+    """Same step through the public API with host buffers: the perturbation goes in
+    from pinned host memory, the data comes back, goes in again for the adjoint,
+    and the gradient comes back."""
+    p = st["plan"]
+    st["dslow"].copy_(host["dslow"], non_blocking=True)
+    st["dden"].copy_(host["dden"], non_blocking=True)
+    p.born(st["rec"], st["bd"], st["bu"], st["dslow"], st["dden"], st["data"])
+    host["data"].copy_(st["data"], non_blocking=True)
+    st["data"].copy_(host["data"], non_blocking=True)
+    p.born(st["rec"], st["bd"], st["bu"], st["gs"], st["gr"], st["data"], adjoint=True)
+    host["gs"].copy_(st["gs"], non_blocking=True)
+    host["gr"].copy_(st["gr"], non_blocking=True)
+
+
+def time_steps(fn, k, barrier):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(k):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    return e0.elapsed_time(e1) / 1e3  # seconds
+
+
+def step_roofline(st, w, reps=20):
+    """Average duration of one NSPS depth step (row + column + row passes) on this
+    workload's wavefield, timed with CUDA events on the launching stream."""
+    import torch
+    p = st["plan"]
+    x = st["bd"][w.nz // 2].clone()
+    for _ in range(3):
+        p.step(w.nz // 2, x, x)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        p.step(w.nz // 2, x, x)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+# ----------------------------------------------------------------------------- CPU arm
+
+class CpuBorn:
+    """FP32 CPU restatement (the oracle in complex64, scipy.fft on all host threads)
+    of one Born forward + adjoint on a slab of the workload: nz_s depth levels and
+    nw_s frequencies at full lateral size."""
+
+    def __init__(self, nz_s=2, nw_s=16):
+        from oracle import wem
+        from pyfwix_b200 import workloads
+
+        self.wem = wem
+        w = workloads.config2(nz=nz_s, nw=nw_s)
+        self.w = w
+        g = wem.Grid(nx=w.nx, ny=w.ny, nw=w.nw, nz=w.nz, dx=w.dx, dy=w.dy, dz=w.dz, ow=w.ow, dw=w.dw,
+                     nref=w.nref, taperx=w.taperx, tapery=w.tapery, eps_scat=w.eps_scat, taylor=w.taylor,
+                     dtype=np.complex64)
+        s2 = w.slow2.astype(np.float64)
+        s = np.sqrt(s2)
+        q = (np.arange(w.nref) * 2 + 1) / (2 * w.nref)
+        sref = np.empty((w.nz, w.nref, w.nw), np.complex64)
+        labels = np.empty((w.nz, w.nw, w.ny, w.nx), np.int64)
+        for iz in range(w.nz):
+            c = np.quantile(s[iz], q) ** 2
+            sref[iz] = c[:, None]
+            labels[iz] = np.argmin(np.abs(s2[iz][..., None] - c), axis=-1)[None]
+        self.slow = np.broadcast_to(s2[:, None], (w.nz, w.nw, w.ny, w.nx)).astype(np.complex64)
+        self.den = np.ones_like(self.slow)
+        self.g, self.st = g, wem.Stepper(g, sref, labels, w.step)
+        self.acq = wem.make_acquisition(g, w.geom)
+        self.cores = os.cpu_count() or 1
+        wem.set_fft_workers(self.cores)
+        try:
+            _, self.bgd, self.bgu = wem.propagate(g, self.st, self.acq, self.slow, self.den, w.wavelet)
+        finally:
+            wem.set_fft_workers(None)
+        self.ds = np.broadcast_to(w.dslow[:, None], self.slow.shape).astype(np.complex64)
+        self.dr = np.zeros_like(self.ds)
+        self.cells = 2 * w.nx * w.ny * w.nw * w.nz
+
+    def step(self):
+        wem = self.wem
+        wem.set_fft_workers(self.cores)
+        try:
+            t0 = time.perf_counter()
+            d = wem.born_forward(self.g, self.st, self.acq, self.slow, self.den, self.bgd, self.bgu, self.ds, self.dr)
+            wem.born_adjoint(self.g, self.st, self.acq, self.slow, self.den, self.bgd, self.bgu,
+                             d.astype(np.complex64))
+            return time.perf_counter() - t0
+        finally:
+            wem.set_fft_workers(None)
+
+    def describe(self, value):
+        w = self.w
+        return {"value": value, "unit": "Gcell-steps/s", "cores": self.cores, "kind": "port",
+                "sample": f"Born fwd+adj on a {w.nz}-level x {w.nw}-frequency slab at {w.nx}x{w.ny} "
+                          f"(complex64 oracle port, scipy.fft workers={self.cores})"}
+
+
+def cpu_baseline():
+    c = CpuBorn()
+    t = c.step()
+    return c.describe(c.cells / t / 1e9)
+
+
+def run_reference(a):
+    ws, rank, local = dist()
+    if rank != 0:
+        return
+    c = CpuBorn(nz_s=2, nw_s=8)
+    for _ in range(max(a.warmup, 0)):
+        c.step()
+    ts = [c.step() for _ in range(a.steps)]
+    t = float(np.mean(ts))
+    v = c.cells / t / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Gcell-steps/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded)",
+            "config": {"workload": "born-nsps-256x256x200-nw128 (CPU sample: 2 levels x 8 frequencies)",
+                       "global_batch": 1, "parallelism": "host threads"},
+            "cpu_baseline": c.describe(v),
+            "e2e": {"value": v, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- main
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    ws, rank, local = dist()
+    if ws > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        barrier = lambda: tdist.barrier(device_ids=[local])
+    else:
+        torch.cuda.set_device(0)
+        barrier = lambda: None
+    device = torch.device("cuda", torch.cuda.current_device())
+    from pyfwix_b200 import workloads
+    w = workloads.CONFIGS[a.config](nz=a.nz)
+    st = setup_born(w, device)
+    for _ in range(a.warmup):
+        born_step(st)
+    torch.cuda.synchronize()
+    from pyfwix_b200 import _lib
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    n0 = _lib.load().fwix_launch_count()
+    t = time_steps(lambda: born_step(st), a.steps, barrier)
+    launches = int(_lib.load().fwix_launch_count() - n0)
+    clk = clocks.stop()
+    if ws > 1:
+        tt = torch.tensor([t], device=device)
+        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+        t = float(tt.item())
+    cells = 2 * w.nx * w.ny * w.nw * w.nz
+    value = ws * cells * a.steps / t / 1e9
+    # end to end through the host buffers
+    e2e = None
+    if not a.no_e2e:
+        host = {k: torch.empty(st[k].shape, dtype=st[k].dtype, pin_memory=True)
+                for k in ("dslow", "dden", "gs", "gr", "data")}
+        host["dslow"].copy_(st["dslow"].cpu())
+        host["dden"].zero_()
+        born_step_e2e(st, host)
+        te = time_steps(lambda: born_step_e2e(st, host), a.steps, barrier)
+        if ws > 1:
+            tt = torch.tensor([te], device=device)
+            tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+            te = float(tt.item())
+        nb = lambda k: host[k].numel() * host[k].element_size()
+        e2e = {"value": ws * cells * a.steps / te / 1e9, "unit": "Gcell-steps/s",
+               "h2d_bytes_per_step": nb("dslow") + nb("dden") + nb("data"),
+               "d2h_bytes_per_step": nb("data") + nb("gs") + nb("gr")}
+    # roofline of the depth step
+    tstep = step_roofline(st, w)
+    cells_step = w.nx * w.ny * w.nw
+    peak, peak_kind = measured_peak()
+    achieved = ALG_BYTES_PER_CELL_STEP * cells_step / tstep / 1e9
+    traffic = profiled_traffic("nsps_step_256x256x128.txt") if (w.nx, w.nw) == (256, 128) else None
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_source": peak_kind,
+            "kernel": "NSPS depth step (row pass + column pass + row pass), 256x256x128",
+            "step_ms": tstep * 1e3, "alg_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP}
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu:
+        cpu = cpu_baseline()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": ws, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": t / a.steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded)",
+                "config": {"workload": w.name + ("" if a.nz is None else f" (nz={w.nz})"),
+                           "global_batch": ws, "seq_len": None, "parallelism": f"shot replicas x{ws}",
+                           "l2": "inputs larger than L2 (background wavefields 2 x %.1f GB)"
+                                 % (st["bd"].numel() * 8 / 1e9)},
+                "gpu_launches": launches, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -98,6 +98,8 @@ typedef struct fwix_traces fwix_traces;
 
 const char* fwix_last_error(void);
 int fwix_version(void);
+/* Kernels this library has enqueued since it was loaded (all plans, all threads). */
+uint64_t fwix_launch_count(void);
 
 /* ---- plan ------------------------------------------------------------------ */
 fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** plan);
@@ -163,11 +165,14 @@ fwix_status fwix_propagate(fwix_plan* plan, const fwix_traces* src, const fwix_t
 fwix_status fwix_migrate(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
                          const void* wavelet, const void* data, float* image, int add,
                          void* stream);
-/* Extended Born: forward (dslow, dden) -> data, adjoint data -> (dslow, dden);
- * dslow/dden are [nz][nw][ny][nx]. */
+/* Extended Born: forward (dslow, dden) -> data, adjoint data -> (dslow, dden).
+ * dslow/dden element (iz, iw, y, x) at iz*nw'*ny*nx + iw*model_w_stride + y*nx + x
+ * with model_w_stride = ny*nx (nw' = nw, the reference domain [nz][nw][ny][nx]) or
+ * 0 (nw' = 1: one perturbation per depth shared by every frequency; the adjoint
+ * then returns the sum over frequency, the transpose of that broadcast). */
 fwix_status fwix_born(fwix_plan* plan, int adjoint, const fwix_traces* rec, const void* bg_down,
-                      const void* bg_up, void* dslow, void* dden, void* data, int add,
-                      void* stream);
+                      const void* bg_up, void* dslow, void* dden, int64_t model_w_stride,
+                      void* data, int add, void* stream);
 
 #ifdef __cplusplus
 }

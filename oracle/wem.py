@@ -216,10 +216,11 @@ def pspi_forward(g, sref_z, labels_z, m, d=None, taper=True):
     d (+)= sum_r mask_r * F^-1( P_r * F(taper * m) ).  The in-place overload
     (``propagator/src/PSPI.cpp:66-83``) is the same map with d = 0."""
     kx, ky, w2 = g.kx(), g.ky(), g.w2()
-    mk = fft2((g.taper()[None, None] if taper else 1.0) * m)
+    tap = g.taper().astype(m.real.dtype) if taper else 1.0
+    mk = fft2(tap * m)
     out = np.zeros_like(m) if d is None else d.copy()
     for r in range(g.nref):
-        P = phase_forward_factor(w2, kx, ky, sref_z[r], g.dz, g.eps)
+        P = phase_forward_factor(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(m.dtype)
         ref = ifft2(mk * P[None])
         out += select(labels_z, r, ref)
     return out.astype(m.dtype, copy=False)
@@ -233,11 +234,11 @@ def pspi_adjoint(g, sref_z, labels_z, d, m=None, taper=False):
     kx, ky, w2 = g.kx(), g.ky(), g.w2()
     mk = np.zeros_like(d)
     for r in range(g.nref):
-        Q = phase_adjoint_factor(w2, kx, ky, sref_z[r], g.dz, g.eps)
+        Q = phase_adjoint_factor(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(d.dtype)
         mk = mk + Q[None] * fft2(select(labels_z, r, d))
     x = ifft2(mk)
     if taper:
-        x = g.taper()[None, None] * x
+        x = g.taper().astype(d.real.dtype)[None, None] * x
     out = x if m is None else m + x
     return out.astype(d.dtype, copy=False)
 
@@ -248,7 +249,7 @@ def nsps_forward(g, sref_z, labels_z, m, d=None):
     kx, ky, w2 = g.kx(), g.ky(), g.w2()
     mk = np.zeros_like(m)
     for r in range(g.nref):
-        P = phase_forward_factor(w2, kx, ky, sref_z[r], g.dz, g.eps)
+        P = phase_forward_factor(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(m.dtype)
         mk = mk + P[None] * fft2(select(labels_z, r, m))
     x = ifft2(mk)
     out = x if d is None else d + x
@@ -262,7 +263,7 @@ def nsps_adjoint(g, sref_z, labels_z, d, m=None):
     dk = fft2(d)
     out = np.zeros_like(d) if m is None else m.copy()
     for r in range(g.nref):
-        Q = phase_adjoint_factor(w2, kx, ky, sref_z[r], g.dz, g.eps)
+        Q = phase_adjoint_factor(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(d.dtype)
         out += select(labels_z, r, ifft2(Q[None] * dk))
     return out.astype(d.dtype, copy=False)
 
@@ -362,32 +363,30 @@ def make_traces(cx, cy, cz, ids, ox, oy, dx, dy, oz, dz, NX, NY):
                   lz.astype(np.float64), np.asarray(ids, dtype=np.int64), valid)
 
 
-def _trace_weights(tr, t, iz_inj):
-    if not tr.valid[t]:
-        return None
-    if iz_inj == tr.iz[t]:
-        z = tr.lz[t]
-    elif iz_inj == tr.iz[t] + 1:
-        z = 1.0 - tr.lz[t]
-    else:
-        return None
-    lx, ly = tr.lx[t], tr.ly[t]
-    return (z * lx * ly, z * (1 - lx) * ly, z * lx * (1 - ly), z * (1 - lx) * (1 - ly))
+def _level_weights(tr, iz_inj):
+    """Active traces at depth level ``iz_inj`` and their four corner weights
+    (``propagator/src/injection.cu:46-71``): lz on level iz, 1-lz on level iz+1."""
+    on0 = tr.valid & (tr.iz == iz_inj)
+    on1 = tr.valid & (tr.iz + 1 == iz_inj)
+    act = np.nonzero(on0 | on1)[0]
+    z = np.where(on0[act], tr.lz[act], 1.0 - tr.lz[act])
+    lx, ly = tr.lx[act], tr.ly[act]
+    w = np.stack([z * lx * ly, z * (1 - lx) * ly, z * lx * (1 - ly), z * (1 - lx) * (1 - ly)])
+    return act, w
 
 
 def inject(tr, traces, wfld, iz_inj):
     """``inj_forward`` (``propagator/src/injection.cu:7-96``): wfld += weights x trace
     at the 4 surrounding nodes of depth level ``iz_inj``."""
     out = wfld.copy()
-    for t in range(len(tr.ix)):
-        w = _trace_weights(tr, t, iz_inj)
-        if w is None:
-            continue
-        s, ix, iy = tr.ids[t], tr.ix[t], tr.iy[t]
-        out[s, :, iy, ix] += w[0] * traces[t]
-        out[s, :, iy, ix + 1] += w[1] * traces[t]
-        out[s, :, iy + 1, ix] += w[2] * traces[t]
-        out[s, :, iy + 1, ix + 1] += w[3] * traces[t]
+    act, w = _level_weights(tr, iz_inj)
+    if len(act) == 0:
+        return out
+    s, ix, iy = tr.ids[act], tr.ix[act], tr.iy[act]
+    tv = traces[act]                                        # [na][nw]
+    for k, (dy, dx) in enumerate(((0, 0), (0, 1), (1, 0), (1, 1))):
+        np.add.at(out, (s[:, None], np.arange(out.shape[1])[None, :], (iy + dy)[:, None], (ix + dx)[:, None]),
+                  w[k][:, None] * tv)
     return out
 
 
@@ -395,13 +394,14 @@ def record(tr, wfld, traces, iz_inj):
     """``inj_adjoint`` (``propagator/src/injection.cu:98-188``): traces += weighted
     gather of the 4 surrounding nodes."""
     out = traces.copy()
-    for t in range(len(tr.ix)):
-        w = _trace_weights(tr, t, iz_inj)
-        if w is None:
-            continue
-        s, ix, iy = tr.ids[t], tr.ix[t], tr.iy[t]
-        out[t] += (w[0] * wfld[s, :, iy, ix] + w[1] * wfld[s, :, iy, ix + 1]
-                   + w[2] * wfld[s, :, iy + 1, ix] + w[3] * wfld[s, :, iy + 1, ix + 1])
+    act, w = _level_weights(tr, iz_inj)
+    if len(act) == 0:
+        return out
+    s, ix, iy = tr.ids[act], tr.ix[act], tr.iy[act]
+    acc = 0
+    for k, (dy, dx) in enumerate(((0, 0), (0, 1), (1, 0), (1, 1))):
+        acc = acc + w[k][:, None] * wfld[s, :, iy + dy, ix + dx]
+    np.add.at(out, act, acc)
     return out
 
 
@@ -494,8 +494,8 @@ def scatter_kfilters(g):
 def scatter_forward(g, slow_slice, u, d=None):
     """``Scatter::cu_forward`` (``propagator/src/Scatter.cpp:76-88``; in place
     ``:104-116``): d (+)= sum_n W_n * F^-1(Q_n * F(u))."""
-    W = scatter_weights(g, slow_slice)
-    Q = scatter_kfilters(g)
+    W = [w.astype(u.dtype) for w in scatter_weights(g, slow_slice)]
+    Q = [q.astype(u.real.dtype) for q in scatter_kfilters(g)]
     uk = fft2(u)
     out = np.zeros_like(u) if d is None else d.copy()
     for n in range(g.taylor + 1):
@@ -506,8 +506,8 @@ def scatter_forward(g, slow_slice, u, d=None):
 def scatter_adjoint(g, slow_slice, d, u=None):
     """``Scatter::cu_adjoint`` (``propagator/src/Scatter.cpp:91-102``; in place
     ``:118-133``): u (+)= sum_n F^-1(Q_n * F(conj(W_n) * d))."""
-    W = scatter_weights(g, slow_slice)
-    Q = scatter_kfilters(g)
+    W = [w.astype(d.dtype) for w in scatter_weights(g, slow_slice)]
+    Q = [q.astype(d.real.dtype) for q in scatter_kfilters(g)]
     out = np.zeros_like(d) if u is None else u.copy()
     for n in range(g.taylor + 1):
         out += ifft2(Q[n][None] * fft2(np.conj(W[n])[None] * d))

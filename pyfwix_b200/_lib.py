@@ -44,6 +44,7 @@ I64 = ctypes.c_int64
 SIGNATURES = {
     "fwix_last_error": [],
     "fwix_version": [],
+    "fwix_launch_count": [],
     "fwix_plan_create": [ctypes.POINTER(FwixDesc), ctypes.POINTER(P)],
     "fwix_plan_destroy": [P],
     "fwix_plan_workspace_bytes": [P, I],
@@ -66,9 +67,10 @@ SIGNATURES = {
     "fwix_upward": [P, I, P, P],
     "fwix_propagate": [P, P, P, P, P, I, P, P, P],
     "fwix_migrate": [P, P, P, P, P, P, I, P],
-    "fwix_born": [P, I, P, P, P, P, P, P, I, P],
+    "fwix_born": [P, I, P, P, P, P, P, I64, P, I, P],
 }
-_RET = {"fwix_last_error": ctypes.c_char_p, "fwix_version": I, "fwix_plan_workspace_bytes": ctypes.c_size_t}
+_RET = {"fwix_last_error": ctypes.c_char_p, "fwix_version": I, "fwix_plan_workspace_bytes": ctypes.c_size_t,
+        "fwix_launch_count": ctypes.c_uint64}
 
 _lib = None
 

@@ -4,6 +4,7 @@
 // numerical operation is a kernel of spectral.cu / pointwise.cu enqueued on the
 // caller's stream.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -15,6 +16,11 @@
 
 using fwix::Dims;
 using fwix::SpecArgs;
+
+namespace fwix {
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace fwix
 
 namespace {
 
@@ -237,10 +243,11 @@ SpecArgs scatter_args(const fwix_plan* p, int iz, const float2* in, float2* out,
 // forward input is the imaging-condition product bg * image (ImagingCondition fwd,
 // imaging_condition.cu:9-55) formed inside the first pass.
 fwix_status do_scatter(fwix_plan* p, int iz, int adjoint, const float2* in, float2* out, int add,
-                       const float2* image, cudaStream_t s) {
+                       const float2* image, long long img_w, cudaStream_t s) {
   SpecArgs a = scatter_args(p, iz, in, out, add);
   if (!adjoint) {
     a.image = image;
+    a.img_w = img_w;
     FWIX_TRY(cu(fwix::row_forward(a, image ? fwix::W_IC : fwix::W_ONE, s), "scatter row pass"));
     FWIX_TRY(cu(fwix::col_type_a(a, fwix::Q_KPOW, s), "scatter column pass"));
     FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_SCAT, 0, s), "scatter inverse row pass"));
@@ -282,18 +289,18 @@ fwix_status do_record(fwix_plan* p, const fwix_traces* tr, int iz, const float2*
 }
 
 // ForwardScattering::cu_forward (Scattering.cpp:43-52): target += step_add(scatter(bg * image)).
-fwix_status fscat_fwd(fwix_plan* p, int iz_prop, const float2* bg, const float2* image, float2* target,
-                      cudaStream_t s) {
-  FWIX_TRY(do_scatter(p, iz_prop, 0, bg, p->wSC(), 0, image, s));
+fwix_status fscat_fwd(fwix_plan* p, int iz_prop, const float2* bg, const float2* image, long long img_w,
+                      float2* target, cudaStream_t s) {
+  FWIX_TRY(do_scatter(p, iz_prop, 0, bg, p->wSC(), 0, image, img_w, s));
   return do_step(p, p->desc.step_kind, iz_prop, FWIX_FWD, p->wSC(), target, 1, s);
 }
 
 // ForwardScattering::cu_adjoint (Scattering.cpp:54-61): gimage += ic_adj(scatter^T(step_adj_add(wfld))).
 fwix_status fscat_adj(fwix_plan* p, int iz_prop, const float2* bg, const float2* wfld, float2* gimage,
-                      cudaStream_t s) {
+                      long long img_w, cudaStream_t s) {
   FWIX_TRY(do_step(p, p->desc.step_kind, iz_prop, FWIX_ADJ_ADD, wfld, p->wSC(), 0, s));
-  FWIX_TRY(do_scatter(p, iz_prop, 1, p->wSC(), p->wSC(), 0, nullptr, s));
-  return cu(fwix::launch_ic_adj(p->d, bg, p->wSC(), gimage, 1, s), "imaging adjoint");
+  FWIX_TRY(do_scatter(p, iz_prop, 1, p->wSC(), p->wSC(), 0, nullptr, 0, s));
+  return cu(fwix::launch_ic_adj(p->d, bg, p->wSC(), gimage, img_w, 1, s), "imaging adjoint");
 }
 
 long long mslice(const fwix_plan* p) { return (long long)p->d.nw * p->d.ny * p->d.nx; }
@@ -306,6 +313,8 @@ extern "C" {
 const char* fwix_last_error(void) { return g_err.c_str(); }
 
 int fwix_version(void) { return 100; }
+
+uint64_t fwix_launch_count(void) { return fwix::g_launches.load(std::memory_order_relaxed); }
 
 fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
   if (!desc || !out) return fail(FWIX_ERR_INVALID, "null descriptor or output");
@@ -459,7 +468,7 @@ fwix_status fwix_scatter(fwix_plan* p, int iz, int adjoint, const void* in, void
   FWIX_TRY(need_model(p));
   FWIX_TRY(need_ws(p, FWIX_WS_STEP));
   FWIX_TRY(check_iz(p, iz));
-  return do_scatter(p, iz, adjoint, (const float2*)in, (float2*)out, add, nullptr, (cudaStream_t)stream);
+  return do_scatter(p, iz, adjoint, (const float2*)in, (float2*)out, add, nullptr, 0, (cudaStream_t)stream);
 }
 
 fwix_status fwix_reflect(fwix_plan* p, int iz, int adjoint, const void* in, void* out, int add, void* stream) {
@@ -473,10 +482,11 @@ fwix_status fwix_imaging(fwix_plan* p, int adjoint, const void* bg, void* image,
                          void* stream) {
   if (!p || !bg || !image || !wfld) return fail(FWIX_ERR_INVALID, "null argument");
   cudaStream_t s = (cudaStream_t)stream;
+  const long long iw = (long long)p->d.ny * p->d.nx;
   if (!adjoint)
-    return cu(fwix::launch_ic_fwd(p->d, (const float2*)bg, (const float2*)image, (float2*)wfld, add, s),
+    return cu(fwix::launch_ic_fwd(p->d, (const float2*)bg, (const float2*)image, iw, (float2*)wfld, add, s),
               "imaging forward");
-  return cu(fwix::launch_ic_adj(p->d, (const float2*)bg, (const float2*)wfld, (float2*)image, add, s),
+  return cu(fwix::launch_ic_adj(p->d, (const float2*)bg, (const float2*)wfld, (float2*)image, iw, add, s),
             "imaging adjoint");
 }
 
@@ -489,7 +499,8 @@ fwix_status fwix_lin_reflect(fwix_plan* p, int iz, int adjoint, void* dmodel, vo
   const long long n = mslice(p);
   return cu(fwix::launch_lin_reflect(p->d, adjoint, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
                                      p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, dm, dm + n,
-                                     dm + 2 * n, dm + 3 * n, (float2*)dr, add, (cudaStream_t)stream),
+                                     dm + 2 * n, dm + 3 * n, (long long)p->d.ny * p->d.nx, (float2*)dr, add,
+                                     (cudaStream_t)stream),
             "linearised reflection");
 }
 
@@ -723,15 +734,20 @@ fwix_status fwix_migrate(fwix_plan* p, const fwix_traces* src, const fwix_traces
 
 // ExtendedBorn::forward / adjoint (ExtendedBorn.cpp:80-453).
 fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const void* bg_down_v,
-                      const void* bg_up_v, void* dslow_v, void* dden_v, void* data_v, int add, void* stream) {
+                      const void* bg_up_v, void* dslow_v, void* dden_v, int64_t model_w_stride, void* data_v,
+                      int add, void* stream) {
   if (!p || !rec || !bg_down_v || !bg_up_v || !dslow_v || !dden_v || !data_v)
     return fail(FWIX_ERR_INVALID, "null argument");
+  const long long plane = (long long)p->d.ny * p->d.nx;
+  if (model_w_stride != 0 && model_w_stride != plane)
+    return fail(FWIX_ERR_INVALID, "model_w_stride must be 0 or ny*nx");
+  const long long mw = model_w_stride;
   FWIX_TRY(need_refs(p));
   FWIX_TRY(need_model(p));
   FWIX_TRY(need_ws(p, FWIX_WS_BORN));
   cudaStream_t s = (cudaStream_t)stream;
   const int nz = p->desc.nz, k = p->desc.step_kind;
-  const long long W = p->d.wfld, M = mslice(p);
+  const long long W = p->d.wfld, M = mw ? mslice(p) : plane;
   const float2* bgd = (const float2*)bg_down_v;
   const float2* bgu = (const float2*)bg_up_v;
   float2* ds = (float2*)dslow_v;
@@ -750,7 +766,7 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
       FWIX_TRY(do_record(p, rec, iz, cur, data, s));
       if (iz == nz - 1) break;  // the last step feeds nothing that is recorded or stored
       FWIX_TRY(do_step(p, k, iz, FWIX_FWD, cur, next, 0, s));
-      FWIX_TRY(fscat_fwd(p, iz, bgd + iz * W, ds + iz * M, next, s));
+      FWIX_TRY(fscat_fwd(p, iz, bgd + iz * W, ds + iz * M, mw, next, s));
     }
     // 2. reflected up by the background (ExtendedBorn.cpp:210-238)
     FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
@@ -765,7 +781,7 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
       FWIX_TRY(do_record(p, rec, iz, A, data, s));
       if (iz > 0) {
         FWIX_TRY(do_step(p, k, iz - 1, FWIX_FWD, A, A, 0, s));
-        FWIX_TRY(fscat_fwd(p, iz - 1, bgu + iz * W, ds + iz * M, A, s));
+        FWIX_TRY(fscat_fwd(p, iz - 1, bgu + iz * W, ds + iz * M, mw, A, s));
       }
     }
     // 4. back scattering (ExtendedBorn.cpp:352-389)
@@ -775,9 +791,9 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
       if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s));
       FWIX_TRY(cu(fwix::launch_lin_reflect(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
                                            p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                           ds + z1 * M, dr + iz * M, dr + z1 * M, DR, 0, s),
+                                           ds + z1 * M, dr + iz * M, dr + z1 * M, mw, DR, 0, s),
                   "linearised reflection"));
-      FWIX_TRY(cu(fwix::launch_ic_fwd(p->d, bgd + iz * W, DR, A, 1, s), "imaging forward"));
+      FWIX_TRY(cu(fwix::launch_ic_fwd(p->d, bgd + iz * W, DR, plane, A, 1, s), "imaging forward"));
       FWIX_TRY(do_record(p, rec, iz, A, data, s));
     }
     return FWIX_OK;
@@ -793,7 +809,7 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
     float2* cur = p->store(iz);
     if (iz > 0) {
       float2* prev = p->store(iz - 1);
-      FWIX_TRY(fscat_adj(p, iz - 1, bgu + iz * W, prev, ds + iz * M, s));
+      FWIX_TRY(fscat_adj(p, iz - 1, bgu + iz * W, prev, ds + iz * M, mw, s));
       FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_INPL, prev, cur, 0, s));
     }
     FWIX_TRY(do_inject(p, rec, iz, data, cur, s));
@@ -803,7 +819,7 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
   FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
   for (int iz = nz - 1; iz >= 0; --iz) {
     if (iz < nz - 1) {
-      FWIX_TRY(fscat_adj(p, iz, bgd + iz * W, A, ds + iz * M, s));
+      FWIX_TRY(fscat_adj(p, iz, bgd + iz * W, A, ds + iz * M, mw, s));
       FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, A, A, 0, s));
     }
     FWIX_TRY(do_reflect(p, iz, 1, p->store(iz), A, 1, s));
@@ -814,10 +830,10 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
   for (int iz = 0; iz < nz; ++iz) {
     const int z1 = lower_iz(p, iz);
     FWIX_TRY(do_inject(p, rec, iz, data, A, s));
-    FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgd + iz * W, A, DR, 0, s), "imaging adjoint"));
+    FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgd + iz * W, A, DR, plane, 0, s), "imaging adjoint"));
     FWIX_TRY(cu(fwix::launch_lin_reflect(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
                                          p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                         ds + z1 * M, dr + iz * M, dr + z1 * M, DR, 1, s),
+                                         ds + z1 * M, dr + iz * M, dr + z1 * M, mw, DR, 1, s),
                 "linearised reflection adjoint"));
     if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, A, A, 0, s));
   }

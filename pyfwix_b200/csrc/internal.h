@@ -9,6 +9,9 @@
 
 namespace fwix {
 
+// Number of kernels this library has enqueued (fwix_launch_count).
+void count_launch(unsigned n = 1);
+
 // Per-cell pre-weights of a forward row pass and post-weights of an inverse row pass.
 enum RowWeight {
   W_ONE = 0,        // 1
@@ -55,7 +58,8 @@ struct SpecArgs {
   long long lab_w;
   const float2* slow;  // s^2 at this depth (unpadded), (iw, y, x) at slow[iw*slow_w + y*nx + x]
   long long slow_w;
-  const float2* image; // imaging-condition image [nw][ny][nx] (W_IC)
+  const float2* image; // imaging-condition image, (iw, y, x) at image[iw*img_w + y*nx + x] (W_IC)
+  long long img_w;     // ny*nx, or 0 for one image shared by every frequency
   float dz, eps, eps_scat;
   float coef[5];
   float norm;          // scale folded into the column multiplier
@@ -85,14 +89,16 @@ cudaError_t launch_taper(const SpecArgs& a, const float2* in, float2* out, int a
 cudaError_t launch_reflect(const Dims& d, int adjoint, const float2* s0, const float2* s1,
                            const float2* r0, const float2* r1, long long mw, const float2* in,
                            float2* out, int add, cudaStream_t s);
-cudaError_t launch_ic_fwd(const Dims& d, const float2* bg, const float2* image, float2* wfld,
-                          int add, cudaStream_t s);
+// image / dm arrays are indexed (iw, y, x) -> iw*img_w + y*nx + x; img_w == 0 means one
+// array shared by every frequency, whose adjoint sums over frequency.
+cudaError_t launch_ic_fwd(const Dims& d, const float2* bg, const float2* image, long long img_w,
+                          float2* wfld, int add, cudaStream_t s);
 cudaError_t launch_ic_adj(const Dims& d, const float2* bg, const float2* wfld, float2* image,
-                          int add, cudaStream_t s);
+                          long long img_w, int add, cudaStream_t s);
 cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, const float2* s1,
                                const float2* r0, const float2* r1, long long mw, float2* dm0,
-                               float2* dm1, float2* dm2, float2* dm3, float2* dr, int add,
-                               cudaStream_t s);
+                               float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
+                               int add, cudaStream_t s);
 cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, float* img, int add,
                              cudaStream_t s);
 cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s);

@@ -46,7 +46,7 @@ __global__ void k_reflect(Dims d, int adjoint, const float2* __restrict__ s0, co
 }
 
 __global__ void k_ic_fwd(Dims d, const float2* __restrict__ bg, const float2* __restrict__ image,
-                         float2* __restrict__ wfld) {
+                         long long img_w, float2* __restrict__ wfld) {
   const long long n = (long long)d.nw * d.ny * d.nx;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -54,7 +54,7 @@ __global__ void k_ic_fwd(Dims d, const float2* __restrict__ bg, const float2* __
     const long long q = i / d.nx;
     const int y = (int)(q % d.ny);
     const int iw = (int)(q / d.ny);
-    const float2 im = image[i];
+    const float2 im = image[iw * img_w + (long long)y * d.nx + x];
     for (int s = 0; s < d.ns; ++s) {
       const long long k = (((long long)s * d.nw + iw) * d.NY + y) * d.NX + x;
       wfld[k] = cadd(wfld[k], cmul(bg[k], im));
@@ -62,19 +62,26 @@ __global__ void k_ic_fwd(Dims d, const float2* __restrict__ bg, const float2* __
   }
 }
 
+// image[w, y, x] (+)= sum_s conj(bg) wfld; with wsum the frequencies are summed as well
+// into image[y, x].
 __global__ void k_ic_adj(Dims d, const float2* __restrict__ bg, const float2* __restrict__ wfld,
-                         float2* __restrict__ image, int add) {
-  const long long n = (long long)d.nw * d.ny * d.nx;
+                         float2* __restrict__ image, int add, int wsum) {
+  const int nwo = wsum ? 1 : d.nw;
+  const int nwi = wsum ? d.nw : 1;
+  const long long n = (long long)nwo * d.ny * d.nx;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const int x = (int)(i % d.nx);
     const long long q = i / d.nx;
     const int y = (int)(q % d.ny);
-    const int iw = (int)(q / d.ny);
+    const int iw0 = (int)(q / d.ny);
     float2 acc = make_float2(0.f, 0.f);
-    for (int s = 0; s < d.ns; ++s) {
-      const long long k = (((long long)s * d.nw + iw) * d.NY + y) * d.NX + x;
-      acc = cadd(acc, cmul_conj(wfld[k], bg[k]));
+    for (int j = 0; j < nwi; ++j) {
+      const int iw = iw0 + j;
+      for (int s = 0; s < d.ns; ++s) {
+        const long long k = (((long long)s * d.nw + iw) * d.NY + y) * d.NX + x;
+        acc = cadd(acc, cmul_conj(wfld[k], bg[k]));
+      }
     }
     image[i] = add ? cadd(image[i], acc) : acc;
   }
@@ -102,32 +109,45 @@ __device__ __forceinline__ LinCoef lin_coef(float2 s0, float2 s1, float2 r0, flo
 
 __global__ void k_lin_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
                               const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw,
-                              float2* dm0, float2* dm1, float2* dm2, float2* dm3, float2* dr, int add) {
-  const long long n = (long long)d.nw * d.ny * d.nx;
+                              float2* dm0, float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
+                              int add) {
+  // forward: one thread per (w, y, x) of dr.  adjoint: one thread per (w, y, x) of dm,
+  // or per (y, x) with a loop over w when dm is shared by every frequency.
+  const int wsum = adjoint && dm_w == 0;
+  const int nwo = wsum ? 1 : d.nw;
+  const long long n = (long long)nwo * d.ny * d.nx;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const int x = (int)(i % d.nx);
     const long long q = i / d.nx;
     const int y = (int)(q % d.ny);
-    const int iw = (int)(q / d.ny);
-    const long long m = iw * mw + (long long)y * d.nx + x;
-    const LinCoef c = lin_coef(s0[m], s1[m], r0[m], r1[m]);
+    const int iw0 = (int)(q / d.ny);
+    const long long yx = (long long)y * d.nx + x;
     if (!adjoint) {
-      float2 v = csub(cmul(c.as, dm0[i]), cmul(c.bs, dm1[i]));
-      v = cadd(v, csub(cmul(c.ar, dm3[i]), cmul(c.br, dm2[i])));
+      const long long m = iw0 * mw + yx, k = iw0 * dm_w + yx;
+      const LinCoef c = lin_coef(s0[m], s1[m], r0[m], r1[m]);
+      float2 v = csub(cmul(c.as, dm0[k]), cmul(c.bs, dm1[k]));
+      v = cadd(v, csub(cmul(c.ar, dm3[k]), cmul(c.br, dm2[k])));
       dr[i] = add ? cadd(dr[i], v) : v;
-    } else {
-      const float2 g = dr[i];
-      const float2 g0 = cmul_conj(g, c.as);
-      const float2 g1 = cscale(cmul_conj(g, c.bs), -1.f);
-      const float2 g3 = cmul_conj(g, c.ar);
-      const float2 g2 = cscale(cmul_conj(g, c.br), -1.f);
-      // dm0 and dm1 alias at the bottom level; the same thread adds both in order.
-      dm0[i] = add ? cadd(dm0[i], g0) : g0;
-      dm1[i] = (add || dm1 == dm0) ? cadd(dm1[i], g1) : g1;
-      dm2[i] = add ? cadd(dm2[i], g2) : g2;
-      dm3[i] = (add || dm3 == dm2) ? cadd(dm3[i], g3) : g3;
+      continue;
     }
+    float2 g0 = make_float2(0.f, 0.f), g1 = g0, g2 = g0, g3 = g0;
+    for (int j = 0; j < (wsum ? d.nw : 1); ++j) {
+      const int iw = iw0 + j;
+      const long long m = iw * mw + yx;
+      const LinCoef c = lin_coef(s0[m], s1[m], r0[m], r1[m]);
+      const float2 g = dr[(long long)iw * d.ny * d.nx + yx];
+      g0 = cadd(g0, cmul_conj(g, c.as));
+      g1 = csub(g1, cmul_conj(g, c.bs));
+      g3 = cadd(g3, cmul_conj(g, c.ar));
+      g2 = csub(g2, cmul_conj(g, c.br));
+    }
+    const long long k = iw0 * dm_w + yx;
+    // dm0 and dm1 (dm2 and dm3) alias at the bottom level; the same thread adds both.
+    dm0[k] = add ? cadd(dm0[k], g0) : g0;
+    dm1[k] = (add || dm1 == dm0) ? cadd(dm1[k], g1) : g1;
+    dm2[k] = add ? cadd(dm2[k], g2) : g2;
+    dm3[k] = (add || dm3 == dm2) ? cadd(dm3[k], g3) : g3;
   }
 }
 
@@ -202,42 +222,49 @@ cudaError_t launch_reflect(const Dims& d, int adjoint, const float2* s0, const f
     if (e != cudaSuccess) return e;
   }
   k_reflect<<<grid1d((long long)d.nw * d.ny * d.nx), 256, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, in, out);
+  count_launch();
   return cudaGetLastError();
 }
 
-cudaError_t launch_ic_fwd(const Dims& d, const float2* bg, const float2* image, float2* wfld, int add,
-                          cudaStream_t s) {
+cudaError_t launch_ic_fwd(const Dims& d, const float2* bg, const float2* image, long long img_w,
+                          float2* wfld, int add, cudaStream_t s) {
   if (!add) {
     cudaError_t e = cudaMemsetAsync(wfld, 0, d.wfld * sizeof(float2), s);
     if (e != cudaSuccess) return e;
   }
-  k_ic_fwd<<<grid1d((long long)d.nw * d.ny * d.nx), 256, 0, s>>>(d, bg, image, wfld);
+  k_ic_fwd<<<grid1d((long long)d.nw * d.ny * d.nx), 256, 0, s>>>(d, bg, image, img_w, wfld);
+  count_launch();
   return cudaGetLastError();
 }
 
-cudaError_t launch_ic_adj(const Dims& d, const float2* bg, const float2* wfld, float2* image, int add,
-                          cudaStream_t s) {
-  k_ic_adj<<<grid1d((long long)d.nw * d.ny * d.nx), 256, 0, s>>>(d, bg, wfld, image, add);
+cudaError_t launch_ic_adj(const Dims& d, const float2* bg, const float2* wfld, float2* image,
+                          long long img_w, int add, cudaStream_t s) {
+  const int wsum = img_w == 0;
+  k_ic_adj<<<grid1d((long long)(wsum ? 1 : d.nw) * d.ny * d.nx), 256, 0, s>>>(d, bg, wfld, image, add, wsum);
+  count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, const float2* s1,
                                const float2* r0, const float2* r1, long long mw, float2* dm0,
-                               float2* dm1, float2* dm2, float2* dm3, float2* dr, int add,
-                               cudaStream_t s) {
-  k_lin_reflect<<<grid1d((long long)d.nw * d.ny * d.nx), 256, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0,
-                                                                        dm1, dm2, dm3, dr, add);
+                               float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
+                               int add, cudaStream_t s) {
+  const long long n = (long long)((adjoint && dm_w == 0) ? 1 : d.nw) * d.ny * d.nx;
+  k_lin_reflect<<<grid1d(n), 256, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3, dm_w, dr, add);
+  count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, float* img, int add,
                              cudaStream_t s) {
   k_image_acc<<<grid1d((long long)d.ny * d.nx), 256, 0, s>>>(d, S, R, img, add);
+  count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s) {
   k_axpy<<<grid1d(n), 256, 0, s>>>(n, x, y);
+  count_launch();
   return cudaGetLastError();
 }
 
@@ -245,6 +272,7 @@ cudaError_t launch_inject(const Dims& d, const InjectLevel& L, const float2* tra
                           cudaStream_t s) {
   if (L.ncell == 0) return cudaSuccess;
   k_inject<<<grid1d((long long)L.ncell * d.nw), 256, 0, s>>>(d, L, traces, wfld);
+  count_launch();
   return cudaGetLastError();
 }
 
@@ -252,6 +280,7 @@ cudaError_t launch_record(const Dims& d, const InjectLevel& L, const float2* wfl
                           cudaStream_t s) {
   if (L.ntr == 0) return cudaSuccess;
   k_record<<<grid1d((long long)L.ntr * d.nw), 256, 0, s>>>(d, L, wfld, traces);
+  count_launch();
   return cudaGetLastError();
 }
 

@@ -66,7 +66,7 @@ __device__ __forceinline__ float2 row_weight(const SpecArgs& a, int t, int iw, i
   if (W == W_SCAT_CONJ) return cmul_conj(v, scat_weight(a, t, iw, y, x));
   // W_IC
   if (y < a.d.ny && x < a.d.nx)
-    return cmul(v, a.image[(long long)iw * a.d.ny * a.d.nx + (long long)y * a.d.nx + x]);
+    return cmul(v, a.image[(long long)iw * a.img_w + (long long)y * a.d.nx + x]);
   return make_float2(0.f, 0.f);
 }
 
@@ -374,6 +374,7 @@ cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_ROWF
+  if (e == cudaSuccess) count_launch();
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -394,6 +395,7 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_ROWI
+  if (e == cudaSuccess) count_launch();
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -414,6 +416,7 @@ cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_COLA
+  if (e == cudaSuccess) count_launch();
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -434,6 +437,7 @@ cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s) {
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_COLB
+  if (e == cudaSuccess) count_launch();
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -449,6 +453,7 @@ cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* ou
     e = ensure_smem(k_col_fft<false>, g.smem);
     if (e == cudaSuccess) k_col_fft<false><<<grid, block, g.smem, s>>>(a, g.TX, g.nxt, in, out, add, scale);
   }
+  if (e == cudaSuccess) count_launch();
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -511,17 +516,20 @@ cudaError_t launch_phase_shift(const SpecArgs& a, int mode, const float2* sref_w
     case Q_PS_INV: k_phase_shift<Q_PS_INV><<<g, 256, 0, s>>>(b, in, out, add); break;
     default: return cudaErrorInvalidValue;
   }
+  count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_select(const SpecArgs& a, int value, const float2* in, float2* out, int add,
                           cudaStream_t s) {
   k_weight<W_MASK><<<grid1d(a.d.wfld), 256, 0, s>>>(a, value, in, out, add);
+  count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_taper(const SpecArgs& a, const float2* in, float2* out, int add, cudaStream_t s) {
   k_weight<W_TAPER><<<grid1d(a.d.wfld), 256, 0, s>>>(a, 0, in, out, add);
+  count_launch();
   return cudaGetLastError();
 }
 

@@ -180,9 +180,15 @@ class Plan:
         return image
 
     def born(self, rec, bg_down, bg_up, dslow, dden, data, adjoint=False, add=False):
+        """Extended Born.  dslow / dden are [nz][nw][ny][nx] (per frequency) or
+        [nz][1][ny][nx] (one perturbation per depth for every frequency)."""
         self.ensure_workspace(L.WS_BORN)
+        nwm = dslow.shape[1] if dslow.dim() == 4 else self.nw
+        if tuple(dslow.shape) != tuple(dden.shape) or nwm not in (1, self.nw):
+            raise ValueError("dslow / dden must both be [nz][nw or 1][ny][nx]")
+        mw = 0 if (nwm == 1 and self.nw > 1) else self.ny * self.nx
         L.check(self.lib.fwix_born(self._h, int(adjoint), rec._h, _p(bg_down), _p(bg_up), _p(dslow), _p(dden),
-                                   _p(data), int(add), _stream()))
+                                   mw, _p(data), int(add), _stream()))
 
     def __del__(self):
         try:

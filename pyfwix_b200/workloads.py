@@ -1,0 +1,128 @@
+"""Seeded synthetic workloads with the shapes, sizes and value distributions of the
+benchmark configurations (there is no public dataset for this path).
+
+config1: PSPI forward modelling + imaging, one shot, 128 x 128 x 100, nw = 64
+         (2-30 Hz), v = 1500 + 0.5 z with a +10 % Gaussian anomaly (sigma 150 m at
+         (640, 640, 500) m), nref = 4 quantile references, 15 Hz Ricker at the
+         surface centre, receivers on every surface node, taper 20 cells.
+config2: Born forward + adjoint with NSPS, one shot, 256 x 256 x 200, nw = 128
+         (3-40 Hz), v = 1500 + 0.4 z times (1 + p), p = Gaussian-filtered white
+         noise (sigma 5 cells) scaled to max |p| = 0.05; reflectivity = 5 flat
+         layers at depths drawn from {10..189}, amplitudes U(-0.1, 0.1) relative to
+         the background s^2.
+
+Seeds are ``numpy.random.default_rng(1000 + config_index)``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def ricker_spectrum(freqs, f0=15.0, dt=0.004, nt=512, t0=0.1):
+    """Direct DTFT W(f) = sum_n r(n dt) exp(-2 pi i f n dt) of a Ricker wavelet."""
+    t = np.arange(nt) * dt
+    a = (np.pi * f0 * (t - t0)) ** 2
+    r = (1 - 2 * a) * np.exp(-a)
+    return np.exp(-2j * np.pi * np.outer(freqs, t)) @ r
+
+
+@dataclass
+class Workload:
+    name: str
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    dy: float
+    dz: float
+    nw: int
+    ow: float
+    dw: float
+    nref: int
+    step: str
+    taperx: int = 20
+    tapery: int = 20
+    padx: int = 0
+    pady: int = 0
+    eps: float = 0.0
+    eps_scat: float = 0.04
+    taylor: int = 1
+    ox: float = 0.0
+    oy: float = 0.0
+    oz: float = 0.0
+    slow2: np.ndarray = None      # [nz][ny][nx] float32, s^2 = 1/v^2
+    geom: dict = field(default_factory=dict)
+    wavelet: np.ndarray = None    # [nsrc][nw] complex64
+    dslow: np.ndarray = None      # Born perturbation [nz][ny][nx] float32 (or None)
+
+    @property
+    def freqs(self):
+        return self.ow + self.dw * np.arange(self.nw)
+
+    @property
+    def cells(self):
+        """x*y*w*z cell-steps of one sweep over all shots."""
+        ns = len(set(self.geom["s_ids"]))
+        return ns * self.nx * self.ny * self.nw * self.nz
+
+    def plan_kwargs(self):
+        return dict(nx=self.nx, ny=self.ny, nw=self.nw, nz=self.nz, dx=self.dx, dy=self.dy,
+                    dz=self.dz, ox=self.ox, oy=self.oy, oz=self.oz, ow=self.ow, dw=self.dw,
+                    padx=self.padx, pady=self.pady, nref=self.nref, eps=self.eps,
+                    taperx=self.taperx, tapery=self.tapery, eps_scat=self.eps_scat,
+                    taylor=self.taylor, step=self.step)
+
+    def surface_receivers(self, shot_id=0):
+        gx, gy = np.meshgrid(self.ox + self.dx * np.arange(self.nx), self.oy + self.dy * np.arange(self.ny))
+        n = gx.size
+        return dict(rx=gx.ravel().astype(np.float32), ry=gy.ravel().astype(np.float32),
+                    rz=np.full(n, self.oz, np.float32), r_ids=np.full(n, shot_id, np.int32))
+
+
+def _coords(w):
+    z = w.oz + w.dz * np.arange(w.nz)
+    y = w.oy + w.dy * np.arange(w.ny)
+    x = w.ox + w.dx * np.arange(w.nx)
+    return np.meshgrid(z, y, x, indexing="ij")
+
+
+def config1(nz=None, seed=1000):
+    w = Workload(name="pspi-model-image-128x128x100-nw64", nx=128, ny=128, nz=nz or 100, dx=10.0, dy=10.0,
+                 dz=10.0, nw=64, ow=2.0, dw=28.0 / 63.0, nref=4, step="pspi")
+    Z, Y, X = _coords(w)
+    v = (1500.0 + 0.5 * Z) * (1 + 0.10 * np.exp(-((X - 640) ** 2 + (Y - 640) ** 2 + (Z - 500) ** 2) / (2 * 150.0 ** 2)))
+    w.slow2 = (1.0 / v ** 2).astype(np.float32)
+    w.geom = dict(sx=np.array([640.0], np.float32), sy=np.array([640.0], np.float32),
+                  sz=np.array([0.0], np.float32), s_ids=np.array([0], np.int32), **w.surface_receivers())
+    w.wavelet = ricker_spectrum(w.freqs)[None, :].astype(np.complex64)
+    return w
+
+
+def config2(nz=None, nw=None, seed=1001):
+    from scipy.ndimage import gaussian_filter
+
+    rng = np.random.default_rng(seed)
+    nz_full = 200
+    w = Workload(name="born-nsps-256x256x200-nw128", nx=256, ny=256, nz=nz or nz_full, dx=10.0, dy=10.0,
+                 dz=10.0, nw=nw or 128, ow=3.0, dw=37.0 / 127.0, nref=4, step="nsps", taperx=20, tapery=20)
+    p = gaussian_filter(rng.standard_normal((nz_full, w.ny, w.nx)), sigma=5)
+    p *= 0.05 / np.max(np.abs(p))
+    Z, Y, X = _coords(w)
+    v = (1500.0 + 0.4 * Z) * (1 + p[: w.nz])
+    w.slow2 = (1.0 / v ** 2).astype(np.float32)
+    depths = rng.choice(np.arange(10, 190), size=5, replace=False)
+    amps = rng.uniform(-0.1, 0.1, size=5)
+    ds = np.zeros((w.nz, w.ny, w.nx), np.float32)
+    for dpt, a in zip(depths, amps):
+        if dpt < w.nz:
+            ds[dpt] = a * w.slow2[dpt]
+    w.dslow = ds
+    w.geom = dict(sx=np.array([w.nx // 2 * w.dx], np.float32), sy=np.array([w.ny // 2 * w.dy], np.float32),
+                  sz=np.array([0.0], np.float32), s_ids=np.array([0], np.int32), **w.surface_receivers())
+    w.wavelet = ricker_spectrum(w.freqs)[None, :].astype(np.complex64)
+    return w
+
+
+CONFIGS = {"config1": config1, "config2": config2}

@@ -117,3 +117,29 @@ def test_born_dot_product_device():
     lhs = np.vdot(r.ravel(), to_host(out).ravel())
     rhs = np.vdot(to_host(gs).ravel(), ms.ravel()) + np.vdot(to_host(gr).ravel(), mr.ravel())
     assert abs((lhs / rhs).real - 1) < 1e-5
+
+
+def test_born_frequency_broadcast_model():
+    """A [nz][1][ny][nx] perturbation equals its per-frequency copy in the forward,
+    and the adjoint returns the frequency sum of the per-frequency gradient."""
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case("nsps", taper=0)
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((len(acq.rec.ix), g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, to_dev(wav), d, bd, bu)
+    ms = crandn(rng, (g.nz, 1, g.ny, g.nx))
+    mr = crandn(rng, (g.nz, 1, g.ny, g.nx))
+    out1 = torch.empty_like(d)
+    p.born(rec, bd, bu, to_dev(ms), to_dev(mr), out1)
+    out2 = torch.empty_like(d)
+    p.born(rec, bd, bu, to_dev(np.repeat(ms, g.nw, 1)), to_dev(np.repeat(mr, g.nw, 1)), out2)
+    assert rel(to_host(out1), to_host(out2)) < 1e-5
+    r = crandn(rng, d.shape)
+    gs1 = torch.empty((g.nz, 1, g.ny, g.nx), dtype=torch.complex64, device="cuda")
+    gr1 = torch.empty_like(gs1)
+    p.born(rec, bd, bu, gs1, gr1, to_dev(r), adjoint=True)
+    gs2 = torch.empty((g.nz, g.nw, g.ny, g.nx), dtype=torch.complex64, device="cuda")
+    gr2 = torch.empty_like(gs2)
+    p.born(rec, bd, bu, gs2, gr2, to_dev(r), adjoint=True)
+    assert rel(to_host(gs1), to_host(gs2).sum(1, keepdims=True)) < 1e-5
+    assert rel(to_host(gr1), to_host(gr2).sum(1, keepdims=True)) < 1e-5
