@@ -174,6 +174,27 @@ fwix_status fwix_born(fwix_plan* plan, int adjoint, const fwix_traces* rec, cons
                       const void* bg_up, void* dslow, void* dden, int64_t model_w_stride,
                       void* data, int add, void* stream);
 
+/* ---- allocation-free depth step ----------------------------------------------
+ * fwix_step_noalloc has no counterpart in the reference.  It is fwix_step for
+ * callers that cannot call cudaMalloc -- for example a host application or
+ * framework that reserves the GPU's memory in its own pool up front and does not
+ * let a library allocate (an allocation there would fail, fragment the pool or
+ * stall the device).  It takes no plan and no workspace: the descriptor is read on
+ * the host and the scratch (tables plus (nref + 1) wavefield-sized intermediates)
+ * lives in one static device array of FWIX_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading this library holds until the process exits.  Larger problems are
+ * rejected with FWIX_ERR_UNSUPPORTED and a message giving the bytes needed.
+ * All calls share that array and it keeps the previous call's contents, so two
+ * calls that overlap on the GPU (other streams, other host threads) race: order
+ * them on one stream.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream capture.
+ * sref / labels / strides are as in fwix_plan_set_refs; in may equal out. */
+#define FWIX_NOALLOC_SCRATCH_BYTES (64ull * 1024ull * 1024ull)
+fwix_status fwix_step_noalloc(const fwix_desc* desc, int kind, int iz, int dir, const void* sref,
+                              const uint8_t* labels, int64_t labels_z_stride,
+                              int64_t labels_w_stride, const void* in, void* out, int add,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

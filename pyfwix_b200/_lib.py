@@ -68,6 +68,7 @@ SIGNATURES = {
     "fwix_propagate": [P, P, P, P, P, I, P, P, P],
     "fwix_migrate": [P, P, P, P, P, P, I, P],
     "fwix_born": [P, I, P, P, P, P, P, I64, P, I, P],
+    "fwix_step_noalloc": [ctypes.POINTER(FwixDesc), I, I, I, P, P, I64, I64, P, P, I, P],
 }
 _RET = {"fwix_last_error": ctypes.c_char_p, "fwix_version": I, "fwix_plan_workspace_bytes": ctypes.c_size_t,
         "fwix_launch_count": ctypes.c_uint64}

@@ -103,6 +103,10 @@ cudaError_t upload(T** dst, const std::vector<T>& v) {
 
 }  // namespace
 
+namespace fwix {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace fwix
+
 struct fwix_plan {
   fwix_desc desc;
   Dims d;

@@ -11,6 +11,8 @@ namespace fwix {
 
 // Number of kernels this library has enqueued (fwix_launch_count).
 void count_launch(unsigned n = 1);
+// Message returned by fwix_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
 
 // Per-cell pre-weights of a forward row pass and post-weights of an inverse row pass.
 enum RowWeight {
