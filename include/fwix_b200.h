@@ -110,6 +110,15 @@ fwix_status fwix_plan_set_workspace(fwix_plan* plan, void* dev_ptr, size_t bytes
  * labels[iz*z_stride + iw*w_stride + y*NX + x] (RefSampler.cpp:27-28, 126-133). */
 fwix_status fwix_plan_set_refs(fwix_plan* plan, const void* sref, const uint8_t* labels,
                                int64_t labels_z_stride, int64_t labels_w_stride);
+/* Optional phase-factor cache.  The factor of a depth step depends only on
+ * (depth, reference, frequency, |kx|, |ky|) (phase_shift.cu:36-55), so with a
+ * cache of fwix_plan_phase_cache_bytes bytes bound, each depth's factors are
+ * computed once, on the first step at that depth, and every later step there
+ * (Born sweeps visit each depth many times) reads them.  Binding NULL disables
+ * it; fwix_plan_set_refs invalidates it.  Calls that use it must be ordered on
+ * one stream (or synchronised), as for the workspace. */
+size_t fwix_plan_phase_cache_bytes(const fwix_plan* plan);
+fwix_status fwix_plan_set_phase_cache(fwix_plan* plan, void* dev_ptr, size_t bytes);
 /* Background s^2 and density, element (iz,iw,y,x) at
  * p[iz*z_stride + iw*w_stride + y*nx + x] (Reflect.h:20-38, Scatter.cpp:68-74). */
 fwix_status fwix_plan_set_model(fwix_plan* plan, const void* slow, const void* den,

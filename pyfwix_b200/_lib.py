@@ -50,6 +50,8 @@ SIGNATURES = {
     "fwix_plan_workspace_bytes": [P, I],
     "fwix_plan_set_workspace": [P, P, ctypes.c_size_t],
     "fwix_plan_set_refs": [P, P, P, I64, I64],
+    "fwix_plan_phase_cache_bytes": [P],
+    "fwix_plan_set_phase_cache": [P, P, ctypes.c_size_t],
     "fwix_plan_set_model": [P, P, P, I64, I64],
     "fwix_fft2d": [P, I, P, P, I, P],
     "fwix_phase_shift": [P, I, P, P, P, I, P],
@@ -71,6 +73,7 @@ SIGNATURES = {
     "fwix_step_noalloc": [ctypes.POINTER(FwixDesc), I, I, I, P, P, I64, I64, P, P, I, P],
 }
 _RET = {"fwix_last_error": ctypes.c_char_p, "fwix_version": I, "fwix_plan_workspace_bytes": ctypes.c_size_t,
+        "fwix_plan_phase_cache_bytes": ctypes.c_size_t,
         "fwix_launch_count": ctypes.c_uint64}
 
 _lib = None

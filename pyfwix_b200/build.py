@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -43,18 +44,35 @@ def nvcc():
     return exe
 
 
-def build(force=False, verbose=False, extra=()):
-    """Compile the library if needed and return its path."""
-    if not force and not _stale():
-        return LIB
-    cmd = [nvcc()] + ARCH + FLAGS + list(extra) + ["-I", INCLUDE, "-I", CSRC] + sources() + ["-o", LIB + ".tmp"]
-    if verbose:
-        print(" ".join(cmd))
+OBJDIR = os.path.join(ROOT, "_build")
+
+
+def _compile(src, extra, verbose):
+    obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
+    cmd = [nvcc()] + ARCH + [f for f in FLAGS if f != "-shared"] + list(extra) + ["-I", INCLUDE, "-I", CSRC,
+                                                                                    "-c", src, "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose and (res.stdout or res.stderr):
-        print(res.stdout + res.stderr)
+        raise RuntimeError(f"nvcc failed on {src}:\n" + res.stdout + res.stderr)
+    return obj, (res.stdout + res.stderr) if verbose else ""
+
+
+def build(force=False, verbose=False, extra=(), jobs=None):
+    """Compile the library if needed (one object per source, in parallel) and
+    return its path."""
+    if not force and not _stale():
+        return LIB
+    os.makedirs(OBJDIR, exist_ok=True)
+    jobs = jobs or max(1, min(len(sources()), os.cpu_count() or 1))
+    with ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(lambda s: _compile(s, extra, verbose), sources()))
+    for _, log in results:
+        if log:
+            print(log)
+    cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC"] + [o for o, _ in results] + ["-o", LIB + ".tmp"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

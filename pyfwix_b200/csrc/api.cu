@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -122,18 +123,25 @@ struct fwix_plan {
   char* ws = nullptr;
   size_t ws_bytes = 0;
   int nterm_max = 1;
+  long long chunk = 1;  // slices per launch: the intermediates of one chunk fit in L2
+  float2* pcache = nullptr;   // phase-factor cache, nz depths (fwix_plan_set_phase_cache)
+  std::vector<char> pbuilt;   // depth iz of the cache holds current factors
+  int pq_nx() const { return d.NX / 2 + 1; }
+  int pq_ny() const { return d.NY / 2 + 1; }
+  long long pdepth() const { return (long long)desc.nref * d.nw * pq_nx() * pq_ny(); }
   float coef[5] = {1.f, 1.f / 2.f, 3.f / 8.f, 5.f / 16.f, 35.f / 128.f};  // Scatter.h:526
 
   size_t wbytes() const { return (size_t)d.wfld * sizeof(float2); }
+  size_t tbytes() const { return (size_t)nterm_max * chunk * d.slice * sizeof(float2); }
   size_t ws_need(int cls) const {
-    size_t b = 2 * (size_t)nterm_max * wbytes();  // t1, t2
+    size_t b = 2 * tbytes();  // t1, t2 for one chunk
     if (cls >= FWIX_WS_SWEEP) b += 3 * wbytes();  // A, B, SC
     if (cls >= FWIX_WS_BORN) b += (size_t)desc.nz * wbytes();  // per-level field store
     return b;
   }
   float2* t1() const { return (float2*)ws; }
-  float2* t2() const { return (float2*)(ws + (size_t)nterm_max * wbytes()); }
-  float2* wA() const { return (float2*)(ws + 2 * (size_t)nterm_max * wbytes()); }
+  float2* t2() const { return (float2*)(ws + tbytes()); }
+  float2* wA() const { return (float2*)(ws + 2 * tbytes()); }
   float2* wB() const { return wA() + d.wfld; }
   float2* wSC() const { return wB() + d.wfld; }
   float2* store(int iz) const { return wSC() + d.wfld * (long long)(1 + iz); }
@@ -163,6 +171,9 @@ struct fwix_plan {
     a.add = add;
     a.t1 = t1();
     a.t2 = t2();
+    a.b0 = 0;
+    a.nb = (long long)d.ns * d.nw;
+    a.tstride = chunk * d.slice;
     return a;
   }
 };
@@ -203,10 +214,40 @@ fwix_status cu(cudaError_t e, const char* what) {
   return FWIX_OK;
 }
 
+// Runs f(args) once per chunk of slices (shot, frequency), each chunk small enough
+// that its intermediates stay in L2 between the row and column passes.
+template <class F>
+fwix_status for_chunks(const fwix_plan* p, SpecArgs a, F f) {
+  const long long B = (long long)p->d.ns * p->d.nw;
+  for (long long b0 = 0; b0 < B; b0 += p->chunk) {
+    a.b0 = b0;
+    a.nb = std::min(p->chunk, B - b0);
+    a.tstride = p->chunk * p->d.slice;
+    FWIX_TRY(f(a));
+  }
+  return FWIX_OK;
+}
+
+// Cached phase factors of depth iz, built on the stream on first use.
+fwix_status phase_factors(fwix_plan* p, int iz, SpecArgs& a, cudaStream_t s) {
+  a.ptab = nullptr;
+  if (!p->pcache) return FWIX_OK;
+  float2* dst = p->pcache + iz * p->pdepth();
+  a.ptab_nx = p->pq_nx();
+  a.ptab_ny = p->pq_ny();
+  if (!p->pbuilt[iz]) {
+    SpecArgs b = a;
+    b.sref = p->sref + (long long)iz * p->desc.nref * p->d.nw;
+    b.nterm = p->desc.nref;
+    FWIX_TRY(cu(fwix::launch_phase_table(b, dst, s), "phase-factor cache"));
+    p->pbuilt[iz] = 1;
+  }
+  a.ptab = dst;
+  return FWIX_OK;
+}
+
 // One depth step: PSPI (PSPI.cpp:6-103) or NSPS (NSPS.cpp:6-45).
-fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, float2* out, int add,
-                    cudaStream_t s) {
-  SpecArgs a = p->args(in, out, add);
+fwix_status step_chunk(fwix_plan* p, int kind, int iz, int dir, SpecArgs a, cudaStream_t s) {
   a.sref = p->sref + (long long)iz * p->desc.nref * p->d.nw;
   a.lab = p->labels + iz * p->lab_z;
   a.lab_w = p->lab_w;
@@ -235,6 +276,13 @@ fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, f
   return FWIX_OK;
 }
 
+fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, float2* out, int add,
+                    cudaStream_t s) {
+  SpecArgs a0 = p->args(in, out, add);
+  FWIX_TRY(phase_factors(p, iz, a0, s));
+  return for_chunks(p, a0, [&](const SpecArgs& a) { return step_chunk(p, kind, iz, dir, a, s); });
+}
+
 SpecArgs scatter_args(const fwix_plan* p, int iz, const float2* in, float2* out, int add) {
   SpecArgs a = p->args(in, out, add);
   a.slow = p->slow + iz * p->m_z;
@@ -246,9 +294,7 @@ SpecArgs scatter_args(const fwix_plan* p, int iz, const float2* in, float2* out,
 // Scatter::cu_forward / cu_adjoint (Scatter.cpp:76-133).  With image != NULL the
 // forward input is the imaging-condition product bg * image (ImagingCondition fwd,
 // imaging_condition.cu:9-55) formed inside the first pass.
-fwix_status do_scatter(fwix_plan* p, int iz, int adjoint, const float2* in, float2* out, int add,
-                       const float2* image, long long img_w, cudaStream_t s) {
-  SpecArgs a = scatter_args(p, iz, in, out, add);
+fwix_status scatter_chunk(int adjoint, const float2* image, long long img_w, SpecArgs a, cudaStream_t s) {
   if (!adjoint) {
     a.image = image;
     a.img_w = img_w;
@@ -261,6 +307,12 @@ fwix_status do_scatter(fwix_plan* p, int iz, int adjoint, const float2* in, floa
     FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_ONE, 0, s), "scatter adjoint inverse row pass"));
   }
   return FWIX_OK;
+}
+
+fwix_status do_scatter(fwix_plan* p, int iz, int adjoint, const float2* in, float2* out, int add,
+                       const float2* image, long long img_w, cudaStream_t s) {
+  SpecArgs a0 = scatter_args(p, iz, in, out, add);
+  return for_chunks(p, a0, [&](const SpecArgs& a) { return scatter_chunk(adjoint, image, img_w, a, s); });
 }
 
 int lower_iz(const fwix_plan* p, int iz) { return iz < p->desc.nz - 1 ? iz + 1 : iz; }
@@ -347,6 +399,13 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
     return fail(FWIX_ERR_UNSUPPORTED, "wavefield sizes must be 2^a 3^b 5^c 7^d and at most 1024");
   }
   p->nterm_max = std::max(q.nref, q.taylor + 1);
+  {
+    // One launch covers every slice unless FWIX_CHUNK_SLICES asks for chunks (smaller
+    // launches keep the intermediates in L2 but leave SMs idle at these sizes).
+    long long c = (long long)q.ns * q.nw;
+    if (const char* env = getenv("FWIX_CHUNK_SLICES")) c = atoll(env);
+    p->chunk = std::max(1LL, std::min(c, (long long)q.ns * q.nw));
+  }
   std::vector<float> w2(q.nw), w(q.nw);
   for (int i = 0; i < q.nw; ++i) {
     // PhaseShift.h:59-70 and Scatter.h:544-556 (float f, then 2 pi f in double)
@@ -391,9 +450,24 @@ fwix_status fwix_plan_set_workspace(fwix_plan* p, void* ptr, size_t bytes) {
   return FWIX_OK;
 }
 
+size_t fwix_plan_phase_cache_bytes(const fwix_plan* p) {
+  return p ? (size_t)p->desc.nz * (size_t)p->pdepth() * sizeof(float2) : 0;
+}
+
+fwix_status fwix_plan_set_phase_cache(fwix_plan* p, void* ptr, size_t bytes) {
+  if (!p) return fail(FWIX_ERR_INVALID, "null plan");
+  if (ptr && bytes < fwix_plan_phase_cache_bytes(p))
+    return fail(FWIX_ERR_WORKSPACE, "phase cache smaller than fwix_plan_phase_cache_bytes");
+  if (((uintptr_t)ptr) % 16 != 0) return fail(FWIX_ERR_INVALID, "phase cache must be 16-byte aligned");
+  p->pcache = (float2*)ptr;
+  p->pbuilt.assign(p->desc.nz, 0);
+  return FWIX_OK;
+}
+
 fwix_status fwix_plan_set_refs(fwix_plan* p, const void* sref, const uint8_t* labels, int64_t z_stride,
                                int64_t w_stride) {
   if (!p || !sref || !labels) return fail(FWIX_ERR_INVALID, "null plan, refs or labels");
+  p->pbuilt.assign(p->desc.nz, 0);  // cached factors belong to the previous references
   p->sref = (const float2*)sref;
   p->labels = labels;
   p->lab_z = z_stride;
@@ -415,16 +489,19 @@ fwix_status fwix_fft2d(fwix_plan* p, int inverse, const void* in, void* out, int
   if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
   FWIX_TRY(need_ws(p, FWIX_WS_STEP));
   cudaStream_t s = (cudaStream_t)stream;
-  SpecArgs a = p->args((const float2*)in, (float2*)out, add);
+  SpecArgs a0 = p->args((const float2*)in, (float2*)out, add);
   const float sc = 1.0f / sqrtf((float)p->d.NX * (float)p->d.NY);
-  if (!inverse) {
-    FWIX_TRY(cu(fwix::row_forward(a, fwix::W_ONE, s), "fft row pass"));
-    FWIX_TRY(cu(fwix::col_fft(a, 0, p->t1(), (float2*)out, add, sc, s), "fft column pass"));
-  } else {
-    FWIX_TRY(cu(fwix::col_fft(a, 1, (const float2*)in, p->t2(), 0, sc, s), "ifft column pass"));
-    FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_ONE, 0, s), "ifft row pass"));
-  }
-  return FWIX_OK;
+  return for_chunks(p, a0, [&](const SpecArgs& a) -> fwix_status {
+    const long long off = a.b0 * p->d.slice;
+    if (!inverse) {
+      FWIX_TRY(cu(fwix::row_forward(a, fwix::W_ONE, s), "fft row pass"));
+      FWIX_TRY(cu(fwix::col_fft(a, 0, p->t1(), (float2*)out + off, add, sc, s), "fft column pass"));
+    } else {
+      FWIX_TRY(cu(fwix::col_fft(a, 1, (const float2*)in + off, p->t2(), 0, sc, s), "ifft column pass"));
+      FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_ONE, 0, s), "ifft row pass"));
+    }
+    return FWIX_OK;
+  });
 }
 
 fwix_status fwix_phase_shift(fwix_plan* p, int mode, const void* sref_w, const void* in, void* out, int add,

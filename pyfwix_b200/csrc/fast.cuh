@@ -1,0 +1,591 @@
+// Register-resident row / column passes for line lengths with a compile-time plan.
+//
+// One group of T lanes (T = 8, 16 or 32; 32 / T groups per warp) owns one line of
+// N = T * E samples and keeps E of them per lane in registers.  The line goes
+// through the radix stages of its plan (mixed-radix Stockham, Govindaraju et al.,
+// SC'08): each stage does E / R radix-R butterflies in registers and, except after
+// the last one, exchanges the samples through the line's own shared-memory region,
+// so stages are separated by __syncwarp() only.  Sample p of a line lives at
+// swz(p) = p ^ ((p >> 3) & 15), which keeps every stage's stores and loads within
+// about one wavefront per half-warp.  All index arithmetic except the lane's own
+// index is compile-time.
+//
+// Layouts: before stage 0 (radix R0) lane t holds element e = b*R0 + r at position
+// t + T*b + r*N/R0; after the last stage (radix Rk) at t + T*b + r*N/Rk.  The
+// inverse runs the stages in reverse order, so its input layout is the forward
+// output layout: a spectrum is multiplied and transformed back in registers.
+//
+// Row passes (lines along x) read and write HBM directly from registers (for a
+// fixed element, consecutive lanes touch consecutive samples) and need no CTA
+// barrier.  Column passes (lines along y) stage a tile of LX columns x NY rows
+// through shared memory so that HBM is read and written in row segments.
+#pragma once
+#include "ops.cuh"
+
+namespace fwix {
+namespace fast {
+
+template <int... Rs>
+struct Radices {
+  static constexpr int NS = sizeof...(Rs);
+  __host__ __device__ static constexpr int get(int s) {
+    constexpr int r[] = {Rs...};
+    return r[s];
+  }
+};
+
+template <int N_, int E_, class RS>
+struct Plan {
+  static constexpr int N = N_;
+  static constexpr int E = E_;
+  static constexpr int T = N_ / E_;    // lanes per line
+  static constexpr int G = 32 / T;     // lines per warp
+  static constexpr int NS = RS::NS;
+  static_assert(T == 8 || T == 16 || T == 32, "a line takes 8, 16 or 32 lanes");
+  __host__ __device__ static constexpr int radix(int s) { return RS::get(s); }
+};
+
+constexpr int kWarps = 8;  // warps per CTA in every pass
+
+template <class P, bool REV>
+struct Order {
+  __host__ __device__ static constexpr int radix(int s) { return REV ? P::radix(P::NS - 1 - s) : P::radix(s); }
+  __host__ __device__ static constexpr int span(int s) { return s == 0 ? 1 : span(s - 1) * radix(s - 1); }
+};
+
+__device__ __forceinline__ int swz(int p) { return p ^ ((p >> 3) & 15); }
+
+template <class P, int R>
+__device__ __forceinline__ int lpos(int t, int e) {
+  return t + P::T * (e / R) + (e % R) * (P::N / R);
+}
+template <class P>
+__device__ __forceinline__ int pos_first(int t, int e) {  // input of the forward transform
+  return lpos<P, P::radix(0)>(t, e);
+}
+template <class P>
+__device__ __forceinline__ int pos_last(int t, int e) {  // output of the forward transform
+  return lpos<P, P::radix(P::NS - 1)>(t, e);
+}
+
+template <class P, bool REV, bool INV, int S>
+__device__ __forceinline__ void stages(float2 (&v)[P::E], int t, const float2* __restrict__ tw, float2* line) {
+  using O = Order<P, REV>;
+  constexpr int R = O::radix(S);
+  constexpr int Ns = O::span(S);
+  constexpr int B = P::E / R;
+  constexpr int tstep = P::N / (Ns * R);
+#pragma unroll
+  for (int b = 0; b < B; ++b) {
+    float2 u[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) u[r] = v[b * R + r];
+    if constexpr (Ns > 1) {
+      const int j = t + P::T * b;
+      const int k = j % Ns;
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const float2 w = tw[k * r * tstep];
+        u[r] = INV ? cmul_conj(u[r], w) : cmul(u[r], w);
+      }
+    }
+    Dft<R, INV>::run(u);
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[b * R + r] = u[r];
+  }
+  if constexpr (S + 1 < P::NS) {
+    constexpr int R2 = O::radix(S + 1);
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const int j = t + P::T * b;
+      const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+      for (int r = 0; r < R; ++r) line[swz(base + r * Ns)] = v[b * R + r];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) v[e] = line[swz(lpos<P, R2>(t, e))];
+    stages<P, REV, INV, S + 1>(v, t, tw, line);
+  }
+}
+
+template <class P>
+__device__ __forceinline__ void fft_fwd(float2 (&v)[P::E], int t, const float2* tw, float2* line) {
+  stages<P, false, false, 0>(v, t, tw, line);
+}
+template <class P>
+__device__ __forceinline__ void fft_inv(float2 (&v)[P::E], int t, const float2* tw, float2* line) {
+  stages<P, true, true, 0>(v, t, tw, line);
+}
+
+__device__ __forceinline__ void load_table(float2* dst, const float2* __restrict__ src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// Asynchronous 8-byte global -> shared copy (zero-filled when !valid).
+__device__ __forceinline__ void cp_async8(float2* dst, const float2* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// ---------------------------------------------------------------- row passes (NX = P::N)
+
+template <class P>
+struct RowGeo {
+  static constexpr int LINE = P::N + (P::T < 32 ? 8 : 0);  // shared-memory stride between lines
+  static constexpr int ROWS = kWarps * P::G;                // rows per CTA
+  static size_t smem() { return ((size_t)kWarps * P::G * LINE + P::N) * sizeof(float2); }
+};
+
+// Per-thread view of a row pass: which row, which lane of the line, its smem line.
+template <class P>
+struct RowCtx {
+  int t;
+  int y;
+  bool live;
+  long long bl, b;
+  int iw;
+  float2* line;
+  float2* tw;
+  __device__ RowCtx(const SpecArgs& a, float2* smem, int nchunk) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / P::T;
+    t = lane % P::T;
+    tw = smem + (size_t)kWarps * P::G * RowGeo<P>::LINE;
+    line = smem + (size_t)(warp * P::G + g) * RowGeo<P>::LINE;
+    bl = blockIdx.x / nchunk;
+    b = a.b0 + bl;
+    y = (int)(blockIdx.x - bl * nchunk) * RowGeo<P>::ROWS + warp * P::G + g;
+    live = y < a.d.NY;
+    iw = (int)(b % a.d.nw);
+  }
+};
+
+// t1[term] = F_x(pre_term * in) for each term.
+template <class P, int PRE>
+__global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int nchunk) {
+  extern __shared__ float2 smem[];
+  RowCtx<P> c(a, smem, nchunk);
+  load_table(c.tw, a.twx, P::N);
+  __syncthreads();
+  float2 raw[P::E];
+  const float2* src = a.in + (c.b * a.d.NY + (c.live ? c.y : 0)) * P::N;
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) raw[e] = c.live ? src[pos_first<P>(c.t, e)] : make_float2(0.f, 0.f);
+  const int nterm = (PRE == W_MASK || PRE == W_SCAT_CONJ) ? a.nterm : 1;
+  for (int term = 0; term < nterm; ++term) {
+    float2 v[P::E];
+#pragma unroll
+    for (int e = 0; e < P::E; ++e)
+      v[e] = c.live ? row_weight<PRE>(a, term, c.iw, c.y, pos_first<P>(c.t, e), raw[e]) : make_float2(0.f, 0.f);
+    fft_fwd<P>(v, c.t, c.tw, c.line);
+    if (c.live) {
+      float2* dst = a.t1 + (long long)term * a.tstride + (c.bl * a.d.NY + c.y) * P::N;
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) dst[pos_last<P>(c.t, e)] = v[e];
+    }
+  }
+}
+
+// out (+)= post * sum_term W_term * F_x^-1(t2[term]); the next term's row is
+// prefetched while the current one is transformed, and with labels the terms
+// that no sample of the warp's rows selects are skipped.
+template <class P, int POST>
+__global__ void __launch_bounds__(kWarps * 32) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
+  extern __shared__ float2 smem[];
+  RowCtx<P> c(a, smem, nchunk);
+  load_table(c.tw, a.twx, P::N);
+  __syncthreads();
+  const int nterm = (POST == W_MASK || POST == W_SCAT) ? a.nterm : 1;
+  float2 acc[P::E];
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) acc[e] = make_float2(0.f, 0.f);
+  uint8_t lab[P::E];
+  unsigned used = 0xffffffffu;
+  if (POST == W_MASK) {
+    const uint8_t* lrow = a.lab + (long long)c.iw * a.lab_w + (long long)(c.live ? c.y : 0) * P::N;
+    unsigned mine = 0;
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) {
+      lab[e] = c.live ? lrow[pos_first<P>(c.t, e)] : 255;
+      if (lab[e] < 32) mine |= 1u << lab[e];
+    }
+    // the warp steps through the union of its lines' terms so that it stays converged
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
+    used = nterm > 32 ? 0xffffffffu : mine;
+  }
+  auto next_term = [&](int from) {
+    int k = from;
+    while (k < nterm && k < 32 && !((used >> k) & 1u)) ++k;
+    return k;
+  };
+  const long long roff = (c.bl * a.d.NY + (c.live ? c.y : 0)) * P::N;
+  int term = next_term(0);
+  float2 pre[P::E];
+  if (term < nterm) {
+    const float2* src = a.t2 + (long long)term * a.tstride + roff;
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) pre[e] = c.live ? src[pos_last<P>(c.t, e)] : make_float2(0.f, 0.f);
+  }
+  while (term < nterm) {
+    float2 v[P::E];
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) v[e] = pre[e];
+    const int nxt = next_term(term + 1);
+    if (nxt < nterm) {
+      const float2* src = a.t2 + (long long)nxt * a.tstride + roff;
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) pre[e] = c.live ? src[pos_last<P>(c.t, e)] : make_float2(0.f, 0.f);
+    }
+    fft_inv<P>(v, c.t, c.tw, c.line);
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) {
+      if (POST == W_MASK) {
+        if ((int)lab[e] == term) acc[e] = v[e];
+      } else if (c.live) {
+        acc[e] = cadd(acc[e], row_weight<POST>(a, term, c.iw, c.y, pos_first<P>(c.t, e), v[e]));
+      }
+    }
+    term = nxt;
+  }
+  if (!c.live) return;
+  float2* dst = a.out + (c.b * a.d.NY + c.y) * P::N;
+  const float ty = post_taper ? a.tapy[c.y] : 1.f;
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) {
+    const int x = pos_first<P>(c.t, e);
+    float2 v = acc[e];
+    if (post_taper) v = cscale(v, a.tapx[x] * ty);
+    if (a.add) v = cadd(dst[x], v);
+    dst[x] = v;
+  }
+}
+
+// ---------------------------------------------------------------- column passes (NY = P::N)
+
+template <class P>
+struct ColGeo {
+  static constexpr int LX = kWarps * P::G;  // columns per CTA
+  static constexpr int LINE = P::N + 1;     // tile stride between columns
+  static size_t smem() { return ((size_t)LX * LINE + P::N) * sizeof(float2); }
+  // Resident CTAs per SM the register allocation is held to: three for plans
+  // of at most 8 samples per lane (about 85 registers), else what fits.
+  static constexpr int kMinBlocks = P::E <= 8 ? 3 : 1;
+  static size_t smem2() { return ((size_t)2 * LX * LINE + P::N) * sizeof(float2); }  // tile, tw, tile
+};
+
+template <class P>
+struct ColCtx {
+  int t, col, x, x0;
+  long long b;
+  int iw;
+  float2* tile;
+  float2* line;
+  float2* tw;
+  __device__ ColCtx(const SpecArgs& a, float2* smem, int nxt) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / P::T;
+    t = lane % P::T;
+    col = warp * P::G + g;
+    tile = smem;
+    line = smem + (size_t)col * ColGeo<P>::LINE;
+    tw = smem + (size_t)ColGeo<P>::LX * ColGeo<P>::LINE;
+    b = blockIdx.x / nxt;
+    x0 = (int)(blockIdx.x - b * nxt) * ColGeo<P>::LX;
+    x = x0 + col;
+    iw = (int)((a.b0 + b) % a.d.nw);
+  }
+};
+
+// Coalesced copy of the CTA's columns of slice-local b between HBM and the tile.
+template <class P>
+__device__ __forceinline__ void cols_to_tile(float2* tile, const float2* __restrict__ g, const SpecArgs& a,
+                                             long long b, int x0) {
+  constexpr int LX = ColGeo<P>::LX;
+  for (int i = threadIdx.x; i < LX * P::N; i += blockDim.x) {
+    const int y = i / LX, cc = i - y * LX;
+    const int x = x0 + cc;
+    if (x < a.d.NX) tile[cc * ColGeo<P>::LINE + swz(y)] = g[b * a.d.slice + (long long)y * a.d.NX + x];
+  }
+}
+template <class P>
+__device__ __forceinline__ void tile_to_cols(const float2* tile, float2* g, const SpecArgs& a, long long b, int x0,
+                                             int add, float scale) {
+  constexpr int LX = ColGeo<P>::LX;
+  for (int i = threadIdx.x; i < LX * P::N; i += blockDim.x) {
+    const int y = i / LX, cc = i - y * LX;
+    const int x = x0 + cc;
+    if (x >= a.d.NX) continue;
+    float2 v = tile[cc * ColGeo<P>::LINE + swz(y)];
+    if (scale != 1.f) v = cscale(v, scale);
+    float2* q = g + b * a.d.slice + (long long)y * a.d.NX + x;
+    if (add) v = cadd(*q, v);
+    *q = v;
+  }
+}
+
+// t2[term] = F_y^-1(Q_term * F_y(t1[0])); the spectrum stays in registers.
+template <class P, int QM>
+__global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_a(const SpecArgs a, int nxt) {
+  extern __shared__ float2 smem[];
+  ColCtx<P> c(a, smem, nxt);
+  load_table(c.tw, a.twy, P::N);
+  cols_to_tile<P>(c.tile, a.t1, a, c.b, c.x0);
+  __syncthreads();
+  float2 psi[P::E];
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) psi[e] = c.line[swz(pos_first<P>(c.t, e))];
+  fft_fwd<P>(psi, c.t, c.tw, c.line);
+  const int xq = c.x < a.d.NX ? c.x : 0;
+  float2 q[P::E];
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) q[e] = qmult<QM>(a, 0, c.iw, xq, pos_last<P>(c.t, e));
+  for (int term = 0; term < a.nterm; ++term) {
+    float2 v[P::E];
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) v[e] = cmul(psi[e], q[e]);
+    if (term + 1 < a.nterm) {
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) q[e] = qmult<QM>(a, term + 1, c.iw, xq, pos_last<P>(c.t, e));
+    }
+    __syncthreads();  // the previous term's tile has been stored
+    fft_inv<P>(v, c.t, c.tw, c.line);
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) c.line[swz(pos_first<P>(c.t, e))] = v[e];
+    __syncthreads();
+    tile_to_cols<P>(c.tile, a.t2 + (long long)term * a.tstride, a, c.b, c.x0, 0, 1.f);
+  }
+}
+
+// Asynchronous copy of the CTA's columns of slice-local b into a tile.
+template <class P>
+__device__ __forceinline__ void cols_to_tile_async(float2* tile, const float2* __restrict__ g, const SpecArgs& a,
+                                                   long long b, int x0) {
+  constexpr int LX = ColGeo<P>::LX;
+  for (int i = threadIdx.x; i < LX * P::N; i += blockDim.x) {
+    const int y = i / LX, cc = i - y * LX;
+    const int x = x0 + cc;
+    const bool ok = x < a.d.NX;
+    cp_async8(tile + cc * ColGeo<P>::LINE + swz(y), g + b * a.d.slice + (long long)y * a.d.NX + (ok ? x : 0), ok);
+  }
+  cp_async_commit();
+}
+
+// t2[0] = F_y^-1(sum_term Q_term * F_y(t1[term])).  Two tiles: the copy engine
+// fills one with the next term while the warps transform the other.
+template <class P, int QM>
+__global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_b(const SpecArgs a, int nxt) {
+  extern __shared__ float2 smem[];
+  ColCtx<P> c(a, smem, nxt);
+  float2* tiles[2] = {c.tile, c.tw + P::N};
+  const long long lineoff = (long long)c.col * ColGeo<P>::LINE;
+  load_table(c.tw, a.twy, P::N);
+  const int xq = c.x < a.d.NX ? c.x : 0;
+  float2 acc[P::E];
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) acc[e] = make_float2(0.f, 0.f);
+  cols_to_tile_async<P>(tiles[0], a.t1, a, c.b, c.x0);
+  for (int term = 0; term < a.nterm; ++term) {
+    __syncthreads();  // every warp is done with the tile the next copy overwrites
+    if (term + 1 < a.nterm) {
+      cols_to_tile_async<P>(tiles[(term + 1) & 1], a.t1 + (long long)(term + 1) * a.tstride, a, c.b, c.x0);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    float2 q[P::E];
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) q[e] = qmult<QM>(a, term, c.iw, xq, pos_last<P>(c.t, e));
+    __syncthreads();  // this term's tile is complete
+    float2* line = tiles[term & 1] + lineoff;
+    float2 v[P::E];
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) v[e] = line[swz(pos_first<P>(c.t, e))];
+    fft_fwd<P>(v, c.t, c.tw, line);
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) acc[e] = cadd(acc[e], cmul(v[e], q[e]));
+  }
+  __syncthreads();
+  fft_inv<P>(acc, c.t, c.tw, c.line);
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) c.line[swz(pos_first<P>(c.t, e))] = acc[e];
+  __syncthreads();
+  tile_to_cols<P>(c.tile, a.t2, a, c.b, c.x0, 0, 1.f);
+}
+
+// out (+)= scale * F_y^{-+1}(in): the column half of a plain 2D transform.
+template <class P, bool INV>
+__global__ void __launch_bounds__(kWarps * 32) k_col_fft(const SpecArgs a, int nxt, const float2* in, float2* out,
+                                                          int add, float scale) {
+  extern __shared__ float2 smem[];
+  ColCtx<P> c(a, smem, nxt);
+  load_table(c.tw, a.twy, P::N);
+  cols_to_tile<P>(c.tile, in, a, c.b, c.x0);
+  __syncthreads();
+  float2 v[P::E];
+  if (!INV) {
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) v[e] = c.line[swz(pos_first<P>(c.t, e))];
+    fft_fwd<P>(v, c.t, c.tw, c.line);
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) c.line[swz(pos_last<P>(c.t, e))] = v[e];
+  } else {
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) v[e] = c.line[swz(pos_last<P>(c.t, e))];
+    fft_inv<P>(v, c.t, c.tw, c.line);
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) c.line[swz(pos_first<P>(c.t, e))] = v[e];
+  }
+  __syncthreads();
+  tile_to_cols<P>(c.tile, out, a, c.b, c.x0, add, scale);
+}
+
+// ---------------------------------------------------------------- launch helpers
+
+template <class K>
+cudaError_t opt_in_smem(K kernel, size_t bytes) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess || bytes <= 48 * 1024) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <class P>
+cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
+  const int nchunk = (a.d.NY + RowGeo<P>::ROWS - 1) / RowGeo<P>::ROWS;
+  const unsigned grid = (unsigned)(a.nb * nchunk);
+  const size_t sm = RowGeo<P>::smem();
+  cudaError_t e;
+#define FWIX_FAST_RF(W)                                                              \
+  case W:                                                                            \
+    e = opt_in_smem(k_row_fwd<P, W>, sm);                                            \
+    if (e == cudaSuccess) k_row_fwd<P, W><<<grid, kWarps * 32, sm, s>>>(a, nchunk);  \
+    break;
+  switch (pre) {
+    FWIX_FAST_RF(W_ONE)
+    FWIX_FAST_RF(W_TAPER)
+    FWIX_FAST_RF(W_MASK)
+    FWIX_FAST_RF(W_SCAT_CONJ)
+    FWIX_FAST_RF(W_IC)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_FAST_RF
+  if (e == cudaSuccess) count_launch();
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <class P>
+cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s) {
+  const int nchunk = (a.d.NY + RowGeo<P>::ROWS - 1) / RowGeo<P>::ROWS;
+  const unsigned grid = (unsigned)(a.nb * nchunk);
+  const size_t sm = RowGeo<P>::smem();
+  cudaError_t e;
+#define FWIX_FAST_RI(W)                                                                          \
+  case W:                                                                                        \
+    e = opt_in_smem(k_row_inv<P, W>, sm);                                                        \
+    if (e == cudaSuccess) k_row_inv<P, W><<<grid, kWarps * 32, sm, s>>>(a, nchunk, post_taper);  \
+    break;
+  switch (post) {
+    FWIX_FAST_RI(W_ONE)
+    FWIX_FAST_RI(W_MASK)
+    FWIX_FAST_RI(W_SCAT)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_FAST_RI
+  if (e == cudaSuccess) count_launch();
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <class P>
+cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
+  const int nxt = (a.d.NX + ColGeo<P>::LX - 1) / ColGeo<P>::LX;
+  const unsigned grid = (unsigned)(a.nb * nxt);
+  const size_t sm = ColGeo<P>::smem();
+  cudaError_t e;
+#define FWIX_FAST_CA(Q)                                                           \
+  case Q:                                                                         \
+    e = opt_in_smem(k_col_a<P, Q>, sm);                                           \
+    if (e == cudaSuccess) k_col_a<P, Q><<<grid, kWarps * 32, sm, s>>>(a, nxt);    \
+    break;
+  switch (qmode) {
+    FWIX_FAST_CA(Q_PS_FWD)
+    FWIX_FAST_CA(Q_PS_ADJ)
+    FWIX_FAST_CA(Q_KPOW)
+    FWIX_FAST_CA(Q_ONE)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_FAST_CA
+  if (e == cudaSuccess) count_launch();
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <class P>
+cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s) {
+  const int nxt = (a.d.NX + ColGeo<P>::LX - 1) / ColGeo<P>::LX;
+  const unsigned grid = (unsigned)(a.nb * nxt);
+  const size_t sm = ColGeo<P>::smem2();
+  cudaError_t e;
+#define FWIX_FAST_CB(Q)                                                           \
+  case Q:                                                                         \
+    e = opt_in_smem(k_col_b<P, Q>, sm);                                           \
+    if (e == cudaSuccess) k_col_b<P, Q><<<grid, kWarps * 32, sm, s>>>(a, nxt);    \
+    break;
+  switch (qmode) {
+    FWIX_FAST_CB(Q_PS_FWD)
+    FWIX_FAST_CB(Q_PS_ADJ)
+    FWIX_FAST_CB(Q_KPOW)
+    FWIX_FAST_CB(Q_ONE)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_FAST_CB
+  if (e == cudaSuccess) count_launch();
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <class P>
+cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add, float scale,
+                    cudaStream_t s) {
+  const int nxt = (a.d.NX + ColGeo<P>::LX - 1) / ColGeo<P>::LX;
+  const unsigned grid = (unsigned)(a.nb * nxt);
+  const size_t sm = ColGeo<P>::smem();
+  cudaError_t e;
+  if (inverse) {
+    e = opt_in_smem(k_col_fft<P, true>, sm);
+    if (e == cudaSuccess) k_col_fft<P, true><<<grid, kWarps * 32, sm, s>>>(a, nxt, in, out, add, scale);
+  } else {
+    e = opt_in_smem(k_col_fft<P, false>, sm);
+    if (e == cudaSuccess) k_col_fft<P, false><<<grid, kWarps * 32, sm, s>>>(a, nxt, in, out, add, scale);
+  }
+  if (e == cudaSuccess) count_launch();
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+}  // namespace fast
+}  // namespace fwix
+
+// One translation unit per line length instantiates the launchers of its plan.
+#define FWIX_FAST_INSTANTIATE(PLAN, TAG)                                                                   \
+  namespace fwix {                                                                                          \
+  namespace fast {                                                                                          \
+  cudaError_t row_forward_##TAG(const SpecArgs& a, int pre, cudaStream_t s) {                               \
+    return row_forward<PLAN>(a, pre, s);                                                                    \
+  }                                                                                                         \
+  cudaError_t row_inverse_##TAG(const SpecArgs& a, int post, int pt, cudaStream_t s) {                      \
+    return row_inverse<PLAN>(a, post, pt, s);                                                               \
+  }                                                                                                         \
+  cudaError_t col_type_a_##TAG(const SpecArgs& a, int q, cudaStream_t s) { return col_type_a<PLAN>(a, q, s); } \
+  cudaError_t col_type_b_##TAG(const SpecArgs& a, int q, cudaStream_t s) { return col_type_b<PLAN>(a, q, s); } \
+  cudaError_t col_fft_##TAG(const SpecArgs& a, int inv, const float2* in, float2* out, int add, float sc,    \
+                            cudaStream_t s) {                                                               \
+    return col_fft<PLAN>(a, inv, in, out, add, sc, s);                                                      \
+  }                                                                                                         \
+  }                                                                                                         \
+  }

@@ -62,25 +62,46 @@ struct SpecArgs {
   long long slow_w;
   const float2* image; // imaging-condition image, (iw, y, x) at image[iw*img_w + y*nx + x] (W_IC)
   long long img_w;     // ny*nx, or 0 for one image shared by every frequency
+  // cached forward phase factors of this depth (x norm), element (ref, iw, |kx|, |ky|)
+  // at ptab[((ref*nw + iw)*ptab_nx + kxq)*ptab_ny + kyq], kxq = min(x, NX-x),
+  // kyq = min(y, NY-y); NULL means evaluate the factors in the kernel
+  const float2* ptab;
+  int ptab_nx, ptab_ny;
   float dz, eps, eps_scat;
   float coef[5];
   float norm;          // scale folded into the column multiplier
   int nterm;           // references (W_MASK) or Taylor terms (W_SCAT)
-  // buffers
+  // buffers.  A launch covers the slices (shot, frequency) b0 .. b0 + nb - 1: in / out
+  // (and the labels, images and tables) are indexed by the global slice b0 + bl,
+  // the intermediates t1 / t2 by the launch-local slice bl, term after term tstride
+  // elements apart.
   const float2* in;    // row-pass input (W_IC: the background wavefield)
   float2* out;         // row-pass output
   int add;
-  float2* t1;          // nterm wavefield-sized buffers, stride d.wfld
+  float2* t1;
   float2* t2;
+  long long b0, nb, tstride;
 };
 
-// Spectral passes (spectral.cu).  Each returns a CUDA error code.
+// Spectral passes (dispatch.cu: register-resident passes for lengths with a
+// compile-time plan, else the generic per-warp passes of spectral.cu).  Each
+// returns a CUDA error code.
+bool fast_length(int n);
 cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s);      // in -> t1[0..nterm)
 cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s);  // t2 -> out
 cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s);     // t1[0] -> t2[0..nterm)
 cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s);     // t1[0..nterm) -> t2[0]
 cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add,
                     float scale, cudaStream_t s);
+cudaError_t generic_row_forward(const SpecArgs& a, int pre, cudaStream_t s);
+cudaError_t generic_row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s);
+cudaError_t generic_col_type_a(const SpecArgs& a, int qmode, cudaStream_t s);
+cudaError_t generic_col_type_b(const SpecArgs& a, int qmode, cudaStream_t s);
+cudaError_t generic_col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add,
+                            float scale, cudaStream_t s);
+
+// Phase-factor cache of one depth (spectral.cu): dst [nref][nw][NX/2+1][NY/2+1].
+cudaError_t launch_phase_table(const SpecArgs& a, float2* dst, cudaStream_t s);
 
 // Pointwise kernels (pointwise.cu).
 cudaError_t launch_phase_shift(const SpecArgs& a, int mode, const float2* sref_w, const float2* in,

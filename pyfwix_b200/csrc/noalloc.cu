@@ -186,6 +186,9 @@ extern "C" fwix_status fwix_step_noalloc(const fwix_desc* desc, int kind, int iz
   a.add = add;
   a.t1 = (float2*)(base + tab);
   a.t2 = a.t1 + (long long)(one_in ? 1 : q.nref) * d.wfld;
+  a.b0 = 0;
+  a.nb = (long long)q.ns * q.nw;
+  a.tstride = d.wfld;
   a.sref = (const float2*)sref + (long long)iz * q.nref * q.nw;
   a.lab = labels + iz * labels_z_stride;
   a.lab_w = labels_w_stride;

@@ -1,0 +1,102 @@
+// Per-cell weights and spectral multipliers shared by the generic (spectral.cu)
+// and the register-resident (fast.cuh) passes.
+#pragma once
+#include "internal.h"
+
+namespace fwix {
+
+// Born weight W_n = (-i w dz / 2) c_n s~^(-1/2-n), s~ = Re s^2 + i (Im s^2 - eps Re s^2),
+// read from the unpadded slice with edge replication into the pad
+// (scatter.cu:61-106 slow_scale, :155-195 scale_by_iw, :240-277 pad_fwd).
+// s~^(-1/2-n) = (1/sqrt(s~)) (1/s~)^n with the principal root.
+__device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, int y, int x) {
+  const int xs = min(x, a.d.nx - 1), ys = min(y, a.d.ny - 1);
+  const float2 s2 = a.slow[(long long)iw * a.slow_w + (long long)ys * a.d.nx + xs];
+  const float2 st = make_float2(s2.x, s2.y - a.eps_scat * s2.x);
+  float2 p = cinv(csqrt_ref(st));
+  if (n > 0) {
+    const float2 is = cinv(st);
+    for (int k = 0; k < n; ++k) p = cmul(p, is);
+  }
+  const float f = 0.5f * a.w[iw] * a.dz * a.coef[n];
+  return rot90<false>(cscale(p, f));
+}
+
+template <int W>
+__device__ __forceinline__ float2 row_weight(const SpecArgs& a, int t, int iw, int y, int x, float2 v) {
+  if (W == W_ONE) return v;
+  if (W == W_TAPER) return cscale(v, a.tapx[x] * a.tapy[y]);
+  if (W == W_MASK) {
+    const uint8_t l = a.lab[(long long)iw * a.lab_w + (long long)y * a.d.NX + x];
+    return (int)l == t ? v : make_float2(0.f, 0.f);
+  }
+  if (W == W_SCAT) return cmul(v, scat_weight(a, t, iw, y, x));
+  if (W == W_SCAT_CONJ) return cmul_conj(v, scat_weight(a, t, iw, y, x));
+  // W_IC
+  if (y < a.d.ny && x < a.d.nx)
+    return cmul(v, a.image[(long long)iw * a.img_w + (long long)y * a.d.nx + x]);
+  return make_float2(0.f, 0.f);
+}
+
+// Column multiplier for term t at (iw, ky[y], kx[x]), scaled by a.norm.
+template <int QM>
+__device__ __forceinline__ float2 qmult(const SpecArgs& a, int t, int iw, int x, int y) {
+  if (QM == Q_ONE) return make_float2(a.norm, 0.f);
+  if (QM == Q_KPOW) {
+    // (|k| / w)^(2t) with |k| / w formed as in scatter.cu:49-50, the power by products
+    if (t == 0) return make_float2(a.norm, 0.f);
+    const float kx = a.kx[x], ky = a.ky[y];
+    const float r = sqrtf(kx * kx + ky * ky) / a.w[iw];
+    const float r2 = r * r;
+    float p = r2;
+    for (int k = 1; k < t; ++k) p *= r2;
+    return make_float2(p * a.norm, 0.f);
+  }
+  const float2 sr = a.sref[t * a.d.nw + iw];
+  const float w2 = a.w2[iw];
+  if ((QM == Q_PS_FWD || QM == Q_PS_ADJ) && a.ptab) {
+    const int kxq = min(x, a.d.NX - x), kyq = min(y, a.d.NY - y);
+    const float2 P = a.ptab[(((long long)t * a.d.nw + iw) * a.ptab_nx + kxq) * a.ptab_ny + kyq];
+    if (QM == Q_PS_FWD) return P;
+    // adjoint factor: conj(P), or P itself where the reference flips Re (b > 0)
+    const float bb = w2 * (sr.y - a.eps * sr.x);
+    return bb > 0.f ? P : cconj(P);
+  }
+  const float kx = a.kx[x], ky = a.ky[y];
+  const float aa = w2 * sr.x - (kx * kx + ky * ky);
+  const float bb = w2 * (sr.y - a.eps * sr.x);
+  float re, im;
+  if (bb == 0.f) {
+    // c = sqrt(a^2) = |a| exactly, so the general branch reduces to one root.
+    if (aa >= 0.f) {
+      re = sqrtf(aa);
+      im = 0.f;
+    } else {
+      re = 0.f;
+      im = -sqrtf(-aa);
+    }
+  } else {
+    // Re = sqrt((c+a)/2), Im = -sqrt((c-a)/2) as phase_shift.cu:38-41, with the
+    // smaller of the two taken from Re |Im| = |b| / 2: the same values without
+    // the cancellation of c - a (or c + a) in float.
+    const float c = sqrtf(aa * aa + bb * bb);
+    if (aa >= 0.f) {
+      re = sqrtf((c + aa) * 0.5f);
+      im = -(fabsf(bb) * 0.5f) / re;
+    } else {
+      im = -sqrtf((c - aa) * 0.5f);
+      re = (fabsf(bb) * 0.5f) / -im;
+    }
+  }
+  if (QM == Q_PS_ADJ && bb > 0.f) re = -re;
+  if (QM == Q_PS_INV) {
+    im = -im;
+    if (bb > 0.f) re = -re;
+  }
+  const float att = (im == 0.f ? 1.f : expf(im * a.dz)) * a.norm;
+  float sn = 0.f, cs = 1.f;
+  if (re != 0.f) sincosf(re * a.dz, &sn, &cs);
+  return QM == Q_PS_FWD ? make_float2(att * cs, -att * sn) : make_float2(att * cs, att * sn);
+}
+
+}  // namespace fwix

@@ -1,7 +1,8 @@
 // Per-cell operators of the path that carry no FFT: reflection, imaging
 // condition, linearised reflection, injection / recording and the migration
-// image.  All are deterministic: a thread owns one (w, y, x) cell and loops over
-// shots, so no floating-point atomics are needed where the reference uses them
+// image.  All are deterministic: a thread owns a (y, x) cell and a fixed set of
+// frequencies and loops over shots, and sums over frequencies are reduced in a
+// fixed order, so no floating-point atomics are needed where the reference uses them
 // (imaging_condition.cu:103-104, lin_reflect.cu:369-384), and the injection is a
 // gather over a host-built list instead of the reference's unsynchronised
 // read-modify-write (injection.cu:89-92).
@@ -25,38 +26,80 @@ __device__ __forceinline__ float2 refl_coef(float2 s0, float2 s1, float2 r0, flo
   return cdiv(csub(a, b), cadd(a, b));
 }
 
-__global__ void k_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
-                          const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw,
-                          const float2* __restrict__ in, float2* __restrict__ out) {
-  const long long n = (long long)d.nw * d.ny * d.nx;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % d.nx);
-    const long long q = i / d.nx;
-    const int y = (int)(q % d.ny);
-    const int iw = (int)(q / d.ny);
-    const long long m = iw * mw + (long long)y * d.nx + x;
-    float2 r = refl_coef(s0[m], s1[m], r0[m], r1[m]);
-    if (adjoint) r = cconj(r);
+// Block shape of the per-cell kernels: 32 consecutive (y, x) cells of the
+// unpadded window by 8 frequency groups.  A thread walks the frequencies
+// iw = threadIdx.y, threadIdx.y + 8, ..., so a coefficient that does not depend
+// on the frequency (model stride mw == 0) is computed once per thread, and a sum
+// over frequencies is finished by a fixed-order reduction of the 8 groups in
+// shared memory.
+constexpr int kCells = 32, kGroups = 8;
+
+struct Cell {
+  int yx, y, x;
+  bool ok;
+};
+__device__ __forceinline__ Cell this_cell(const Dims& d) {
+  Cell c;
+  c.yx = blockIdx.x * kCells + threadIdx.x;
+  c.ok = c.yx < d.ny * d.nx;
+  c.y = c.ok ? c.yx / d.nx : 0;
+  c.x = c.ok ? c.yx - c.y * d.nx : 0;
+  return c;
+}
+__device__ __forceinline__ long long wf_index(const Dims& d, int s, int iw, const Cell& c) {
+  return (((long long)s * d.nw + iw) * d.NY + c.y) * d.NX + c.x;
+}
+
+// Sums v over the 8 frequency groups of each cell in a fixed order; thread
+// (x, 0) gets the total.
+template <int K>
+__device__ __forceinline__ void reduce_groups(float2 (&v)[K]) {
+  __shared__ float2 red[K][kGroups][kCells];
+#pragma unroll
+  for (int k = 0; k < K; ++k) red[k][threadIdx.y][threadIdx.x] = v[k];
+  __syncthreads();
+  if (threadIdx.y == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float2 t = red[k][0][threadIdx.x];
+#pragma unroll
+      for (int g = 1; g < kGroups; ++g) t = cadd(t, red[k][g][threadIdx.x]);
+      v[k] = t;
+    }
+  }
+}
+
+unsigned cell_blocks(const Dims& d) { return (unsigned)((d.ny * d.nx + kCells - 1) / kCells); }
+
+__global__ void __launch_bounds__(kCells * kGroups)
+    k_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
+              const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw,
+              const float2* __restrict__ in, float2* __restrict__ out) {
+  const Cell c = this_cell(d);
+  if (!c.ok) return;
+  float2 r = make_float2(0.f, 0.f);
+  for (int iw = threadIdx.y; iw < d.nw; iw += kGroups) {
+    if (mw != 0 || iw == (int)threadIdx.y) {
+      const long long m = iw * mw + c.yx;
+      r = refl_coef(s0[m], s1[m], r0[m], r1[m]);
+      if (adjoint) r = cconj(r);
+    }
     for (int s = 0; s < d.ns; ++s) {
-      const long long k = (((long long)s * d.nw + iw) * d.NY + y) * d.NX + x;
+      const long long k = wf_index(d, s, iw, c);
       out[k] = cadd(out[k], cmul(in[k], r));
     }
   }
 }
 
-__global__ void k_ic_fwd(Dims d, const float2* __restrict__ bg, const float2* __restrict__ image,
-                         long long img_w, float2* __restrict__ wfld) {
-  const long long n = (long long)d.nw * d.ny * d.nx;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % d.nx);
-    const long long q = i / d.nx;
-    const int y = (int)(q % d.ny);
-    const int iw = (int)(q / d.ny);
-    const float2 im = image[iw * img_w + (long long)y * d.nx + x];
+__global__ void __launch_bounds__(kCells * kGroups)
+    k_ic_fwd(Dims d, const float2* __restrict__ bg, const float2* __restrict__ image, long long img_w,
+             float2* __restrict__ wfld) {
+  const Cell c = this_cell(d);
+  if (!c.ok) return;
+  for (int iw = threadIdx.y; iw < d.nw; iw += kGroups) {
+    const float2 im = image[iw * img_w + c.yx];
     for (int s = 0; s < d.ns; ++s) {
-      const long long k = (((long long)s * d.nw + iw) * d.NY + y) * d.NX + x;
+      const long long k = wf_index(d, s, iw, c);
       wfld[k] = cadd(wfld[k], cmul(bg[k], im));
     }
   }
@@ -64,27 +107,27 @@ __global__ void k_ic_fwd(Dims d, const float2* __restrict__ bg, const float2* __
 
 // image[w, y, x] (+)= sum_s conj(bg) wfld; with wsum the frequencies are summed as well
 // into image[y, x].
-__global__ void k_ic_adj(Dims d, const float2* __restrict__ bg, const float2* __restrict__ wfld,
-                         float2* __restrict__ image, int add, int wsum) {
-  const int nwo = wsum ? 1 : d.nw;
-  const int nwi = wsum ? d.nw : 1;
-  const long long n = (long long)nwo * d.ny * d.nx;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % d.nx);
-    const long long q = i / d.nx;
-    const int y = (int)(q % d.ny);
-    const int iw0 = (int)(q / d.ny);
-    float2 acc = make_float2(0.f, 0.f);
-    for (int j = 0; j < nwi; ++j) {
-      const int iw = iw0 + j;
-      for (int s = 0; s < d.ns; ++s) {
-        const long long k = (((long long)s * d.nw + iw) * d.NY + y) * d.NX + x;
-        acc = cadd(acc, cmul_conj(wfld[k], bg[k]));
-      }
+__global__ void __launch_bounds__(kCells * kGroups)
+    k_ic_adj(Dims d, const float2* __restrict__ bg, const float2* __restrict__ wfld, float2* __restrict__ image,
+             int add, int wsum) {
+  const Cell c = this_cell(d);
+  float2 acc[1] = {make_float2(0.f, 0.f)};
+  for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups) {
+    float2 t = make_float2(0.f, 0.f);
+    for (int s = 0; s < d.ns; ++s) {
+      const long long k = wf_index(d, s, iw, c);
+      t = cadd(t, cmul_conj(wfld[k], bg[k]));
     }
-    image[i] = add ? cadd(image[i], acc) : acc;
+    if (wsum) {
+      acc[0] = cadd(acc[0], t);
+    } else {
+      float2* o = image + (long long)iw * d.ny * d.nx + c.yx;
+      *o = add ? cadd(*o, t) : t;
+    }
   }
+  if (!wsum) return;
+  reduce_groups<1>(acc);
+  if (threadIdx.y == 0 && c.ok) image[c.yx] = add ? cadd(image[c.yx], acc[0]) : acc[0];
 }
 
 // Coefficients of drefl_forward (lin_reflect.cu:248-292).
@@ -107,66 +150,69 @@ __device__ __forceinline__ LinCoef lin_coef(float2 s0, float2 s1, float2 r0, flo
   return c;
 }
 
-__global__ void k_lin_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
-                              const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw,
-                              float2* dm0, float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
-                              int add) {
-  // forward: one thread per (w, y, x) of dr.  adjoint: one thread per (w, y, x) of dm,
-  // or per (y, x) with a loop over w when dm is shared by every frequency.
+// forward: dr[w, y, x] (+)= as dm0 - bs dm1 + ar dm3 - br dm2.  adjoint: the
+// conjugate-transposed sums into dm[w] (dm_w != 0) or into dm shared by every
+// frequency (dm_w == 0, summed over w).
+__global__ void __launch_bounds__(kCells * kGroups)
+    k_lin_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
+                  const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw, float2* dm0,
+                  float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr, int add) {
+  const Cell c = this_cell(d);
+  const long long plane = (long long)d.ny * d.nx;
   const int wsum = adjoint && dm_w == 0;
-  const int nwo = wsum ? 1 : d.nw;
-  const long long n = (long long)nwo * d.ny * d.nx;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % d.nx);
-    const long long q = i / d.nx;
-    const int y = (int)(q % d.ny);
-    const int iw0 = (int)(q / d.ny);
-    const long long yx = (long long)y * d.nx + x;
+  LinCoef cf;
+  float2 g[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups) {
+    if (mw != 0 || iw == (int)threadIdx.y) {
+      const long long m = iw * mw + c.yx;
+      cf = lin_coef(s0[m], s1[m], r0[m], r1[m]);
+    }
+    const long long i = iw * plane + c.yx, k = iw * dm_w + c.yx;
     if (!adjoint) {
-      const long long m = iw0 * mw + yx, k = iw0 * dm_w + yx;
-      const LinCoef c = lin_coef(s0[m], s1[m], r0[m], r1[m]);
-      float2 v = csub(cmul(c.as, dm0[k]), cmul(c.bs, dm1[k]));
-      v = cadd(v, csub(cmul(c.ar, dm3[k]), cmul(c.br, dm2[k])));
+      float2 v = csub(cmul(cf.as, dm0[k]), cmul(cf.bs, dm1[k]));
+      v = cadd(v, csub(cmul(cf.ar, dm3[k]), cmul(cf.br, dm2[k])));
       dr[i] = add ? cadd(dr[i], v) : v;
       continue;
     }
-    float2 g0 = make_float2(0.f, 0.f), g1 = g0, g2 = g0, g3 = g0;
-    for (int j = 0; j < (wsum ? d.nw : 1); ++j) {
-      const int iw = iw0 + j;
-      const long long m = iw * mw + yx;
-      const LinCoef c = lin_coef(s0[m], s1[m], r0[m], r1[m]);
-      const float2 g = dr[(long long)iw * d.ny * d.nx + yx];
-      g0 = cadd(g0, cmul_conj(g, c.as));
-      g1 = csub(g1, cmul_conj(g, c.bs));
-      g3 = cadd(g3, cmul_conj(g, c.ar));
-      g2 = csub(g2, cmul_conj(g, c.br));
+    const float2 gi = dr[i];
+    const float2 t0 = cmul_conj(gi, cf.as), t1 = cscale(cmul_conj(gi, cf.bs), -1.f);
+    const float2 t3 = cmul_conj(gi, cf.ar), t2 = cscale(cmul_conj(gi, cf.br), -1.f);
+    if (wsum) {
+      g[0] = cadd(g[0], t0);
+      g[1] = cadd(g[1], t1);
+      g[2] = cadd(g[2], t2);
+      g[3] = cadd(g[3], t3);
+    } else {
+      // dm0 and dm1 (dm2 and dm3) alias at the bottom level; the same thread adds both.
+      dm0[k] = add ? cadd(dm0[k], t0) : t0;
+      dm1[k] = (add || dm1 == dm0) ? cadd(dm1[k], t1) : t1;
+      dm2[k] = add ? cadd(dm2[k], t2) : t2;
+      dm3[k] = (add || dm3 == dm2) ? cadd(dm3[k], t3) : t3;
     }
-    const long long k = iw0 * dm_w + yx;
-    // dm0 and dm1 (dm2 and dm3) alias at the bottom level; the same thread adds both.
-    dm0[k] = add ? cadd(dm0[k], g0) : g0;
-    dm1[k] = (add || dm1 == dm0) ? cadd(dm1[k], g1) : g1;
-    dm2[k] = add ? cadd(dm2[k], g2) : g2;
-    dm3[k] = (add || dm3 == dm2) ? cadd(dm3[k], g3) : g3;
   }
+  if (!wsum) return;
+  reduce_groups<4>(g);
+  if (threadIdx.y != 0 || !c.ok) return;
+  const long long k = c.yx;
+  dm0[k] = add ? cadd(dm0[k], g[0]) : g[0];
+  dm1[k] = (add || dm1 == dm0) ? cadd(dm1[k], g[1]) : g[1];
+  dm2[k] = add ? cadd(dm2[k], g[2]) : g[2];
+  dm3[k] = (add || dm3 == dm2) ? cadd(dm3[k], g[3]) : g[3];
 }
 
-__global__ void k_image_acc(Dims d, const float2* __restrict__ S, const float2* __restrict__ R,
-                            float* __restrict__ img, int add) {
-  const long long n = (long long)d.ny * d.nx;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % d.nx);
-    const int y = (int)(i / d.nx);
-    float acc = 0.f;
-    for (int s = 0; s < d.ns; ++s)
-      for (int iw = 0; iw < d.nw; ++iw) {
-        const long long k = (((long long)s * d.nw + iw) * d.NY + y) * d.NX + x;
-        const float2 a = S[k], b = R[k];
-        acc += a.x * b.x + a.y * b.y;  // Re(conj(S) R)
-      }
-    img[i] = add ? img[i] + acc : acc;
-  }
+__global__ void __launch_bounds__(kCells * kGroups)
+    k_image_acc(Dims d, const float2* __restrict__ S, const float2* __restrict__ R, float* __restrict__ img,
+                int add) {
+  const Cell c = this_cell(d);
+  float2 acc[1] = {make_float2(0.f, 0.f)};
+  for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups)
+    for (int s = 0; s < d.ns; ++s) {
+      const long long k = wf_index(d, s, iw, c);
+      const float2 a = S[k], b = R[k];
+      acc[0].x += a.x * b.x + a.y * b.y;  // Re(conj(S) R)
+    }
+  reduce_groups<1>(acc);
+  if (threadIdx.y == 0 && c.ok) img[c.yx] = add ? img[c.yx] + acc[0].x : acc[0].x;
 }
 
 __global__ void k_axpy(long long n, const float2* __restrict__ x, float2* __restrict__ y) {
@@ -180,8 +226,8 @@ __global__ void k_inject(Dims d, InjectLevel L, const float2* __restrict__ trace
   const long long n = (long long)L.ncell * d.nw;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int iw = (int)(i % d.nw);
-    const int e = (int)(i / d.nw);
+    const int e = (int)(i % L.ncell);
+    const int iw = (int)(i / L.ncell);
     float2 acc = make_float2(0.f, 0.f);
     for (int k = L.start[e]; k < L.start[e + 1]; ++k)
       acc = cadd(acc, cscale(traces[(long long)L.trace[k] * d.nw + iw], L.weight[k]));
@@ -197,8 +243,8 @@ __global__ void k_record(Dims d, InjectLevel L, const float2* __restrict__ wfld,
   const long long n = (long long)L.ntr * d.nw;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int iw = (int)(i % d.nw);
-    const int e = (int)(i / d.nw);
+    const int e = (int)(i % L.ntr);
+    const int iw = (int)(i / L.ntr);
     const long long cell = L.rcell[e];
     const long long shot = cell / d.slice, yx = cell - shot * d.slice;
     const float2* p = wfld + (shot * d.nw + iw) * d.slice + yx;
@@ -221,7 +267,7 @@ cudaError_t launch_reflect(const Dims& d, int adjoint, const float2* s0, const f
     cudaError_t e = cudaMemsetAsync(out, 0, d.wfld * sizeof(float2), s);
     if (e != cudaSuccess) return e;
   }
-  k_reflect<<<grid1d((long long)d.nw * d.ny * d.nx), 256, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, in, out);
+  k_reflect<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, in, out);
   count_launch();
   return cudaGetLastError();
 }
@@ -232,15 +278,14 @@ cudaError_t launch_ic_fwd(const Dims& d, const float2* bg, const float2* image, 
     cudaError_t e = cudaMemsetAsync(wfld, 0, d.wfld * sizeof(float2), s);
     if (e != cudaSuccess) return e;
   }
-  k_ic_fwd<<<grid1d((long long)d.nw * d.ny * d.nx), 256, 0, s>>>(d, bg, image, img_w, wfld);
+  k_ic_fwd<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, bg, image, img_w, wfld);
   count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_ic_adj(const Dims& d, const float2* bg, const float2* wfld, float2* image,
                           long long img_w, int add, cudaStream_t s) {
-  const int wsum = img_w == 0;
-  k_ic_adj<<<grid1d((long long)(wsum ? 1 : d.nw) * d.ny * d.nx), 256, 0, s>>>(d, bg, wfld, image, add, wsum);
+  k_ic_adj<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, bg, wfld, image, add, img_w == 0);
   count_launch();
   return cudaGetLastError();
 }
@@ -249,15 +294,14 @@ cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, con
                                const float2* r0, const float2* r1, long long mw, float2* dm0,
                                float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
                                int add, cudaStream_t s) {
-  const long long n = (long long)((adjoint && dm_w == 0) ? 1 : d.nw) * d.ny * d.nx;
-  k_lin_reflect<<<grid1d(n), 256, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3, dm_w, dr, add);
+  k_lin_reflect<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3, dm_w, dr, add);
   count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, float* img, int add,
                              cudaStream_t s) {
-  k_image_acc<<<grid1d((long long)d.ny * d.nx), 256, 0, s>>>(d, S, R, img, add);
+  k_image_acc<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, S, R, img, add);
   count_launch();
   return cudaGetLastError();
 }

@@ -11,7 +11,7 @@
 #include <mutex>
 #include <utility>
 
-#include "internal.h"
+#include "ops.cuh"
 
 namespace fwix {
 
@@ -37,87 +37,6 @@ cudaError_t ensure_smem(K kernel, size_t bytes) {
   return e;
 }
 
-// Born weight W_n = (-i w dz / 2) c_n s~^(-1/2-n), s~ = Re s^2 + i (Im s^2 - eps Re s^2),
-// read from the unpadded slice with edge replication into the pad
-// (scatter.cu:61-106 slow_scale, :155-195 scale_by_iw, :240-277 pad_fwd).
-// s~^(-1/2-n) = (1/sqrt(s~)) (1/s~)^n with the principal root.
-__device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, int y, int x) {
-  const int xs = min(x, a.d.nx - 1), ys = min(y, a.d.ny - 1);
-  const float2 s2 = a.slow[(long long)iw * a.slow_w + (long long)ys * a.d.nx + xs];
-  const float2 st = make_float2(s2.x, s2.y - a.eps_scat * s2.x);
-  float2 p = cinv(csqrt_ref(st));
-  if (n > 0) {
-    const float2 is = cinv(st);
-    for (int k = 0; k < n; ++k) p = cmul(p, is);
-  }
-  const float f = 0.5f * a.w[iw] * a.dz * a.coef[n];
-  return rot90<false>(cscale(p, f));
-}
-
-template <int W>
-__device__ __forceinline__ float2 row_weight(const SpecArgs& a, int t, int iw, int y, int x, float2 v) {
-  if (W == W_ONE) return v;
-  if (W == W_TAPER) return cscale(v, a.tapx[x] * a.tapy[y]);
-  if (W == W_MASK) {
-    const uint8_t l = a.lab[(long long)iw * a.lab_w + (long long)y * a.d.NX + x];
-    return (int)l == t ? v : make_float2(0.f, 0.f);
-  }
-  if (W == W_SCAT) return cmul(v, scat_weight(a, t, iw, y, x));
-  if (W == W_SCAT_CONJ) return cmul_conj(v, scat_weight(a, t, iw, y, x));
-  // W_IC
-  if (y < a.d.ny && x < a.d.nx)
-    return cmul(v, a.image[(long long)iw * a.img_w + (long long)y * a.d.nx + x]);
-  return make_float2(0.f, 0.f);
-}
-
-// Column multiplier for term t at (iw, ky[y], kx[x]), scaled by a.norm.
-template <int QM>
-__device__ __forceinline__ float2 qmult(const SpecArgs& a, int t, int iw, int x, int y) {
-  if (QM == Q_ONE) return make_float2(a.norm, 0.f);
-  const float kx = a.kx[x], ky = a.ky[y];
-  if (QM == Q_KPOW) {
-    if (t == 0) return make_float2(a.norm, 0.f);
-    const float k2 = kx * kx + ky * ky;
-    return make_float2(powf(sqrtf(k2) / a.w[iw], 2.0f * t) * a.norm, 0.f);
-  }
-  const float2 sr = a.sref[t * a.d.nw + iw];
-  const float w2 = a.w2[iw];
-  const float aa = w2 * sr.x - (kx * kx + ky * ky);
-  const float bb = w2 * (sr.y - a.eps * sr.x);
-  float re, im;
-  if (bb == 0.f) {
-    // c = sqrt(a^2) = |a| exactly, so the general branch reduces to one root.
-    if (aa >= 0.f) {
-      re = sqrtf(aa);
-      im = 0.f;
-    } else {
-      re = 0.f;
-      im = -sqrtf(-aa);
-    }
-  } else {
-    // Re = sqrt((c+a)/2), Im = -sqrt((c-a)/2) as phase_shift.cu:38-41, with the
-    // smaller of the two taken from Re |Im| = |b| / 2: the same values without
-    // the cancellation of c - a (or c + a) in float.
-    const float c = sqrtf(aa * aa + bb * bb);
-    if (aa >= 0.f) {
-      re = sqrtf((c + aa) * 0.5f);
-      im = -(fabsf(bb) * 0.5f) / re;
-    } else {
-      im = -sqrtf((c - aa) * 0.5f);
-      re = (fabsf(bb) * 0.5f) / -im;
-    }
-  }
-  if (QM == Q_PS_ADJ && bb > 0.f) re = -re;
-  if (QM == Q_PS_INV) {
-    im = -im;
-    if (bb > 0.f) re = -re;
-  }
-  const float att = (im == 0.f ? 1.f : expf(im * a.dz)) * a.norm;
-  float sn = 0.f, cs = 1.f;
-  if (re != 0.f) sincosf(re * a.dz, &sn, &cs);
-  return QM == Q_PS_FWD ? make_float2(att * cs, -att * sn) : make_float2(att * cs, att * sn);
-}
-
 // ---------------------------------------------------------------- row passes
 
 template <int PRE>
@@ -131,19 +50,20 @@ __global__ void __launch_bounds__(256) k_row_forward(const SpecArgs a, int nchun
   float2* lineB = lineA + NX;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.twx[i];
   __syncthreads();
-  const long long b = blockIdx.x / nchunk;
-  const int chunk = blockIdx.x - (int)(b * nchunk);
+  const long long bl = blockIdx.x / nchunk, b = a.b0 + bl;
+  const int chunk = blockIdx.x - (int)(bl * nchunk);
   const int iw = (int)(b % a.d.nw);
   const int nterm = (PRE == W_MASK || PRE == W_SCAT || PRE == W_SCAT_CONJ) ? a.nterm : 1;
   for (int y = chunk * nwarp + warp; y < a.d.NY; y += nchunk * nwarp) {
     const long long roff = (b * a.d.NY + y) * NX;
+    const long long loff = (bl * a.d.NY + y) * NX;
     for (int x = lane; x < NX; x += 32) lineIn[x] = a.in[roff + x];
     __syncwarp();
     for (int t = 0; t < nterm; ++t) {
       for (int x = lane; x < NX; x += 32) lineA[x] = row_weight<PRE>(a, t, iw, y, x, lineIn[x]);
       __syncwarp();
       const float2* r = warp_fft<false>(lineA, lineB, 1, a.px, tw, lane);
-      float2* o = a.t1 + (long long)t * a.d.wfld + roff;
+      float2* o = a.t1 + (long long)t * a.tstride + loff;
       for (int x = lane; x < NX; x += 32) o[x] = r[x];
       __syncwarp();
     }
@@ -161,12 +81,13 @@ __global__ void __launch_bounds__(256) k_row_inverse(const SpecArgs a, int nchun
   float2* lineB = lineA + NX;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.twx[i];
   __syncthreads();
-  const long long b = blockIdx.x / nchunk;
-  const int chunk = blockIdx.x - (int)(b * nchunk);
+  const long long bl = blockIdx.x / nchunk, b = a.b0 + bl;
+  const int chunk = blockIdx.x - (int)(bl * nchunk);
   const int iw = (int)(b % a.d.nw);
   const int nterm = (POST == W_MASK || POST == W_SCAT || POST == W_SCAT_CONJ) ? a.nterm : 1;
   for (int y = chunk * nwarp + warp; y < a.d.NY; y += nchunk * nwarp) {
     const long long roff = (b * a.d.NY + y) * NX;
+    const long long loff = (bl * a.d.NY + y) * NX;
     for (int x = lane; x < NX; x += 32) acc[x] = make_float2(0.f, 0.f);
     for (int t = 0; t < nterm; ++t) {
       if (POST == W_MASK) {
@@ -176,7 +97,7 @@ __global__ void __launch_bounds__(256) k_row_inverse(const SpecArgs a, int nchun
         for (int x = lane; x < NX; x += 32) hit |= ((int)lrow[x] == t);
         if (!__any_sync(0xffffffffu, hit)) continue;
       }
-      const float2* src = a.t2 + (long long)t * a.d.wfld + roff;
+      const float2* src = a.t2 + (long long)t * a.tstride + loff;
       for (int x = lane; x < NX; x += 32) lineA[x] = src[x];
       __syncwarp();
       const float2* r = warp_fft<true>(lineA, lineB, 1, a.px, tw, lane);
@@ -244,7 +165,7 @@ __global__ void __launch_bounds__(256) k_col_a(const SpecArgs a, int TX, int nxt
   for (int i = threadIdx.x; i < NY; i += blockDim.x) s.tw[i] = a.twy[i];
   const long long b = blockIdx.x / nxt;
   const int x0 = (int)(blockIdx.x - b * nxt) * TX;
-  const int iw = (int)(b % a.d.nw);
+  const int iw = (int)((a.b0 + b) % a.d.nw);
   tile_load(s.T0, TS, a.t1 + b * a.d.slice, NX, NY, x0, TX);
   __syncthreads();
   for (int c = warp; c < TX; c += nwarp) warp_fft<false>(s.T0 + c, s.T1 + c, TS, a.py, s.tw, lane);
@@ -261,7 +182,7 @@ __global__ void __launch_bounds__(256) k_col_a(const SpecArgs a, int TX, int nxt
       warp_fft<true>(G + c, H + c, TS, a.py, s.tw, lane);
     }
     __syncthreads();
-    tile_store(R, TS, a.t2 + (long long)t * a.d.wfld + b * a.d.slice, NX, NY, x0, TX, 0, 1.f);
+    tile_store(R, TS, a.t2 + (long long)t * a.tstride + b * a.d.slice, NX, NY, x0, TX, 0, 1.f);
     __syncthreads();
   }
 }
@@ -275,12 +196,12 @@ __global__ void __launch_bounds__(256) k_col_b(const SpecArgs a, int TX, int nxt
   for (int i = threadIdx.x; i < NY; i += blockDim.x) s.tw[i] = a.twy[i];
   const long long b = blockIdx.x / nxt;
   const int x0 = (int)(blockIdx.x - b * nxt) * TX;
-  const int iw = (int)(b % a.d.nw);
+  const int iw = (int)((a.b0 + b) % a.d.nw);
   float2* Z = s.T2;
   for (int i = threadIdx.x; i < NY * TS; i += blockDim.x) Z[i] = make_float2(0.f, 0.f);
   const bool odd = a.py.npass & 1;
   for (int t = 0; t < a.nterm; ++t) {
-    tile_load(s.T0, TS, a.t1 + (long long)t * a.d.wfld + b * a.d.slice, NX, NY, x0, TX);
+    tile_load(s.T0, TS, a.t1 + (long long)t * a.tstride + b * a.d.slice, NX, NY, x0, TX);
     __syncthreads();
     float2* F = odd ? s.T1 : s.T0;
     for (int c = warp; c < TX; c += nwarp) {
@@ -353,11 +274,11 @@ long long nblocks(long long slices, long long per) { return slices * per; }
 
 }  // namespace
 
-// ---------------------------------------------------------------- host launchers
+// ---------------------------------------------------------------- host launchers (generic lengths)
 
-cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
+cudaError_t generic_row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
   RowGeom g = row_geom(a.d);
-  const long long blocks = nblocks((long long)a.d.ns * a.d.nw, g.nchunk);
+  const long long blocks = nblocks(a.nb, g.nchunk);
   dim3 grid((unsigned)blocks), block(32 * g.nwarp);
   cudaError_t e = cudaSuccess;
 #define FWIX_ROWF(W)                                                      \
@@ -378,9 +299,9 @@ cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s) {
+cudaError_t generic_row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s) {
   RowGeom g = row_geom(a.d);
-  const long long blocks = nblocks((long long)a.d.ns * a.d.nw, g.nchunk);
+  const long long blocks = nblocks(a.nb, g.nchunk);
   dim3 grid((unsigned)blocks), block(32 * g.nwarp);
   cudaError_t e = cudaSuccess;
 #define FWIX_ROWI(W)                                                                  \
@@ -399,9 +320,9 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
+cudaError_t generic_col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
   ColGeom g = col_geom(a.d);
-  dim3 grid((unsigned)((long long)a.d.ns * a.d.nw * g.nxt)), block(32 * g.nwarp);
+  dim3 grid((unsigned)(a.nb * g.nxt)), block(32 * g.nwarp);
   cudaError_t e = cudaSuccess;
 #define FWIX_COLA(Q)                                                              \
   case Q:                                                                         \
@@ -420,9 +341,9 @@ cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s) {
+cudaError_t generic_col_type_b(const SpecArgs& a, int qmode, cudaStream_t s) {
   ColGeom g = col_geom(a.d);
-  dim3 grid((unsigned)((long long)a.d.ns * a.d.nw * g.nxt)), block(32 * g.nwarp);
+  dim3 grid((unsigned)(a.nb * g.nxt)), block(32 * g.nwarp);
   cudaError_t e = cudaSuccess;
 #define FWIX_COLB(Q)                                                              \
   case Q:                                                                         \
@@ -441,10 +362,10 @@ cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s) {
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add,
+cudaError_t generic_col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add,
                     float scale, cudaStream_t s) {
   ColGeom g = col_geom(a.d);
-  dim3 grid((unsigned)((long long)a.d.ns * a.d.nw * g.nxt)), block(32 * g.nwarp);
+  dim3 grid((unsigned)(a.nb * g.nxt)), block(32 * g.nwarp);
   cudaError_t e;
   if (inverse) {
     e = ensure_smem(k_col_fft<true>, g.smem);
@@ -516,6 +437,31 @@ cudaError_t launch_phase_shift(const SpecArgs& a, int mode, const float2* sref_w
     case Q_PS_INV: k_phase_shift<Q_PS_INV><<<g, 256, 0, s>>>(b, in, out, add); break;
     default: return cudaErrorInvalidValue;
   }
+  count_launch();
+  return cudaGetLastError();
+}
+
+// Forward phase factors x norm of one depth for every (ref, w, |kx|, |ky|): the
+// same arithmetic as the in-kernel evaluation (k depends on |index| only).
+__global__ void k_phase_table(const SpecArgs a, float2* dst) {
+  const long long n = (long long)a.nterm * a.d.nw * a.ptab_nx * a.ptab_ny;
+  SpecArgs b = a;
+  b.ptab = nullptr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int kyq = (int)(i % a.ptab_ny);
+    long long q = i / a.ptab_ny;
+    const int kxq = (int)(q % a.ptab_nx);
+    q /= a.ptab_nx;
+    const int iw = (int)(q % a.d.nw);
+    const int r = (int)(q / a.d.nw);
+    dst[i] = qmult<Q_PS_FWD>(b, r, iw, kxq, kyq);
+  }
+}
+
+cudaError_t launch_phase_table(const SpecArgs& a, float2* dst, cudaStream_t s) {
+  const long long n = (long long)a.nterm * a.d.nw * a.ptab_nx * a.ptab_ny;
+  k_phase_table<<<grid1d(n), 256, 0, s>>>(a, dst);
   count_launch();
   return cudaGetLastError();
 }

@@ -76,8 +76,25 @@ class Plan:
             L.check(self.lib.fwix_plan_set_workspace(self._h, _p(self._ws), need))
         return self._ws
 
-    def set_refs(self, sref, labels):
-        """sref [nz][nref][nw] complex; labels [nz][nw or 1][NY][NX] integer."""
+    def enable_phase_cache(self, max_fraction=0.4):
+        """Bind a phase-factor cache (each depth's factors computed once and reused)
+        when it fits in ``max_fraction`` of the device's free memory.  Returns
+        whether the cache is on."""
+        need = int(self.lib.fwix_plan_phase_cache_bytes(self._h))
+        free, _ = torch.cuda.mem_get_info(self.device)
+        if need == 0 or need > max_fraction * free:
+            return False
+        self._keep["pcache"] = torch.empty(need, dtype=torch.uint8, device=self.device)
+        L.check(self.lib.fwix_plan_set_phase_cache(self._h, _p(self._keep["pcache"]), need))
+        return True
+
+    def disable_phase_cache(self):
+        L.check(self.lib.fwix_plan_set_phase_cache(self._h, ctypes.c_void_p(0), 0))
+        self._keep.pop("pcache", None)
+
+    def set_refs(self, sref, labels, phase_cache=True):
+        """sref [nz][nref][nw] complex; labels [nz][nw or 1][NY][NX] integer.  With
+        ``phase_cache`` a phase-factor cache is bound when memory allows."""
         sref = _c64(sref, self.device)
         if tuple(sref.shape) != (self.nz, self.nref, self.nw):
             raise ValueError(f"sref shape {tuple(sref.shape)} != {(self.nz, self.nref, self.nw)}")
@@ -92,6 +109,8 @@ class Plan:
         zst = labels.shape[1] * self.NY * self.NX
         L.check(self.lib.fwix_plan_set_refs(self._h, _p(sref), _p(labels), zst, wst))
         self._keep["sref"], self._keep["labels"] = sref, labels
+        if phase_cache and "pcache" not in self._keep:
+            self.enable_phase_cache()
         return sref, labels
 
     def set_model(self, slow, den):

@@ -88,6 +88,8 @@ def test_select_and_taper():
 
 STEP_CASES = [
     dict(nx=24, ny=20, padx=0, pady=0, eps=0.0, complex_refs=False, labels_per_w=True),
+    dict(nx=192, ny=320, padx=0, pady=0, eps=0.0, complex_refs=False, labels_per_w=True),
+    dict(nx=380, ny=100, padx=4, pady=0, eps=0.01, complex_refs=True, labels_per_w=False),
     dict(nx=32, ny=28, padx=8, pady=4, eps=0.02, complex_refs=True, labels_per_w=False),
     dict(nx=100, ny=60, padx=28, pady=4, eps=0.0, complex_refs=False, labels_per_w=False),
 ]
@@ -141,11 +143,12 @@ def test_step_dot_product():
         assert dot_err(m, Am, d, Atd) < 1e-5
 
 
-@pytest.mark.parametrize("taylor,pad", [(0, 0), (1, 0), (2, 8)])
-def test_scatter(taylor, pad):
+@pytest.mark.parametrize("taylor,pad,nx,ny", [(0, 0, 24, 20), (1, 0, 24, 20), (2, 8, 24, 20), (1, 0, 128, 64),
+                                              (2, 8, 120, 60)])
+def test_scatter(taylor, pad, nx, ny):
     """Scatter forward / adjoint (Scatter.cpp:76-102), padded slowness replicated
     into the pad (scatter.cu:240-277)."""
-    g, rng, sref, labels, slow, den = make_case(nx=24, ny=20, nw=4, nz=3, padx=pad, pady=pad // 2, taylor=taylor)
+    g, rng, sref, labels, slow, den = make_case(nx=nx, ny=ny, nw=4, nz=3, padx=pad, pady=pad // 2, taylor=taylor)
     p = make_plan(g, 2, sref, labels, slow, den)
     x = wavefield(rng, 2, g)
     d0 = wavefield(rng, 2, g)
@@ -215,3 +218,48 @@ def test_injection_record():
         p.inject(tr, iz, d, to_dev(wf), adjoint=True)
         ref = wem.record(tr_o, wf, np.zeros_like(trace), iz)
         assert np.linalg.norm(to_host(d) - ref) <= TOL * max(np.linalg.norm(ref), 1.0)
+
+
+@pytest.mark.parametrize("chunk", ["1", "3"])
+def test_chunked_steps(monkeypatch, chunk):
+    """Steps and the Born scatter run in chunks of slices whose intermediates stay in
+    L2; forcing small chunks must not change the result."""
+    monkeypatch.setenv("FWIX_CHUNK_SLICES", chunk)
+    g, rng, sref, labels, slow, den = make_case(nx=64, ny=40, nw=4, nz=2, nref=3, padx=0, pady=0)
+    lab = oracle_labels(labels, g)
+    for kind in ("pspi", "nsps"):
+        p = make_plan(g, 2, sref, labels, slow, den, step=kind)
+        x = wavefield(rng, 2, g)
+        fwd = wem.pspi_forward if kind == "pspi" else wem.nsps_forward
+        y = to_host(p.step(1, to_dev(x), torch.empty(p.wshape, dtype=torch.complex64, device="cuda")))
+        assert rel(y, fwd(g, sref[1], lab[1], x)) < TOL
+        y = to_host(p.scatter(1, to_dev(x), torch.empty(p.wshape, dtype=torch.complex64, device="cuda"), adjoint=True))
+        assert rel(y, wem.scatter_adjoint(g, slow[1], x)) < TOL
+        y = to_host(p.fft2d(to_dev(x), torch.empty(p.wshape, dtype=torch.complex64, device="cuda"), inverse=True))
+        assert rel(y, wem.ifft2(x)) < TOL
+
+
+@pytest.mark.parametrize("complex_refs,eps", [(False, 0.0), (True, 0.03)])
+def test_phase_cache_matches_inline(complex_refs, eps):
+    """Steps read the cached factors when a phase cache is bound; results equal
+    the in-kernel evaluation, including the adjoint's b > 0 branch."""
+    g, rng, sref, labels, _, _ = make_case(nx=64, ny=64, nw=4, nz=3, nref=3, eps=eps, complex_refs=complex_refs)
+    if complex_refs:
+        sref = sref.copy()
+        sref[:, 1, :] += 1j * abs(sref[:, 1, :]) * 0.3  # Im s2 > eps Re s2: b > 0 for this reference
+    x = wavefield(rng, 2, g)
+    outs = {}
+    for cached in (False, True):
+        for kind in ("pspi", "nsps"):
+            p = make_plan(g, 2, sref, labels, step=kind)
+            if not cached:
+                p.disable_phase_cache()
+            else:
+                assert "pcache" in p._keep
+            for d in (0, 1, 2):
+                for iz in (2, 0, 2):
+                    outs[(cached, kind, d, iz)] = to_host(p.step(iz, to_dev(x), torch.empty(p.wshape, dtype=torch.complex64,
+                                                                                            device="cuda"), direction=d))
+    for k, v in outs.items():
+        if k[0]:
+            assert rel(v, outs[(False,) + k[1:]]) < 1e-6, k

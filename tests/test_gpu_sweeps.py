@@ -30,8 +30,8 @@ def test_down_up(kind):
         assert rel(y, fn(st, g.nz, x)) < TOL
 
 
-def _acq_case(kind="pspi", taper=3, pad=4, nz=7):
-    g, rng, sref, labels, slow, den = make_case(nx=32, ny=24, nw=4, nz=nz, nref=3, padx=pad, pady=pad,
+def _acq_case(kind="pspi", taper=3, pad=4, nz=7, nx=32, ny=24):
+    g, rng, sref, labels, slow, den = make_case(nx=nx, ny=ny, nw=4, nz=nz, nref=3, padx=pad, pady=pad,
                                                 taperx=taper, tapery=taper)
     slow = slow.copy()
     slow[nz - 3:] *= 1.8  # reflector
@@ -48,9 +48,9 @@ def _acq_case(kind="pspi", taper=3, pad=4, nz=7):
     return g, rng, st, acq, p, src, rec, wav, slow, den
 
 
-@pytest.mark.parametrize("kind", ["pspi", "nsps"])
-def test_propagate(kind):
-    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind)
+@pytest.mark.parametrize("kind,nx,ny,pad", [("pspi", 32, 24, 4), ("nsps", 32, 24, 4), ("pspi", 96, 60, 4)])
+def test_propagate(kind, nx, ny, pad):
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind, nx=nx, ny=ny, pad=pad)
     data, bgd, bgu = wem.propagate(g, st, acq, slow, den, wav)
     bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
     bu = torch.empty_like(bd)
@@ -75,9 +75,12 @@ def test_migrate():
     assert rel(out.cpu().numpy(), img) < TOL
 
 
-@pytest.mark.parametrize("kind,taper", [("pspi", 3), ("nsps", 0)])
-def test_born(kind, taper):
-    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind, taper=taper)
+@pytest.mark.parametrize("kind,taper,nx,ny,pad", [("pspi", 3, 32, 24, 4), ("nsps", 0, 32, 24, 4),
+                                                 ("pspi", 3, 64, 64, 0), ("nsps", 2, 60, 44, 4)])
+def test_born(kind, taper, nx, ny, pad):
+    """Born forward / adjoint; 64 x 64 exercises the register-resident passes,
+    the other sizes the generic ones."""
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind, taper=taper, nx=nx, ny=ny, pad=pad)
     data, bgd, bgu = wem.propagate(g, st, acq, slow, den, wav)
     bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
     bu = torch.empty_like(bd)
