@@ -55,6 +55,43 @@ struct Order {
 
 __device__ __forceinline__ int swz(int p) { return p ^ ((p >> 3) & 15); }
 
+// Twiddles in shared memory, one table per stage and order: stage S (span Ns,
+// radix R) reads W_N^(k r N / (Ns R)) for k = j mod Ns and r = 1..R-1 at
+// (r - 1) Ns + k, so the lanes of a warp read consecutive entries (no bank
+// conflicts).  The forward-order tables come first, then the reversed-order
+// (inverse transform) ones; together they hold about 2 N values.
+template <class P, bool REV>
+struct TwLayout {
+  using O = Order<P, REV>;
+  __host__ __device__ static constexpr int count(int s) { return O::span(s) > 1 ? (O::radix(s) - 1) * O::span(s) : 0; }
+  __host__ __device__ static constexpr int offset(int s) { return s == 0 ? 0 : offset(s - 1) + count(s - 1); }
+  __host__ __device__ static constexpr int total() { return offset(P::NS); }
+};
+template <class P>
+constexpr int tw_size() {
+  return TwLayout<P, false>::total() + TwLayout<P, true>::total();
+}
+
+template <class P, bool REV, int S>
+__device__ __forceinline__ void fill_stage_tw(float2* dst, const float2* __restrict__ tw) {
+  if constexpr (S < P::NS) {
+    using O = Order<P, REV>;
+    constexpr int Ns = O::span(S), R = O::radix(S), cnt = TwLayout<P, REV>::count(S);
+    constexpr int off = TwLayout<P, REV>::offset(S), tstep = P::N / (Ns * R);
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const int r = i / Ns + 1, k = i - (r - 1) * Ns;
+      dst[off + i] = tw[k * r * tstep];
+    }
+    fill_stage_tw<P, REV, S + 1>(dst, tw);
+  }
+}
+// Fills both orders' tables from the plain table tw[m] = exp(-2 pi i m / N).
+template <class P>
+__device__ __forceinline__ void load_stage_tw(float2* dst, const float2* __restrict__ tw) {
+  fill_stage_tw<P, false, 0>(dst, tw);
+  fill_stage_tw<P, true, 0>(dst + TwLayout<P, false>::total(), tw);
+}
+
 template <class P, int R>
 __device__ __forceinline__ int lpos(int t, int e) {
   return t + P::T * (e / R) + (e % R) * (P::N / R);
@@ -74,7 +111,6 @@ __device__ __forceinline__ void stages(float2 (&v)[P::E], int t, const float2* _
   constexpr int R = O::radix(S);
   constexpr int Ns = O::span(S);
   constexpr int B = P::E / R;
-  constexpr int tstep = P::N / (Ns * R);
 #pragma unroll
   for (int b = 0; b < B; ++b) {
     float2 u[R];
@@ -85,7 +121,7 @@ __device__ __forceinline__ void stages(float2 (&v)[P::E], int t, const float2* _
       const int k = j % Ns;
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const float2 w = tw[k * r * tstep];
+        const float2 w = tw[TwLayout<P, REV>::offset(S) + (r - 1) * Ns + k];
         u[r] = INV ? cmul_conj(u[r], w) : cmul(u[r], w);
       }
     }
@@ -116,11 +152,7 @@ __device__ __forceinline__ void fft_fwd(float2 (&v)[P::E], int t, const float2* 
 }
 template <class P>
 __device__ __forceinline__ void fft_inv(float2 (&v)[P::E], int t, const float2* tw, float2* line) {
-  stages<P, true, true, 0>(v, t, tw, line);
-}
-
-__device__ __forceinline__ void load_table(float2* dst, const float2* __restrict__ src, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  stages<P, true, true, 0>(v, t, tw + TwLayout<P, false>::total(), line);
 }
 
 // Asynchronous 8-byte global -> shared copy (zero-filled when !valid).
@@ -138,7 +170,7 @@ template <class P>
 struct RowGeo {
   static constexpr int LINE = P::N + (P::T < 32 ? 8 : 0);  // shared-memory stride between lines
   static constexpr int ROWS = kWarps * P::G;                // rows per CTA
-  static size_t smem() { return ((size_t)kWarps * P::G * LINE + P::N) * sizeof(float2); }
+  static size_t smem() { return ((size_t)kWarps * P::G * LINE + tw_size<P>()) * sizeof(float2); }
 };
 
 // Per-thread view of a row pass: which row, which lane of the line, its smem line.
@@ -170,7 +202,7 @@ template <class P, int PRE>
 __global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int nchunk) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
-  load_table(c.tw, a.twx, P::N);
+  load_stage_tw<P>(c.tw, a.twx);
   __syncthreads();
   float2 raw[P::E];
   const float2* src = a.in + (c.b * a.d.NY + (c.live ? c.y : 0)) * P::N;
@@ -198,7 +230,7 @@ template <class P, int POST>
 __global__ void __launch_bounds__(kWarps * 32) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
-  load_table(c.tw, a.twx, P::N);
+  load_stage_tw<P>(c.tw, a.twx);
   __syncthreads();
   const int nterm = (POST == W_MASK || POST == W_SCAT) ? a.nterm : 1;
   float2 acc[P::E];
@@ -271,12 +303,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_inv(const SpecArgs a, int n
 template <class P>
 struct ColGeo {
   static constexpr int LX = kWarps * P::G;  // columns per CTA
-  static constexpr int LINE = P::N + 1;     // tile stride between columns
-  static size_t smem() { return ((size_t)LX * LINE + P::N) * sizeof(float2); }
+  // Tile stride between columns: with 8 columns a warp's tile copy covers 4
+  // rows x 8 columns, conflict-free for a stride of 2 (mod 16) samples; with 16
+  // or 32 columns an odd stride is, and 5 also suits the line exchanges.
+  static constexpr int LINE = P::N + (LX == 8 ? 2 : 5);
+  static size_t smem() { return ((size_t)LX * LINE + tw_size<P>()) * sizeof(float2); }
   // Resident CTAs per SM the register allocation is held to: three for plans
   // of at most 8 samples per lane (about 85 registers), else what fits.
   static constexpr int kMinBlocks = P::E <= 8 ? 3 : 1;
-  static size_t smem2() { return ((size_t)2 * LX * LINE + P::N) * sizeof(float2); }  // tile, tw, tile
+  static size_t smem2() { return ((size_t)2 * LX * LINE + tw_size<P>()) * sizeof(float2); }  // tile, tw, tile
 };
 
 template <class P>
@@ -334,7 +369,7 @@ template <class P, int QM>
 __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_a(const SpecArgs a, int nxt) {
   extern __shared__ float2 smem[];
   ColCtx<P> c(a, smem, nxt);
-  load_table(c.tw, a.twy, P::N);
+  load_stage_tw<P>(c.tw, a.twy);
   cols_to_tile<P>(c.tile, a.t1, a, c.b, c.x0);
   __syncthreads();
   float2 psi[P::E];
@@ -383,9 +418,9 @@ template <class P, int QM>
 __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_b(const SpecArgs a, int nxt) {
   extern __shared__ float2 smem[];
   ColCtx<P> c(a, smem, nxt);
-  float2* tiles[2] = {c.tile, c.tw + P::N};
+  float2* tiles[2] = {c.tile, c.tw + tw_size<P>()};
   const long long lineoff = (long long)c.col * ColGeo<P>::LINE;
-  load_table(c.tw, a.twy, P::N);
+  load_stage_tw<P>(c.tw, a.twy);
   const int xq = c.x < a.d.NX ? c.x : 0;
   float2 acc[P::E];
 #pragma unroll
@@ -426,7 +461,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_col_fft(const SpecArgs a, int n
                                                           int add, float scale) {
   extern __shared__ float2 smem[];
   ColCtx<P> c(a, smem, nxt);
-  load_table(c.tw, a.twy, P::N);
+  load_stage_tw<P>(c.tw, a.twy);
   cols_to_tile<P>(c.tile, in, a, c.b, c.x0);
   __syncthreads();
   float2 v[P::E];

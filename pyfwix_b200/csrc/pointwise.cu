@@ -221,40 +221,63 @@ __global__ void k_axpy(long long n, const float2* __restrict__ x, float2* __rest
     y[i] = cadd(y[i], x[i]);
 }
 
+// Injection and recording move data between traces [trace][w] (frequency
+// fastest) and the wavefield [shot][w][y][x] (x fastest).  A block takes 32
+// listed cells (or receivers) x 32 frequencies and transposes through shared
+// memory, so that both sides are touched in contiguous runs.  Cells within a
+// level's list are distinct, and so are receivers, so no two threads write
+// the same element.
+
 // wfld[shot, w, y, x] += sum_k weight_k * traces[trace_k, w] for each listed cell.
-__global__ void k_inject(Dims d, InjectLevel L, const float2* __restrict__ traces, float2* wfld) {
-  const long long n = (long long)L.ncell * d.nw;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int e = (int)(i % L.ncell);
-    const int iw = (int)(i / L.ncell);
+__global__ void __launch_bounds__(256) k_inject(Dims d, InjectLevel L, const float2* __restrict__ traces,
+                                                float2* wfld) {
+  __shared__ float2 tile[32][33];
+  const int e0 = blockIdx.x * 32, w0 = blockIdx.y * 32;
+  const int iw = w0 + threadIdx.x;
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int e = e0 + k;
     float2 acc = make_float2(0.f, 0.f);
-    for (int k = L.start[e]; k < L.start[e + 1]; ++k)
-      acc = cadd(acc, cscale(traces[(long long)L.trace[k] * d.nw + iw], L.weight[k]));
-    const long long cell = L.cell[e];
-    const long long shot = cell / d.slice, yx = cell - shot * d.slice;
-    const long long k = (shot * d.nw + iw) * d.slice + yx;
-    wfld[k] = cadd(wfld[k], acc);
+    if (e < L.ncell && iw < d.nw)
+      for (int j = L.start[e]; j < L.start[e + 1]; ++j)
+        acc = cadd(acc, cscale(traces[(long long)L.trace[j] * d.nw + iw], L.weight[j]));
+    tile[k][threadIdx.x] = acc;
+  }
+  __syncthreads();
+  const int e = e0 + threadIdx.x;
+  if (e >= L.ncell) return;
+  const long long cell = L.cell[e];
+  const long long shot = cell / d.slice, yx = cell - shot * d.slice;
+  for (int f = threadIdx.y; f < 32 && w0 + f < d.nw; f += 8) {
+    const long long k = (shot * d.nw + w0 + f) * d.slice + yx;
+    wfld[k] = cadd(wfld[k], tile[threadIdx.x][f]);
   }
 }
 
 // traces[t, w] += sum of the four corner weights times the wavefield.
-__global__ void k_record(Dims d, InjectLevel L, const float2* __restrict__ wfld, float2* traces) {
-  const long long n = (long long)L.ntr * d.nw;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int e = (int)(i % L.ntr);
-    const int iw = (int)(i / L.ntr);
+__global__ void __launch_bounds__(256) k_record(Dims d, InjectLevel L, const float2* __restrict__ wfld,
+                                                float2* traces) {
+  __shared__ float2 tile[32][33];
+  const int e0 = blockIdx.x * 32, w0 = blockIdx.y * 32;
+  const int e = e0 + threadIdx.x;
+  if (e < L.ntr) {
     const long long cell = L.rcell[e];
     const long long shot = cell / d.slice, yx = cell - shot * d.slice;
-    const float2* p = wfld + (shot * d.nw + iw) * d.slice + yx;
     const float4 w = L.rw[e];
-    float2 v = cscale(p[0], w.x);
-    v = cadd(v, cscale(p[1], w.y));
-    v = cadd(v, cscale(p[d.NX], w.z));
-    v = cadd(v, cscale(p[d.NX + 1], w.w));
-    const long long t = (long long)L.rtrace[e] * d.nw + iw;
-    traces[t] = cadd(traces[t], v);
+    for (int f = threadIdx.y; f < 32 && w0 + f < d.nw; f += 8) {
+      const float2* p = wfld + (shot * d.nw + w0 + f) * d.slice + yx;
+      float2 v = cscale(p[0], w.x);
+      v = cadd(v, cscale(p[1], w.y));
+      v = cadd(v, cscale(p[d.NX], w.z));
+      v = cadd(v, cscale(p[d.NX + 1], w.w));
+      tile[f][threadIdx.x] = v;
+    }
+  }
+  __syncthreads();
+  const int iw = w0 + threadIdx.x;
+  if (iw >= d.nw) return;
+  for (int k = threadIdx.y; k < 32 && e0 + k < L.ntr; k += 8) {
+    const long long t = (long long)L.rtrace[e0 + k] * d.nw + iw;
+    traces[t] = cadd(traces[t], tile[threadIdx.x][k]);
   }
 }
 
@@ -315,7 +338,8 @@ cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s)
 cudaError_t launch_inject(const Dims& d, const InjectLevel& L, const float2* traces, float2* wfld,
                           cudaStream_t s) {
   if (L.ncell == 0) return cudaSuccess;
-  k_inject<<<grid1d((long long)L.ncell * d.nw), 256, 0, s>>>(d, L, traces, wfld);
+  const dim3 grid((unsigned)((L.ncell + 31) / 32), (unsigned)((d.nw + 31) / 32));
+  k_inject<<<grid, dim3(32, 8), 0, s>>>(d, L, traces, wfld);
   count_launch();
   return cudaGetLastError();
 }
@@ -323,7 +347,8 @@ cudaError_t launch_inject(const Dims& d, const InjectLevel& L, const float2* tra
 cudaError_t launch_record(const Dims& d, const InjectLevel& L, const float2* wfld, float2* traces,
                           cudaStream_t s) {
   if (L.ntr == 0) return cudaSuccess;
-  k_record<<<grid1d((long long)L.ntr * d.nw), 256, 0, s>>>(d, L, wfld, traces);
+  const dim3 grid((unsigned)((L.ntr + 31) / 32), (unsigned)((d.nw + 31) / 32));
+  k_record<<<grid, dim3(32, 8), 0, s>>>(d, L, wfld, traces);
   count_launch();
   return cudaGetLastError();
 }

@@ -1,0 +1,233 @@
+"""The drop-in operator surface (``fwix/CudaWEM.py`` / ``fwix/CudaOperator.py``
+class names and ``forward/adjoint(add, model, data)`` calls) against the FP64
+oracle, with operands passed the ways the reference's callers pass them:
+vectors with hypercubes, host numpy arrays (results written back in place) and
+device tensors.  Mirrors the reference's operator tests
+(``propagator/tests/*_test.cpp``: forward / adjoint / dot product per operator)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import wem
+from pyfwix_b200 import CudaWEM, vectors
+from pyfwix_b200.CudaOperator import cuFFT2d
+from tests.conftest import cdot, crandn, dot_err
+from tests.gpu_helpers import make_case, oracle_labels, rel
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+TOL_SWEEP = 1e-4
+
+
+def _axes(g, nz=None):
+    return vectors.Hypercube([vectors.Axis(g.nx, g.ox, g.dx), vectors.Axis(g.ny, g.oy, g.dy),
+                              vectors.Axis(g.nw, g.ow, g.dw), vectors.Axis(nz or g.nz, g.oz, g.dz)])
+
+
+def _wf_hyper(g, ns):
+    return vectors.Hypercube([vectors.Axis(g.NX, g.ox, g.dx), vectors.Axis(g.NY, g.oy, g.dy),
+                              vectors.Axis(g.nw, g.ow, g.dw), vectors.Axis(ns)])
+
+
+def _par(g, **kw):
+    p = dict(nref=g.nref, padx=g.padx, pady=g.pady, eps=g.eps, taperx=g.taperx, tapery=g.tapery,
+             eps_scat=g.eps_scat, taylor=g.taylor)
+    p.update(kw)
+    return p
+
+
+def test_cufft2d_host_and_device_operands():
+    rng = np.random.default_rng(3)
+    x = crandn(rng, (3, 2, 40, 48)).astype(np.complex64)
+    y = np.zeros_like(x)
+    op = cuFFT2d(x, y)
+    op.forward(False, x, y)                         # host numpy, written back in place
+    assert rel(y, wem.fft2(x.astype(np.complex128))) < TOL
+    xd = torch.as_tensor(x).cuda()
+    yd = torch.as_tensor(y).cuda()
+    op.adjoint(True, xd, yd)                        # device tensors, add
+    assert rel(xd.cpu().numpy(), x + wem.ifft2(y.astype(np.complex128))) < TOL
+
+
+def test_phase_shift_operator():
+    g, rng, sref, _, _, _ = make_case(nx=32, ny=24, nw=4, nz=1, eps=0.02, complex_refs=True)
+    m = vectors.Vector(_wf_hyper(g, 2), crandn(rng, (2, g.nw, g.NY, g.NX)), device="cuda")
+    d = m.cloneSpace()
+    op = CudaWEM.PhaseShift(m, d, g.dz, g.eps)
+    op.set_slow(sref[0, 1])
+    op.forward(False, m, d)
+    fac = wem.phase_forward_factor(g.w2(), g.kx(), g.ky(), sref[0, 1], g.dz, g.eps)
+    x = m.arr.cpu().numpy()
+    assert rel(d.arr.cpu().numpy(), x * fac[None]) < TOL
+    y = crandn(rng, x.shape)
+    dd = vectors.Vector(_wf_hyper(g, 2), y, device="cuda")
+    mm = m.cloneSpace()
+    op.adjoint(False, mm, dd)
+    adj = wem.phase_adjoint_factor(g.w2(), g.kx(), g.ky(), sref[0, 1], g.dz, g.eps)
+    assert rel(mm.arr.cpu().numpy(), y * adj[None]) < TOL
+
+
+def _slow_model(g, rng, per_w=True):
+    s0 = (1 / 1800.0) ** 2
+    nwm = g.nw if per_w else 1
+    s2 = s0 * (1 + 0.3 * rng.random((g.nz, 1, g.ny, g.nx))) * np.ones((1, nwm, 1, 1))
+    return s2.astype(np.complex64)
+
+
+@pytest.mark.parametrize("cls,kind", [(CudaWEM.PSPI, "pspi"), (CudaWEM.NSPS, "nsps")])
+def test_one_step_operators(cls, kind):
+    g, rng, _, _, _, _ = make_case(nx=36, ny=30, nw=4, nz=3, nref=3, padx=4, pady=2)
+    s2 = vectors.Vector(_axes(g), _slow_model(g, rng), device="cuda")
+    m = vectors.Vector(_wf_hyper(g, 2), crandn(rng, (2, g.nw, g.NY, g.NX)), device="cuda")
+    d = m.cloneSpace()
+    op = cls(m, d, s2, _par(g))
+    sref = op.plan._keep["sref"].cpu().numpy().astype(np.complex128)
+    lab = oracle_labels(op.plan._keep["labels"].cpu().numpy(), g)
+    for iz in range(g.nz):
+        op.set_depth(iz)
+        op.forward(False, m, d)
+        x = m.arr.cpu().numpy().astype(np.complex128)
+        ref = (wem.pspi_forward(g, sref[iz], lab[iz], x, taper=True) if kind == "pspi"
+               else wem.nsps_forward(g, sref[iz], lab[iz], x))
+        assert rel(d.arr.cpu().numpy(), ref) < TOL
+        # add-version adjoint (PSPI: no taper, as in the reference)
+        y = crandn(rng, x.shape)
+        dv = vectors.Vector(_wf_hyper(g, 2), y, device="cuda")
+        mv = m.cloneSpace()
+        op.adjoint(False, mv, dv)
+        ref = (wem.pspi_adjoint(g, sref[iz], lab[iz], y, taper=False) if kind == "pspi"
+               else wem.nsps_adjoint(g, sref[iz], lab[iz], y))
+        assert rel(mv.arr.cpu().numpy(), ref) < TOL
+
+
+def test_injection_operator():
+    g, rng, _, _, _, _ = make_case(nx=32, ny=24, nw=3, nz=6, padx=4, pady=4)
+    cx = rng.uniform(0, 330, 12).astype(np.float32)
+    cy = rng.uniform(0, 300, 12).astype(np.float32)
+    cz = rng.uniform(0, 35, 12).astype(np.float32)
+    ids = rng.integers(0, 2, 12).astype(np.int32)
+    tr = crandn(rng, (12, g.nw)).astype(np.complex64)
+    wf = np.zeros((2, g.nw, g.NY, g.NX), np.complex64)
+    wfv = vectors.Vector(_wf_hyper(g, 2), wf)
+    op = CudaWEM.Injection(tr, wfv, g.oz, g.dz, cx, cy, cz, ids)
+    otr = wem.make_traces(cx, cy, cz, ids, g.ox, g.oy, g.dx, g.dy, g.oz, g.dz, g.NX, g.NY)
+    for iz in range(4):
+        op.set_depth(iz)
+        op.forward(False, tr, wfv)
+        ref = wem.inject(otr, tr.astype(np.complex128), np.zeros(wf.shape, np.complex128), iz)
+        assert rel(wfv.arr.numpy(), ref) < TOL
+        w = crandn(rng, wf.shape)
+        got = np.zeros_like(tr)
+        op.adjoint(False, got, w)
+        refr = wem.record(otr, w, np.zeros(tr.shape, np.complex128), iz)
+        if np.linalg.norm(refr) > 0:
+            assert rel(got, refr) < TOL
+
+
+@pytest.mark.parametrize("cls,fwd,adj", [(CudaWEM.Downward, wem.downward, wem.downward_adjoint),
+                                         (CudaWEM.Upward, wem.upward, wem.upward_adjoint)])
+def test_sweep_operators(cls, fwd, adj):
+    g, rng, _, _, _, _ = make_case(nx=32, ny=24, nw=3, nz=5, nref=3, padx=4, pady=4)
+    s2 = _slow_model(g, rng)
+    x = crandn(rng, (2, g.nw, g.NY, g.NX)).astype(np.complex64)
+    out = np.zeros_like(x)
+    par = dict(_par(g), ox=g.ox, dx=g.dx, oy=g.oy, dy=g.dy, oz=g.oz, dz=g.dz, ow=g.ow, dw=g.dw)
+    op = cls(x, out, s2, par)                               # bare arrays, axes from par
+    sref = op.plan._keep["sref"].cpu().numpy().astype(np.complex128)
+    lab = oracle_labels(op.plan._keep["labels"].cpu().numpy(), g)
+    st = wem.Stepper(g, sref, lab, "pspi")
+    op.forward(False, x, out)
+    assert rel(out, fwd(st, g.nz, x.astype(np.complex128))) < TOL_SWEEP
+    w = torch.as_tensor(x).cuda()
+    op.adjoint(w)                                           # one-argument in-place form
+    assert rel(w.cpu().numpy(), adj(st, g.nz, x.astype(np.complex128))) < TOL_SWEEP
+
+
+def _acq(g, rng):
+    geom = dict(sx=np.array([80.0, 200.0], np.float32), sy=np.array([96.0, 120.0], np.float32),
+                sz=np.array([0.0, 5.0], np.float32), s_ids=np.array([7, 3], np.int32),
+                rx=np.linspace(0, 300, 16).astype(np.float32), ry=np.full(16, 100.0, np.float32),
+                rz=np.zeros(16, np.float32), r_ids=np.array([7, 3] * 8, np.int32))
+    wav = crandn(rng, (2, g.nw)).astype(np.complex64)
+    return geom, wav
+
+
+def _born_setup(kind="pspi"):
+    g, rng, _, _, _, _ = make_case(nx=32, ny=24, nw=3, nz=6, nref=3, padx=4, pady=4, taperx=0, tapery=0)
+    s2 = _slow_model(g, rng)
+    s2[g.nz - 2:] *= 1.6
+    den = (1.0 + 0.2 * rng.random(s2.shape)).astype(np.complex64)
+    model = vectors.SuperVector(vectors.Vector(_axes(g), s2), vectors.Vector(_axes(g), den))
+    geom, wav = _acq(g, rng)
+    data = np.zeros((16, g.nw), np.complex64)
+    prop = CudaWEM.Propagator(model, data, wav, _par(g, step=kind), geom)
+    return g, rng, s2, den, model, geom, wav, data, prop
+
+
+def _oracle_of(prop, g, kind="pspi"):
+    sref = prop.plan._keep["sref"].cpu().numpy().astype(np.complex128)
+    lab = oracle_labels(prop.plan._keep["labels"].cpu().numpy(), g)
+    return wem.Stepper(g, sref, lab, kind)
+
+
+@pytest.mark.parametrize("kind", ["pspi", "nsps"])
+def test_propagator_and_born(kind):
+    g, rng, s2, den, model, geom, wav, data, prop = _born_setup(kind)
+    prop.forward(False, model, data)
+    st = _oracle_of(prop, g, kind)
+    acq = wem.make_acquisition(g, geom)
+    ref, bgd, bgu = wem.propagate(g, st, acq, s2.astype(np.complex128), den.astype(np.complex128),
+                                  wav.astype(np.complex128))
+    assert rel(data, ref) < TOL_SWEEP
+    dm = vectors.SuperVector(vectors.Vector(_axes(g), crandn(rng, s2.shape) * 1e-3),
+                             vectors.Vector(_axes(g), crandn(rng, s2.shape) * 1e-2))
+    born = CudaWEM.ExtendedBorn(dm, data, model, prop)
+    d1 = np.zeros_like(data)
+    born.forward(False, dm, d1)
+    refb = wem.born_forward(g, st, acq, s2.astype(np.complex128), den.astype(np.complex128), bgd, bgu,
+                            dm[0].arr.numpy().astype(np.complex128), dm[1].arr.numpy().astype(np.complex128))
+    assert rel(d1, refb) < TOL_SWEEP
+    r = crandn(rng, data.shape).astype(np.complex64)
+    g_ = dm.cloneSpace()
+    born.adjoint(False, g_, r)
+    gs, gr = wem.born_adjoint(g, st, acq, s2.astype(np.complex128), den.astype(np.complex128), bgd, bgu,
+                              r.astype(np.complex128))
+    assert rel(g_[0].arr.numpy(), gs) < TOL_SWEEP
+    assert rel(g_[1].arr.numpy(), gr) < TOL_SWEEP
+    # dot product through the surface: <B dm, r> vs <dm, B^T r>
+    lhs = cdot(r, d1)
+    rhs = cdot(g_[0].arr.numpy(), dm[0].arr.numpy()) + cdot(g_[1].arr.numpy(), dm[1].arr.numpy())
+    assert abs(lhs / rhs - 1) < 1e-4
+
+
+def test_born_adjoint_add_and_workers_flow():
+    """The call sequence of ``fwix/workers.py:62-76``: forward model, residual,
+    objective, Born adjoint into a zeroed gradient."""
+    g, rng, s2, den, model, geom, wav, data, prop = _born_setup()
+    d_obs = crandn(rng, data.shape).astype(np.complex64) * 1e-3
+    res = np.zeros_like(data)
+    grad = model.cloneSpace()
+    born = CudaWEM.ExtendedBorn(grad, res, model, prop)
+    prop.forward(False, model, res)
+    res -= d_obs
+    obj = float(np.real(np.vdot(res, res)))
+    assert obj > 0
+    born.adjoint(False, grad, res)
+    g1 = [v.arr.clone() for v in grad.vecs]
+    born.adjoint(True, grad, res)                             # add doubles it
+    for a, b in zip(g1, grad.vecs):
+        assert rel(b.arr.numpy(), 2 * a.numpy()) < 1e-6
+
+
+def test_refsampler_surface():
+    g, rng, _, _, _, _ = make_case(nx=32, ny=24, nw=3, nz=4, nref=3, padx=4, pady=2)
+    s2 = _slow_model(g, rng)
+    rs = CudaWEM.RefSampler(vectors.Vector(_axes(g), s2), dict(nref=3, padx=4, pady=2))
+    assert rs.get_ref_slow(2, 1).shape == (g.nw,)
+    lab = rs.get_ref_labels(2)
+    assert lab.shape == (g.nw, g.NY, g.NX) and lab.min() >= 0 and lab.max() < 3
+    # labels pick the nearest reference
+    refs = np.stack([rs.get_ref_slow(2, r) for r in range(3)])
+    near = np.argmin(np.abs(s2[2][None].astype(np.complex128) - refs[:, :, None, None]), axis=0)
+    assert np.mean(lab[:, :g.ny, :g.nx] == near) > 0.999

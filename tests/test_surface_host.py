@@ -1,0 +1,69 @@
+"""Host-side logic of the operator surface that needs no GPU: hypercube and
+vector conventions (SEP axis order, conjugating dot product), shot-id
+remapping and its error (``propagator/src/Propagator.cpp:28-59``), the
+required padding keys (``propagator/src/Propagator.cpp:63-71``) and axes taken
+from ``par`` for bare arrays."""
+import numpy as np
+import pytest
+import torch
+
+from pyfwix_b200 import CudaWEM, vectors
+
+
+def test_hypercube_axis_order():
+    h = vectors.Hypercube([vectors.Axis(8, 0, 10), vectors.Axis(6, 5, 12), vectors.Axis(3, 2, 0.5),
+                           vectors.Axis(4, 0, 10)])
+    assert h.shape == (4, 3, 6, 8)
+    assert h.getAxis(1).n == 8 and h.getAxis(4).n == 4
+    assert h.getN123() == 4 * 3 * 6 * 8 and h.getNdim() == 4
+    assert h.checkSame(vectors.Hypercube(h.getAxes()))
+    assert not h.checkSame(vectors.Hypercube.from_shape(h.shape))
+
+
+def test_vector_ops():
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal((3, 4)) + 1j * rng.standard_normal((3, 4))
+    b = rng.standard_normal((3, 4)) + 1j * rng.standard_normal((3, 4))
+    va, vb = vectors.Vector(a), vectors.Vector(b)
+    assert abs(va.dot(vb) - np.vdot(a, b)) < 1e-4 * abs(np.vdot(a, b))
+    vc = va.clone().scaleAdd(vb, 2.0, -1.0)
+    assert np.allclose(vc.arr.numpy(), 2 * a - b, atol=1e-5)
+    assert va.cloneSpace().norm() == 0.0
+    sv = vectors.SuperVector(va, vb)
+    assert abs(sv.dot(sv) - (np.vdot(a, a) + np.vdot(b, b))) < 1e-3
+    with pytest.raises(ValueError):
+        vectors.Vector(vectors.Hypercube.from_shape((2, 2)), np.zeros((3, 3)))
+
+
+def test_remap_ids_dense_sorted():
+    s, r, ns = CudaWEM._remap_ids([10, 31, 21, 10], [21, 21, 10, 31])
+    assert ns == 3
+    assert list(s) == [0, 2, 1, 0] and list(r) == [1, 1, 0, 2]
+    with pytest.raises(RuntimeError, match="Shot ID not present"):
+        CudaWEM._remap_ids([1, 2], [1, 3])
+
+
+def test_padding_keys_required():
+    with pytest.raises(RuntimeError, match="negative padx/pady"):
+        CudaWEM._pads({"nref": 2})
+    assert CudaWEM._pads({"padx": 4, "pady": 0}) == (4, 0)
+
+
+def test_axes_from_par_for_bare_arrays():
+    par = dict(ox=1.0, dx=10.0, oy=2.0, dy=12.0, oz=0.0, dz=5.0, ow=3.0, dw=0.25)
+    h = CudaWEM._hyper(np.zeros((7, 5, 6, 8), np.complex64), par, "model")
+    x, y, w, z = h.getAxes()
+    assert (x.n, x.o, x.d) == (8, 1.0, 10.0) and (y.n, y.d) == (6, 12.0)
+    assert (w.n, w.o, w.d) == (5, 3.0, 0.25) and (z.n, z.d) == (7, 5.0)
+    v = vectors.Vector(h, torch.zeros(h.shape, dtype=torch.complex64))
+    assert CudaWEM._hyper(v) is h
+
+
+def test_store_writes_back_into_numpy_and_tensors():
+    t = torch.arange(6, dtype=torch.float32).to(torch.complex64)
+    a = np.zeros(6, np.complex64)
+    CudaWEM._store(a, t)
+    assert np.array_equal(a, t.numpy())
+    b = torch.zeros(2, 3, dtype=torch.complex64)
+    CudaWEM._store(b, t)
+    assert torch.equal(b.reshape(-1), t)
