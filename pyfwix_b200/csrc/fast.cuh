@@ -209,11 +209,21 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int n
 #pragma unroll
   for (int e = 0; e < P::E; ++e) raw[e] = c.live ? src[pos_first<P>(c.t, e)] : make_float2(0.f, 0.f);
   const int nterm = (PRE == W_MASK || PRE == W_SCAT_CONJ) ? a.nterm : 1;
+  uint8_t lab[P::E];
+  if (PRE == W_MASK) {
+    const uint8_t* lrow = a.lab + (long long)c.iw * a.lab_w + (long long)(c.live ? c.y : 0) * P::N;
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) lab[e] = c.live ? lrow[pos_first<P>(c.t, e)] : 255;
+  }
   for (int term = 0; term < nterm; ++term) {
     float2 v[P::E];
 #pragma unroll
-    for (int e = 0; e < P::E; ++e)
-      v[e] = c.live ? row_weight<PRE>(a, term, c.iw, c.y, pos_first<P>(c.t, e), raw[e]) : make_float2(0.f, 0.f);
+    for (int e = 0; e < P::E; ++e) {
+      if (PRE == W_MASK)
+        v[e] = (int)lab[e] == term ? raw[e] : make_float2(0.f, 0.f);
+      else
+        v[e] = c.live ? row_weight<PRE>(a, term, c.iw, c.y, pos_first<P>(c.t, e), raw[e]) : make_float2(0.f, 0.f);
+    }
     fft_fwd<P>(v, c.t, c.tw, c.line);
     if (c.live) {
       float2* dst = a.t1 + (long long)term * a.tstride + (c.bl * a.d.NY + c.y) * P::N;
@@ -341,26 +351,46 @@ struct ColCtx {
 template <class P>
 __device__ __forceinline__ void cols_to_tile(float2* tile, const float2* __restrict__ g, const SpecArgs& a,
                                              long long b, int x0) {
-  constexpr int LX = ColGeo<P>::LX;
-  for (int i = threadIdx.x; i < LX * P::N; i += blockDim.x) {
-    const int y = i / LX, cc = i - y * LX;
-    const int x = x0 + cc;
-    if (x < a.d.NX) tile[cc * ColGeo<P>::LINE + swz(y)] = g[b * a.d.slice + (long long)y * a.d.NX + x];
+  constexpr int LX = ColGeo<P>::LX, NT = kWarps * 32;
+  static_assert((LX * P::N) % NT == 0, "tile is a whole number of CTA sweeps");
+  const int cc = threadIdx.x % LX, x = x0 + cc;
+  if (x >= a.d.NX) return;
+  const float2* src = g + b * a.d.slice + x;
+#pragma unroll 4
+  for (int k = 0; k < LX * P::N / NT; ++k) {
+    const int y = (int)(threadIdx.x + k * NT) / LX;
+    tile[cc * ColGeo<P>::LINE + swz(y)] = src[(long long)y * a.d.NX];
   }
 }
 template <class P>
 __device__ __forceinline__ void tile_to_cols(const float2* tile, float2* g, const SpecArgs& a, long long b, int x0,
                                              int add, float scale) {
-  constexpr int LX = ColGeo<P>::LX;
-  for (int i = threadIdx.x; i < LX * P::N; i += blockDim.x) {
-    const int y = i / LX, cc = i - y * LX;
-    const int x = x0 + cc;
-    if (x >= a.d.NX) continue;
+  constexpr int LX = ColGeo<P>::LX, NT = kWarps * 32;
+  const int cc = threadIdx.x % LX, x = x0 + cc;
+  if (x >= a.d.NX) return;
+  float2* dst = g + b * a.d.slice + x;
+#pragma unroll 4
+  for (int k = 0; k < LX * P::N / NT; ++k) {
+    const int y = (int)(threadIdx.x + k * NT) / LX;
     float2 v = tile[cc * ColGeo<P>::LINE + swz(y)];
     if (scale != 1.f) v = cscale(v, scale);
-    float2* q = g + b * a.d.slice + (long long)y * a.d.NX + x;
+    float2* q = dst + (long long)y * a.d.NX;
     if (add) v = cadd(*q, v);
     *q = v;
+  }
+}
+
+// Column multipliers of term t for this lane's spectrum samples (forward-output
+// layout), from the phase table when one is bound.
+template <class P, int QM>
+__device__ __forceinline__ void col_factors(const SpecArgs& a, int t, int iw, int x, int lane_t, float2 (&q)[P::E]) {
+  if ((QM == Q_PS_FWD || QM == Q_PS_ADJ) && a.ptab) {
+    const QCol qc = qcol<QM>(a, t, iw, x);
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) q[e] = qcol_get(a, qc, pos_last<P>(lane_t, e));
+  } else {
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) q[e] = qmult<QM>(a, t, iw, x, pos_last<P>(lane_t, e));
   }
 }
 
@@ -378,16 +408,12 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_a(co
   fft_fwd<P>(psi, c.t, c.tw, c.line);
   const int xq = c.x < a.d.NX ? c.x : 0;
   float2 q[P::E];
-#pragma unroll
-  for (int e = 0; e < P::E; ++e) q[e] = qmult<QM>(a, 0, c.iw, xq, pos_last<P>(c.t, e));
+  col_factors<P, QM>(a, 0, c.iw, xq, c.t, q);
   for (int term = 0; term < a.nterm; ++term) {
     float2 v[P::E];
 #pragma unroll
     for (int e = 0; e < P::E; ++e) v[e] = cmul(psi[e], q[e]);
-    if (term + 1 < a.nterm) {
-#pragma unroll
-      for (int e = 0; e < P::E; ++e) q[e] = qmult<QM>(a, term + 1, c.iw, xq, pos_last<P>(c.t, e));
-    }
+    if (term + 1 < a.nterm) col_factors<P, QM>(a, term + 1, c.iw, xq, c.t, q);
     __syncthreads();  // the previous term's tile has been stored
     fft_inv<P>(v, c.t, c.tw, c.line);
     __syncwarp();
@@ -402,12 +428,14 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_a(co
 template <class P>
 __device__ __forceinline__ void cols_to_tile_async(float2* tile, const float2* __restrict__ g, const SpecArgs& a,
                                                    long long b, int x0) {
-  constexpr int LX = ColGeo<P>::LX;
-  for (int i = threadIdx.x; i < LX * P::N; i += blockDim.x) {
-    const int y = i / LX, cc = i - y * LX;
-    const int x = x0 + cc;
-    const bool ok = x < a.d.NX;
-    cp_async8(tile + cc * ColGeo<P>::LINE + swz(y), g + b * a.d.slice + (long long)y * a.d.NX + (ok ? x : 0), ok);
+  constexpr int LX = ColGeo<P>::LX, NT = kWarps * 32;
+  const int cc = threadIdx.x % LX, x = x0 + cc;
+  const bool ok = x < a.d.NX;
+  const float2* src = g + b * a.d.slice + (ok ? x : 0);
+#pragma unroll 4
+  for (int k = 0; k < LX * P::N / NT; ++k) {
+    const int y = (int)(threadIdx.x + k * NT) / LX;
+    cp_async8(tile + cc * ColGeo<P>::LINE + swz(y), src + (long long)y * a.d.NX, ok);
   }
   cp_async_commit();
 }
@@ -435,8 +463,7 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_b(co
       cp_async_wait<0>();
     }
     float2 q[P::E];
-#pragma unroll
-    for (int e = 0; e < P::E; ++e) q[e] = qmult<QM>(a, term, c.iw, xq, pos_last<P>(c.t, e));
+    col_factors<P, QM>(a, term, c.iw, xq, c.t, q);
     __syncthreads();  // this term's tile is complete
     float2* line = tiles[term & 1] + lineoff;
     float2 v[P::E];

@@ -20,6 +20,22 @@ struct Fft1D {
   int radix[FWIX_MAX_PASS];
 };
 
+// Complex arithmetic.  On sm_100 the packed FP32 pair instructions
+// (__fadd2_rn / __fmul2_rn / __ffma2_rn) do both components in one
+// instruction; each component is rounded exactly as the scalar form would be.
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {  // (ax bx - ay by, ax by + ay bx)
+  const float2 t = __fmul2_rn(make_float2(a.x, a.x), b);
+  return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), t);
+}
+__device__ __forceinline__ float2 cmul_conj(float2 a, float2 b) {  // a * conj(b)
+  const float2 t = __fmul2_rn(a, make_float2(b.x, b.x));
+  return __ffma2_rn(make_float2(a.y, -a.x), make_float2(b.y, b.y), t);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+#else
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -29,6 +45,7 @@ __device__ __forceinline__ float2 cmul_conj(float2 a, float2 b) {  // a * conj(b
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+#endif
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 // multiply by -i (forward) or +i (inverse)
 template <bool INV>

@@ -99,4 +99,29 @@ __device__ __forceinline__ float2 qmult(const SpecArgs& a, int t, int iw, int x,
   return QM == Q_PS_FWD ? make_float2(att * cs, -att * sn) : make_float2(att * cs, att * sn);
 }
 
+// Phase-table view of one column (fixed x) for one term: the factors of every
+// ky of that column are then one load each (qcol_get).  Only for the cached
+// phase-shift path (a.ptab set, Q_PS_FWD / Q_PS_ADJ).
+struct QCol {
+  const float2* p;
+  bool flip;  // adjoint: conj(P) unless the reference's b > 0 branch applies
+};
+template <int QM>
+__device__ __forceinline__ QCol qcol(const SpecArgs& a, int t, int iw, int x) {
+  QCol q;
+  const int kxq = min(x, a.d.NX - x);
+  q.p = a.ptab + (((long long)t * a.d.nw + iw) * a.ptab_nx + kxq) * a.ptab_ny;
+  if (QM == Q_PS_ADJ) {
+    const float2 sr = a.sref[t * a.d.nw + iw];
+    q.flip = !(a.w2[iw] * (sr.y - a.eps * sr.x) > 0.f);
+  } else {
+    q.flip = false;
+  }
+  return q;
+}
+__device__ __forceinline__ float2 qcol_get(const SpecArgs& a, const QCol& q, int y) {
+  const float2 P = q.p[min(y, a.d.NY - y)];
+  return q.flip ? cconj(P) : P;
+}
+
 }  // namespace fwix
