@@ -73,6 +73,9 @@ enum { FWIX_FWD = 0, FWIX_ADJ_ADD = 1, FWIX_ADJ_INPL = 2 };
 /* PhaseShift modes (phase_shift.cu:7-61, :125-184, :248-305). */
 enum { FWIX_PS_FWD = 0, FWIX_PS_ADJ = 1, FWIX_PS_INV = 2 };
 
+/* Smooth-step modes (fwix_smooth_step). */
+enum { FWIX_SMOOTH_FWD = 0, FWIX_SMOOTH_ADJ = 1, FWIX_SMOOTH_DERIV = 2 };
+
 /* Workspace classes for fwix_plan_workspace_bytes. */
 enum { FWIX_WS_STEP = 0, FWIX_WS_SWEEP = 1, FWIX_WS_BORN = 2 };
 
@@ -150,6 +153,29 @@ fwix_status fwix_imaging(fwix_plan* plan, int adjoint, const void* bg, void* ima
  * drho(iz), drho(iz+1)) <-> dr [nw][ny][nx]. */
 fwix_status fwix_lin_reflect(fwix_plan* plan, int iz, int adjoint, void* dmodel, void* dr, int add,
                              void* stream);
+
+/* ---- differentiable ("smooth") step ------------------------------------------
+ * No reference counterpart: the reference's PSPI selects the nearest reference
+ * per cell (propagator/src/selector.cu:29-35), so its output depends on the
+ * slowness only through piecewise-constant labels and has no usable gradient.
+ * The smooth step interpolates between the two references that bracket the
+ * local slowness s (hat functions over the references sorted ascending,
+ * clamped at both ends) and applies the split-step correction
+ * SS_r = exp(-i w (s - s_r) dz):
+ *   FWD   out (+)= sum_r w_r(s) SS_r F^-1(P_r F(taper in))
+ *   ADJ   out (+)= its exact transpose
+ *   DERIV out (+)= sum_r (w_r'(s) - i w dz w_r(s)) SS_r F^-1(P_r F(taper in))
+ *                  (the derivative of FWD with respect to s, cell by cell)
+ * P_r are the phase factors of the complex references bound by
+ * fwix_plan_set_refs (s_r^2 for every frequency; labels are not used). */
+/* slow_pad [nz][NY][NX] (edge-replicated s), sref_real [nz][nref] ascending. */
+fwix_status fwix_plan_set_smooth(fwix_plan* plan, const float* slow_pad, const float* sref_real);
+fwix_status fwix_smooth_step(fwix_plan* plan, int iz, int mode, const void* in, void* out, int add,
+                             void* stream);
+/* out[y][x] (+)= Re sum_{shots, w} conj(a) b over the padded slice (padded != 0,
+ * out is [NY][NX]) or the model window (out is [ny][nx]). */
+fwix_status fwix_correlate(fwix_plan* plan, const void* a, const void* b, float* out, int add, int padded,
+                           void* stream);
 
 /* ---- acquisition ------------------------------------------------------------ */
 /* Host coordinate arrays; ids are dense shot indices in [0, ns). */

@@ -732,3 +732,181 @@ def migrate(g, stepper, acq, wavelet, data):
         S = stepper.fwd(iz, S)
         R = stepper.adj(iz, R)
     return img
+
+
+# --------------------------------------------------------------------------
+# differentiable ("smooth") PSPI step and the adjoint-state FWI gradient.
+# No reference counterpart: the reference's PSPI selects the nearest reference
+# per cell (``propagator/src/selector.cu:29-35``), so its output is piecewise
+# constant in the slowness.  The smooth step interpolates between the two
+# references bracketing the local slowness s (hat functions on the sorted
+# references, clamped at both ends) with the split-step correction
+# exp(-i w (s - s_r) dz); the phase factors P_r are the reference's
+# (``propagator/src/phase_shift.cu:7-61``) for s_r^2.  This section restates
+# that definition in FP64 as the oracle of the B200 smooth step, and derives
+# the gradient of J = 1/2 |d(s) - d_obs|^2 for the Propagator's modelling
+# (down pass, reflection, up pass; ``propagator/src/Propagator.cpp:121-221``)
+# with density 1 and the references held fixed.
+# --------------------------------------------------------------------------
+
+def hat_weights(s, refs):
+    """Weights w_r(s) and derivatives w_r'(s), each [nref] + s.shape."""
+    refs = np.asarray(refs, dtype=np.float64)
+    s = np.asarray(s, dtype=np.float64)
+    n = len(refs)
+    w = np.zeros((n,) + s.shape)
+    dw = np.zeros_like(w)
+    if n == 1:
+        w[0] = 1.0
+        return w, dw
+    lo, hi = s <= refs[0], s >= refs[-1]
+    mid = ~(lo | hi)
+    j = np.clip(np.searchsorted(refs, s, side="right") - 1, 0, n - 2)
+    span = refs[j + 1] - refs[j]
+    u = (s - refs[j]) / span
+    for r in range(n):
+        w[r] = np.where(mid & (j == r), 1 - u, 0.0) + np.where(mid & (j + 1 == r), u, 0.0)
+        dw[r] = np.where(mid & (j == r), -1.0 / span, 0.0) + np.where(mid & (j + 1 == r), 1.0 / span, 0.0)
+    w[0][lo] = 1.0
+    w[n - 1][hi] = 1.0
+    return w, dw
+
+
+def _smooth_terms(g, refs_z, s_pad_z):
+    """Per reference: phase factors P_r [nw][NY][NX] (s_r^2 for every frequency),
+    split-step factors SS_r and hat weights / derivatives on the padded slice."""
+    kx, ky, w2, w = g.kx(), g.ky(), g.w2(), g.w()
+    wt, dwt = hat_weights(s_pad_z, refs_z)
+    out = []
+    for r, sr in enumerate(refs_z):
+        sref_w = np.full(g.nw, float(sr) ** 2, dtype=np.complex128)
+        P = phase_forward_factor(w2, kx, ky, sref_w, g.dz, g.eps)
+        Pa = phase_adjoint_factor(w2, kx, ky, sref_w, g.dz, g.eps)
+        SS = np.exp(-1j * w[:, None, None] * (s_pad_z[None] - sr) * g.dz)
+        out.append((P, Pa, SS, wt[r][None], dwt[r][None]))
+    return out
+
+
+def smooth_forward(g, refs_z, s_pad_z, psi):
+    """psi' = sum_r w_r SS_r F^-1(P_r F(taper psi))."""
+    mk = fft2(psi * g.taper()[None, None])
+    out = np.zeros_like(psi, dtype=np.complex128)
+    for P, _, SS, wt, _ in _smooth_terms(g, refs_z, s_pad_z):
+        out += (wt * SS)[None] * ifft2(P[None] * mk)
+    return out
+
+
+def smooth_adjoint(g, refs_z, s_pad_z, d):
+    """Exact transpose of smooth_forward: taper F^-1(sum_r P_r^adj F(w_r conj(SS_r) d))."""
+    mk = np.zeros_like(d, dtype=np.complex128)
+    for _, Pa, SS, wt, _ in _smooth_terms(g, refs_z, s_pad_z):
+        mk += Pa[None] * fft2((wt * np.conj(SS))[None] * d)
+    return ifft2(mk) * g.taper()[None, None]
+
+
+def smooth_deriv(g, refs_z, s_pad_z, psi):
+    """Cell-wise derivative of smooth_forward with respect to s:
+    sum_r (w_r' - i w dz w_r) SS_r F^-1(P_r F(taper psi))."""
+    mk = fft2(psi * g.taper()[None, None])
+    w = g.w()[:, None, None]
+    out = np.zeros_like(psi, dtype=np.complex128)
+    for P, _, SS, wt, dwt in _smooth_terms(g, refs_z, s_pad_z):
+        out += ((dwt - 1j * w * g.dz * wt) * SS)[None] * ifft2(P[None] * mk)
+    return out
+
+
+def pad_edge(g, s):
+    """[nz][ny][nx] -> [nz][NY][NX] by edge replication."""
+    return np.pad(s, ((0, 0), (0, g.pady), (0, g.padx)), mode="edge")
+
+
+def fold_edge(g, gp):
+    """Transpose of pad_edge: padded-cell contributions summed into the edge cells."""
+    out = gp[:, :g.ny, :g.nx].copy()
+    out[:, :, g.nx - 1] += gp[:, :g.ny, g.nx:].sum(axis=2)
+    out[:, g.ny - 1, :] += gp[:, g.ny:, :g.nx].sum(axis=1)
+    out[:, g.ny - 1, g.nx - 1] += gp[:, g.ny:, g.nx:].sum(axis=(1, 2))
+    return out
+
+
+def smooth_refs(s, nref, spread=1e-3):
+    """Reference slownesses per depth: nref values evenly spaced over the slice's
+    [min, max] (a slice narrower than spread * mean is widened to that)."""
+    s = np.asarray(s, dtype=np.float64)
+    lo, hi = s.min(axis=(1, 2)), s.max(axis=(1, 2))
+    mid, half = 0.5 * (lo + hi), 0.5 * (hi - lo)
+    half = np.maximum(half, 0.5 * spread * mid)
+    if nref == 1:
+        return mid[:, None]
+    return mid[:, None] + half[:, None] * np.linspace(-1.0, 1.0, nref)[None, :]
+
+
+def smooth_propagate(g, refs, s, acq, wavelet):
+    """Modelling with the smooth step: the Propagator's down pass, reflection
+    (density 1: r = (s0 - s1) / (s0 + s1), bottom r = 0) and up pass.  Returns
+    (data, D, U): D[iz] the down field after injection at iz, U[iz] the up
+    field after the step, reflection and recording at iz."""
+    sp = pad_edge(g, s)
+    s2 = np.repeat((np.asarray(s, np.float64) ** 2)[:, None].astype(np.complex128), g.nw, axis=1)
+    den = np.ones_like(s2)
+    data = np.zeros((len(acq.rec.ix), g.nw), dtype=np.complex128)
+    D = np.zeros((acq.ns, g.nw, g.NY, g.NX), dtype=np.complex128)
+    Ds, Us = [None] * g.nz, [None] * g.nz
+    for iz in range(g.nz):
+        D = inject(acq.src, wavelet, D, iz)
+        data = record(acq.rec, D, data, iz)
+        Ds[iz] = D.copy()
+        D = smooth_forward(g, refs[iz], sp[iz], D)
+    U = np.zeros_like(D)
+    for iz in range(g.nz - 1, -1, -1):
+        U = smooth_forward(g, refs[iz], sp[iz], U)
+        U = reflect_forward(g, s2, den, iz, Ds[iz], U)
+        data = record(acq.rec, U, data, iz)
+        Us[iz] = U.copy()
+    return data, Ds, Us
+
+
+def smooth_objective(g, refs, s, acq, wavelet, d_obs):
+    data, _, _ = smooth_propagate(g, refs, s, acq, wavelet)
+    r = data - d_obs
+    return 0.5 * float(np.real(np.vdot(r, r)))
+
+
+def smooth_gradient(g, refs, s, acq, wavelet, d_obs):
+    """(J, dJ/ds [nz][ny][nx]) by the adjoint-state method.
+
+    mu_iz (adjoint of U_iz) = Rec_iz^H r + S_{iz-1}^H mu_{iz-1}, downward;
+    nu_iz (adjoint of D_iz) = Rec_iz^H r + conj(R_iz) mu_iz + S_iz^H nu_{iz+1}, upward;
+    dJ/ds collects Re<mu_iz, dS_iz(U_{iz+1})>, Re<nu_{iz+1}, dS_iz(D_iz)> and
+    Re<mu_iz, dR_iz D_iz>, summed over shots and frequencies."""
+    s = np.asarray(s, np.float64)
+    data, Ds, Us = smooth_propagate(g, refs, s, acq, wavelet)
+    res = data - d_obs
+    J = 0.5 * float(np.real(np.vdot(res, res)))
+    sp = pad_edge(g, s)
+    s2 = np.repeat((s ** 2)[:, None].astype(np.complex128), g.nw, axis=1)
+    den = np.ones_like(s2)
+    gpad = np.zeros((g.nz, g.NY, g.NX))
+    grefl = np.zeros((g.nz, g.ny, g.nx))
+    corr = lambda a, b: np.real(np.sum(np.conj(a) * b, axis=(0, 1)))
+    mus = [None] * g.nz
+    mu = np.zeros_like(Ds[0])
+    for iz in range(g.nz):
+        if iz > 0:
+            mu = smooth_adjoint(g, refs[iz - 1], sp[iz - 1], mu)
+        mu = inject(acq.rec, res, mu, iz)
+        mus[iz] = mu.copy()
+        if iz + 1 < g.nz:
+            gpad[iz] += corr(mu, smooth_deriv(g, refs[iz], sp[iz], Us[iz + 1]))
+            c = corr(mu[:, :, :g.ny, :g.nx], Ds[iz][:, :, :g.ny, :g.nx])
+            s0, s1 = s[iz], s[iz + 1]
+            grefl[iz] += c * 2 * s1 / (s0 + s1) ** 2
+            grefl[iz + 1] += c * (-2 * s0) / (s0 + s1) ** 2
+    nu = np.zeros_like(Ds[0])
+    for iz in range(g.nz - 1, -1, -1):
+        if iz + 1 < g.nz:
+            gpad[iz] += corr(nu, smooth_deriv(g, refs[iz], sp[iz], Ds[iz]))
+        nu = smooth_adjoint(g, refs[iz], sp[iz], nu)
+        nu = reflect_adjoint(g, s2, den, iz, mus[iz], nu)
+        nu = inject(acq.rec, res, nu, iz)
+    return J, fold_edge(g, gpad) + grefl

@@ -18,6 +18,7 @@ STATUS = {0: "FWIX_OK", -1: "FWIX_ERR_INVALID", -2: "FWIX_ERR_UNSUPPORTED", -3: 
 STEP_PSPI, STEP_NSPS = 0, 1
 FWD, ADJ_ADD, ADJ_INPL = 0, 1, 2
 PS_FWD, PS_ADJ, PS_INV = 0, 1, 2
+SMOOTH_FWD, SMOOTH_ADJ, SMOOTH_DERIV = 0, 1, 2
 WS_STEP, WS_SWEEP, WS_BORN = 0, 1, 2
 
 
@@ -58,6 +59,9 @@ SIGNATURES = {
     "fwix_select": [P, I, I, P, P, I, P],
     "fwix_taper": [P, P, P, I, P],
     "fwix_step": [P, I, I, I, P, P, I, P],
+    "fwix_plan_set_smooth": [P, P, P],
+    "fwix_smooth_step": [P, I, I, P, P, I, P],
+    "fwix_correlate": [P, P, P, P, I, I, P],
     "fwix_scatter": [P, I, I, P, P, I, P],
     "fwix_reflect": [P, I, I, P, P, I, P],
     "fwix_imaging": [P, I, P, P, P, I, P],

@@ -124,6 +124,8 @@ struct fwix_plan {
   size_t ws_bytes = 0;
   int nterm_max = 1;
   long long chunk = 1;  // slices per launch: the intermediates of one chunk fit in L2
+  const float* sm_s = nullptr;    // smooth step: padded slowness [nz][NY][NX]
+  const float* sm_ref = nullptr;  // smooth step: sorted real reference slownesses [nz][nref]
   float2* pcache = nullptr;   // phase-factor cache, nz depths (fwix_plan_set_phase_cache)
   std::vector<char> pbuilt;   // depth iz of the cache holds current factors
   int pq_nx() const { return d.NX / 2 + 1; }
@@ -281,6 +283,33 @@ fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, f
   SpecArgs a0 = p->args(in, out, add);
   FWIX_TRY(phase_factors(p, iz, a0, s));
   return for_chunks(p, a0, [&](const SpecArgs& a) { return step_chunk(p, kind, iz, dir, a, s); });
+}
+
+fwix_status need_smooth(const fwix_plan* p) {
+  if (!p->sm_s || !p->sm_ref || !p->sref)
+    return fail(FWIX_ERR_STATE, "smooth-step slowness / references not bound (fwix_plan_set_smooth, fwix_plan_set_refs)");
+  return FWIX_OK;
+}
+
+// Smooth PSPI step (no reference counterpart): forward
+//   out (+)= sum_r w_r(s) SS_r F^-1(P_r F(taper in)),
+// its exact transpose, and the derivative with respect to the local slowness
+//   out (+)= sum_r (w_r' - i w dz w_r) SS_r F^-1(P_r F(taper in)).
+fwix_status smooth_chunk(fwix_plan* p, int iz, int mode, SpecArgs a, cudaStream_t s) {
+  a.sref = p->sref + (long long)iz * p->desc.nref * p->d.nw;
+  a.sm_s = p->sm_s + (long long)iz * p->d.slice;
+  a.sm_ref = p->sm_ref + (long long)iz * p->desc.nref;
+  a.sm_n = p->desc.nref;
+  a.nterm = p->desc.nref;
+  if (mode == FWIX_SMOOTH_ADJ) {
+    FWIX_TRY(cu(fwix::row_forward(a, fwix::W_SMOOTH_CONJ, s), "smooth adjoint row pass"));
+    FWIX_TRY(cu(fwix::col_type_b(a, fwix::Q_PS_ADJ, s), "smooth adjoint column pass"));
+    return cu(fwix::row_inverse(a, fwix::W_ONE, 1, s), "smooth adjoint inverse row pass");
+  }
+  FWIX_TRY(cu(fwix::row_forward(a, fwix::W_TAPER, s), "smooth row pass"));
+  FWIX_TRY(cu(fwix::col_type_a(a, fwix::Q_PS_FWD, s), "smooth column pass"));
+  return cu(fwix::row_inverse(a, mode == FWIX_SMOOTH_DERIV ? fwix::W_SMOOTH_DERIV : fwix::W_SMOOTH, 0, s),
+            "smooth inverse row pass");
 }
 
 SpecArgs scatter_args(const fwix_plan* p, int iz, const float2* in, float2* out, int add) {
@@ -542,6 +571,35 @@ fwix_status fwix_step(fwix_plan* p, int kind, int iz, int dir, const void* in, v
   FWIX_TRY(need_ws(p, FWIX_WS_STEP));
   FWIX_TRY(check_iz(p, iz));
   return do_step(p, kind, iz, dir, (const float2*)in, (float2*)out, add, (cudaStream_t)stream);
+}
+
+fwix_status fwix_plan_set_smooth(fwix_plan* p, const float* slow_pad, const float* sref_real) {
+  if (!p) return fail(FWIX_ERR_INVALID, "null plan");
+  p->sm_s = slow_pad;
+  p->sm_ref = sref_real;
+  return FWIX_OK;
+}
+
+fwix_status fwix_smooth_step(fwix_plan* p, int iz, int mode, const void* in, void* out, int add, void* stream) {
+  if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  if (mode != FWIX_SMOOTH_FWD && mode != FWIX_SMOOTH_ADJ && mode != FWIX_SMOOTH_DERIV)
+    return fail(FWIX_ERR_INVALID, "unknown smooth-step mode");
+  FWIX_TRY(need_smooth(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  FWIX_TRY(check_iz(p, iz));
+  cudaStream_t s = (cudaStream_t)stream;
+  SpecArgs a0 = p->args((const float2*)in, (float2*)out, add);
+  FWIX_TRY(phase_factors(p, iz, a0, s));
+  return for_chunks(p, a0, [&](const SpecArgs& a) { return smooth_chunk(p, iz, mode, a, s); });
+}
+
+fwix_status fwix_correlate(fwix_plan* p, const void* a, const void* b, float* out, int add, int padded,
+                           void* stream) {
+  if (!p || !a || !b || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (padded)
+    return cu(fwix::launch_correlate_padded(p->d, (const float2*)a, (const float2*)b, out, add, s), "correlate");
+  return cu(fwix::launch_image_acc(p->d, (const float2*)a, (const float2*)b, out, add, s), "correlate");
 }
 
 fwix_status fwix_scatter(fwix_plan* p, int iz, int adjoint, const void* in, void* out, int add, void* stream) {

@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int n
   const float2* src = a.in + (c.b * a.d.NY + (c.live ? c.y : 0)) * P::N;
 #pragma unroll
   for (int e = 0; e < P::E; ++e) raw[e] = c.live ? src[pos_first<P>(c.t, e)] : make_float2(0.f, 0.f);
-  const int nterm = (PRE == W_MASK || PRE == W_SCAT_CONJ) ? a.nterm : 1;
+  const int nterm = multi_term(PRE) ? a.nterm : 1;
   uint8_t lab[P::E];
   if (PRE == W_MASK) {
     const uint8_t* lrow = a.lab + (long long)c.iw * a.lab_w + (long long)(c.live ? c.y : 0) * P::N;
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_inv(const SpecArgs a, int n
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
   __syncthreads();
-  const int nterm = (POST == W_MASK || POST == W_SCAT) ? a.nterm : 1;
+  const int nterm = multi_term(POST) ? a.nterm : 1;
   float2 acc[P::E];
 #pragma unroll
   for (int e = 0; e < P::E; ++e) acc[e] = make_float2(0.f, 0.f);
@@ -537,6 +537,7 @@ cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
     FWIX_FAST_RF(W_MASK)
     FWIX_FAST_RF(W_SCAT_CONJ)
     FWIX_FAST_RF(W_IC)
+    FWIX_FAST_RF(W_SMOOTH_CONJ)
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_FAST_RF
@@ -559,6 +560,8 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
     FWIX_FAST_RI(W_ONE)
     FWIX_FAST_RI(W_MASK)
     FWIX_FAST_RI(W_SCAT)
+    FWIX_FAST_RI(W_SMOOTH)
+    FWIX_FAST_RI(W_SMOOTH_DERIV)
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_FAST_RI

@@ -21,8 +21,20 @@ enum RowWeight {
   W_MASK = 2,       // labels == term                        (selector.cu:29-35)
   W_SCAT = 3,       // Born weight W_n                       (scatter.cu:61-106,155-195)
   W_SCAT_CONJ = 4,  // conj(W_n)
-  W_IC = 5          // bg * image on the unpadded window      (imaging_condition.cu:39-52)
+  W_IC = 5,         // bg * image on the unpadded window      (imaging_condition.cu:39-52)
+  // differentiable ("smooth") step, no reference counterpart: per reference r a
+  // hat-function weight w_r(s) of the local slowness s between the sorted
+  // reference slownesses, times the split-step factor SS_r = exp(-i w (s - s_r) dz)
+  W_SMOOTH = 6,       // w_r SS_r
+  W_SMOOTH_CONJ = 7,  // w_r conj(SS_r)
+  W_SMOOTH_DERIV = 8  // d(w_r SS_r)/ds = (w_r' - i w dz w_r) SS_r
 };
+
+// Weights that run one pass per term (reference or Taylor term).
+__host__ __device__ constexpr bool multi_term(int w) {
+  return w == W_MASK || w == W_SCAT || w == W_SCAT_CONJ || w == W_SMOOTH || w == W_SMOOTH_CONJ ||
+         w == W_SMOOTH_DERIV;
+}
 
 // Spectral multipliers applied between the column FFTs.
 enum ColMult {
@@ -67,6 +79,11 @@ struct SpecArgs {
   // kyq = min(y, NY-y); NULL means evaluate the factors in the kernel
   const float2* ptab;
   int ptab_nx, ptab_ny;
+  // smooth step: padded local slowness [NY][NX] and the sorted real reference
+  // slownesses [sm_n] of this depth
+  const float* sm_s;
+  const float* sm_ref;
+  int sm_n;
   float dz, eps, eps_scat;
   float coef[5];
   float norm;          // scale folded into the column multiplier
@@ -124,6 +141,9 @@ cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, con
                                int add, cudaStream_t s);
 cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, float* img, int add,
                              cudaStream_t s);
+// img[y][x] (+)= Re sum_{s,w} conj(S) R over the padded NY x NX slice.
+cudaError_t launch_correlate_padded(const Dims& d, const float2* S, const float2* R, float* img, int add,
+                                    cudaStream_t s);
 cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s);
 
 // Acquisition kernels (pointwise.cu).  A depth level's injection is a gather

@@ -22,8 +22,59 @@ __device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, 
   return rot90<false>(cscale(p, f));
 }
 
+// Hat-function interpolation weight of reference t at slowness s and its
+// derivative, on references sorted ascending (clamped to the end references
+// outside their range, where the derivative is 0).
+struct Hat {
+  float w, dw;
+};
+__device__ __forceinline__ Hat hat_weight(const float* ref, int n, int t, float s) {
+  Hat h = {0.f, 0.f};
+  if (n == 1) {
+    h.w = 1.f;
+    return h;
+  }
+  if (s <= ref[0]) {
+    h.w = t == 0 ? 1.f : 0.f;
+    return h;
+  }
+  if (s >= ref[n - 1]) {
+    h.w = t == n - 1 ? 1.f : 0.f;
+    return h;
+  }
+  int j = 0;
+  while (j < n - 2 && s >= ref[j + 1]) ++j;
+  const float span = ref[j + 1] - ref[j];
+  const float u = (s - ref[j]) / span;
+  if (t == j) {
+    h.w = 1.f - u;
+    h.dw = -1.f / span;
+  } else if (t == j + 1) {
+    h.w = u;
+    h.dw = 1.f / span;
+  }
+  return h;
+}
+
+// w_r SS_r (W_SMOOTH), w_r conj(SS_r) (W_SMOOTH_CONJ) or (w_r' - i w dz w_r) SS_r
+// (W_SMOOTH_DERIV) for reference t at cell (y, x) of frequency iw.
+template <int W>
+__device__ __forceinline__ float2 smooth_factor(const SpecArgs& a, int t, int iw, int y, int x) {
+  const float s = a.sm_s[(long long)y * a.d.NX + x];
+  const Hat h = hat_weight(a.sm_ref, a.sm_n, t, s);
+  if (h.w == 0.f && h.dw == 0.f) return make_float2(0.f, 0.f);
+  const float wdz = a.w[iw] * a.dz;
+  float sn, cs;
+  sincosf(wdz * (s - a.sm_ref[t]), &sn, &cs);
+  const float2 ss = make_float2(cs, -sn);  // exp(-i w (s - s_t) dz)
+  if (W == W_SMOOTH) return cscale(ss, h.w);
+  if (W == W_SMOOTH_CONJ) return cscale(cconj(ss), h.w);
+  return cmul(make_float2(h.dw, -wdz * h.w), ss);
+}
+
 template <int W>
 __device__ __forceinline__ float2 row_weight(const SpecArgs& a, int t, int iw, int y, int x, float2 v) {
+  if (W == W_SMOOTH || W == W_SMOOTH_CONJ || W == W_SMOOTH_DERIV) return cmul(v, smooth_factor<W>(a, t, iw, y, x));
   if (W == W_ONE) return v;
   if (W == W_TAPER) return cscale(v, a.tapx[x] * a.tapy[y]);
   if (W == W_MASK) {

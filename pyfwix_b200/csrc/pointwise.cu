@@ -329,6 +329,16 @@ cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, fl
   return cudaGetLastError();
 }
 
+cudaError_t launch_correlate_padded(const Dims& d, const float2* S, const float2* R, float* img, int add,
+                                    cudaStream_t s) {
+  Dims full = d;  // iterate over the padded slice: the cell window is the whole NY x NX
+  full.nx = d.NX;
+  full.ny = d.NY;
+  k_image_acc<<<cell_blocks(full), dim3(kCells, kGroups), 0, s>>>(full, S, R, img, add);
+  count_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s) {
   k_axpy<<<grid1d(n), 256, 0, s>>>(n, x, y);
   count_launch();

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(256) k_row_forward(const SpecArgs a, int nchun
   const long long bl = blockIdx.x / nchunk, b = a.b0 + bl;
   const int chunk = blockIdx.x - (int)(bl * nchunk);
   const int iw = (int)(b % a.d.nw);
-  const int nterm = (PRE == W_MASK || PRE == W_SCAT || PRE == W_SCAT_CONJ) ? a.nterm : 1;
+  const int nterm = multi_term(PRE) ? a.nterm : 1;
   for (int y = chunk * nwarp + warp; y < a.d.NY; y += nchunk * nwarp) {
     const long long roff = (b * a.d.NY + y) * NX;
     const long long loff = (bl * a.d.NY + y) * NX;
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_row_inverse(const SpecArgs a, int nchun
   const long long bl = blockIdx.x / nchunk, b = a.b0 + bl;
   const int chunk = blockIdx.x - (int)(bl * nchunk);
   const int iw = (int)(b % a.d.nw);
-  const int nterm = (POST == W_MASK || POST == W_SCAT || POST == W_SCAT_CONJ) ? a.nterm : 1;
+  const int nterm = multi_term(POST) ? a.nterm : 1;
   for (int y = chunk * nwarp + warp; y < a.d.NY; y += nchunk * nwarp) {
     const long long roff = (b * a.d.NY + y) * NX;
     const long long loff = (bl * a.d.NY + y) * NX;
@@ -292,6 +292,7 @@ cudaError_t generic_row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
     FWIX_ROWF(W_MASK)
     FWIX_ROWF(W_SCAT_CONJ)
     FWIX_ROWF(W_IC)
+    FWIX_ROWF(W_SMOOTH_CONJ)
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_ROWF
@@ -313,6 +314,8 @@ cudaError_t generic_row_inverse(const SpecArgs& a, int post, int post_taper, cud
     FWIX_ROWI(W_ONE)
     FWIX_ROWI(W_MASK)
     FWIX_ROWI(W_SCAT)
+    FWIX_ROWI(W_SMOOTH)
+    FWIX_ROWI(W_SMOOTH_DERIV)
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_ROWI

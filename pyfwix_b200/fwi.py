@@ -1,0 +1,289 @@
+"""FWI gradient with respect to slowness: modelling with the differentiable
+("smooth") depth step and its adjoint-state gradient, behind a
+``torch.autograd.Function``.
+
+The reference's gradient is ``ExtendedBorn.adjoint`` of the data residual
+(``fwix/workers.py:62-76``), a Born-linearised operator on s^2 per frequency.
+Its modelling selects the nearest reference slowness per cell
+(``propagator/src/selector.cu:29-35``), so the data depend on the slowness
+only through piecewise-constant labels and cannot be differentiated cell by
+cell.  Here the modelling keeps the reference's structure -- down pass with
+source injection and recording, reflection, up pass with recording
+(``propagator/src/Propagator.cpp:121-221``) -- with the smooth step
+(``fwix_smooth_step``: interpolation between the two bracketing references
+plus the split-step correction) so that J(s) = 1/2 |d(s) - d_obs|^2 has an exact
+gradient:
+
+  mu_iz = Rec_iz^H r + S_{iz-1}^H mu_{iz-1}                      (iz = 0 .. nz-1)
+  nu_iz = Rec_iz^H r + conj(R_iz) mu_iz + S_iz^H nu_{iz+1}       (iz = nz-1 .. 0)
+  dJ/ds = Re sum_{shots,w} [conj(mu_iz) dS_iz(U_{iz+1}) + conj(nu_{iz+1}) dS_iz(D_iz)]
+          + dR/ds terms Re sum conj(mu_iz) D_iz
+
+with D / U the down / up fields, R_iz = (s_iz - s_iz+1) / (s_iz + s_iz+1)
+(density 1, ``propagator/src/reflect.cu:42-45``) and the reference
+slownesses of each depth held fixed.  Every operator is a kernel of
+libfwix_b200.so; this module only sequences them.
+
+Storage: the down and up fields of every depth and the mu field of every depth
+are kept in device memory (``checkpoint=None``), or, with ``checkpoint=k``,
+only every k-th down / up / mu field is kept and each k-level segment is
+recomputed from its checkpoint when the backward sweeps reach it.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .plan import Plan
+
+
+def smooth_refs(s, nref, spread=1e-3):
+    """Reference slownesses per depth: nref values evenly spaced over the
+    slice's [min, max] (slices narrower than spread * mean are widened)."""
+    s = torch.as_tensor(s, dtype=torch.float64)
+    lo = s.amin(dim=(1, 2))
+    hi = s.amax(dim=(1, 2))
+    mid, half = 0.5 * (lo + hi), 0.5 * (hi - lo)
+    half = torch.maximum(half, 0.5 * spread * mid)
+    if nref == 1:
+        return mid[:, None]
+    return mid[:, None] + half[:, None] * torch.linspace(-1.0, 1.0, nref, dtype=torch.float64, device=s.device)
+
+
+def pad_edge(s, padx, pady):
+    """[nz][ny][nx] -> [nz][ny+pady][nx+padx], edge replicated."""
+    if padx == 0 and pady == 0:
+        return s
+    return torch.nn.functional.pad(s[None], (0, padx, 0, pady), mode="replicate")[0]
+
+
+def fold_edge(gp, ny, nx):
+    """Transpose of pad_edge."""
+    out = gp[:, :ny, :nx].clone()
+    out[:, :, nx - 1] += gp[:, :ny, nx:].sum(dim=2)
+    out[:, ny - 1, :] += gp[:, ny:, :nx].sum(dim=1)
+    out[:, ny - 1, nx - 1] += gp[:, ny:, nx:].sum(dim=(1, 2))
+    return out
+
+
+def _get(par, key, default=None):
+    v = par.get(key, default) if hasattr(par, "get") else getattr(par, key, default)
+    return default if v is None else v
+
+
+class SmoothFWI:
+    """One shot batch: plan, acquisition and stored fields.
+
+    ``par`` holds the grid axes (``ox, dx, oy, dy, oz, dz, ow, dw``; frequencies
+    in Hz) and the step keys (``nref, padx, pady, eps, taperx, tapery``);
+    optional ``refs`` ([nz][nref], fixed reference slownesses) and
+    ``checkpoint`` (k)."""
+
+    def __init__(self, shape, geometry, wavelet, par, device=None):
+        nz, ny, nx = shape
+        wav = torch.as_tensor(wavelet)
+        self.device = torch.device(device) if device is not None else (
+            wav.device if wav.is_cuda else torch.device("cuda", torch.cuda.current_device()))
+        self.par = par
+        nw = wav.shape[1]
+        from .CudaWEM import _remap_ids
+        s_ids, r_ids, ns = _remap_ids(geometry["s_ids"], geometry["r_ids"])
+        self.padx, self.pady = int(_get(par, "padx", 0)), int(_get(par, "pady", 0))
+        self.plan = Plan(nx=nx, ny=ny, nw=nw, ns=ns, nz=nz, dx=_get(par, "dx", 1.0), dy=_get(par, "dy", 1.0),
+                         dz=_get(par, "dz", 1.0), ox=_get(par, "ox", 0.0), oy=_get(par, "oy", 0.0),
+                         oz=_get(par, "oz", 0.0), ow=_get(par, "ow", 1.0), dw=_get(par, "dw", 1.0),
+                         padx=self.padx, pady=self.pady, nref=int(_get(par, "nref", 2)),
+                         eps=float(_get(par, "eps", 0.0)), taperx=int(_get(par, "taperx", 0)),
+                         tapery=int(_get(par, "tapery", 0)), step="pspi", device=self.device)
+        p = self.plan
+        self.src = p.traces(geometry["sx"], geometry["sy"], geometry["sz"], s_ids)
+        self.rec = p.traces(geometry["rx"], geometry["ry"], geometry["rz"], r_ids)
+        self.wavelet = wav.to(self.device, torch.complex64).contiguous()
+        self.ntrace = len(np.asarray(geometry["rx"]))
+        k = _get(par, "checkpoint", None)
+        self.k = None if k in (None, 0, 1) else int(k)
+        self.refs_fixed = _get(par, "refs", None)
+        p.ensure_workspace(L.WS_STEP)
+
+    # ---------------------------------------------------------------- state
+    def set_slowness(self, s):
+        """Binds s [nz][ny][nx] (float): padded slowness, references, and s^2 /
+        density 1 for the reflection coefficients."""
+        p = self.plan
+        s = torch.as_tensor(s).to(self.device, torch.float32).contiguous()
+        self.s = s
+        refs = self.refs_fixed if self.refs_fixed is not None else smooth_refs(s, p.nref)
+        self.refs = torch.as_tensor(refs).to(self.device, torch.float32)
+        p.set_smooth(pad_edge(s, self.padx, self.pady), self.refs)
+        s2 = (s.double() ** 2)[:, None].to(torch.complex64)
+        p.set_model(s2, torch.ones_like(s2))
+
+    def _field(self):
+        return torch.zeros(self.plan.wshape, dtype=torch.complex64, device=self.device)
+
+    # ---------------------------------------------------------------- modelling
+    def _down_step(self, iz, D, data, store):
+        p = self.plan
+        p.inject(self.src, iz, self.wavelet, D)
+        p.inject(self.rec, iz, data, D, adjoint=True)
+        if store is not None:
+            store.copy_(D)
+        p.smooth_step(iz, D, D)
+
+    def _up_step(self, iz, U, Dz, data):
+        p = self.plan
+        p.smooth_step(iz, U, U)
+        p.reflect(iz, Dz, U, add=True)
+        p.inject(self.rec, iz, data, U, adjoint=True)
+
+    def model(self, s, keep=True):
+        """Data [ntrace][nw] for slowness s; with keep the fields the gradient
+        needs are stored (all depths, or every k-th)."""
+        self.set_slowness(s)
+        p, nz = self.plan, self.plan.nz
+        data = torch.zeros((self.ntrace, p.nw), dtype=torch.complex64, device=self.device)
+        D = self._field()
+        if self.k is None:
+            self.Ds = [self._field() for _ in range(nz)]
+            for iz in range(nz):
+                self._down_step(iz, D, data, self.Ds[iz])
+            U = self._field()
+            self.Us = [None] * nz
+            for iz in range(nz - 1, -1, -1):
+                self._up_step(iz, U, self.Ds[iz], data)
+                if keep:
+                    self.Us[iz] = U.clone()
+            if not keep:
+                self.Ds = self.Us = None
+            return data
+        k = self.k
+        self.Dck = {}
+        for iz in range(nz):
+            if iz % k == 0:
+                self.Dck[iz] = D.clone()   # the field before injection at iz
+            self._down_step(iz, D, data, None)
+        self.Uck = {nz: self._field()}
+        U = self._field()
+        for a in reversed(range(0, nz, k)):
+            seg = self._segment_D(a)
+            for iz in range(min(a + k, nz) - 1, a - 1, -1):
+                self._up_step(iz, U, seg[iz - a], data)
+            self.Uck[a] = U.clone()
+        return data
+
+    def _segment_D(self, a):
+        """Down fields D_a .. D_{a+k-1} (after injection) recomputed from the
+        checkpoint at a, without recording."""
+        p, nz = self.plan, self.plan.nz
+        D = self.Dck[a].clone()
+        out = []
+        for iz in range(a, min(a + self.k, nz)):
+            p.inject(self.src, iz, self.wavelet, D)
+            out.append(D.clone())
+            p.smooth_step(iz, D, D)
+        return out
+
+    def _segment_U(self, a, Dseg):
+        """Up fields U_a .. U_{a+k} of a segment, from the checkpoint at a+k."""
+        p, nz = self.plan, self.plan.nz
+        top = min(a + self.k, nz)
+        U = self.Uck[top].clone()
+        out = {top: U.clone()}
+        for iz in range(top - 1, a - 1, -1):
+            p.smooth_step(iz, U, U)
+            p.reflect(iz, Dseg[iz - a], U, add=True)
+            out[iz] = U.clone()
+        return out
+
+    # ---------------------------------------------------------------- gradient
+    def gradient(self, res):
+        """dJ/ds [nz][ny][nx] (float32) for the residual res = d - d_obs, after
+        model(s, keep=True)."""
+        p, nz = self.plan, self.plan.nz
+        res = torch.as_tensor(res).to(self.device, torch.complex64).contiguous()
+        gpad = torch.zeros((nz, p.NY, p.NX), dtype=torch.float32, device=self.device)
+        crefl = torch.zeros((nz, p.ny, p.nx), dtype=torch.float32, device=self.device)
+        G = self._field()
+        if self.k is None:
+            Dget = lambda iz: self.Ds[iz]
+            Uget = lambda iz: self.Us[iz]
+            mus = [None] * nz
+            mu = self._field()
+            for iz in range(nz):
+                self._mu_level(iz, mu, res, Dget(iz), Uget(iz + 1) if iz + 1 < nz else None, gpad, crefl, G)
+                mus[iz] = mu.clone()
+            nu = self._field()
+            for iz in range(nz - 1, -1, -1):
+                self._nu_level(iz, nu, res, Dget(iz), mus[iz], gpad, G)
+        else:
+            k = self.k
+            mu = self._field()
+            self.Mck = {}
+            for a in range(0, nz, k):
+                self.Mck[a] = mu.clone()  # mu_{a-1} (zero for a = 0)
+                Dseg = self._segment_D(a)
+                Useg = self._segment_U(a, Dseg)
+                for iz in range(a, min(a + k, nz)):
+                    self._mu_level(iz, mu, res, Dseg[iz - a], Useg[iz + 1] if iz + 1 < nz else None,
+                                   gpad, crefl, G)
+            nu = self._field()
+            for a in reversed(range(0, nz, k)):
+                Dseg = self._segment_D(a)
+                mseg = []
+                m = self.Mck[a].clone()
+                for iz in range(a, min(a + k, nz)):
+                    if iz > 0:
+                        p.smooth_step(iz - 1, m, m, mode=L.SMOOTH_ADJ)
+                    p.inject(self.rec, iz, res, m)
+                    mseg.append(m.clone())
+                for iz in range(min(a + k, nz) - 1, a - 1, -1):
+                    self._nu_level(iz, nu, res, Dseg[iz - a], mseg[iz - a], gpad, G)
+        # reflection coefficients r_iz = (s_iz - s_iz+1) / (s_iz + s_iz+1)
+        s = self.s
+        grefl = torch.zeros_like(crefl)
+        if nz > 1:
+            s0, s1 = s[:-1], s[1:]
+            den = (s0 + s1) ** 2
+            grefl[:-1] += crefl[:-1] * (2 * s1 / den)
+            grefl[1:] += crefl[:-1] * (-2 * s0 / den)
+        return fold_edge(gpad, p.ny, p.nx) + grefl
+
+    def _mu_level(self, iz, mu, res, Dz, Unext, gpad, crefl, G):
+        p = self.plan
+        if iz > 0:
+            p.smooth_step(iz - 1, mu, mu, mode=L.SMOOTH_ADJ)
+        p.inject(self.rec, iz, res, mu)
+        if Unext is not None:
+            p.smooth_step(iz, Unext, G, mode=L.SMOOTH_DERIV)
+            p.correlate(mu, G, gpad[iz], add=True, padded=True)
+            p.correlate(mu, Dz, crefl[iz], add=True, padded=False)
+
+    def _nu_level(self, iz, nu, res, Dz, muz, gpad, G):
+        p = self.plan
+        if iz + 1 < p.nz:
+            p.smooth_step(iz, Dz, G, mode=L.SMOOTH_DERIV)
+            p.correlate(nu, G, gpad[iz], add=True, padded=True)
+        p.smooth_step(iz, nu, nu, mode=L.SMOOTH_ADJ)
+        p.reflect(iz, muz, nu, adjoint=True, add=True)
+        p.inject(self.rec, iz, res, nu)
+
+
+class FWIGradient(torch.autograd.Function):
+    """J = 1/2 |d(s) - d_obs|^2 for slowness s [nz][ny][nx] (float32, device);
+    backward returns dJ/ds.  ``FWIGradient.apply(s, wavelet, geometry, d_obs, par)``."""
+
+    @staticmethod
+    def forward(ctx, s, wavelet, geometry, d_obs, par):
+        prob = SmoothFWI(tuple(s.shape), geometry, wavelet, par, device=s.device if s.is_cuda else None)
+        data = prob.model(s.detach(), keep=True)
+        res = data - torch.as_tensor(d_obs).to(prob.device, torch.complex64)
+        ctx.prob, ctx.res = prob, res
+        J = 0.5 * torch.sum(res.real.double() ** 2 + res.imag.double() ** 2)
+        return J.to(s.dtype) if s.is_floating_point() else J
+
+    @staticmethod
+    def backward(ctx, gJ):
+        g = ctx.prob.gradient(ctx.res)
+        ctx.prob = ctx.res = None
+        return (gJ * g).to(gJ.dtype), None, None, None, None

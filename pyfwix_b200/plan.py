@@ -129,7 +129,34 @@ class Plan:
         self._keep["slow"], self._keep["den"] = slow, den
         return slow, den
 
+    def set_smooth(self, slow_pad, sref_real):
+        """Smooth step inputs: padded slowness [nz][NY][NX] and sorted real
+        reference slownesses [nz][nref] (float).  Also binds the references'
+        phase factors (s_r^2 for every frequency) through set_refs."""
+        sp = torch.as_tensor(slow_pad).to(device=self.device, dtype=torch.float32).contiguous()
+        sr = torch.as_tensor(sref_real).to(device=self.device, dtype=torch.float32).contiguous()
+        if tuple(sp.shape) != (self.nz, self.NY, self.NX) or tuple(sr.shape) != (self.nz, self.nref):
+            raise ValueError("smooth inputs must be [nz][NY][NX] and [nz][nref]")
+        if self.nref > 1 and not bool(torch.all(sr[:, 1:] > sr[:, :-1])):
+            raise ValueError("reference slownesses must increase strictly within each depth")
+        sref2 = (sr.double() ** 2)[:, :, None].expand(self.nz, self.nref, self.nw).to(torch.complex64)
+        labels = torch.zeros((self.nz, 1, self.NY, self.NX), dtype=torch.uint8, device=self.device)
+        self.set_refs(sref2, labels)
+        L.check(self.lib.fwix_plan_set_smooth(self._h, _p(sp), _p(sr)))
+        self._keep["sm_s"], self._keep["sm_ref"] = sp, sr
+        return sp, sr
+
     # ------------------------------------------------------------------ operators
+    def smooth_step(self, iz, inp, out, mode=L.SMOOTH_FWD, add=False):
+        self.ensure_workspace(L.WS_STEP)
+        L.check(self.lib.fwix_smooth_step(self._h, iz, mode, _p(inp), _p(out), int(add), _stream()))
+        return out
+
+    def correlate(self, a, b, out, add=False, padded=True):
+        """out (+)= Re sum_{shots, w} conj(a) b, [NY][NX] (padded) or [ny][nx]."""
+        L.check(self.lib.fwix_correlate(self._h, _p(a), _p(b), _p(out), int(add), int(padded), _stream()))
+        return out
+
     def fft2d(self, inp, out, inverse=False, add=False):
         self.ensure_workspace(L.WS_STEP)
         L.check(self.lib.fwix_fft2d(self._h, int(inverse), _p(inp), _p(out), int(add), _stream()))

@@ -1,0 +1,94 @@
+"""The differentiable step and the FWI gradient on the device against the FP64
+oracle (oracle/wem.py, smooth section): the smooth step forward / adjoint /
+slowness derivative per depth (1e-5 relative L2, and its dot test), and the
+adjoint-state gradient of J = 1/2 |d(s) - d_obs|^2 from full storage and from
+depth checkpoints, within the 1e-3 gradient tolerance of the FP64 oracle run of
+the same operator; FWIGradient's autograd backward equals that gradient."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import wem
+from tests.conftest import crandn
+from tests.gpu_helpers import rel, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(nx=32, ny=24, nw=4, nz=5, nref=3, padx=4, pady=4, seed=0):
+    rng = np.random.default_rng(seed)
+    g = wem.Grid(nx=nx, ny=ny, nw=nw, nz=nz, dx=10.0, dy=10.0, dz=10.0, ow=6.0, dw=3.0, padx=padx, pady=pady,
+                 nref=nref, taperx=3, tapery=3)
+    s = (1 / 1800.0) * (1 + 0.12 * rng.random((nz, ny, nx)))
+    s[nz // 2:] *= 1.25
+    geom = dict(sx=np.array([150.0], np.float32), sy=np.array([110.0], np.float32), sz=np.array([0.0], np.float32),
+                s_ids=np.array([0], np.int32), rx=np.linspace(0, 300, 14).astype(np.float32),
+                ry=np.full(14, 120.0, np.float32), rz=np.zeros(14, np.float32), r_ids=np.zeros(14, np.int32))
+    wav = crandn(rng, (1, nw))
+    par = dict(nref=nref, padx=padx, pady=pady, taperx=3, tapery=3, eps=0.0, ox=0.0, oy=0.0, oz=0.0, dx=10.0,
+               dy=10.0, dz=10.0, ow=6.0, dw=3.0)
+    return g, rng, s, geom, wav, par
+
+
+@pytest.mark.parametrize("nx,ny", [(32, 24), (60, 60)])
+def test_smooth_step_modes(nx, ny):
+    from pyfwix_b200 import _lib as L
+    from pyfwix_b200.fwi import SmoothFWI
+    g, rng, s, geom, wav, par = _case(nx=nx, ny=ny)
+    prob = SmoothFWI(s.shape, geom, wav, par)
+    prob.set_slowness(torch.as_tensor(s, dtype=torch.float32))
+    refs = prob.refs.cpu().numpy().astype(np.float64)
+    sp = wem.pad_edge(g, s.astype(np.float32).astype(np.float64))
+    p = prob.plan
+    x = crandn(rng, (1, g.nw, g.NY, g.NX))
+    y = crandn(rng, x.shape)
+    for iz in (0, 3):
+        out = torch.empty_like(to_dev(x))
+        got = to_host(p.smooth_step(iz, to_dev(x), out, mode=L.SMOOTH_FWD))
+        assert rel(got, wem.smooth_forward(g, refs[iz], sp[iz], x)) < 1e-5
+        got = to_host(p.smooth_step(iz, to_dev(y), out, mode=L.SMOOTH_ADJ))
+        assert rel(got, wem.smooth_adjoint(g, refs[iz], sp[iz], y)) < 1e-5
+        got = to_host(p.smooth_step(iz, to_dev(x), out, mode=L.SMOOTH_DERIV))
+        assert rel(got, wem.smooth_deriv(g, refs[iz], sp[iz], x)) < 1e-5
+        # dot test of the device pair
+        fx = to_host(p.smooth_step(iz, to_dev(x), torch.empty_like(out)))
+        ay = to_host(p.smooth_step(iz, to_dev(y), torch.empty_like(out), mode=L.SMOOTH_ADJ))
+        assert abs(np.vdot(y, fx) / np.vdot(ay, x) - 1) < 1e-5
+
+
+@pytest.mark.parametrize("checkpoint", [None, 2])
+def test_gradient_matches_oracle(checkpoint):
+    from pyfwix_b200.fwi import SmoothFWI
+    g, rng, s, geom, wav, par = _case()
+    s = s.astype(np.float32)
+    s_true = (s * (1 + 0.03 * np.exp(-((np.arange(g.nx) - 16) ** 2)[None, None, :] / 20.0))).astype(np.float32)
+    prob = SmoothFWI(s.shape, geom, wav, dict(par, checkpoint=checkpoint))
+    d_obs = prob.model(torch.as_tensor(s_true), keep=False)
+    refs = prob.refs  # references of s_true; hold them fixed for both runs
+    prob = SmoothFWI(s.shape, geom, wav, dict(par, checkpoint=checkpoint, refs=refs))
+    data = prob.model(torch.as_tensor(s), keep=True)
+    res = data - d_obs
+    grad = prob.gradient(res).cpu().numpy()
+    acq = wem.make_acquisition(g, geom)
+    refs64 = refs.cpu().numpy().astype(np.float64)
+    d_obs_o = wem.smooth_propagate(g, refs64, s_true.astype(np.float64), acq, wav)[0]
+    J_o, grad_o = wem.smooth_gradient(g, refs64, s.astype(np.float64), acq, wav, d_obs_o)
+    assert rel(to_host(data), wem.smooth_propagate(g, refs64, s.astype(np.float64), acq, wav)[0]) < 1e-4
+    assert rel(grad, grad_o) < 1e-3
+
+
+def test_autograd_function():
+    from pyfwix_b200.fwi import FWIGradient, SmoothFWI
+    g, rng, s, geom, wav, par = _case(nz=4)
+    s = s.astype(np.float32)
+    prob = SmoothFWI(s.shape, geom, wav, par)
+    d_obs = prob.model(torch.as_tensor(s * 1.01), keep=False)
+    par = dict(par, refs=prob.refs)
+    st = torch.as_tensor(s, device="cuda").requires_grad_(True)
+    J = FWIGradient.apply(st, torch.as_tensor(wav).cuda(), geom, d_obs, par)
+    J.backward()
+    acq = wem.make_acquisition(g, geom)
+    refs64 = prob.refs.cpu().numpy().astype(np.float64)
+    J_o, grad_o = wem.smooth_gradient(g, refs64, s.astype(np.float64), acq, wav, to_host(d_obs))
+    assert abs(float(J.detach()) / J_o - 1) < 1e-4
+    assert rel(st.grad.cpu().numpy(), grad_o) < 1e-3

@@ -350,3 +350,51 @@ def test_extended_born_taper_quirk(rng):
     gs, gr = wem.born_adjoint(g, st, acq, slow, den, bgd, bgu, d)
     ratio = np.vdot(d.ravel(), Am.ravel()) / np.vdot(gs.ravel(), ms.ravel())
     assert abs(ratio.real - 1) > 1e-6
+
+
+def test_smooth_step_dot_and_derivative(rng):
+    g = wem.Grid(nx=16, ny=12, nw=3, nz=3, dx=10, dy=10, dz=10, ow=5, dw=4, padx=4, pady=4, nref=3, taperx=2,
+                 tapery=2)
+    s = 1 / 1800 * (1 + 0.1 * rng.random((g.nz, g.ny, g.nx)))
+    refs = wem.smooth_refs(s, g.nref)
+    sp = wem.pad_edge(g, s)
+    x = crandn(rng, (2, g.nw, g.NY, g.NX))
+    y = crandn(rng, x.shape)
+    a = np.vdot(y, wem.smooth_forward(g, refs[1], sp[1], x))
+    b = np.vdot(wem.smooth_adjoint(g, refs[1], sp[1], y), x)
+    assert abs(a / b - 1) < 1e-12
+    k = (1, 5, 7)
+    h = 1e-7 * s[k]
+
+    def step_with(v):
+        ss = s.copy()
+        ss[k] = v
+        return wem.smooth_forward(g, refs[1], wem.pad_edge(g, ss)[1], x)
+    fd = (step_with(s[k] + h) - step_with(s[k] - h)) / (2 * h)
+    der = wem.smooth_deriv(g, refs[1], sp[1], x)
+    assert np.abs(fd[:, :, 5, 7] - der[:, :, 5, 7]).max() < 1e-6 * np.abs(der[:, :, 5, 7]).max()
+
+
+def test_smooth_gradient_matches_central_differences(rng):
+    """The adjoint-state gradient of the FP64 oracle against central finite
+    differences of its objective (references fixed), relative step 1e-6."""
+    g = wem.Grid(nx=16, ny=12, nw=3, nz=4, dx=10, dy=10, dz=10, ow=5, dw=4, padx=4, pady=4, nref=3, taperx=2,
+                 tapery=2)
+    s = 1 / 1800 * (1 + 0.1 * rng.random((g.nz, g.ny, g.nx)))
+    s[2:] *= 1.3
+    refs = wem.smooth_refs(s, g.nref)
+    geom = dict(sx=[70.0], sy=[50.0], sz=[0.0], s_ids=[0], rx=list(np.linspace(0, 150, 10)), ry=[60.0] * 10,
+                rz=[0.0] * 10, r_ids=[0] * 10)
+    acq = wem.make_acquisition(g, geom)
+    wav = crandn(rng, (1, g.nw))
+    d_obs = wem.smooth_propagate(g, refs, s * 1.02, acq, wav)[0]
+    J, grad = wem.smooth_gradient(g, refs, s, acq, wav, d_obs)
+    cells = [(0, 3, 4), (1, 6, 7), (2, 11, 15), (2, 5, 5), (3, 8, 2), (1, 0, 15)]
+    for k in cells:
+        h = 1e-6 * s[k]
+        sp_, sm_ = s.copy(), s.copy()
+        sp_[k] += h
+        sm_[k] -= h
+        fd = (wem.smooth_objective(g, refs, sp_, acq, wav, d_obs) -
+              wem.smooth_objective(g, refs, sm_, acq, wav, d_obs)) / (2 * h)
+        assert abs(grad[k] - fd) <= 1e-5 * max(abs(fd), 1e-3 * np.abs(grad).max()), (k, grad[k], fd)
