@@ -279,8 +279,9 @@ fwix_status step_chunk(fwix_plan* p, int kind, int iz, int dir, SpecArgs a, cuda
 }
 
 fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, float2* out, int add,
-                    cudaStream_t s) {
+                    cudaStream_t s, const float2* in2 = nullptr) {
   SpecArgs a0 = p->args(in, out, add);
+  a0.in2 = in2;  // the step of in + in2 (linear: one step instead of two)
   FWIX_TRY(phase_factors(p, iz, a0, s));
   return for_chunks(p, a0, [&](const SpecArgs& a) { return step_chunk(p, kind, iz, dir, a, s); });
 }
@@ -371,21 +372,6 @@ fwix_status do_record(fwix_plan* p, const fwix_traces* tr, int iz, const float2*
   const fwix::InjectLevel* L = level_of(tr, iz);
   if (!L) return FWIX_OK;
   return cu(fwix::launch_record(p->d, *L, wfld, traces, s), "record");
-}
-
-// ForwardScattering::cu_forward (Scattering.cpp:43-52): target += step_add(scatter(bg * image)).
-fwix_status fscat_fwd(fwix_plan* p, int iz_prop, const float2* bg, const float2* image, long long img_w,
-                      float2* target, cudaStream_t s) {
-  FWIX_TRY(do_scatter(p, iz_prop, 0, bg, p->wSC(), 0, image, img_w, s));
-  return do_step(p, p->desc.step_kind, iz_prop, FWIX_FWD, p->wSC(), target, 1, s);
-}
-
-// ForwardScattering::cu_adjoint (Scattering.cpp:54-61): gimage += ic_adj(scatter^T(step_adj_add(wfld))).
-fwix_status fscat_adj(fwix_plan* p, int iz_prop, const float2* bg, const float2* wfld, float2* gimage,
-                      long long img_w, cudaStream_t s) {
-  FWIX_TRY(do_step(p, p->desc.step_kind, iz_prop, FWIX_ADJ_ADD, wfld, p->wSC(), 0, s));
-  FWIX_TRY(do_scatter(p, iz_prop, 1, p->wSC(), p->wSC(), 0, nullptr, 0, s));
-  return cu(fwix::launch_ic_adj(p->d, bg, p->wSC(), gimage, img_w, 1, s), "imaging adjoint");
 }
 
 long long mslice(const fwix_plan* p) { return (long long)p->d.nw * p->d.ny * p->d.nx; }
@@ -895,39 +881,36 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
   float2* A = p->wA();
   float2* DR = p->wB();  // [nw][ny][nx] scratch for the linearised reflection
   const size_t wb = p->wbytes();
+  // The reference runs four sweeps each way (ExtendedBorn.cpp:152-453), every
+  // scattered source propagated by a step of its own.  All operators are linear,
+  // so sources that feed the same recursion are summed before one step:
+  // step(A) + step(scat) = step(A + scat).  The forward keeps one downward and one
+  // upward recursion, the adjoint one downward and one upward; the results equal
+  // the four-sweep operators up to float rounding.
+  float2* SC = p->wSC();
+  const bool pspi = k == FWIX_STEP_PSPI;
   if (!adjoint) {
     if (!add) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
-    // 1. down scattering (ExtendedBorn.cpp:152-178); store[iz] holds the field before step iz
+    // down scattering (ExtendedBorn.cpp:152-178): store[iz] = dD_iz, the field
+    // recorded at iz; dD_iz+1 = S_iz(dD_iz + Scat_iz(bg_down_iz * ds_iz))
     FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
     for (int iz = 0; iz < nz; ++iz) {
-      float2* cur = p->store(iz);
-      float2* next = iz < nz - 1 ? p->store(iz + 1) : A;
-      FWIX_TRY(do_record(p, rec, iz, cur, data, s));
-      if (iz == nz - 1) break;  // the last step feeds nothing that is recorded or stored
-      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, cur, next, 0, s));
-      FWIX_TRY(fscat_fwd(p, iz, bgd + iz * W, ds + iz * M, mw, next, s));
+      FWIX_TRY(do_record(p, rec, iz, p->store(iz), data, s));
+      if (iz == nz - 1) break;
+      FWIX_TRY(do_scatter(p, iz, 0, bgd + iz * W, SC, 0, ds + iz * M, mw, s));
+      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, p->store(iz), p->store(iz + 1), 0, s, SC));
     }
-    // 2. reflected up by the background (ExtendedBorn.cpp:210-238)
-    FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
-    for (int iz = nz - 1; iz >= 0; --iz) {
-      if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s));
-      FWIX_TRY(do_reflect(p, iz, 0, p->store(iz), A, 1, s));
-      FWIX_TRY(do_record(p, rec, iz, A, data, s));
-    }
-    // 3. up scattering (ExtendedBorn.cpp:282-311)
-    FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
-    for (int iz = nz - 1; iz >= 0; --iz) {
-      FWIX_TRY(do_record(p, rec, iz, A, data, s));
-      if (iz > 0) {
-        FWIX_TRY(do_step(p, k, iz - 1, FWIX_FWD, A, A, 0, s));
-        FWIX_TRY(fscat_fwd(p, iz - 1, bgu + iz * W, ds + iz * M, mw, A, s));
-      }
-    }
-    // 4. back scattering (ExtendedBorn.cpp:352-389)
+    // one upward recursion for the reflected down-scattered field (:210-238), the
+    // up scattering (:282-311) and the back scattering (:352-389):
+    //   Z_iz = S_iz(Z_iz+1 + Scat_iz(bg_up_iz+1 * ds_iz+1)) + R_iz dD_iz + bg_down_iz * dR_iz
     FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
     for (int iz = nz - 1; iz >= 0; --iz) {
       const int z1 = lower_iz(p, iz);
-      if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s));
+      if (iz < nz - 1) {
+        FWIX_TRY(do_scatter(p, iz, 0, bgu + (iz + 1) * W, SC, 0, ds + (iz + 1) * M, mw, s));
+        FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s, SC));
+      }
+      FWIX_TRY(do_reflect(p, iz, 0, p->store(iz), A, 1, s));
       FWIX_TRY(cu(fwix::launch_lin_reflect(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
                                            p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
                                            ds + z1 * M, dr + iz * M, dr + z1 * M, mw, DR, 0, s),
@@ -941,40 +924,56 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
     FWIX_CU(cudaMemsetAsync(ds, 0, (size_t)nz * M * sizeof(float2), s));
     FWIX_CU(cudaMemsetAsync(dr, 0, (size_t)nz * M * sizeof(float2), s));
   }
-  // up-scattering adjoint (ExtendedBorn.cpp:313-349); store[iz] keeps the adjoint
-  // up-going field that the reflected sweep consumes
+  // The scattering adjoints step with the add-version adjoint (no taper,
+  // Scattering.cpp:54-61), the recursions with the in-place adjoint (taper last,
+  // PSPI.cpp:85-103); for PSPI the second is the taper of the first, so one
+  // add-version step serves both.  (NSPS has no taper: the two coincide.)
+  SpecArgs ta = p->args(nullptr, nullptr, 0);
+  auto taper_into = [&](const float2* u, float2* out) {
+    return cu(fwix::launch_taper(ta, u, out, 0, s), "taper");
+  };
+  // downward: zeta_iz = Rec_iz^H d + S_iz-1^H zeta_iz-1 (the adjoint of the upward
+  // recursion), kept in store[iz]; it feeds the up-scattering adjoint (:313-349)
+  // and the back-scattering adjoint (:391-453), which needs no steps of its own
   FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
   for (int iz = 0; iz < nz; ++iz) {
+    const int z1 = lower_iz(p, iz);
     float2* cur = p->store(iz);
     if (iz > 0) {
-      float2* prev = p->store(iz - 1);
-      FWIX_TRY(fscat_adj(p, iz - 1, bgu + iz * W, prev, ds + iz * M, mw, s));
-      FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_INPL, prev, cur, 0, s));
+      if (pspi) {
+        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, p->store(iz - 1), SC, 0, s));
+        FWIX_TRY(taper_into(SC, cur));
+        FWIX_TRY(do_scatter(p, iz - 1, 1, SC, SC, 0, nullptr, 0, s));
+      } else {
+        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, p->store(iz - 1), cur, 0, s));
+        FWIX_TRY(do_scatter(p, iz - 1, 1, cur, SC, 0, nullptr, 0, s));
+      }
+      FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgu + iz * W, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
     }
     FWIX_TRY(do_inject(p, rec, iz, data, cur, s));
-  }
-  // reflected and direct down-scattering adjoints (ExtendedBorn.cpp:240-280 and
-  // :180-208) share the recursion, so their sources are summed in one sweep
-  FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
-  for (int iz = nz - 1; iz >= 0; --iz) {
-    if (iz < nz - 1) {
-      FWIX_TRY(fscat_adj(p, iz, bgd + iz * W, A, ds + iz * M, mw, s));
-      FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, A, A, 0, s));
-    }
-    FWIX_TRY(do_reflect(p, iz, 1, p->store(iz), A, 1, s));
-    FWIX_TRY(do_inject(p, rec, iz, data, A, s));
-  }
-  // back-scattering adjoint (ExtendedBorn.cpp:391-453)
-  FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
-  for (int iz = 0; iz < nz; ++iz) {
-    const int z1 = lower_iz(p, iz);
-    FWIX_TRY(do_inject(p, rec, iz, data, A, s));
-    FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgd + iz * W, A, DR, plane, 0, s), "imaging adjoint"));
+    FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgd + iz * W, cur, DR, plane, 0, s), "imaging adjoint"));
     FWIX_TRY(cu(fwix::launch_lin_reflect(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
                                          p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
                                          ds + z1 * M, dr + iz * M, dr + z1 * M, mw, DR, 1, s),
                 "linearised reflection adjoint"));
-    if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, A, A, 0, s));
+  }
+  // upward: eta_iz = Rec_iz^H d + conj(R_iz) zeta_iz + S_iz^H eta_iz+1, the adjoint of
+  // the down-scattering recursion (reflected :240-280 and direct :180-208)
+  FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+  for (int iz = nz - 1; iz >= 0; --iz) {
+    if (iz < nz - 1) {
+      if (pspi) {
+        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, SC, 0, s));
+        FWIX_TRY(taper_into(SC, A));
+        FWIX_TRY(do_scatter(p, iz, 1, SC, SC, 0, nullptr, 0, s));
+      } else {
+        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, A, 0, s));
+        FWIX_TRY(do_scatter(p, iz, 1, A, SC, 0, nullptr, 0, s));
+      }
+      FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgd + iz * W, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
+    }
+    FWIX_TRY(do_reflect(p, iz, 1, p->store(iz), A, 1, s));
+    FWIX_TRY(do_inject(p, rec, iz, data, A, s));
   }
   return FWIX_OK;
 }

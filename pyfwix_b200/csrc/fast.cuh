@@ -205,9 +205,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int n
   load_stage_tw<P>(c.tw, a.twx);
   __syncthreads();
   float2 raw[P::E];
-  const float2* src = a.in + (c.b * a.d.NY + (c.live ? c.y : 0)) * P::N;
+  const long long roff = (c.b * a.d.NY + (c.live ? c.y : 0)) * P::N;
+  const float2* src = a.in + roff;
 #pragma unroll
   for (int e = 0; e < P::E; ++e) raw[e] = c.live ? src[pos_first<P>(c.t, e)] : make_float2(0.f, 0.f);
+  if (a.in2 && c.live) {
+    const float2* src2 = a.in2 + roff;
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) raw[e] = cadd(raw[e], src2[pos_first<P>(c.t, e)]);
+  }
   const int nterm = multi_term(PRE) ? a.nterm : 1;
   uint8_t lab[P::E];
   if (PRE == W_MASK) {

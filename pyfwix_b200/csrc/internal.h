@@ -93,6 +93,7 @@ struct SpecArgs {
   // the intermediates t1 / t2 by the launch-local slice bl, term after term tstride
   // elements apart.
   const float2* in;    // row-pass input (W_IC: the background wavefield)
+  const float2* in2;   // optional second row-pass input added to `in` (NULL: none)
   float2* out;         // row-pass output
   int add;
   float2* t1;

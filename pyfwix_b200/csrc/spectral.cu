@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(256) k_row_forward(const SpecArgs a, int nchun
   for (int y = chunk * nwarp + warp; y < a.d.NY; y += nchunk * nwarp) {
     const long long roff = (b * a.d.NY + y) * NX;
     const long long loff = (bl * a.d.NY + y) * NX;
-    for (int x = lane; x < NX; x += 32) lineIn[x] = a.in[roff + x];
+    for (int x = lane; x < NX; x += 32) lineIn[x] = a.in2 ? cadd(a.in[roff + x], a.in2[roff + x]) : a.in[roff + x];
     __syncwarp();
     for (int t = 0; t < nterm; ++t) {
       for (int x = lane; x < NX; x += 32) lineA[x] = row_weight<PRE>(a, t, iw, y, x, lineIn[x]);
