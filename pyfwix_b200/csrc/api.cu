@@ -124,6 +124,7 @@ struct fwix_plan {
   size_t ws_bytes = 0;
   int nterm_max = 1;
   long long chunk = 1;  // slices per launch: the intermediates of one chunk fit in L2
+  float2* scat_tab = nullptr;     // scatter weights of one depth, [taylor+1][NY][NX]
   const float* sm_s = nullptr;    // smooth step: padded slowness [nz][NY][NX]
   const float* sm_ref = nullptr;  // smooth step: sorted real reference slownesses [nz][nref]
   float2* pcache = nullptr;   // phase-factor cache, nz depths (fwix_plan_set_phase_cache)
@@ -342,6 +343,11 @@ fwix_status scatter_chunk(int adjoint, const float2* image, long long img_w, Spe
 fwix_status do_scatter(fwix_plan* p, int iz, int adjoint, const float2* in, float2* out, int add,
                        const float2* image, long long img_w, cudaStream_t s) {
   SpecArgs a0 = scatter_args(p, iz, in, out, add);
+  if (p->m_w == 0) {
+    // one slowness for every frequency: the powers of s~ are a per-cell table
+    FWIX_TRY(cu(fwix::launch_scat_table(a0, p->scat_tab, s), "scatter weights"));
+    a0.scat_tab = p->scat_tab;
+  }
   return for_chunks(p, a0, [&](const SpecArgs& a) { return scatter_chunk(adjoint, image, img_w, a, s); });
 }
 
@@ -438,6 +444,8 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
   if (e == cudaSuccess) e = upload(&p->w, w);
   if (e == cudaSuccess) e = upload(&p->tapx, taper_table(p->d.NX, q.taperx));
   if (e == cudaSuccess) e = upload(&p->tapy, taper_table(p->d.NY, q.tapery));
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&p->scat_tab, (size_t)(q.taylor + 1) * p->d.slice * sizeof(float2));
   if (e != cudaSuccess) {
     fwix_plan_destroy(p);
     return fail(FWIX_ERR_CUDA, std::string("plan tables: ") + cudaGetErrorString(e));
@@ -448,7 +456,7 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
 
 fwix_status fwix_plan_destroy(fwix_plan* p) {
   if (!p) return FWIX_OK;
-  void* ptrs[] = {p->twx, p->twy, p->kx, p->ky, p->w2, p->w, p->tapx, p->tapy};
+  void* ptrs[] = {p->twx, p->twy, p->kx, p->ky, p->w2, p->w, p->tapx, p->tapy, p->scat_tab};
   for (void* v : ptrs)
     if (v) cudaFree(v);
   delete p;
@@ -879,7 +887,6 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
   float2* dr = (float2*)dden_v;
   float2* data = (float2*)data_v;
   float2* A = p->wA();
-  float2* DR = p->wB();  // [nw][ny][nx] scratch for the linearised reflection
   const size_t wb = p->wbytes();
   // The reference runs four sweeps each way (ExtendedBorn.cpp:152-453), every
   // scattered source propagated by a step of its own.  All operators are linear,
@@ -911,11 +918,10 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
         FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s, SC));
       }
       FWIX_TRY(do_reflect(p, iz, 0, p->store(iz), A, 1, s));
-      FWIX_TRY(cu(fwix::launch_lin_reflect(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
-                                           p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                           ds + z1 * M, dr + iz * M, dr + z1 * M, mw, DR, 0, s),
+      FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                              p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
+                                              ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bgd + iz * W, A, 1, s),
                   "linearised reflection"));
-      FWIX_TRY(cu(fwix::launch_ic_fwd(p->d, bgd + iz * W, DR, plane, A, 1, s), "imaging forward"));
       FWIX_TRY(do_record(p, rec, iz, A, data, s));
     }
     return FWIX_OK;
@@ -951,10 +957,9 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
       FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgu + iz * W, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
     }
     FWIX_TRY(do_inject(p, rec, iz, data, cur, s));
-    FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgd + iz * W, cur, DR, plane, 0, s), "imaging adjoint"));
-    FWIX_TRY(cu(fwix::launch_lin_reflect(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
-                                         p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                         ds + z1 * M, dr + iz * M, dr + z1 * M, mw, DR, 1, s),
+    FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                            p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
+                                            ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bgd + iz * W, cur, 1, s),
                 "linearised reflection adjoint"));
   }
   // upward: eta_iz = Rec_iz^H d + conj(R_iz) zeta_iz + S_iz^H eta_iz+1, the adjoint of

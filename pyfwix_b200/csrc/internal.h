@@ -72,6 +72,8 @@ struct SpecArgs {
   long long lab_w;
   const float2* slow;  // s^2 at this depth (unpadded), (iw, y, x) at slow[iw*slow_w + y*nx + x]
   long long slow_w;
+  // when slow_w == 0: s~^(-1/2-n) of the padded slice, [nterm][NY][NX] (NULL: computed per cell)
+  const float2* scat_tab;
   const float2* image; // imaging-condition image, (iw, y, x) at image[iw*img_w + y*nx + x] (W_IC)
   long long img_w;     // ny*nx, or 0 for one image shared by every frequency
   // cached forward phase factors of this depth (x norm), element (ref, iw, |kx|, |ky|)
@@ -118,6 +120,10 @@ cudaError_t generic_col_type_b(const SpecArgs& a, int qmode, cudaStream_t s);
 cudaError_t generic_col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add,
                             float scale, cudaStream_t s);
 
+// Powers s~^(-1/2-n), n < nterm, of the edge-padded slowness slice (slow_w == 0):
+// dst [nterm][NY][NX] (spectral.cu).
+cudaError_t launch_scat_table(const SpecArgs& a, float2* dst, cudaStream_t s);
+
 // Phase-factor cache of one depth (spectral.cu): dst [nref][nw][NX/2+1][NY/2+1].
 cudaError_t launch_phase_table(const SpecArgs& a, float2* dst, cudaStream_t s);
 
@@ -140,6 +146,12 @@ cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, con
                                const float2* r0, const float2* r1, long long mw, float2* dm0,
                                float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
                                int add, cudaStream_t s);
+// Linearised reflection fused with the imaging condition: forward wf (+)= bg * LR(dm)
+// on every shot; adjoint dm (+)= LR^H(sum_s conj(bg) wf).
+cudaError_t launch_lin_reflect_ic(const Dims& d, int adjoint, const float2* s0, const float2* s1,
+                                  const float2* r0, const float2* r1, long long mw, float2* dm0, float2* dm1,
+                                  float2* dm2, float2* dm3, long long dm_w, const float2* bg, float2* wf, int add,
+                                  cudaStream_t s);
 cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, float* img, int add,
                              cudaStream_t s);
 // img[y][x] (+)= Re sum_{s,w} conj(S) R over the padded NY x NX slice.

@@ -9,7 +9,7 @@ namespace fwix {
 // read from the unpadded slice with edge replication into the pad
 // (scatter.cu:61-106 slow_scale, :155-195 scale_by_iw, :240-277 pad_fwd).
 // s~^(-1/2-n) = (1/sqrt(s~)) (1/s~)^n with the principal root.
-__device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, int y, int x) {
+__device__ __forceinline__ float2 scat_power(const SpecArgs& a, int n, int iw, int y, int x) {
   const int xs = min(x, a.d.nx - 1), ys = min(y, a.d.ny - 1);
   const float2 s2 = a.slow[(long long)iw * a.slow_w + (long long)ys * a.d.nx + xs];
   const float2 st = make_float2(s2.x, s2.y - a.eps_scat * s2.x);
@@ -18,7 +18,20 @@ __device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, 
     const float2 is = cinv(st);
     for (int k = 0; k < n; ++k) p = cmul(p, is);
   }
+  return p;
+}
+
+__device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, int y, int x) {
   const float f = 0.5f * a.w[iw] * a.dz * a.coef[n];
+  if (a.scat_tab) return rot90<false>(cscale(a.scat_tab[((long long)n * a.d.NY + y) * a.d.NX + x], f));
+  const int xs = min(x, a.d.nx - 1), ys = min(y, a.d.ny - 1);
+  const float2 s2 = a.slow[(long long)iw * a.slow_w + (long long)ys * a.d.nx + xs];
+  const float2 st = make_float2(s2.x, s2.y - a.eps_scat * s2.x);
+  float2 p = cinv(csqrt_ref(st));
+  if (n > 0) {
+    const float2 is = cinv(st);
+    for (int k = 0; k < n; ++k) p = cmul(p, is);
+  }
   return rot90<false>(cscale(p, f));
 }
 
@@ -94,11 +107,10 @@ template <int QM>
 __device__ __forceinline__ float2 qmult(const SpecArgs& a, int t, int iw, int x, int y) {
   if (QM == Q_ONE) return make_float2(a.norm, 0.f);
   if (QM == Q_KPOW) {
-    // (|k| / w)^(2t) with |k| / w formed as in scatter.cu:49-50, the power by products
+    // (|k| / w)^(2t) (scatter.cu:49-50), the power by products
     if (t == 0) return make_float2(a.norm, 0.f);
     const float kx = a.kx[x], ky = a.ky[y];
-    const float r = sqrtf(kx * kx + ky * ky) / a.w[iw];
-    const float r2 = r * r;
+    const float r2 = (kx * kx + ky * ky) / a.w2[iw];  // (|k| / w)^2
     float p = r2;
     for (int k = 1; k < t; ++k) p *= r2;
     return make_float2(p * a.norm, 0.f);

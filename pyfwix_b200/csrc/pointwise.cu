@@ -153,10 +153,16 @@ __device__ __forceinline__ LinCoef lin_coef(float2 s0, float2 s1, float2 r0, flo
 // forward: dr[w, y, x] (+)= as dm0 - bs dm1 + ar dm3 - br dm2.  adjoint: the
 // conjugate-transposed sums into dm[w] (dm_w != 0) or into dm shared by every
 // frequency (dm_w == 0, summed over w).
+// With IC the reflectivity perturbation dr is not stored: the forward adds
+// bg * dr to the wavefield wf of every shot (the imaging-condition forward,
+// imaging_condition.cu:9-55) and the adjoint takes dr = sum_s conj(bg) wf (its
+// adjoint, :57-108), which saves writing and re-reading dr.
+template <bool IC>
 __global__ void __launch_bounds__(kCells * kGroups)
     k_lin_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
                   const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw, float2* dm0,
-                  float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr, int add) {
+                  float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr, int add,
+                  const float2* __restrict__ bg, float2* wf) {
   const Cell c = this_cell(d);
   const long long plane = (long long)d.ny * d.nx;
   const int wsum = adjoint && dm_w == 0;
@@ -171,10 +177,26 @@ __global__ void __launch_bounds__(kCells * kGroups)
     if (!adjoint) {
       float2 v = csub(cmul(cf.as, dm0[k]), cmul(cf.bs, dm1[k]));
       v = cadd(v, csub(cmul(cf.ar, dm3[k]), cmul(cf.br, dm2[k])));
-      dr[i] = add ? cadd(dr[i], v) : v;
+      if (IC) {
+        for (int sh = 0; sh < d.ns; ++sh) {
+          const long long q = wf_index(d, sh, iw, c);
+          wf[q] = cadd(wf[q], cmul(bg[q], v));
+        }
+      } else {
+        dr[i] = add ? cadd(dr[i], v) : v;
+      }
       continue;
     }
-    const float2 gi = dr[i];
+    float2 gi;
+    if (IC) {
+      gi = make_float2(0.f, 0.f);
+      for (int sh = 0; sh < d.ns; ++sh) {
+        const long long q = wf_index(d, sh, iw, c);
+        gi = cadd(gi, cmul_conj(wf[q], bg[q]));
+      }
+    } else {
+      gi = dr[i];
+    }
     const float2 t0 = cmul_conj(gi, cf.as), t1 = cscale(cmul_conj(gi, cf.bs), -1.f);
     const float2 t3 = cmul_conj(gi, cf.ar), t2 = cscale(cmul_conj(gi, cf.br), -1.f);
     if (wsum) {
@@ -317,7 +339,18 @@ cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, con
                                const float2* r0, const float2* r1, long long mw, float2* dm0,
                                float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
                                int add, cudaStream_t s) {
-  k_lin_reflect<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3, dm_w, dr, add);
+  k_lin_reflect<false><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1,
+                                                                       dm2, dm3, dm_w, dr, add, nullptr, nullptr);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lin_reflect_ic(const Dims& d, int adjoint, const float2* s0, const float2* s1,
+                                  const float2* r0, const float2* r1, long long mw, float2* dm0, float2* dm1,
+                                  float2* dm2, float2* dm3, long long dm_w, const float2* bg, float2* wf, int add,
+                                  cudaStream_t s) {
+  k_lin_reflect<true><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1,
+                                                                      dm2, dm3, dm_w, nullptr, add, bg, wf);
   count_launch();
   return cudaGetLastError();
 }

@@ -476,6 +476,22 @@ cudaError_t launch_select(const SpecArgs& a, int value, const float2* in, float2
   return cudaGetLastError();
 }
 
+__global__ void k_scat_table(const SpecArgs a, float2* dst) {
+  const long long n = (long long)a.nterm * a.d.slice;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i / a.d.slice);
+    const long long yx = i - (long long)t * a.d.slice;
+    const int y = (int)(yx / a.d.NX), x = (int)(yx - (long long)y * a.d.NX);
+    dst[i] = scat_power(a, t, 0, y, x);
+  }
+}
+
+cudaError_t launch_scat_table(const SpecArgs& a, float2* dst, cudaStream_t s) {
+  k_scat_table<<<grid1d((long long)a.nterm * a.d.slice), 256, 0, s>>>(a, dst);
+  count_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_taper(const SpecArgs& a, const float2* in, float2* out, int add, cudaStream_t s) {
   k_weight<W_TAPER><<<grid1d(a.d.wfld), 256, 0, s>>>(a, 0, in, out, add);
   count_launch();
