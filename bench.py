@@ -51,6 +51,8 @@ def args_():
     ap.add_argument("--nz", type=int, default=None, help="override depth count (quick runs only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fwi", action="store_true", help="skip the FWI-gradient timing")
+    ap.add_argument("--fwi-nz", type=int, default=None, help="depth levels of the FWI workload (quick runs)")
     return ap.parse_args()
 
 
@@ -208,6 +210,43 @@ def step_roofline(st, w, reps=20):
     return e0.elapsed_time(e1) / 1e3 / reps
 
 
+def fwi_gradient_timing(device, nz=None, checkpoint="auto"):
+    """Seconds per shot of the autograd FWI gradient (FWIGradient forward =
+    modelling + misfit, backward = adjoint-state gradient) on one shot of the
+    384 x 384 x 300 workload, timed with CUDA events; the observed data are
+    modelled first in the true model (untimed)."""
+    import torch
+
+    from pyfwix_b200 import workloads
+    from pyfwix_b200.fwi import FWIGradient, SmoothFWI
+    w, s_true, s0 = workloads.config4(nz=nz)
+    par = dict(nref=w.nref, padx=0, pady=0, taperx=w.taperx, tapery=w.tapery, eps=0.0, ox=w.ox, oy=w.oy,
+               oz=w.oz, dx=w.dx, dy=w.dy, dz=w.dz, ow=w.ow, dw=w.dw, checkpoint=checkpoint)
+    wav = torch.as_tensor(w.wavelet).to(device)
+    prob = SmoothFWI(s_true.shape, w.geom, wav, dict(par, checkpoint=None), device=device)
+    d_obs = prob.model(torch.as_tensor(s_true), keep=False)
+    refs = prob.refs.clone()
+    del prob
+    torch.cuda.empty_cache()
+    par["refs"] = refs
+    s = torch.as_tensor(s0, device=device).requires_grad_(True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    J = FWIGradient.apply(s, wav, w.geom, d_obs, par)
+    ev[1].record()
+    J.backward()
+    ev[2].record()
+    torch.cuda.synchronize()
+    t_fwd, t_bwd = ev[0].elapsed_time(ev[1]) / 1e3, ev[1].elapsed_time(ev[2]) / 1e3
+    assert torch.isfinite(s.grad).all()
+    cells = w.nx * w.ny * w.nw * w.nz
+    return {"workload": w.name + ("" if nz is None else f" (nz={w.nz})") + ", 1 shot of 8",
+            "s_per_shot": t_fwd + t_bwd, "forward_s_per_shot": t_fwd, "gradient_s_per_shot": t_bwd,
+            "grad_over_forward": (t_fwd + t_bwd) / t_fwd, "checkpoint": FWIGradient.last_storage,
+            "forward_gcell_steps_per_s": 2 * cells / t_fwd / 1e9, "objective": float(J.detach())}
+
+
 # ----------------------------------------------------------------------------- CPU arm
 
 class CpuBorn:
@@ -358,6 +397,12 @@ def main():
             "traffic": traffic, "peak_source": peak_kind,
             "kernel": "NSPS depth step (row pass + column pass + row pass), 256x256x128",
             "step_ms": tstep * 1e3, "alg_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP}
+    bg_gb = st["bd"].numel() * 8 / 1e9
+    fwi = None
+    if not a.no_fwi:
+        del st
+        torch.cuda.empty_cache()
+        fwi = fwi_gradient_timing(device, nz=a.fwi_nz)
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu:
         cpu = cpu_baseline()
@@ -368,8 +413,9 @@ def main():
                 "config": {"workload": w.name + ("" if a.nz is None else f" (nz={w.nz})"),
                            "global_batch": ws, "seq_len": None, "parallelism": f"shot replicas x{ws}",
                            "l2": "inputs larger than L2 (background wavefields 2 x %.1f GB)"
-                                 % (st["bd"].numel() * 8 / 1e9)},
-                "gpu_launches": launches, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+                                 % bg_gb},
+                "gpu_launches": launches, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "fwi_grad": fwi}
         print(json.dumps(line), flush=True)
     if ws > 1:
         tdist.destroy_process_group()

@@ -221,8 +221,28 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int n
 #pragma unroll
     for (int e = 0; e < P::E; ++e) lab[e] = c.live ? lrow[pos_first<P>(c.t, e)] : 255;
   }
+  // smooth weights: terms that no sample of the warp's rows supports are zero rows
+  unsigned used = 0xffffffffu;
+  if (PRE == W_SMOOTH_CONJ && a.sm_n <= 32) {
+    unsigned mine = 0;
+    const float* srow = a.sm_s + (long long)(c.live ? c.y : 0) * P::N;
+#pragma unroll
+    for (int e = 0; e < P::E; ++e)
+      if (c.live) mine |= hat_support(a.sm_ref, a.sm_n, srow[pos_first<P>(c.t, e)]);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
+    used = mine;
+  }
   for (int term = 0; term < nterm; ++term) {
     float2 v[P::E];
+    if (!((used >> (term & 31)) & 1u)) {
+      if (c.live) {
+        float2* dst = a.t1 + (long long)term * a.tstride + (c.bl * a.d.NY + c.y) * P::N;
+#pragma unroll
+        for (int e = 0; e < P::E; ++e) dst[pos_last<P>(c.t, e)] = make_float2(0.f, 0.f);
+      }
+      continue;
+    }
 #pragma unroll
     for (int e = 0; e < P::E; ++e) {
       if (PRE == W_MASK)
@@ -266,6 +286,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_inv(const SpecArgs a, int n
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
     used = nterm > 32 ? 0xffffffffu : mine;
+  } else if ((POST == W_SMOOTH || POST == W_SMOOTH_DERIV) && a.sm_n <= 32) {
+    unsigned mine = 0;
+    const float* srow = a.sm_s + (long long)(c.live ? c.y : 0) * P::N;
+#pragma unroll
+    for (int e = 0; e < P::E; ++e)
+      if (c.live) mine |= hat_support(a.sm_ref, a.sm_n, srow[pos_first<P>(c.t, e)]);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
+    used = mine;
   }
   auto next_term = [&](int from) {
     int k = from;

@@ -69,6 +69,16 @@ __device__ __forceinline__ Hat hat_weight(const float* ref, int n, int t, float 
   return h;
 }
 
+// Terms whose hat weight or its derivative can be nonzero at slowness s (bit r
+// for reference r; only the bracketing pair, or one end reference outside).
+__device__ __forceinline__ unsigned hat_support(const float* ref, int n, float s) {
+  if (n == 1 || s <= ref[0]) return 1u;
+  if (s >= ref[n - 1]) return 1u << (n - 1);
+  int j = 0;
+  while (j < n - 2 && s >= ref[j + 1]) ++j;
+  return 3u << j;
+}
+
 // w_r SS_r (W_SMOOTH), w_r conj(SS_r) (W_SMOOTH_CONJ) or (w_r' - i w dz w_r) SS_r
 // (W_SMOOTH_DERIV) for reference t at cell (y, x) of frequency iw.
 template <int W>

@@ -27,7 +27,9 @@ libfwix_b200.so; this module only sequences them.
 Storage: the down and up fields of every depth and the mu field of every depth
 are kept in device memory (``checkpoint=None``), or, with ``checkpoint=k``,
 only every k-th down / up / mu field is kept and each k-level segment is
-recomputed from its checkpoint when the backward sweeps reach it.
+recomputed from its checkpoint when the backward sweeps reach it;
+``checkpoint="auto"`` (the default) stores everything when it fits in device
+memory and picks the interval otherwise.
 """
 from __future__ import annotations
 
@@ -78,7 +80,7 @@ class SmoothFWI:
     ``par`` holds the grid axes (``ox, dx, oy, dy, oz, dz, ow, dw``; frequencies
     in Hz) and the step keys (``nref, padx, pady, eps, taperx, tapery``);
     optional ``refs`` ([nz][nref], fixed reference slownesses) and
-    ``checkpoint`` (k)."""
+    ``checkpoint`` (k, None for full storage, or "auto")."""
 
     def __init__(self, shape, geometry, wavelet, par, device=None):
         nz, ny, nx = shape
@@ -101,10 +103,27 @@ class SmoothFWI:
         self.rec = p.traces(geometry["rx"], geometry["ry"], geometry["rz"], r_ids)
         self.wavelet = wav.to(self.device, torch.complex64).contiguous()
         self.ntrace = len(np.asarray(geometry["rx"]))
-        k = _get(par, "checkpoint", None)
-        self.k = None if k in (None, 0, 1) else int(k)
+        self.k = self._storage(_get(par, "checkpoint", "auto"))
         self.refs_fixed = _get(par, "refs", None)
         p.ensure_workspace(L.WS_STEP)
+
+    def _storage(self, k):
+        """None (every depth stored) or the checkpoint interval.  "auto" stores every
+        depth when the down, up and mu fields of all depths fit in 60 % of the
+        free device memory, else takes the smallest interval in 4, 8, ..., 256
+        whose checkpoints plus segment buffers fit."""
+        if k != "auto":
+            return None if k in (None, 0, 1) else int(k)
+        p = self.plan
+        wb = p.ns * p.nw * p.NY * p.NX * 8
+        free, _ = torch.cuda.mem_get_info(self.device)
+        budget = 0.6 * free
+        if 3 * p.nz * wb + 4 * wb <= budget:
+            return None
+        for k in (4, 8, 16, 32, 64, 128, 256):
+            if (3 * (-(-p.nz // k)) + 2 * k + 4) * wb <= budget:
+                return k
+        return 256
 
     # ---------------------------------------------------------------- state
     def set_slowness(self, s):
@@ -273,9 +292,12 @@ class FWIGradient(torch.autograd.Function):
     """J = 1/2 |d(s) - d_obs|^2 for slowness s [nz][ny][nx] (float32, device);
     backward returns dJ/ds.  ``FWIGradient.apply(s, wavelet, geometry, d_obs, par)``."""
 
+    last_storage = None  # "every depth" or the checkpoint interval of the last call
+
     @staticmethod
     def forward(ctx, s, wavelet, geometry, d_obs, par):
         prob = SmoothFWI(tuple(s.shape), geometry, wavelet, par, device=s.device if s.is_cuda else None)
+        FWIGradient.last_storage = "every depth" if prob.k is None else prob.k
         data = prob.model(s.detach(), keep=True)
         res = data - torch.as_tensor(d_obs).to(prob.device, torch.complex64)
         ctx.prob, ctx.res = prob, res

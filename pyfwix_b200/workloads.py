@@ -10,6 +10,11 @@ config2: Born forward + adjoint with NSPS, one shot, 256 x 256 x 200, nw = 128
          noise (sigma 5 cells) scaled to max |p| = 0.05; reflectivity = 5 flat
          layers at depths drawn from {10..189}, amplitudes U(-0.1, 0.1) relative to
          the background s^2.
+config4: FWI gradient, PSPI smooth step, 384 x 384 x 300, nw = 96 (3-30 Hz), nref 4,
+         true model v = 1500 + 0.5 z times (1 + three Gaussian anomalies of +-8 %,
+         sigma 150 m, at seeded centres), starting model the background; 8 sources
+         at seeded surface positions (shot s uses source s), receivers on every
+         surface node, depth checkpoints every 16 levels.
 
 Seeds are ``numpy.random.default_rng(1000 + config_index)``.
 """
@@ -123,6 +128,32 @@ def config2(nz=None, nw=None, seed=1001):
                   sz=np.array([0.0], np.float32), s_ids=np.array([0], np.int32), **w.surface_receivers())
     w.wavelet = ricker_spectrum(w.freqs)[None, :].astype(np.complex64)
     return w
+
+
+def config4(nz=None, shot=0, seed=1003):
+    """FWI gradient workload; returns (Workload with the starting model, true slowness
+    s_true [nz][ny][nx] float32, starting slowness s0 [nz][ny][nx] float32)."""
+    rng = np.random.default_rng(seed)
+    nz_full = 300
+    w = Workload(name="fwi-smooth-pspi-384x384x300-nw96", nx=384, ny=384, nz=nz or nz_full, dx=10.0, dy=10.0,
+                 dz=10.0, nw=96, ow=3.0, dw=27.0 / 95.0, nref=4, step="pspi", taperx=20, tapery=20)
+    Z, Y, X = _coords(w)
+    v0 = 1500.0 + 0.5 * Z
+    pert = np.zeros_like(v0)
+    for _ in range(3):
+        cx, cy = rng.uniform(0.25, 0.75, 2) * np.array([w.nx * w.dx, w.ny * w.dy])
+        cz = rng.uniform(0.25, 0.75) * nz_full * w.dz
+        amp = rng.choice([-0.08, 0.08])
+        pert += amp * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2 + (Z - cz) ** 2) / (2 * 150.0 ** 2))
+    s_true = (1.0 / (v0 * (1 + pert))).astype(np.float32)
+    s0 = (1.0 / v0).astype(np.float32)
+    src = rng.uniform(0.1, 0.9, size=(8, 2)) * np.array([w.nx * w.dx, w.ny * w.dy])
+    sx, sy = src[shot]
+    w.geom = dict(sx=np.array([sx], np.float32), sy=np.array([sy], np.float32), sz=np.array([0.0], np.float32),
+                  s_ids=np.array([0], np.int32), **w.surface_receivers())
+    w.wavelet = ricker_spectrum(w.freqs)[None, :].astype(np.complex64)
+    w.slow2 = s0 ** 2
+    return w, s_true, s0
 
 
 CONFIGS = {"config1": config1, "config2": config2}
