@@ -53,6 +53,8 @@ def args_():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fwi", action="store_true", help="skip the FWI-gradient timing")
     ap.add_argument("--fwi-nz", type=int, default=None, help="depth levels of the FWI workload (quick runs)")
+    ap.add_argument("--profile-step", choices=["pspi", "nsps", "pspi-adj", "nsps-adj"], default=None,
+                    help="run one depth step of the workload's wavefield and exit (for ncu captures)")
     return ap.parse_args()
 
 
@@ -334,10 +336,36 @@ def run_reference(a):
 
 # ----------------------------------------------------------------------------- main
 
+def profile_step(a):
+    """One depth step on the workload's wavefield (random data), nothing else:
+    the launch a kernel profiler captures."""
+    import torch
+
+    from pyfwix_b200 import _lib as L
+    from pyfwix_b200 import refsampler, workloads
+    from pyfwix_b200.plan import Plan
+    torch.cuda.set_device(0)
+    w = workloads.CONFIGS[a.config](nz=2)
+    kind, adj = a.profile_step.split("-")[0], a.profile_step.endswith("-adj")
+    kw = w.plan_kwargs()
+    kw["step"] = kind
+    plan = Plan(ns=1, device="cuda", **kw)
+    s2 = torch.as_tensor(w.slow2)[:, None].cuda()
+    sref, labels = refsampler.sample(s2, w.nref, w.padx, w.pady)
+    plan.set_refs(refsampler.expand_refs(sref, w.nw), labels)
+    x = torch.randn(plan.wshape, dtype=torch.complex64, device="cuda")
+    plan.step(0, x, x, direction=L.ADJ_INPL if adj else L.FWD)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_step": a.profile_step, "workload": w.name, "ok": True}))
+
+
 def main():
     a = args_()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.profile_step:
+        profile_step(a)
         return
     import torch
     ws, rank, local = dist()

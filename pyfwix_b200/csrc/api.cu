@@ -124,6 +124,7 @@ struct fwix_plan {
   size_t ws_bytes = 0;
   int nterm_max = 1;
   long long chunk = 1;  // slices per launch: the intermediates of one chunk fit in L2
+  bool fused = false;   // 256 x 256 slices: one-launch cluster step (fused256.cu), opt-in
   float2* scat_tab = nullptr;     // scatter weights of one depth, [taylor+1][NY][NX]
   const float* sm_s = nullptr;    // smooth step: padded slowness [nz][NY][NX]
   const float* sm_ref = nullptr;  // smooth step: sorted real reference slownesses [nz][nref]
@@ -255,6 +256,7 @@ fwix_status step_chunk(fwix_plan* p, int kind, int iz, int dir, SpecArgs a, cuda
   a.lab = p->labels + iz * p->lab_z;
   a.lab_w = p->lab_w;
   a.nterm = p->desc.nref;
+  if (p->fused && fwix::fused_step_available()) return cu(fwix::fused_step(a, kind, dir, s), "fused step");
   if (kind == FWIX_STEP_PSPI) {
     if (dir == FWIX_FWD) {
       FWIX_TRY(cu(fwix::row_forward(a, fwix::W_TAPER, s), "pspi row pass"));
@@ -426,6 +428,12 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
     long long c = (long long)q.ns * q.nw;
     if (const char* env = getenv("FWIX_CHUNK_SLICES")) c = atoll(env);
     p->chunk = std::max(1LL, std::min(c, (long long)q.ns * q.nw));
+  }
+  {
+    // The one-launch cluster step is opt-in (FWIX_FUSED=1): measured on B200 it
+    // is slower than the three-launch step at these sizes.
+    const char* env = getenv("FWIX_FUSED");
+    p->fused = p->d.NX == 256 && p->d.NY == 256 && env && env[0] == '1';
   }
   std::vector<float> w2(q.nw), w(q.nw);
   for (int i = 0; i < q.nw; ++i) {

@@ -124,6 +124,11 @@ cudaError_t generic_col_fft(const SpecArgs& a, int inverse, const float2* in, fl
 // dst [nterm][NY][NX] (spectral.cu).
 cudaError_t launch_scat_table(const SpecArgs& a, float2* dst, cudaStream_t s);
 
+// One PSPI / NSPS depth step of 256 x 256 slices in one cluster launch
+// (fused256.cu); available when the device runs 8-CTA clusters of it.
+bool fused_step_available();
+cudaError_t fused_step(const SpecArgs& a, int kind, int dir, cudaStream_t s);
+
 // Phase-factor cache of one depth (spectral.cu): dst [nref][nw][NX/2+1][NY/2+1].
 cudaError_t launch_phase_table(const SpecArgs& a, float2* dst, cudaStream_t s);
 

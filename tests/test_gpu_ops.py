@@ -92,6 +92,8 @@ STEP_CASES = [
     dict(nx=380, ny=100, padx=4, pady=0, eps=0.01, complex_refs=True, labels_per_w=False),
     dict(nx=32, ny=28, padx=8, pady=4, eps=0.02, complex_refs=True, labels_per_w=False),
     dict(nx=100, ny=60, padx=28, pady=4, eps=0.0, complex_refs=False, labels_per_w=False),
+    dict(nx=256, ny=256, padx=0, pady=0, eps=0.0, complex_refs=False, labels_per_w=False),
+    dict(nx=248, ny=252, padx=8, pady=4, eps=0.01, complex_refs=True, labels_per_w=True),
 ]
 
 
@@ -129,6 +131,27 @@ def test_nsps_step(case):
         assert rel(y, wem.nsps_forward(g, sref[iz], lab[iz], x, d0)) < TOL
         y = to_host(p.step(iz, to_dev(x), to_dev(d0), direction=1, add=True))
         assert rel(y, wem.nsps_adjoint(g, sref[iz], lab[iz], x, d0)) < TOL
+
+
+@pytest.mark.parametrize("kind", ["pspi", "nsps"])
+def test_fused_step_matches_three_launch_step(kind, monkeypatch):
+    """The 256 x 256 cluster step against the three-launch step on the same
+    inputs (FWIX_FUSED=1 at plan creation selects the former), in place and
+    with accumulation, every direction."""
+    g, rng, sref, labels, _, _ = make_case(nx=256, ny=256, nw=3, nz=2, nref=4, padx=0, pady=0, eps=0.01,
+                                           complex_refs=True, labels_per_w=False, taperx=20, tapery=20)
+    p_three = make_plan(g, 2, sref, labels, step=kind)
+    monkeypatch.setenv("FWIX_FUSED", "1")
+    p_fused = make_plan(g, 2, sref, labels, step=kind)
+    x = wavefield(rng, 2, g)
+    d0 = wavefield(rng, 2, g)
+    for direction in (0, 1, 2):
+        a = to_host(p_fused.step(1, to_dev(x), to_dev(d0), direction=direction, add=True))
+        b = to_host(p_three.step(1, to_dev(x), to_dev(d0), direction=direction, add=True))
+        assert rel(a, b) < 1e-5, (direction, rel(a, b))
+        xin = to_dev(x)
+        a = to_host(p_fused.step(0, xin, xin, direction=direction))
+        assert rel(a, to_host(p_three.step(0, to_dev(x), to_dev(d0), direction=direction))) < 1e-5
 
 
 def test_step_dot_product():
