@@ -34,10 +34,15 @@ struct Radices {
   }
 };
 
-template <int N_, int E_, class RS>
+// SW selects the sample placement of the line exchanges: 0 puts sample p at
+// p ^ ((p >> 3) & 15), 1 at p + (p >> 4) (conflict-free for radix-16 stages on
+// 16-lane lines); LINE_EXTRA is the room the second needs past N.
+template <int N_, int E_, class RS, int SW_ = 0>
 struct Plan {
   static constexpr int N = N_;
   static constexpr int E = E_;
+  static constexpr int SW = SW_;
+  static constexpr int LINE_EXTRA = SW_ == 1 ? N_ / 16 : 0;
   static constexpr int T = N_ / E_;    // lanes per line
   static constexpr int G = 32 / T;     // lines per warp
   static constexpr int NS = RS::NS;
@@ -54,6 +59,10 @@ struct Order {
 };
 
 __device__ __forceinline__ int swz(int p) { return p ^ ((p >> 3) & 15); }
+template <class P>
+__device__ __forceinline__ int xswz(int p) {  // exchange placement of plan P
+  return P::SW == 1 ? p + (p >> 4) : swz(p);
+}
 
 // Twiddles in shared memory, one table per stage and order: stage S (span Ns,
 // radix R) reads W_N^(k r N / (Ns R)) for k = j mod Ns and r = 1..R-1 at
@@ -137,11 +146,11 @@ __device__ __forceinline__ void stages(float2 (&v)[P::E], int t, const float2* _
       const int j = t + P::T * b;
       const int base = (j / Ns) * Ns * R + (j % Ns);
 #pragma unroll
-      for (int r = 0; r < R; ++r) line[swz(base + r * Ns)] = v[b * R + r];
+      for (int r = 0; r < R; ++r) line[xswz<P>(base + r * Ns)] = v[b * R + r];
     }
     __syncwarp();
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) v[e] = line[swz(lpos<P, R2>(t, e))];
+    for (int e = 0; e < P::E; ++e) v[e] = line[xswz<P>(lpos<P, R2>(t, e))];
     stages<P, REV, INV, S + 1>(v, t, tw, line);
   }
 }
@@ -168,7 +177,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 template <class P>
 struct RowGeo {
-  static constexpr int LINE = P::N + (P::T < 32 ? 8 : 0);  // shared-memory stride between lines
+  // shared-memory stride between lines
+  static constexpr int LINE = P::N + (P::LINE_EXTRA > (P::T < 32 ? 8 : 0) ? P::LINE_EXTRA : (P::T < 32 ? 8 : 0));
   static constexpr int ROWS = kWarps * P::G;                // rows per CTA
   static size_t smem() { return ((size_t)kWarps * P::G * LINE + tw_size<P>()) * sizeof(float2); }
 };
@@ -671,8 +681,10 @@ cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* ou
 }  // namespace fast
 }  // namespace fwix
 
-// One translation unit per line length instantiates the launchers of its plan.
-#define FWIX_FAST_INSTANTIATE(PLAN, TAG)                                                                   \
+// One translation unit per line length instantiates the launchers of its plan
+// (FWIX_FAST_INSTANTIATE2: one plan for the row passes, another for the columns).
+#define FWIX_FAST_INSTANTIATE(PLAN, TAG) FWIX_FAST_INSTANTIATE2(PLAN, PLAN, TAG)
+#define FWIX_FAST_INSTANTIATE2(PLAN, CPLAN, TAG)                                                                   \
   namespace fwix {                                                                                          \
   namespace fast {                                                                                          \
   cudaError_t row_forward_##TAG(const SpecArgs& a, int pre, cudaStream_t s) {                               \
@@ -681,11 +693,11 @@ cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* ou
   cudaError_t row_inverse_##TAG(const SpecArgs& a, int post, int pt, cudaStream_t s) {                      \
     return row_inverse<PLAN>(a, post, pt, s);                                                               \
   }                                                                                                         \
-  cudaError_t col_type_a_##TAG(const SpecArgs& a, int q, cudaStream_t s) { return col_type_a<PLAN>(a, q, s); } \
-  cudaError_t col_type_b_##TAG(const SpecArgs& a, int q, cudaStream_t s) { return col_type_b<PLAN>(a, q, s); } \
+  cudaError_t col_type_a_##TAG(const SpecArgs& a, int q, cudaStream_t s) { return col_type_a<CPLAN>(a, q, s); } \
+  cudaError_t col_type_b_##TAG(const SpecArgs& a, int q, cudaStream_t s) { return col_type_b<CPLAN>(a, q, s); } \
   cudaError_t col_fft_##TAG(const SpecArgs& a, int inv, const float2* in, float2* out, int add, float sc,    \
                             cudaStream_t s) {                                                               \
-    return col_fft<PLAN>(a, inv, in, out, add, sc, s);                                                      \
+    return col_fft<CPLAN>(a, inv, in, out, add, sc, s);                                                     \
   }                                                                                                         \
   }                                                                                                         \
   }

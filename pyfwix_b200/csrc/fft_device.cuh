@@ -161,6 +161,44 @@ struct Dft<5, INV> {
   }
 };
 
+// Radix 16 as 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2; radix-4 transforms over n1,
+// twiddles W16^(n2 k1), radix-4 transforms over n2.
+template <bool INV>
+__device__ __forceinline__ float2 tw16(float2 a, float c, float s) {  // a * (c -+ i s)
+  return INV ? cmul(a, make_float2(c, s)) : cmul(a, make_float2(c, -s));
+}
+template <bool INV>
+struct Dft<16, INV> {
+  static __device__ __forceinline__ void run(float2 (&v)[16]) {
+    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+    const float h = 0.70710678118654752440f;
+    float2 y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      float2 u[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+      Dft<4, INV>::run(u);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = u[k1];
+    }
+    y[1][1] = tw16<INV>(y[1][1], c1, s1);   // W^1
+    y[1][2] = tw16<INV>(y[1][2], h, h);     // W^2
+    y[1][3] = tw16<INV>(y[1][3], s1, c1);   // W^3
+    y[2][1] = tw16<INV>(y[2][1], h, h);     // W^2
+    y[2][2] = rot90<INV>(y[2][2]);          // W^4
+    y[2][3] = tw16<INV>(y[2][3], -h, h);    // W^6
+    y[3][1] = tw16<INV>(y[3][1], s1, c1);   // W^3
+    y[3][2] = tw16<INV>(y[3][2], -h, h);    // W^6
+    y[3][3] = tw16<INV>(y[3][3], -c1, -s1); // W^9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      float2 u[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+      Dft<4, INV>::run(u);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = u[k2];
+    }
+  }
+};
+
 // Radix 7 from the symmetric pair form y_m = v0 + sum_k cos(2 pi k m/7) t_k -+
 // i sum_k sin(2 pi k m/7) u_k with t_k = v_k + v_{7-k}, u_k = v_k - v_{7-k}.
 template <bool INV>
