@@ -44,7 +44,7 @@ from .plan import Plan
 from .vectors import Axis, Hypercube, SuperVector, Vector
 
 __all__ = ["Propagator", "ExtendedBorn", "PhaseShift", "RefSampler", "PSPI", "NSPS", "Injection",
-           "Downward", "Upward"]
+           "Downward", "Upward", "WindowPropagator", "WindowExtendedBorn"]
 
 
 # ---------------------------------------------------------------------- helpers
@@ -156,11 +156,16 @@ def _pads(par):
     return padx, pady
 
 
-def _plan_from_slow(slow_hyper, par, ns, device, nz=None, padx=None, pady=None):
+def _plan_from_slow(slow_hyper, par, ns, device, nz=None, padx=None, pady=None, nw=None):
+    """Plan for a model hypercube (x, y, w, z); ``nw`` overrides the frequency count
+    for a model whose frequency axis has length 1 (shared by every frequency)."""
     x, y, w, z = _grid_from_model(slow_hyper)
     if padx is None:
         padx, pady = _pads(par)
-    return Plan(nx=x.n, ny=y.n, nw=w.n, ns=ns, nz=z.n if nz is None else nz, dx=x.d, dy=y.d, dz=z.d,
+    if nw is not None and w.n not in (1, nw):
+        raise RuntimeError("Error: model hypercube does not match the slow_hyper")
+    return Plan(nx=x.n, ny=y.n, nw=w.n if nw is None else nw, ns=ns, nz=z.n if nz is None else nz,
+                dx=x.d, dy=y.d, dz=z.d,
                 ox=x.o, oy=y.o, oz=z.o, ow=w.o, dw=w.d, padx=padx, pady=pady,
                 nref=int(_get(par, "nref", 1)), eps=float(_get(par, "eps", 0.0)),
                 taperx=int(_get(par, "taperx", 0)), tapery=int(_get(par, "tapery", 0)),
@@ -178,8 +183,10 @@ def _refs(plan, slow2, par):
 
 
 # ---------------------------------------------------------------------- operators
-class Propagator:
-    """Nonlinear modelling: wavelet -> recorded data for a [s^2, density] model.
+class WindowPropagator:
+    """Nonlinear modelling on one model window (the whole model it is given):
+    wavelet -> recorded data for a [s^2, density] model.  ``Propagator`` runs one
+    of these per (shot group, frequency band) pair.
 
     The background down- and up-going wavefields of the last ``forward`` stay in
     device memory (lossless, every depth) for :class:`ExtendedBorn`; the reference
@@ -196,10 +203,9 @@ class Propagator:
         self.nbatches = tuple(nbatches)
         g = geometry
         s_ids, r_ids, ns = _remap_ids(g["s_ids"], g["r_ids"])
-        self.plan = _plan_from_slow(self.slow_hyper, par, ns, self.device)
-        if len(self.range_shape) != 2 or self.range_shape[1] != self.plan.nw or \
-                self.range_shape[0] != len(np.asarray(g["rx"])):
+        if len(self.range_shape) != 2 or self.range_shape[0] != len(np.asarray(g["rx"])):
             raise RuntimeError("Error: data hypercube does not match the range")
+        self.plan = _plan_from_slow(self.slow_hyper, par, ns, self.device, nw=self.range_shape[1])
         self.src = self.plan.traces(g["sx"], g["sy"], g["sz"], s_ids)
         self.rec = self.plan.traces(g["rx"], g["ry"], g["rz"], r_ids)
         self.wavelet = _dev(wavelet, self.device)
@@ -235,10 +241,10 @@ class Propagator:
         return 1.0
 
 
-class ExtendedBorn:
+class WindowExtendedBorn:
     """Extended Born modelling (domain [ds^2, drho], range data) about the
-    background ``slow_den`` of ``propagator``; ``adjoint`` is the FWI gradient
-    (``fwix/workers.py:76``)."""
+    background ``slow_den`` of a ``WindowPropagator``; ``adjoint`` is the FWI
+    gradient (``fwix/workers.py:76``)."""
 
     def __init__(self, model, data, slow_den, propagator):
         self.prop = propagator
@@ -496,3 +502,26 @@ class Downward(_Sweep):
 class Upward(_Sweep):
     """Depth nz-1 -> 0 continuation (``propagator/src/OneWay.cpp:50-79``)."""
     up = True
+
+
+# The reference's Python Propagator always builds a StreamingPropagator
+# (``fwix/CudaWEM.py:10-18``): shots and frequencies in ``nbatches`` groups, each
+# on the window of the model its sources and receivers cover (plus ``ginsu_x`` /
+# ``ginsu_y``).  These two keep that behaviour on top of the window classes.
+from .streaming import StreamingExtendedBorn, StreamingPropagator  # noqa: E402
+
+
+class Propagator(StreamingPropagator):
+    """Nonlinear modelling: wavelet -> recorded data for a [s^2, density] model,
+    per (shot group, frequency band) on its acquisition window
+    (``propagator/src/StreamingPropagator.cpp``, ``Propagator.cpp:121-221``).
+
+    The background down- and up-going wavefields of the last ``forward`` stay in
+    device memory (lossless, every depth) for :class:`ExtendedBorn`; the reference
+    keeps ZFP-compressed copies on disk (``propagator/src/WavefieldPool.cpp``)."""
+
+
+class ExtendedBorn(StreamingExtendedBorn):
+    """Extended Born modelling (domain [ds^2, drho], range data) about the
+    background ``slow_den`` of ``propagator``; ``adjoint`` is the FWI gradient
+    (``fwix/workers.py:76``, ``propagator/src/StreamingExtendedBorn.cpp``)."""

@@ -145,9 +145,11 @@ def test_sweep_operators(cls, fwd, adj):
 
 
 def _acq(g, rng):
+    # receivers spread over the whole model, so that the acquisition window is the model
     geom = dict(sx=np.array([80.0, 200.0], np.float32), sy=np.array([96.0, 120.0], np.float32),
                 sz=np.array([0.0, 5.0], np.float32), s_ids=np.array([7, 3], np.int32),
-                rx=np.linspace(0, 300, 16).astype(np.float32), ry=np.full(16, 100.0, np.float32),
+                rx=np.linspace(0, (g.nx - 1) * g.dx, 16).astype(np.float32),
+                ry=np.linspace(0, (g.ny - 1) * g.dy, 16).astype(np.float32),
                 rz=np.zeros(16, np.float32), r_ids=np.array([7, 3] * 8, np.int32))
     wav = crandn(rng, (2, g.nw)).astype(np.complex64)
     return geom, wav
@@ -166,8 +168,9 @@ def _born_setup(kind="pspi"):
 
 
 def _oracle_of(prop, g, kind="pspi"):
-    sref = prop.plan._keep["sref"].cpu().numpy().astype(np.complex128)
-    lab = oracle_labels(prop.plan._keep["labels"].cpu().numpy(), g)
+    plan = prop.pairs[0].prop.plan if hasattr(prop, "pairs") else prop.plan
+    sref = plan._keep["sref"].cpu().numpy().astype(np.complex128)
+    lab = oracle_labels(plan._keep["labels"].cpu().numpy(), g)
     return wem.Stepper(g, sref, lab, kind)
 
 
@@ -231,3 +234,71 @@ def test_refsampler_surface():
     refs = np.stack([rs.get_ref_slow(2, r) for r in range(3)])
     near = np.argmin(np.abs(s2[2][None].astype(np.complex128) - refs[:, :, None, None]), axis=0)
     assert np.mean(lab[:, :g.ny, :g.nx] == near) > 0.999
+
+
+def test_streaming_batches_windows_and_bands():
+    """nbatches = (2 shot groups, 2 frequency bands) with aperture windows
+    (ginsu) against the FP64 oracle run on each pair's window and added into
+    the global data / gradient at the pair's receivers, band and window
+    (StreamingPropagator.cpp:327-470); Born dot test through the surface."""
+    from pyfwix_b200 import streaming
+    # taper 0: the reference's PSPI Born pair is adjoint only without taper
+    g, rng, _, _, _, _ = make_case(nx=56, ny=40, nw=4, nz=5, nref=3, padx=4, pady=4, taperx=0, tapery=0)
+    s2 = _slow_model(g, rng)
+    s2[g.nz - 2:] *= 1.5
+    den = (1.0 + 0.2 * rng.random(s2.shape)).astype(np.complex64)
+    model = vectors.SuperVector(vectors.Vector(_axes(g), s2), vectors.Vector(_axes(g), den))
+    sx = np.array([60.0, 150.0, 330.0, 430.0], np.float32)
+    geom = dict(sx=sx, sy=np.full(4, 180.0, np.float32), sz=np.zeros(4, np.float32),
+                s_ids=np.array([11, 12, 13, 14], np.int32))
+    rx, ry, rid = [], [], []
+    for k, x in enumerate(sx):
+        rx += list(x + np.linspace(-40, 40, 5))
+        ry += [170.0, 190.0, 200.0, 210.0, 230.0]
+        rid += [11 + k] * 5
+    geom.update(rx=np.clip(np.array(rx, np.float32), 0, 540), ry=np.array(ry, np.float32),
+                rz=np.zeros(len(rx), np.float32), r_ids=np.array(rid, np.int32))
+    wav = crandn(rng, (4, g.nw)).astype(np.complex64)
+    par = _par(g, ginsu_x=30.0, ginsu_y=20.0)
+    data = np.zeros((len(rx), g.nw), np.complex64)
+    prop = CudaWEM.Propagator(model, data, wav, par, geom, nbatches=(2, 2))
+    assert len(prop.pairs) == 4 and len({p.window for p in prop.pairs}) == 2
+    prop.forward(False, model, data)
+    ref = np.zeros(data.shape, np.complex128)
+    grids = []
+    for p in prop.pairs:
+        x0, x1, y0, y1 = p.window
+        pl = p.prop.plan
+        gw = wem.Grid(nx=x1 - x0 + 1, ny=y1 - y0 + 1, nw=p.nf, nz=g.nz, dx=g.dx, dy=g.dy, dz=g.dz,
+                      ox=g.ox + x0 * g.dx, oy=g.oy + y0 * g.dy, oz=g.oz, ow=g.ow + p.f0 * g.dw, dw=g.dw,
+                      padx=pl.NX - pl.nx, pady=pl.NY - pl.ny, nref=g.nref, taperx=g.taperx, tapery=g.tapery)
+        pg = prop._pair_geometry(p)
+        acq = wem.make_acquisition(gw, pg)
+        st = _oracle_of(p.prop, gw)
+        sw = s2[:, p.f0:p.f0 + p.nf, y0:y1 + 1, x0:x1 + 1].astype(np.complex128)
+        dw_ = den[:, p.f0:p.f0 + p.nf, y0:y1 + 1, x0:x1 + 1].astype(np.complex128)
+        d, bgd, bgu = wem.propagate(gw, st, acq, sw, dw_, wav[p.src_idx][:, p.f0:p.f0 + p.nf].astype(np.complex128))
+        ref[np.ix_(p.rec_idx, np.arange(p.f0, p.f0 + p.nf))] += d
+        grids.append((gw, st, acq, sw, dw_, bgd, bgu))
+    assert rel(data, ref) < TOL_SWEEP
+    # Born adjoint against the per-window oracle, and the surface dot test
+    born = CudaWEM.ExtendedBorn(model.cloneSpace(), data, model, prop)
+    r = crandn(rng, data.shape).astype(np.complex64)
+    gmod = model.cloneSpace()
+    born.adjoint(False, gmod, r)
+    gs_ref = np.zeros(s2.shape, np.complex128)
+    for p, (gw, st, acq, sw, dw_, bgd, bgu) in zip(prop.pairs, grids):
+        x0, x1, y0, y1 = p.window
+        rr = r[p.rec_idx][:, p.f0:p.f0 + p.nf].astype(np.complex128)
+        gs, gr = wem.born_adjoint(gw, st, acq, sw, dw_, bgd, bgu, rr)
+        gs_ref[:, p.f0:p.f0 + p.nf, y0:y1 + 1, x0:x1 + 1] += gs
+    assert rel(gmod[0].arr.numpy(), gs_ref) < TOL_SWEEP
+    dm = vectors.SuperVector(vectors.Vector(_axes(g), crandn(rng, s2.shape) * 1e-3),
+                             vectors.Vector(_axes(g), crandn(rng, s2.shape) * 1e-2))
+    d1 = np.zeros_like(data)
+    born.forward(False, dm, d1)
+    lhs = cdot(r, d1)
+    rhs = cdot(gmod[0].arr.numpy(), dm[0].arr.numpy()) + cdot(gmod[1].arr.numpy(), dm[1].arr.numpy())
+    assert abs(lhs / rhs - 1) < 1e-4
+    assert streaming.window_indices([60.0], [180.0], (56, 0.0, 10.0), (40, 0.0, 10.0), 30.0, 20.0) == (3, 9, 16, 20)
+    assert [streaming.next_fft_length(n) for n in (23, 26, 49, 97)] == [24, 27, 49, 98]
