@@ -173,6 +173,17 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// Labels of a lane's samples, four to a 32-bit word (fewer registers than a byte
+// array, which the compiler keeps one per register).
+template <int E>
+struct Labels {
+  uint32_t w[(E + 3) / 4];
+  __device__ __forceinline__ void set(int e, uint32_t v) {
+    w[e / 4] = (e % 4 == 0 ? 0u : w[e / 4]) | ((v & 0xffu) << (8 * (e % 4)));
+  }
+  __device__ __forceinline__ int get(int e) const { return (int)((w[e / 4] >> (8 * (e % 4))) & 0xffu); }
+};
+
 // ---------------------------------------------------------------- row passes (NX = P::N)
 
 template <class P>
@@ -209,7 +220,7 @@ struct RowCtx {
 
 // t1[term] = F_x(pre_term * in) for each term.
 template <class P, int PRE>
-__global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int nchunk) {
+__global__ void __launch_bounds__(kWarps * 32, multi_term(PRE) && P::E == 16 ? 2 : 0) k_row_fwd(const SpecArgs a, int nchunk) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
@@ -225,11 +236,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int n
     for (int e = 0; e < P::E; ++e) raw[e] = cadd(raw[e], src2[pos_first<P>(c.t, e)]);
   }
   const int nterm = multi_term(PRE) ? a.nterm : 1;
-  uint8_t lab[P::E];
+  Labels<P::E> lab;
   if (PRE == W_MASK) {
     const uint8_t* lrow = a.lab + (long long)c.iw * a.lab_w + (long long)(c.live ? c.y : 0) * P::N;
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) lab[e] = c.live ? lrow[pos_first<P>(c.t, e)] : 255;
+    for (int e = 0; e < P::E; ++e) lab.set(e, c.live ? lrow[pos_first<P>(c.t, e)] : 255u);
   }
   // smooth weights: terms that no sample of the warp's rows supports are zero rows
   unsigned used = 0xffffffffu;
@@ -256,7 +267,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int n
 #pragma unroll
     for (int e = 0; e < P::E; ++e) {
       if (PRE == W_MASK)
-        v[e] = (int)lab[e] == term ? raw[e] : make_float2(0.f, 0.f);
+        v[e] = lab.get(e) == term ? raw[e] : make_float2(0.f, 0.f);
       else
         v[e] = c.live ? row_weight<PRE>(a, term, c.iw, c.y, pos_first<P>(c.t, e), raw[e]) : make_float2(0.f, 0.f);
     }
@@ -273,7 +284,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_fwd(const SpecArgs a, int n
 // prefetched while the current one is transformed, and with labels the terms
 // that no sample of the warp's rows selects are skipped.
 template <class P, int POST>
-__global__ void __launch_bounds__(kWarps * 32) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
+__global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && P::E == 16 ? 2 : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
@@ -282,15 +293,16 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_inv(const SpecArgs a, int n
   float2 acc[P::E];
 #pragma unroll
   for (int e = 0; e < P::E; ++e) acc[e] = make_float2(0.f, 0.f);
-  uint8_t lab[P::E];
+  Labels<P::E> lab;
   unsigned used = 0xffffffffu;
   if (POST == W_MASK) {
     const uint8_t* lrow = a.lab + (long long)c.iw * a.lab_w + (long long)(c.live ? c.y : 0) * P::N;
     unsigned mine = 0;
 #pragma unroll
     for (int e = 0; e < P::E; ++e) {
-      lab[e] = c.live ? lrow[pos_first<P>(c.t, e)] : 255;
-      if (lab[e] < 32) mine |= 1u << lab[e];
+      const uint32_t l = c.live ? lrow[pos_first<P>(c.t, e)] : 255u;
+      lab.set(e, l);
+      if (l < 32) mine |= 1u << l;
     }
     // the warp steps through the union of its lines' terms so that it stays converged
 #pragma unroll
@@ -333,7 +345,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_row_inv(const SpecArgs a, int n
 #pragma unroll
     for (int e = 0; e < P::E; ++e) {
       if (POST == W_MASK) {
-        if ((int)lab[e] == term) acc[e] = v[e];
+        if (lab.get(e) == term) acc[e] = v[e];
       } else if (c.live) {
         acc[e] = cadd(acc[e], row_weight<POST>(a, term, c.iw, c.y, pos_first<P>(c.t, e), v[e]));
       }
