@@ -375,9 +375,10 @@ struct ColGeo {
   // or 32 columns an odd stride is, and 5 also suits the line exchanges.
   static constexpr int LINE = P::N + (LX == 8 ? 2 : 5);
   static size_t smem() { return ((size_t)LX * LINE + tw_size<P>()) * sizeof(float2); }
-  // Resident CTAs per SM the register allocation is held to: three for plans
-  // of at most 8 samples per lane (about 85 registers), else what fits.
-  static constexpr int kMinBlocks = P::E <= 8 ? 3 : 1;
+  // Resident CTAs per SM the register allocation is held to: four for plans of
+  // at most 8 samples per lane (64 registers; the few spills stay in L1 and the
+  // extra warps hide more latency than they cost), else what fits.
+  static constexpr int kMinBlocks = P::E <= 8 ? 4 : 1;
   static size_t smem2() { return ((size_t)2 * LX * LINE + tw_size<P>()) * sizeof(float2); }  // tile, tw, tile
 };
 
