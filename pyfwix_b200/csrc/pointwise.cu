@@ -76,10 +76,19 @@ __global__ void __launch_bounds__(kCells * kGroups)
               const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw,
               const float2* __restrict__ in, float2* __restrict__ out) {
   const Cell c = this_cell(d);
+  // one model for every frequency: the first group forms each cell's coefficient once
+  __shared__ float2 rs[kCells];
+  if (mw == 0) {
+    if (threadIdx.y == 0 && c.ok) {
+      const float2 r = refl_coef(s0[c.yx], s1[c.yx], r0[c.yx], r1[c.yx]);
+      rs[threadIdx.x] = adjoint ? cconj(r) : r;
+    }
+    __syncthreads();
+  }
   if (!c.ok) return;
-  float2 r = make_float2(0.f, 0.f);
+  float2 r = mw == 0 ? rs[threadIdx.x] : make_float2(0.f, 0.f);
   for (int iw = threadIdx.y; iw < d.nw; iw += kGroups) {
-    if (mw != 0 || iw == (int)threadIdx.y) {
+    if (mw != 0) {
       const long long m = iw * mw + c.yx;
       r = refl_coef(s0[m], s1[m], r0[m], r1[m]);
       if (adjoint) r = cconj(r);
@@ -167,9 +176,16 @@ __global__ void __launch_bounds__(kCells * kGroups)
   const long long plane = (long long)d.ny * d.nx;
   const int wsum = adjoint && dm_w == 0;
   LinCoef cf;
+  // one model for every frequency: the first group forms each cell's coefficients once
+  __shared__ LinCoef cs[kCells];
+  if (mw == 0) {
+    if (threadIdx.y == 0 && c.ok) cs[threadIdx.x] = lin_coef(s0[c.yx], s1[c.yx], r0[c.yx], r1[c.yx]);
+    __syncthreads();
+    cf = cs[threadIdx.x];
+  }
   float2 g[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
   for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups) {
-    if (mw != 0 || iw == (int)threadIdx.y) {
+    if (mw != 0) {
       const long long m = iw * mw + c.yx;
       cf = lin_coef(s0[m], s1[m], r0[m], r1[m]);
     }
