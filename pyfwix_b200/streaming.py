@@ -241,10 +241,19 @@ class StreamingExtendedBorn:
         sp = self.sp
         self._ensure()
         out = _dev(data, sp.device) if add else _dev(data, sp.device, zero=True)
+        main = torch.cuda.current_stream(sp.device)
+        results = []
         for p, born in zip(sp.pairs, self.borns):
             dm = sp._window_model(p, model)
             d = torch.zeros((len(p.rec_idx), p.nf), dtype=torch.complex64, device=sp.device)
-            born.forward(False, dm, d)
+            p.stream.wait_stream(main)
+            with torch.cuda.stream(p.stream):
+                born.forward(False, dm, d)
+            results.append((p, d, dm))
+        # sums in pair order on the caller's stream: the result does not depend on
+        # which pair finishes first
+        for p, d, _ in results:
+            main.wait_stream(p.stream)
             rows = torch.as_tensor(p.rec_idx, device=sp.device)
             out[rows, p.f0:p.f0 + p.nf] += d
         _store(data, out)
@@ -254,14 +263,22 @@ class StreamingExtendedBorn:
         self._ensure()
         ds_t, dr_t = (_dev(m, sp.device, zero=not add) for m in _model_pair(model))
         d_all = _dev(data, sp.device)
+        main = torch.cuda.current_stream(sp.device)
+        shared = ds_t.shape[1] == 1
+        results = []
         for p, born in zip(sp.pairs, self.borns):
             x0, x1, y0, y1 = p.window
-            shared = ds_t.shape[1] == 1
             nf = 1 if shared else p.nf
             gs = torch.zeros((ds_t.shape[0], nf, y1 - y0 + 1, x1 - x0 + 1), dtype=torch.complex64, device=sp.device)
             gr = torch.zeros_like(gs)
             d = d_all[torch.as_tensor(p.rec_idx, device=sp.device)][:, p.f0:p.f0 + p.nf].contiguous()
-            born.adjoint(False, [gs, gr], d)
+            p.stream.wait_stream(main)
+            with torch.cuda.stream(p.stream):
+                born.adjoint(False, [gs, gr], d)
+            results.append((p, gs, gr, d))
+        for p, gs, gr, _ in results:
+            main.wait_stream(p.stream)
+            x0, x1, y0, y1 = p.window
             f = slice(0, 1) if shared else slice(p.f0, p.f0 + p.nf)
             ds_t[:, f, y0:y1 + 1, x0:x1 + 1] += gs
             dr_t[:, f, y0:y1 + 1, x0:x1 + 1] += gr

@@ -67,3 +67,35 @@ def test_store_writes_back_into_numpy_and_tensors():
     b = torch.zeros(2, 3, dtype=torch.complex64)
     CudaWEM._store(b, t)
     assert torch.equal(b.reshape(-1), t)
+
+
+def test_window_indices_floor_ceil_clip_and_degenerate():
+    """Acquisition window of a shot group (``propagator/src/StreamingPropagator.cpp:357-393``):
+    floor of the low edge, ceil of the high edge, clipped to the axis, the whole
+    axis when the box collapses to one sample."""
+    from pyfwix_b200.streaming import window_indices
+    ax = (100, 0.0, 10.0)
+    ay = (50, 5.0, 20.0)
+    # x in [123, 456] +- 30 -> [93, 486] m -> ix [9, 49]; y in [105, 305] +- 0 -> iy [5, 15]
+    assert window_indices([123.0, 456.0], [105.0, 305.0], ax, ay, 30.0, 0.0) == (9, 49, 5, 15)
+    # clipped at both ends
+    assert window_indices([-50.0, 2000.0], [0.0, 2000.0], ax, ay, 0.0, 0.0) == (0, 99, 0, 49)
+    # one point, no ginsu: the box is degenerate on both axes -> whole axes
+    assert window_indices([200.0], [205.0], ax, ay) == (0, 99, 0, 49)
+    # no points -> whole model
+    assert window_indices([], [], ax, ay) == (0, 99, 0, 49)
+
+
+def test_next_fft_length_and_even_split():
+    from pyfwix_b200.streaming import next_fft_length, split_even
+    assert [next_fft_length(n) for n in (1, 11, 13, 17, 23, 97, 256, 257)] == [1, 12, 14, 18, 24, 98, 256, 270]
+    for n in range(1, 1100):
+        m = next_fft_length(n)
+        k = m
+        for f in (2, 3, 5, 7):
+            while k % f == 0:
+                k //= f
+        assert k == 1 and m >= n
+    assert split_even(10, 3) == [4, 3, 3]
+    assert split_even(2, 5) == [1, 1]
+    assert sum(split_even(128, 7)) == 128
