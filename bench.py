@@ -53,6 +53,10 @@ def args_():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fwi", action="store_true", help="skip the FWI-gradient timing")
     ap.add_argument("--fwi-nz", type=int, default=None, help="depth levels of the FWI workload (quick runs)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched forward+imaging timing")
+    ap.add_argument("--batched-nz", type=int, default=None, help="depth levels of the batched workload (quick runs)")
+    ap.add_argument("--batched-shots", type=int, default=32)
+    ap.add_argument("--batched-streams", type=int, default=8)
     ap.add_argument("--profile-step", choices=["pspi", "nsps", "pspi-adj", "nsps-adj"], default=None,
                     help="run one depth step of the workload's wavefield and exit (for ncu captures)")
     return ap.parse_args()
@@ -249,6 +253,54 @@ def fwi_gradient_timing(device, nz=None, checkpoint="auto"):
             "forward_gcell_steps_per_s": 2 * cells / t_fwd / 1e9, "objective": float(J.detach())}
 
 
+def batched_timing(device, nshots=32, nz=None, nstreams=8):
+    """Batched forward + imaging (32 shots of uneven grid and band, each migrated:
+    source and receiver wavefields continued in lockstep, image summed over
+    frequency at every level) run three ways on the same instances -- shot after
+    shot on one stream ("plain", the per-shot path), over CUDA streams, and
+    replayed from one captured CUDA graph -- each timed with CUDA events over one
+    pass after a warm-up pass.  Cell-steps count both continued wavefields."""
+    import torch
+
+    from pyfwix_b200 import workloads
+    from pyfwix_b200.batch import MigrationBatch
+    ws = workloads.config3(nshots=nshots, nz=nz)
+    t0 = time.perf_counter()
+    b = MigrationBatch(ws, device=device, nstreams=nstreams)
+    b.model_data()
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    cells = 2 * b.cells
+    out = {"workload": f"config3 batched forward+imaging, {nshots} shots, nx=ny in 128-384, nz={ws[0].nz}, "
+                       f"48-160 frequencies each, PSPI nref 6",
+           "cell_steps": cells, "nstreams": len(b.streams), "setup_s": setup_s}
+
+    def once(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    b.run_plain()                      # warm-up
+    t_plain = once(b.run_plain)
+    t_streams = once(b.run_streams)
+    t1 = time.perf_counter()
+    b.capture()
+    out["graph_capture_s"] = time.perf_counter() - t1
+    b.run_graph()                      # warm-up (graph upload)
+    t_graph = once(b.run_graph)
+    for k, t in (("plain", t_plain), ("streams", t_streams), ("graph", t_graph)):
+        out[k + "_gcell_steps_per_s"] = cells / t / 1e9
+        out[k + "_s"] = t
+    out["graph_over_plain"] = t_plain / t_graph
+    del b
+    torch.cuda.empty_cache()
+    return out
+
+
 # ----------------------------------------------------------------------------- CPU arm
 
 class CpuBorn:
@@ -426,11 +478,13 @@ def main():
             "kernel": "NSPS depth step (row pass + column pass + row pass), 256x256x128",
             "step_ms": tstep * 1e3, "alg_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP}
     bg_gb = st["bd"].numel() * 8 / 1e9
-    fwi = None
+    fwi = batched = None
+    del st
+    torch.cuda.empty_cache()
     if not a.no_fwi:
-        del st
-        torch.cuda.empty_cache()
         fwi = fwi_gradient_timing(device, nz=a.fwi_nz)
+    if ws == 1 and not a.no_batched:
+        batched = batched_timing(device, nshots=a.batched_shots, nz=a.batched_nz, nstreams=a.batched_streams)
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu:
         cpu = cpu_baseline()
@@ -443,7 +497,7 @@ def main():
                            "l2": "inputs larger than L2 (background wavefields 2 x %.1f GB)"
                                  % bg_gb},
                 "gpu_launches": launches, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "fwi_grad": fwi}
+                "fwi_grad": fwi, "batched": batched}
         print(json.dumps(line), flush=True)
     if ws > 1:
         tdist.destroy_process_group()

@@ -191,8 +191,10 @@ fwix_status fwix_inject(fwix_plan* plan, const fwix_traces* tr, int iz, int adjo
 /* Downward / Upward continuation in place over all nz levels. */
 fwix_status fwix_downward(fwix_plan* plan, int adjoint, void* wfld, void* stream);
 fwix_status fwix_upward(fwix_plan* plan, int adjoint, void* wfld, void* stream);
-/* Nonlinear modelling wavelet -> data.  bg_down / bg_up: [nz] wavefields (may be
- * NULL when the Born operators are not needed). */
+/* Nonlinear modelling wavelet -> data.  bg_down: [nz] wavefields, required (the up
+ * pass reflects the down field of every depth); on return it holds the down field
+ * of every depth.  bg_up: [nz] wavefields receiving the up field of every depth, or
+ * NULL when the Born operators are not needed. */
 fwix_status fwix_propagate(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
                            const void* wavelet, void* data, int add, void* bg_down, void* bg_up,
                            void* stream);

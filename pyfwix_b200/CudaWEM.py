@@ -44,7 +44,7 @@ from .plan import Plan
 from .vectors import Axis, Hypercube, SuperVector, Vector
 
 __all__ = ["Propagator", "ExtendedBorn", "PhaseShift", "RefSampler", "PSPI", "NSPS", "Injection",
-           "Downward", "Upward", "WindowPropagator", "WindowExtendedBorn"]
+           "Downward", "Upward", "WindowPropagator", "WindowExtendedBorn", "slowness_model"]
 
 
 # ---------------------------------------------------------------------- helpers
@@ -511,6 +511,16 @@ class Upward(_Sweep):
 from .streaming import StreamingExtendedBorn, StreamingPropagator  # noqa: E402
 
 
+def slowness_model(s_real):
+    """[s^2, density] model of a real slowness s [nz][ny][nx]: complex s^2 with a
+    frequency axis of length 1 (shared by every frequency), density 1."""
+    s = torch.as_tensor(s_real)
+    if s.dim() != 3:
+        raise ValueError(f"s_real must be [nz][ny][nx], got {tuple(s.shape)}")
+    s2 = (s.double() ** 2)[:, None].to(torch.complex64).contiguous()
+    return [s2, torch.ones_like(s2)]
+
+
 class Propagator(StreamingPropagator):
     """Nonlinear modelling: wavelet -> recorded data for a [s^2, density] model,
     per (shot group, frequency band) on its acquisition window
@@ -518,7 +528,60 @@ class Propagator(StreamingPropagator):
 
     The background down- and up-going wavefields of the last ``forward`` stay in
     device memory (lossless, every depth) for :class:`ExtendedBorn`; the reference
-    keeps ZFP-compressed copies on disk (``propagator/src/WavefieldPool.cpp``)."""
+    keeps ZFP-compressed copies on disk (``propagator/src/WavefieldPool.cpp``).
+
+    Shortcuts beyond the reference's arguments: ``s_real`` (a real slowness
+    [nz][ny][nx]) stands for the model [s^2, 1] (``model`` may then be None, in
+    the constructor and in ``forward``; ``par`` carries the axes), and
+    ``mode="smooth"`` models with the differentiable step (interpolation between
+    the two bracketing references plus the split-step correction, density 1,
+    the whole model in one batch) that ``fwi.FWIGradient`` differentiates;
+    ``mode="parity"`` (default) is the reference's selection step."""
+
+    def __init__(self, model, data, wavelet, par, geometry, nbatches=(1, 1), bands=None, mode="parity",
+                 s_real=None):
+        if mode not in ("parity", "smooth"):
+            raise ValueError(f"mode must be 'parity' or 'smooth', got {mode!r}")
+        self.mode = mode
+        self.s_real = s_real
+        self._s_model = None
+        if s_real is not None:
+            model = self._s_model = slowness_model(s_real)
+        elif model is None:
+            raise ValueError("Propagator needs a model or s_real")
+        super().__init__(model, data, wavelet, par, geometry, nbatches, bands)
+        self._smooth = None
+
+    def _slowness_of(self, model):
+        if model is None:
+            if self.s_real is None:
+                raise ValueError("forward needs a model (no s_real was given)")
+            return torch.as_tensor(self.s_real)
+        s2, _ = _model_pair(model)
+        t = torch.as_tensor(_raw(s2))
+        if t.dim() != 4 or t.shape[1] != 1:
+            raise ValueError("mode='smooth' needs a frequency-independent model [nz][1][ny][nx] or s_real")
+        return torch.sqrt(t[:, 0].real.double()).float()
+
+    def forward(self, add, model, data):
+        if self.mode == "parity":
+            if model is None and self._s_model is None:
+                raise ValueError("forward needs a model (no s_real was given)")
+            return super().forward(add, model if model is not None else self._s_model, data)
+        from .fwi import SmoothFWI
+        s = self._slowness_of(model)
+        if self._smooth is None:
+            ax = self.ax
+            par = {k: _get(self.par, k) for k in ("nref", "padx", "pady", "eps", "taperx", "tapery", "checkpoint",
+                                                   "refs") if _get(self.par, k) is not None}
+            par.update(ox=ax[0].o, dx=ax[0].d, oy=ax[1].o, dy=ax[1].d, ow=ax[2].o, dw=ax[2].d, oz=ax[3].o,
+                       dz=ax[3].d)
+            self._smooth = SmoothFWI(tuple(s.shape), {k: v for k, v in self.g.items()}, self.wavelet, par,
+                                     device=self.device)
+        d = self._smooth.model(s.to(self.device), keep=False)
+        out = _dev(data, self.device) if add else _dev(data, self.device, zero=True)
+        out += d
+        _store(data, out)
 
 
 class ExtendedBorn(StreamingExtendedBorn):

@@ -20,6 +20,10 @@
 // barrier.  Column passes (lines along y) stage a tile of LX columns x NY rows
 // through shared memory so that HBM is read and written in row segments.
 #pragma once
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "ops.cuh"
 
 namespace fwix {
@@ -220,7 +224,7 @@ struct RowCtx {
 
 // t1[term] = F_x(pre_term * in) for each term.
 template <class P, int PRE>
-__global__ void __launch_bounds__(kWarps * 32, multi_term(PRE) && P::E == 16 ? 2 : 0) k_row_fwd(const SpecArgs a, int nchunk) {
+__global__ void __launch_bounds__(kWarps * 32, multi_term(PRE) && (P::E == 16 || P::E == 12) ? 2 : 0) k_row_fwd(const SpecArgs a, int nchunk) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(PRE) && P::E == 16 ? 2
 // prefetched while the current one is transformed, and with labels the terms
 // that no sample of the warp's rows selects are skipped.
 template <class P, int POST>
-__global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && P::E == 16 ? 2 : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
+__global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 || P::E == 12) ? 2 : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
@@ -378,7 +382,7 @@ struct ColGeo {
   // Resident CTAs per SM the register allocation is held to: four for plans of
   // at most 8 samples per lane (64 registers; the few spills stay in L1 and the
   // extra warps hide more latency than they cost), else what fits.
-  static constexpr int kMinBlocks = P::E <= 8 ? 4 : 1;
+  static constexpr int kMinBlocks = P::E <= 8 ? 4 : P::E <= 12 ? 2 : 1;
   static size_t smem2() { return ((size_t)2 * LX * LINE + tw_size<P>()) * sizeof(float2); }  // tile, tw, tile
 };
 
@@ -571,11 +575,25 @@ __global__ void __launch_bounds__(kWarps * 32) k_col_fft(const SpecArgs a, int n
 
 // ---------------------------------------------------------------- launch helpers
 
+// Sets the shared-memory carveout and, above 48 KB, the dynamic shared-memory limit
+// of a kernel, once per (kernel, device, size): the attribute calls cost more host
+// time than the launch itself, and the depth loops launch every pass per level.
 template <class K>
 cudaError_t opt_in_smem(K kernel, size_t bytes) {
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  if (e != cudaSuccess || bytes <= 48 * 1024) return e;
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const auto key = std::make_pair((const void*)kernel, dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e == cudaSuccess && bytes > 48 * 1024)
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done[key] = bytes;
+  return e;
 }
 
 template <class P>

@@ -10,6 +10,12 @@ config2: Born forward + adjoint with NSPS, one shot, 256 x 256 x 200, nw = 128
          noise (sigma 5 cells) scaled to max |p| = 0.05; reflectivity = 5 flat
          layers at depths drawn from {10..189}, amplitudes U(-0.1, 0.1) relative to
          the background s^2.
+config3: batched forward + imaging, 32 shots, each on its own grid: nx = ny drawn
+         from {128, 192, 256, 320, 384}, nz = 200, d = 10 m, a band of 48-160
+         frequencies (step 43/159 Hz) placed at random within 2-45 Hz; velocity of
+         the config1 family (1500 + 0.5 z, +10 % Gaussian anomaly, sigma 150 m) with
+         the anomaly centre drawn per shot over the middle half of the grid; PSPI,
+         nref = 6; source at the grid centre, receivers on every surface node.
 config4: FWI gradient, PSPI smooth step, 384 x 384 x 300, nw = 96 (3-30 Hz), nref 4,
          true model v = 1500 + 0.5 z times (1 + three Gaussian anomalies of +-8 %,
          sigma 150 m, at seeded centres), starting model the background; 8 sources
@@ -58,6 +64,7 @@ class Workload:
     oy: float = 0.0
     oz: float = 0.0
     slow2: np.ndarray = None      # [nz][ny][nx] float32, s^2 = 1/v^2
+    anomaly: tuple = None         # (cx, cy, cz) of the +10 % anomaly; slow2 then comes from slow2_on()
     geom: dict = field(default_factory=dict)
     wavelet: np.ndarray = None    # [nsrc][nw] complex64
     dslow: np.ndarray = None      # Born perturbation [nz][ny][nx] float32 (or None)
@@ -154,6 +161,44 @@ def config4(nz=None, shot=0, seed=1003):
     w.wavelet = ricker_spectrum(w.freqs)[None, :].astype(np.complex64)
     w.slow2 = s0 ** 2
     return w, s_true, s0
+
+
+def config3(nshots=32, nz=None, seed=1002):
+    """Batched forward + imaging: a list of single-shot Workloads of uneven grid and
+    band.  Their s^2 is generated on the device by ``slow2_on`` (the 32 models
+    hold about 2 GB)."""
+    rng = np.random.default_rng(seed)
+    dw = 43.0 / 159.0
+    out = []
+    for i in range(nshots):
+        n = int(rng.choice([128, 192, 256, 320, 384]))
+        nw = int(rng.integers(48, 161))
+        ow = 2.0 + float(rng.integers(0, 160 - nw + 1)) * dw
+        w = Workload(name=f"shot{i}-{n}x{n}x{nz or 200}-nw{nw}", nx=n, ny=n, nz=nz or 200, dx=10.0, dy=10.0,
+                     dz=10.0, nw=nw, ow=ow, dw=dw, nref=6, step="pspi", taperx=20, tapery=20)
+        cx, cy = rng.uniform(0.25, 0.75, 2) * n * w.dx
+        cz = float(rng.uniform(0.25, 0.75)) * 200 * w.dz
+        w.anomaly = (float(cx), float(cy), cz)
+        w.geom = dict(sx=np.array([n // 2 * w.dx], np.float32), sy=np.array([n // 2 * w.dy], np.float32),
+                      sz=np.array([0.0], np.float32), s_ids=np.array([0], np.int32), **w.surface_receivers())
+        w.wavelet = ricker_spectrum(w.freqs)[None, :].astype(np.complex64)
+        out.append(w)
+    return out
+
+
+def slow2_on(w, device):
+    """s^2 [nz][ny][nx] (float32, on ``device``) of a config1-family workload:
+    v = (1500 + 0.5 z) (1 + 0.10 exp(-|r - c|^2 / (2 150^2)))."""
+    import torch
+    if w.anomaly is None:
+        return torch.as_tensor(w.slow2).to(device)
+    cx, cy, cz = w.anomaly
+    z = (w.oz + w.dz * torch.arange(w.nz, device=device, dtype=torch.float64))[:, None, None]
+    y = (w.oy + w.dy * torch.arange(w.ny, device=device, dtype=torch.float64))[None, :, None]
+    x = (w.ox + w.dx * torch.arange(w.nx, device=device, dtype=torch.float64))[None, None, :]
+    v = (1500.0 + 0.5 * z) * (1 + 0.10 * torch.exp(-((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2)
+                                                    / (2 * 150.0 ** 2)))
+    return (1.0 / v ** 2).float().contiguous()
 
 
 CONFIGS = {"config1": config1, "config2": config2}

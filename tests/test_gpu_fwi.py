@@ -92,3 +92,35 @@ def test_autograd_function():
     J_o, grad_o = wem.smooth_gradient(g, refs64, s.astype(np.float64), acq, wav, to_host(d_obs))
     assert abs(float(J.detach()) / J_o - 1) < 1e-4
     assert rel(st.grad.cpu().numpy(), grad_o) < 1e-3
+
+
+def test_propagator_s_real_and_smooth_mode():
+    """Propagator shortcuts: ``s_real`` stands for the model [s^2, 1] (same data
+    as passing that model), and ``mode="smooth"`` models with the differentiable
+    step (the FP64 oracle's smooth modelling with the same references)."""
+    from pyfwix_b200 import CudaWEM
+    g, rng, s, geom, wav, par = _case()
+    s = s.astype(np.float32)
+    # the receivers lie on one line y = 120 m: an aperture (ginsu) that covers the
+    # model keeps the parity runs from windowing the model down to two rows
+    par = dict(par, ginsu_x=1e4, ginsu_y=1e4)
+    d1 = np.zeros((len(geom["rx"]), g.nw), np.complex64)
+    p1 = CudaWEM.Propagator(None, d1, wav, par, geom, s_real=s)
+    p1.forward(False, None, d1)
+    model = CudaWEM.slowness_model(s)
+    d2 = np.zeros_like(d1)
+    p2 = CudaWEM.Propagator(model, d2, wav, par, geom)
+    p2.forward(False, model, d2)
+    assert np.abs(d1).max() > 0 and rel(d1, d2) < 1e-6
+    d3 = np.zeros_like(d1)
+    p3 = CudaWEM.Propagator(None, d3, wav, par, geom, mode="smooth", s_real=s)
+    p3.forward(False, None, d3)
+    refs64 = p3._smooth.refs.cpu().numpy().astype(np.float64)
+    acq = wem.make_acquisition(g, geom)
+    ref = wem.smooth_propagate(g, refs64, s.astype(np.float64), acq, wav)[0]
+    assert rel(d3, ref) < 1e-4
+    d4 = d3.copy()
+    p3.forward(True, None, d4)   # add
+    assert rel(d4, 2 * ref) < 1e-4
+    with pytest.raises(ValueError):
+        CudaWEM.Propagator(None, d1, wav, par, geom, mode="bogus", s_real=s)
