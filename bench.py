@@ -57,6 +57,9 @@ def args_():
     ap.add_argument("--batched-nz", type=int, default=None, help="depth levels of the batched workload (quick runs)")
     ap.add_argument("--batched-shots", type=int, default=32)
     ap.add_argument("--batched-streams", type=int, default=8)
+    ap.add_argument("--profile-n", type=int, default=None, help="lateral size of the profiled step (default: the workload's)")
+    ap.add_argument("--profile-nw", type=int, default=96)
+    ap.add_argument("--profile-nref", type=int, default=4)
     ap.add_argument("--profile-step", choices=["pspi", "nsps", "pspi-adj", "nsps-adj"], default=None,
                     help="run one depth step of the workload's wavefield and exit (for ncu captures)")
     return ap.parse_args()
@@ -397,7 +400,17 @@ def profile_step(a):
     from pyfwix_b200 import refsampler, workloads
     from pyfwix_b200.plan import Plan
     torch.cuda.set_device(0)
-    w = workloads.CONFIGS[a.config](nz=2)
+    if a.profile_n:
+        # a step of another lateral size: config1-family velocity with 5 % seeded noise
+        n, nw = a.profile_n, a.profile_nw
+        w = workloads.Workload(name=f"step-{n}x{n}-nw{nw}-nref{a.profile_nref}", nx=n, ny=n, nz=2, dx=10.0,
+                               dy=10.0, dz=10.0, nw=nw, ow=3.0, dw=27.0 / max(nw - 1, 1), nref=a.profile_nref,
+                               step="pspi")
+        rng = np.random.default_rng(1000 + n)
+        v = (1500.0 + 0.5 * 10.0 * np.arange(2))[:, None, None] * (1 + 0.05 * rng.random((2, n, n)))
+        w.slow2 = (1.0 / v ** 2).astype(np.float32)
+    else:
+        w = workloads.CONFIGS[a.config](nz=2)
     kind, adj = a.profile_step.split("-")[0], a.profile_step.endswith("-adj")
     kw = w.plan_kwargs()
     kw["step"] = kind

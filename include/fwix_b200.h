@@ -117,9 +117,12 @@ fwix_status fwix_plan_set_refs(fwix_plan* plan, const void* sref, const uint8_t*
  * (depth, reference, frequency, |kx|, |ky|) (phase_shift.cu:36-55), so with a
  * cache of fwix_plan_phase_cache_bytes bytes bound, each depth's factors are
  * computed once, on the first step at that depth, and every later step there
- * (Born sweeps visit each depth many times) reads them.  Binding NULL disables
- * it; fwix_plan_set_refs invalidates it.  Calls that use it must be ordered on
- * one stream (or synchronised), as for the workspace. */
+ * (Born sweeps visit each depth many times) reads them.  A smaller cache of k
+ * depths (at least fwix_plan_phase_cache_bytes / nz bytes each) keeps depth iz
+ * in slot iz mod k and rebuilds a slot when another depth has taken it: one
+ * depth is enough for the two steps per level of a lockstep migration.
+ * Binding NULL disables it; fwix_plan_set_refs invalidates it.  Calls that use
+ * it must be ordered on one stream (or synchronised), as for the workspace. */
 size_t fwix_plan_phase_cache_bytes(const fwix_plan* plan);
 fwix_status fwix_plan_set_phase_cache(fwix_plan* plan, void* dev_ptr, size_t bytes);
 /* Background s^2 and density, element (iz,iw,y,x) at

@@ -42,6 +42,8 @@ class Instance:
         s2 = slow2[:, None]                                                  # [nz][1][ny][nx]
         sref, labels = refsampler.sample(s2, w.nref, w.padx, w.pady)
         p.set_refs(refsampler.expand_refs(sref, w.nw), labels, phase_cache=False)
+        # one depth of phase factors, shared by the source and receiver steps of a level
+        p.enable_phase_cache(depths=1)
         s2c = s2.to(torch.complex64)
         p.set_model(s2c, torch.ones_like(s2c))
         g = w.geom

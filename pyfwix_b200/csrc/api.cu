@@ -128,8 +128,9 @@ struct fwix_plan {
   float2* scat_tab = nullptr;     // scatter weights of one depth, [taylor+1][NY][NX]
   const float* sm_s = nullptr;    // smooth step: padded slowness [nz][NY][NX]
   const float* sm_ref = nullptr;  // smooth step: sorted real reference slownesses [nz][nref]
-  float2* pcache = nullptr;   // phase-factor cache, nz depths (fwix_plan_set_phase_cache)
-  std::vector<char> pbuilt;   // depth iz of the cache holds current factors
+  float2* pcache = nullptr;   // phase-factor cache of pslots depths (fwix_plan_set_phase_cache)
+  int pslots = 0;             // depth iz lives in slot iz % pslots
+  std::vector<int> pslot_iz;  // depth whose current factors a slot holds, -1 for none
   int pq_nx() const { return d.NX / 2 + 1; }
   int pq_ny() const { return d.NY / 2 + 1; }
   long long pdepth() const { return (long long)desc.nref * d.nw * pq_nx() * pq_ny(); }
@@ -236,15 +237,16 @@ fwix_status for_chunks(const fwix_plan* p, SpecArgs a, F f) {
 fwix_status phase_factors(fwix_plan* p, int iz, SpecArgs& a, cudaStream_t s) {
   a.ptab = nullptr;
   if (!p->pcache) return FWIX_OK;
-  float2* dst = p->pcache + iz * p->pdepth();
+  const int slot = iz % p->pslots;
+  float2* dst = p->pcache + slot * p->pdepth();
   a.ptab_nx = p->pq_nx();
   a.ptab_ny = p->pq_ny();
-  if (!p->pbuilt[iz]) {
+  if (p->pslot_iz[slot] != iz) {
     SpecArgs b = a;
     b.sref = p->sref + (long long)iz * p->desc.nref * p->d.nw;
     b.nterm = p->desc.nref;
     FWIX_TRY(cu(fwix::launch_phase_table(b, dst, s), "phase-factor cache"));
-    p->pbuilt[iz] = 1;
+    p->pslot_iz[slot] = iz;
   }
   a.ptab = dst;
   return FWIX_OK;
@@ -487,18 +489,20 @@ size_t fwix_plan_phase_cache_bytes(const fwix_plan* p) {
 
 fwix_status fwix_plan_set_phase_cache(fwix_plan* p, void* ptr, size_t bytes) {
   if (!p) return fail(FWIX_ERR_INVALID, "null plan");
-  if (ptr && bytes < fwix_plan_phase_cache_bytes(p))
-    return fail(FWIX_ERR_WORKSPACE, "phase cache smaller than fwix_plan_phase_cache_bytes");
+  const size_t depth_bytes = (size_t)p->pdepth() * sizeof(float2);
+  if (ptr && bytes < depth_bytes)
+    return fail(FWIX_ERR_WORKSPACE, "phase cache smaller than one depth (fwix_plan_phase_cache_bytes / nz)");
   if (((uintptr_t)ptr) % 16 != 0) return fail(FWIX_ERR_INVALID, "phase cache must be 16-byte aligned");
   p->pcache = (float2*)ptr;
-  p->pbuilt.assign(p->desc.nz, 0);
+  p->pslots = ptr ? (int)std::min<size_t>((size_t)p->desc.nz, bytes / depth_bytes) : 0;
+  p->pslot_iz.assign(std::max(p->pslots, 1), -1);
   return FWIX_OK;
 }
 
 fwix_status fwix_plan_set_refs(fwix_plan* p, const void* sref, const uint8_t* labels, int64_t z_stride,
                                int64_t w_stride) {
   if (!p || !sref || !labels) return fail(FWIX_ERR_INVALID, "null plan, refs or labels");
-  p->pbuilt.assign(p->desc.nz, 0);  // cached factors belong to the previous references
+  p->pslot_iz.assign(std::max(p->pslots, 1), -1);  // cached factors belong to the previous references
   p->sref = (const float2*)sref;
   p->labels = labels;
   p->lab_z = z_stride;

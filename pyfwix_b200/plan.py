@@ -76,11 +76,14 @@ class Plan:
             L.check(self.lib.fwix_plan_set_workspace(self._h, _p(self._ws), need))
         return self._ws
 
-    def enable_phase_cache(self, max_fraction=0.4):
+    def enable_phase_cache(self, max_fraction=0.4, depths=None):
         """Bind a phase-factor cache (each depth's factors computed once and reused)
-        when it fits in ``max_fraction`` of the device's free memory.  Returns
-        whether the cache is on."""
+        of every depth, or of ``depths`` depths in rotation, when it fits in
+        ``max_fraction`` of the device's free memory.  Returns whether the cache
+        is on."""
         need = int(self.lib.fwix_plan_phase_cache_bytes(self._h))
+        if depths is not None:
+            need = need // self.nz * max(1, min(int(depths), self.nz))
         free, _ = torch.cuda.mem_get_info(self.device)
         if need == 0 or need > max_fraction * free:
             return False
