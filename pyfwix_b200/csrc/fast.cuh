@@ -41,8 +41,44 @@ struct Radices {
 // SW selects the sample placement of the line exchanges: 0 puts sample p at
 // p ^ ((p >> 3) & 15), 1 at p + (p >> 4) (conflict-free for radix-16 stages on
 // 16-lane lines); LINE_EXTRA is the room the second needs past N.
-template <int N_, int E_, class RS, int SW_ = 0>
+// Placement of each line exchange of a plan, one code per exchange: the forward
+// transform's exchanges (after stages 0 .. NS-2) first, then the inverse's.  -1
+// keeps the plan's default placement (xswz), 0 is p itself, any other code
+// a | m << 4 | mask << 8 places sample p at p ^ (((p >> a) * m) & mask), which
+// stays within the aligned block of mask + 1 samples; a plan may only use codes
+// that permute 0 .. N-1 (with m = 1 every a does: bit i of the result is bit i
+// of p plus bit i + a).  Chosen per exchange so that the stores of one stage and
+// the loads of the next hit as few shared-memory banks twice as possible (the
+// strides of an exchange depend on its stage).
+template <int... Cs>
+struct XSw {
+  static constexpr int n = sizeof...(Cs);
+  __host__ __device__ static constexpr int get(int i) {
+    constexpr int c[] = {Cs..., -1};
+    return c[i];
+  }
+};
+using NoXSw = XSw<>;
+constexpr int xs(int a, int m, int mask) { return a | m << 4 | mask << 8; }  // code of p ^ (((p >> a) * m) & mask)
+// Whether every code of XS maps 0 .. N-1 onto itself one to one.
+template <int N, class XS>
+constexpr bool xsw_permutes() {
+  for (int i = 0; i < XS::n; ++i) {
+    const int c = XS::get(i);
+    if (c <= 0) continue;
+    bool seen[N] = {};
+    for (int p = 0; p < N; ++p) {
+      const int q = p ^ (((p >> (c & 15)) * ((c >> 4) & 15)) & (c >> 8));
+      if (q < 0 || q >= N || seen[q]) return false;
+      seen[q] = true;
+    }
+  }
+  return true;
+}
+
+template <int N_, int E_, class RS, int SW_ = 0, class XS_ = NoXSw>
 struct Plan {
+  using XS = XS_;
   static constexpr int N = N_;
   static constexpr int E = E_;
   static constexpr int SW = SW_;
@@ -51,6 +87,8 @@ struct Plan {
   static constexpr int G = 32 / T;     // lines per warp
   static constexpr int NS = RS::NS;
   static_assert(T == 8 || T == 16 || T == 32, "a line takes 8, 16 or 32 lanes");
+  static_assert(XS::n == 0 || XS::n == 2 * (NS - 1), "one exchange placement per exchange of each direction");
+  static_assert(xsw_permutes<N_, XS_>(), "an exchange placement must permute the line");
   __host__ __device__ static constexpr int radix(int s) { return RS::get(s); }
 };
 
@@ -66,6 +104,18 @@ __device__ __forceinline__ int swz(int p) { return p ^ ((p >> 3) & 15); }
 template <class P>
 __device__ __forceinline__ int xswz(int p) {  // exchange placement of plan P
   return P::SW == 1 ? p + (p >> 4) : swz(p);
+}
+// Placement of exchange S of the forward (REV false) or inverse transform.
+template <class P, bool REV, int S>
+__device__ __forceinline__ int xch(int p) {
+  constexpr int c = P::XS::n ? P::XS::get((REV ? P::NS - 1 : 0) + S) : -1;
+  if constexpr (c < 0) {
+    return xswz<P>(p);
+  } else if constexpr (c == 0) {
+    return p;
+  } else {
+    return p ^ (((p >> (c & 15)) * ((c >> 4) & 15)) & (c >> 8));
+  }
 }
 
 // Twiddles in shared memory, one table per stage and order: stage S (span Ns,
@@ -150,11 +200,11 @@ __device__ __forceinline__ void stages(float2 (&v)[P::E], int t, const float2* _
       const int j = t + P::T * b;
       const int base = (j / Ns) * Ns * R + (j % Ns);
 #pragma unroll
-      for (int r = 0; r < R; ++r) line[xswz<P>(base + r * Ns)] = v[b * R + r];
+      for (int r = 0; r < R; ++r) line[xch<P, REV, S>(base + r * Ns)] = v[b * R + r];
     }
     __syncwarp();
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) v[e] = line[xswz<P>(lpos<P, R2>(t, e))];
+    for (int e = 0; e < P::E; ++e) v[e] = line[xch<P, REV, S>(lpos<P, R2>(t, e))];
     stages<P, REV, INV, S + 1>(v, t, tw, line);
   }
 }

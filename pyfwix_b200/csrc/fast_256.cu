@@ -5,5 +5,5 @@
 #include "fast.cuh"
 
 using FwixRowPlan256 = fwix::fast::Plan<256, 16, fwix::fast::Radices<16, 16>, 1>;
-using FwixColPlan256 = fwix::fast::Plan<256, 8, fwix::fast::Radices<8, 8, 4>>;
+using FwixColPlan256 = fwix::fast::Plan<256, 8, fwix::fast::Radices<8, 8, 4>, 0, fwix::fast::XSw<-1, -1, fwix::fast::xs(2, 1, 15), -1>>;
 FWIX_FAST_INSTANTIATE2(FwixRowPlan256, FwixColPlan256, 256)
