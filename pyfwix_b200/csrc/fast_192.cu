@@ -1,9 +1,11 @@
 // Register-resident passes for lines of 192 samples: 16 lanes x 12 samples,
-// radix stages 4,4,4,3.
+// radix stages 12, 4, 4 (the radix-12 butterfly is a prime-factor 4 x 3
+// transform, so the first stage needs no twiddles and the line is exchanged
+// through shared memory once less than with radix-4 stages throughout).
 // The exchange placements (XSw) are the ones with the fewest shared-memory
 // bank conflicts for this plan's strides, per exchange.
 #include "fast.cuh"
 
-using FwixPlan192 = fwix::fast::Plan<192, 12, fwix::fast::Radices<4,4,4,3>, 0,
-                                        fwix::fast::XSw<fwix::fast::xs(2, 1, 15), fwix::fast::xs(2, 1, 15), -1, 0, 0, -1>>;
+using FwixPlan192 = fwix::fast::Plan<192, 12, fwix::fast::Radices<12, 4, 4>, 0,
+    fwix::fast::XSw<fwix::fast::xs(2, 1, 15), -1, fwix::fast::xs(2, 1, 15), fwix::fast::xs(2, 1, 15)>>;
 FWIX_FAST_INSTANTIATE(FwixPlan192, 192)

@@ -1,9 +1,11 @@
 // Register-resident passes for lines of 640 samples: 32 lanes x 20 samples,
-// radix stages 4,4,4,2,5.
+// radix stages 20, 4, 4, 2 (the radix-20 butterfly is a prime-factor 4 x 5
+// transform, so the first stage needs no twiddles and the line is exchanged
+// through shared memory once less than with radix-4 stages throughout).
 // The exchange placements (XSw) are the ones with the fewest shared-memory
 // bank conflicts for this plan's strides, per exchange.
 #include "fast.cuh"
 
-using FwixPlan640 = fwix::fast::Plan<640, 20, fwix::fast::Radices<4,4,4,2,5>, 0,
-                                        fwix::fast::XSw<fwix::fast::xs(2, 1, 15), fwix::fast::xs(2, 1, 15), -1, -1, 0, 0, fwix::fast::xs(5, 7, 15), fwix::fast::xs(4, 15, 15)>>;
+using FwixPlan640 = fwix::fast::Plan<640, 20, fwix::fast::Radices<20, 4, 4, 2>, 0,
+    fwix::fast::XSw<fwix::fast::xs(2, 1, 15), fwix::fast::xs(4, 7, 7), -1, fwix::fast::xs(1, 1, 15), -1, fwix::fast::xs(2, 1, 15)>>;
 FWIX_FAST_INSTANTIATE(FwixPlan640, 640)

@@ -199,6 +199,41 @@ struct Dft<16, INV> {
   }
 };
 
+// Radix 4 N2 for N2 = 3, 5 by the prime-factor (Good-Thomas) mapping, which needs
+// no twiddles between the two transforms: input n = (N2 n1 + 4 n2) mod N, radix-N2
+// transforms over n2, radix-4 transforms over n1, output k = k1 (mod 4),
+// k = k2 (mod N2), i.e. k = (A k1 + B k2) mod N with A = N2 (N2^-1 mod 4) and
+// B = 4 (4^-1 mod N2): (9, 4) for 12, (5, 16) for 20.
+template <int N2, int A, int B, bool INV>
+__device__ __forceinline__ void dft_pfa4(float2 (&v)[4 * N2]) {
+  constexpr int N = 4 * N2;
+  float2 y[4][N2];
+#pragma unroll
+  for (int n1 = 0; n1 < 4; ++n1) {
+    float2 u[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) u[n2] = v[(N2 * n1 + 4 * n2) % N];
+    Dft<N2, INV>::run(u);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) y[n1][k2] = u[k2];
+  }
+#pragma unroll
+  for (int k2 = 0; k2 < N2; ++k2) {
+    float2 u[4] = {y[0][k2], y[1][k2], y[2][k2], y[3][k2]};
+    Dft<4, INV>::run(u);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) v[(A * k1 + B * k2) % N] = u[k1];
+  }
+}
+template <bool INV>
+struct Dft<12, INV> {
+  static __device__ __forceinline__ void run(float2 (&v)[12]) { dft_pfa4<3, 9, 4, INV>(v); }
+};
+template <bool INV>
+struct Dft<20, INV> {
+  static __device__ __forceinline__ void run(float2 (&v)[20]) { dft_pfa4<5, 5, 16, INV>(v); }
+};
+
 // Radix 7 from the symmetric pair form y_m = v0 + sum_k cos(2 pi k m/7) t_k -+
 // i sum_k sin(2 pi k m/7) u_k with t_k = v_k + v_{7-k}, u_k = v_k - v_{7-k}.
 template <bool INV>

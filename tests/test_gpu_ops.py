@@ -15,7 +15,8 @@ TOL = 1e-5
 
 
 @pytest.mark.parametrize("NX,NY", [(16, 16), (20, 12), (100, 100), (128, 128), (192, 40), (320, 24),
-                                   (384, 10), (512, 8), (1000, 4), (30, 1024), (1, 8)])
+                                   (384, 10), (512, 8), (1000, 4), (30, 1024), (1, 8), (96, 160), (160, 96),
+                                   (640, 384), (384, 192), (64, 640), (20, 320)])
 def test_fft2d(NX, NY):
     """cuFFT2d forward / adjoint (operator/src/FFT.cpp:36-55) and the FFT tests of
     operator/tests/operator_unit_test.cpp:36-99."""
@@ -94,6 +95,8 @@ STEP_CASES = [
     dict(nx=100, ny=60, padx=28, pady=4, eps=0.0, complex_refs=False, labels_per_w=False),
     dict(nx=256, ny=256, padx=0, pady=0, eps=0.0, complex_refs=False, labels_per_w=False),
     dict(nx=248, ny=252, padx=8, pady=4, eps=0.01, complex_refs=True, labels_per_w=True),
+    dict(nx=380, ny=380, padx=4, pady=4, eps=0.0, complex_refs=False, labels_per_w=False),
+    dict(nx=96, ny=160, padx=0, pady=0, eps=0.01, complex_refs=True, labels_per_w=True),
 ]
 
 
