@@ -214,6 +214,61 @@ fwix_status fwix_born(fwix_plan* plan, int adjoint, const fwix_traces* rec, cons
                       const void* bg_up, void* dslow, void* dden, int64_t model_w_stride,
                       void* data, int add, void* stream);
 
+/* ---- one-call forms of the depth steps and the image --------------------------
+ * fwix_pspi_step / fwix_nsps_step: PSPI::cu_forward / cu_adjoint
+ * (propagator/src/PSPI.cpp:6-103) and NSPS (propagator/src/NSPS.cpp:6-45) at
+ * level iz, overwriting psi_out (psi_in may equal psi_out).  adjoint: 0 forward,
+ * 1 the add-version adjoint (PSPI.cpp:26-44, no taper), 2 the in-place adjoint
+ * (PSPI.cpp:85-103, taper last); the same as fwix_step with that direction. */
+fwix_status fwix_pspi_step(fwix_plan* plan, int iz, const void* psi_in, void* psi_out, int adjoint,
+                           void* stream);
+fwix_status fwix_nsps_step(fwix_plan* plan, int iz, const void* psi_in, void* psi_out, int adjoint,
+                           void* stream);
+/* Imaging condition of one level summed over frequency and shots
+ * (imaging_condition.cu:57-108 with the sum over w of Scattering.cpp:104-111):
+ * image[y][x] (+)= sum_w Re sum_s conj(S) R over the unpadded window; S, R are
+ * wavefields [ns][nw][NY][NX], image is float [ny][nx]. */
+fwix_status fwix_image_accumulate(fwix_plan* plan, const void* S, const void* R, float* image, int add,
+                                  void* stream);
+
+/* ---- batched sweeps over many instances --------------------------------------
+ * fwix_sweep runs one sweep for each of ninst instances -- shots of their own
+ * grid, band, references and buffers, each described by its plan and the
+ * arrays below -- the way the reference's StreamingPropagator runs its
+ * propagators on TBB threads, one CUDA stream each
+ * (propagator/src/StreamingPropagator.cpp).  Instances are assigned largest
+ * first (nx*ny*nw*nz*ns) to the least loaded of the nstreams streams given;
+ * every stream first waits for the work already enqueued on `stream`, and
+ * `stream` waits for all of them at the end, so the call is stream ordered on
+ * `stream` like the others (and can be captured into a CUDA graph from it).
+ * With nstreams == 0 everything runs on `stream`.  Instances must not share a
+ * plan.  Per kind, the instance fields used:
+ *   DOWN / UP  : wfld (in place), adjoint        fwix_downward / fwix_upward
+ *   MODEL      : src, rec, wavelet, data, add, bg_down, bg_up   fwix_propagate
+ *   IMAGE      : src, rec, wavelet, data, image, add            fwix_migrate
+ *   BORN_FWD   : rec, bg_down, bg_up, dslow, dden, model_w_stride, data, add
+ *   BORN_ADJ   : the same, data in, (dslow, dden) out           fwix_born */
+enum { FWIX_SWEEP_DOWN = 0, FWIX_SWEEP_UP = 1, FWIX_SWEEP_MODEL = 2, FWIX_SWEEP_IMAGE = 3,
+       FWIX_SWEEP_BORN_FWD = 4, FWIX_SWEEP_BORN_ADJ = 5 };
+typedef struct fwix_instance {
+  fwix_plan* plan;
+  const fwix_traces* src;
+  const fwix_traces* rec;
+  const void* wavelet;
+  void* data;
+  void* wfld;
+  float* image;
+  void* bg_down;
+  void* bg_up;
+  void* dslow;
+  void* dden;
+  int64_t model_w_stride;
+  int adjoint;
+  int add;
+} fwix_instance;
+fwix_status fwix_sweep(int kind, const fwix_instance* insts, int ninst, void* const* streams, int nstreams,
+                       void* stream);
+
 /* ---- allocation-free depth step ----------------------------------------------
  * fwix_step_noalloc has no counterpart in the reference.  It is fwix_step for
  * callers that cannot call cudaMalloc -- for example a host application or

@@ -41,6 +41,15 @@ P = ctypes.c_void_p
 I = ctypes.c_int
 I64 = ctypes.c_int64
 
+
+class FwixInstance(ctypes.Structure):
+    """fwix_instance: one instance of a batched sweep (fwix_sweep)."""
+    _fields_ = [
+        ("plan", P), ("src", P), ("rec", P), ("wavelet", P), ("data", P), ("wfld", P), ("image", P),
+        ("bg_down", P), ("bg_up", P), ("dslow", P), ("dden", P), ("model_w_stride", I64),
+        ("adjoint", I), ("add", I),
+    ]
+
 # name -> argtypes (all return fwix_status as int unless listed in _RET)
 SIGNATURES = {
     "fwix_last_error": [],
@@ -75,7 +84,12 @@ SIGNATURES = {
     "fwix_migrate": [P, P, P, P, P, P, I, P],
     "fwix_born": [P, I, P, P, P, P, P, I64, P, I, P],
     "fwix_step_noalloc": [ctypes.POINTER(FwixDesc), I, I, I, P, P, I64, I64, P, P, I, P],
+    "fwix_pspi_step": [P, I, P, P, I, P],
+    "fwix_nsps_step": [P, I, P, P, I, P],
+    "fwix_image_accumulate": [P, P, P, P, I, P],
+    "fwix_sweep": [I, ctypes.POINTER(FwixInstance), I, ctypes.POINTER(P), I, P],
 }
+SWEEP_DOWN, SWEEP_UP, SWEEP_MODEL, SWEEP_IMAGE, SWEEP_BORN_FWD, SWEEP_BORN_ADJ = range(6)
 _RET = {"fwix_last_error": ctypes.c_char_p, "fwix_version": I, "fwix_plan_workspace_bytes": ctypes.c_size_t,
         "fwix_plan_phase_cache_bytes": ctypes.c_size_t,
         "fwix_launch_count": ctypes.c_uint64}

@@ -7,9 +7,9 @@ plan.  The reference runs such a batch as ``StreamingPropagator`` instances on
 TBB threads, one CUDA stream each (``propagator/src/StreamingPropagator.cpp``),
 and images each shot with ``ExtendedBorn``'s imaging condition
 (``propagator/src/imaging_condition.cu:9-108``).  Here the instances are
-spread over a fixed set of CUDA streams (largest first, each to the stream with
-the least work queued), so the kernels of small shots fill the SMs that large
-ones leave idle, and the whole batch -- every instance's depth loop -- can be
+spread over a fixed set of CUDA streams by ``fwix_sweep`` (largest first, each
+to the stream with the least work queued), so the kernels of small shots fill
+the SMs that large ones leave idle, and the whole batch -- every instance's depth loop -- can be
 captured once into one CUDA graph and replayed, which takes the host out of
 the loop: one graph launch per batch instead of ~10 kernel launches per depth
 and shot.
@@ -22,14 +22,12 @@ in the same order on its own buffers.
 """
 from __future__ import annotations
 
-import heapq
-
 import numpy as np
 import torch
 
 from . import _lib as L
 from . import refsampler
-from .plan import Plan
+from .plan import Plan, sweep
 
 
 class Instance:
@@ -83,19 +81,7 @@ class MigrationBatch:
         with torch.cuda.device(self.device):
             self.inst = [Instance(w, self.device, slow2_fn(w, self.device)) for w in workloads]
             self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, int(nstreams)))]
-        self.assign = self._balance()
         self.graph = None
-
-    def _balance(self):
-        """Instances per stream: largest first onto the least-loaded stream."""
-        order = sorted(range(len(self.inst)), key=lambda i: (-self.inst[i].cells, i))
-        heap = [(0, k) for k in range(len(self.streams))]
-        lanes = [[] for _ in self.streams]
-        for i in order:
-            load, k = heapq.heappop(heap)
-            lanes[k].append(i)
-            heapq.heappush(heap, (load + self.inst[i].cells, k))
-        return lanes
 
     @property
     def cells(self):
@@ -113,15 +99,10 @@ class MigrationBatch:
             i.migrate()
 
     def _enqueue_streams(self):
-        main = torch.cuda.current_stream(self.device)
-        for k, lane in enumerate(self.assign):
-            s = self.streams[k]
-            s.wait_stream(main)
-            with torch.cuda.stream(s):
-                for i in lane:
-                    self.inst[i].migrate()
-        for s in self.streams:
-            main.wait_stream(s)
+        # fwix_sweep assigns the instances (largest first onto the least loaded
+        # stream) and forks / joins them on the caller's stream
+        sweep(L.SWEEP_IMAGE, [dict(plan=i.plan, src=i.src, rec=i.rec, wavelet=i.wavelet, data=i.data,
+                                   image=i.image) for i in self.inst], self.streams)
 
     def run_streams(self):
         """All shots at once over the streams, joined back into the current stream."""

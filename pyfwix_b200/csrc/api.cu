@@ -995,4 +995,101 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
   return FWIX_OK;
 }
 
+
+// ---------------------------------------------------------------- one-call forms
+fwix_status fwix_pspi_step(fwix_plan* p, int iz, const void* in, void* out, int adjoint, void* stream) {
+  return fwix_step(p, FWIX_STEP_PSPI, iz, adjoint, in, out, 0, stream);
+}
+
+fwix_status fwix_nsps_step(fwix_plan* p, int iz, const void* in, void* out, int adjoint, void* stream) {
+  return fwix_step(p, FWIX_STEP_NSPS, iz, adjoint, in, out, 0, stream);
+}
+
+fwix_status fwix_image_accumulate(fwix_plan* p, const void* S, const void* R, float* image, int add,
+                                  void* stream) {
+  return fwix_correlate(p, S, R, image, add, 0, stream);
+}
+
+// ---------------------------------------------------------------- batched sweeps
+namespace {
+
+fwix_status sweep_one(int kind, const fwix_instance& in, void* s) {
+  switch (kind) {
+    case FWIX_SWEEP_DOWN: return fwix_downward(in.plan, in.adjoint, in.wfld, s);
+    case FWIX_SWEEP_UP: return fwix_upward(in.plan, in.adjoint, in.wfld, s);
+    case FWIX_SWEEP_MODEL:
+      return fwix_propagate(in.plan, in.src, in.rec, in.wavelet, in.data, in.add, in.bg_down, in.bg_up, s);
+    case FWIX_SWEEP_IMAGE: return fwix_migrate(in.plan, in.src, in.rec, in.wavelet, in.data, in.image, in.add, s);
+    case FWIX_SWEEP_BORN_FWD:
+    case FWIX_SWEEP_BORN_ADJ:
+      return fwix_born(in.plan, kind == FWIX_SWEEP_BORN_ADJ, in.rec, in.bg_down, in.bg_up, in.dslow, in.dden,
+                       in.model_w_stride, in.data, in.add, s);
+    default: return fail(FWIX_ERR_INVALID, "unknown sweep kind");
+  }
+}
+
+}  // namespace
+
+fwix_status fwix_sweep(int kind, const fwix_instance* insts, int ninst, void* const* streams, int nstreams,
+                       void* stream) {
+  if (ninst < 0 || (ninst > 0 && !insts) || nstreams < 0 || (nstreams > 0 && !streams))
+    return fail(FWIX_ERR_INVALID, "null or negative instance / stream list");
+  if (kind < FWIX_SWEEP_DOWN || kind > FWIX_SWEEP_BORN_ADJ) return fail(FWIX_ERR_INVALID, "unknown sweep kind");
+  for (int i = 0; i < ninst; ++i) {
+    if (!insts[i].plan) return fail(FWIX_ERR_INVALID, "instance " + std::to_string(i) + " has no plan");
+    for (int j = 0; j < i; ++j)
+      if (insts[j].plan == insts[i].plan)
+        return fail(FWIX_ERR_INVALID, "instances " + std::to_string(j) + " and " + std::to_string(i) +
+                                          " share a plan (its workspace would be used by two streams)");
+  }
+  if (nstreams == 0) {
+    for (int i = 0; i < ninst; ++i) FWIX_TRY(sweep_one(kind, insts[i], stream));
+    return FWIX_OK;
+  }
+  // largest first onto the least loaded stream
+  std::vector<int> order(ninst);
+  for (int i = 0; i < ninst; ++i) order[i] = i;
+  auto cost = [&](int i) {
+    const fwix_desc& q = insts[i].plan->desc;
+    return (double)insts[i].plan->d.NX * insts[i].plan->d.NY * q.nw * q.ns * q.nz;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  std::vector<double> load(nstreams, 0.0);
+  std::vector<std::vector<int>> lanes(nstreams);
+  for (int i : order) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    lanes[k].push_back(i);
+    load[k] += cost(i);
+  }
+  cudaStream_t main = (cudaStream_t)stream;
+  cudaEvent_t fork = nullptr;
+  FWIX_CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  fwix_status st = FWIX_OK;
+  std::vector<cudaEvent_t> joins;
+  cudaError_t e = cudaEventRecord(fork, main);
+  for (int k = 0; k < nstreams && e == cudaSuccess && st == FWIX_OK; ++k) {
+    if (lanes[k].empty()) continue;
+    cudaStream_t sk = (cudaStream_t)streams[k];
+    e = cudaStreamWaitEvent(sk, fork, 0);
+    for (size_t j = 0; j < lanes[k].size() && e == cudaSuccess && st == FWIX_OK; ++j)
+      st = sweep_one(kind, insts[lanes[k][j]], sk);
+    cudaEvent_t join = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+      joins.push_back(join);
+      e = cudaEventRecord(join, sk);
+    }
+  }
+  // the caller's stream waits for every lane enqueued so far, also after a failure
+  for (cudaEvent_t j : joins) {
+    const cudaError_t w = cudaStreamWaitEvent(main, j, 0);
+    if (e == cudaSuccess) e = w;
+    cudaEventDestroy(j);
+  }
+  cudaEventDestroy(fork);
+  if (st != FWIX_OK) return st;
+  if (e != cudaSuccess) return fail(FWIX_ERR_CUDA, std::string("fwix_sweep: ") + cudaGetErrorString(e));
+  return FWIX_OK;
+}
+
 }  // extern "C"

@@ -276,3 +276,36 @@ class Traces:
                 self._h = ctypes.c_void_p()
         except Exception:
             pass
+
+
+def _addr(t):
+    return t.data_ptr() if t is not None else None
+
+
+def sweep(kind, instances, streams=()):
+    """One batched sweep (``fwix_sweep``) over instances, each a dict with its
+    ``plan`` and the arrays of that sweep kind (``src``, ``rec``: Traces;
+    ``wavelet``, ``data``, ``wfld``, ``image``, ``bg_down``, ``bg_up``, ``dslow``,
+    ``dden``: tensors; ``adjoint``, ``add``: flags).  Instances run on the given
+    torch streams (largest first onto the least loaded), joined back into the
+    current stream; no streams runs them one after the other on it."""
+    n = len(instances)
+    arr = (L.FwixInstance * max(n, 1))()
+    for k, d in enumerate(instances):
+        plan = d["plan"]
+        plan.ensure_workspace(L.WS_BORN if kind in (L.SWEEP_BORN_FWD, L.SWEEP_BORN_ADJ) else
+                              L.WS_SWEEP if kind in (L.SWEEP_MODEL, L.SWEEP_IMAGE) else L.WS_STEP)
+        mw = 0
+        if d.get("dslow") is not None:
+            ds = d["dslow"]
+            mw = 0 if (ds.shape[1] == 1 and plan.nw > 1) else plan.ny * plan.nx
+        arr[k] = L.FwixInstance(
+            plan=plan._h.value, src=d["src"]._h.value if d.get("src") is not None else None,
+            rec=d["rec"]._h.value if d.get("rec") is not None else None,
+            wavelet=_addr(d.get("wavelet")), data=_addr(d.get("data")), wfld=_addr(d.get("wfld")),
+            image=_addr(d.get("image")), bg_down=_addr(d.get("bg_down")), bg_up=_addr(d.get("bg_up")),
+            dslow=_addr(d.get("dslow")), dden=_addr(d.get("dden")), model_w_stride=mw,
+            adjoint=int(d.get("adjoint", 0)), add=int(d.get("add", 0)))
+    hs = (ctypes.c_void_p * max(len(streams), 1))(*[s.cuda_stream for s in streams])
+    lib = L.load()
+    L.check(lib.fwix_sweep(int(kind), arr, n, hs, len(streams), _stream()))

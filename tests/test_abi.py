@@ -47,3 +47,37 @@ def test_invalid_descriptor_is_an_error_not_an_exit():
     assert st == -2 and b"2^a 3^b 5^c" in lib.fwix_last_error()
     with pytest.raises(_lib.FwixError):
         _lib.check(-4)
+
+
+def test_instance_struct_layout_matches_header(tmp_path):
+    """The ctypes mirror of fwix_instance has the C struct's size and field
+    offsets (compiled here with the system C compiler from the header)."""
+    import shutil
+    import subprocess
+    from pyfwix_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    fields = [f for f, _ in _lib.FwixInstance._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "fwix_b200.h"\nint main(void) {\n'
+                   '  printf("%zu", sizeof(fwix_instance));\n'
+                   + "".join(f'  printf(" %zu", offsetof(fwix_instance, {f}));\n' for f in fields)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [ctypes.sizeof(_lib.FwixInstance)] + [getattr(_lib.FwixInstance, f).offset for f in fields]
+    assert got == want
+
+
+def test_sweep_argument_checks_without_gpu():
+    """fwix_sweep rejects a bad kind or a negative count before touching the GPU,
+    and an empty batch with no streams is a no-op."""
+    from pyfwix_b200 import _lib
+    lib = _lib.load()
+    assert lib.fwix_sweep(99, None, 0, None, 0, None) == -1
+    assert b"kind" in lib.fwix_last_error()
+    assert lib.fwix_sweep(_lib.SWEEP_IMAGE, None, -1, None, 0, None) == -1
+    assert b"instance" in lib.fwix_last_error()
+    assert lib.fwix_sweep(_lib.SWEEP_IMAGE, None, 0, None, 0, None) == 0
