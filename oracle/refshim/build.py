@@ -47,7 +47,7 @@ def build(force=False):
            "-Xcompiler", "-fPIC", "-w",
            "-I", os.path.join(HERE, "stub"), "-I", os.path.join(REF, "operator", "src"),
            "-I", os.path.join(REF, "propagator", "src"),
-           os.path.join(HERE, "shim.cu")] + sources() + ["-o", LIB + ".tmp"]
+           os.path.join(HERE, "shim.cu")] + sources() + ["-lcufft", "-o", LIB + ".tmp"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("reference shim build failed:\n" + res.stdout + res.stderr)

@@ -12,6 +12,8 @@
 // around a caller pointer (n / o / d fastest axis first) and frees it after
 // the launch.  Every entry point synchronises the device before returning and
 // returns the CUDA error code (0 = success).
+#include <cufft.h>
+
 #include <new>
 #include <vector>
 
@@ -147,6 +149,66 @@ int refshim_scale_by_iw(int adjoint, int NX, int NY, int nw, int ns, const float
 int refshim_pad(int nx, int ny, int NX, int NY, int nw, const void* in, void* out) {
   Header m(in, {nx, ny, nw}), d(out, {NX, NY, nw});
   pad_fwd<<<kGrid3, kBlock3>>>(m.v, d.v);
+  return done();
+}
+
+// PSPI::cu_forward (propagator/src/PSPI.cpp:6-24) replayed with the reference's
+// kernels and cuFFT on the default stream, for timing the reference's own GPU
+// depth step: data->zero(); taper->cu_forward(0, model, model_k);
+// fft2d->cu_forward(model_k); per reference: ps->cu_forward(0, model_k,
+// wfld_ref) (zero, then ps_forward); fft2d->cu_adjoint(wfld_ref);
+// select->cu_forward(1, wfld_ref, data).  Launch shapes as the reference's
+// Propagator hands them to its operators (propagator/src/Propagator.cpp:20-21:
+// grid {32, 4, 4}, block {16, 16, 4}; Selector.h: 256-thread blocks over every
+// sample).  Two differences, both in the reference's favour: the cuFFT plans
+// carry no store callback (operator/src/fft_callback.cu scales every stored
+// element by 1/sqrt(NX NY); here the outputs are NX NY times the unitary ones
+// and that work is not done), and the per-depth host-to-device copies of the
+// labels and reference slownesses (Selector.h set_labels, PhaseShift.h
+// set_slow) are not made: labels [nw][NY][NX] int32 and sref [nref][nw] are
+// already on the device.  One warm-up step, then `reps` steps between CUDA
+// events; *ms receives the mean time per step.
+int refshim_pspi_forward_timed(int NX, int NY, int nw, int ns, int nref, const float* w2, const float* kx,
+                               const float* ky, const void* sref, const int* labels, float dz, float eps, int tapx,
+                               int tapy, const void* in, void* out, void* model_k, void* wfld_ref, int reps,
+                               float* ms) {
+  Header m(in, {NX, NY, nw, ns}), d(out, {NX, NY, nw, ns}), mk(model_k, {NX, NY, nw, ns}),
+      wr(wfld_ref, {NX, NY, nw, ns});
+  cufftHandle plan;
+  int dims[2] = {NY, NX};
+  if (cufftPlanMany(&plan, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nw * ns) != CUFFT_SUCCESS) return -1;
+  const size_t bytes = (size_t)NX * NY * nw * ns * sizeof(cuFloatComplex);
+  const dim3 g(32, 4, 4), b(16, 16, 4);
+  const unsigned sel_grid = (unsigned)(((size_t)NX * NY * nw * ns + 255) / 256);
+  cufftComplex* K = (cufftComplex*)model_k;
+  cufftComplex* W = (cufftComplex*)wfld_ref;
+  auto step = [&]() {
+    cudaMemsetAsync(out, 0, bytes);
+    cudaMemsetAsync(model_k, 0, bytes);
+    taper_forward<<<g, b>>>(m.v, mk.v, tapx, tapy);
+    cufftExecC2C(plan, K, K, CUFFT_FORWARD);
+    for (int r = 0; r < nref; ++r) {
+      cudaMemsetAsync(wfld_ref, 0, bytes);
+      ps_forward<<<g, b>>>(mk.v, wr.v, w2, kx, ky, (const cuFloatComplex*)sref + (size_t)r * nw, dz, eps);
+      cufftExecC2C(plan, W, W, CUFFT_INVERSE);
+      select_forward<<<sel_grid, 256>>>(wr.v, d.v, r, labels);
+    }
+  };
+  step();
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaDeviceSynchronize();
+  cudaEventRecord(e0);
+  for (int i = 0; i < reps; ++i) step();
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  *ms = t / (float)(reps > 0 ? reps : 1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cufftDestroy(plan);
   return done();
 }
 
