@@ -60,7 +60,8 @@ def args_():
     ap.add_argument("--profile-n", type=int, default=None, help="lateral size of the profiled step (default: the workload's)")
     ap.add_argument("--profile-nw", type=int, default=96)
     ap.add_argument("--profile-nref", type=int, default=4)
-    ap.add_argument("--profile-step", choices=["pspi", "nsps", "pspi-adj", "nsps-adj"], default=None,
+    ap.add_argument("--profile-step", choices=["pspi", "nsps", "pspi-adj", "nsps-adj", "smooth", "smooth-adj"],
+                    default=None,
                     help="run one depth step of the workload's wavefield and exit (for ncu captures)")
     return ap.parse_args()
 
@@ -400,6 +401,20 @@ def profile_step(a):
     from pyfwix_b200 import refsampler, workloads
     from pyfwix_b200.plan import Plan
     torch.cuda.set_device(0)
+    if a.profile_step.startswith("smooth"):
+        # one differentiable step of the FWI workload (384 x 384 x 96, true model, depth 1)
+        from pyfwix_b200.fwi import SmoothFWI
+        w, s_true, _ = workloads.config4(nz=2)
+        par = dict(nref=w.nref, padx=0, pady=0, taperx=w.taperx, tapery=w.tapery, eps=0.0, ox=w.ox, oy=w.oy,
+                   oz=w.oz, dx=w.dx, dy=w.dy, dz=w.dz, ow=w.ow, dw=w.dw, checkpoint=None)
+        prob = SmoothFWI(s_true.shape, w.geom, torch.as_tensor(w.wavelet).cuda(), par, device="cuda")
+        prob.set_slowness(torch.as_tensor(s_true))
+        x = torch.randn(prob.plan.wshape, dtype=torch.complex64, device="cuda")
+        mode = {"smooth": L.SMOOTH_FWD, "smooth-adj": L.SMOOTH_ADJ}[a.profile_step]
+        prob.plan.smooth_step(1, x, torch.empty_like(x), mode=mode)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_step": a.profile_step, "workload": w.name, "ok": True}))
+        return
     if a.profile_n:
         # a step of another lateral size: config1-family velocity with 5 % seeded noise
         n, nw = a.profile_n, a.profile_nw

@@ -92,7 +92,8 @@ struct Plan {
   __host__ __device__ static constexpr int radix(int s) { return RS::get(s); }
 };
 
-constexpr int kWarps = 8;  // warps per CTA in every pass
+constexpr int kWarps = 8;       // warps per CTA in every pass
+constexpr int kMaxHatRefs = 32;  // smooth-step references the row passes stage in shared memory
 
 template <class P, bool REV>
 struct Order {
@@ -245,8 +246,56 @@ struct RowGeo {
   // shared-memory stride between lines
   static constexpr int LINE = P::N + (P::LINE_EXTRA > (P::T < 32 ? 8 : 0) ? P::LINE_EXTRA : (P::T < 32 ? 8 : 0));
   static constexpr int ROWS = kWarps * P::G;                // rows per CTA
-  static size_t smem() { return ((size_t)kWarps * P::G * LINE + tw_size<P>()) * sizeof(float2); }
+  // after the twiddles: the smooth step's references and inverse spans (kMaxHatRefs each)
+  static size_t smem() { return ((size_t)kWarps * P::G * LINE + tw_size<P>() + kMaxHatRefs) * sizeof(float2); }
 };
+
+// Smooth-step references of the row passes, staged in shared memory once per CTA:
+// ref[0 .. n) and inv[j] = 1 / (ref[j+1] - ref[j]).  With more references than
+// kMaxHatRefs the passes fall back to the per-term weights of row_weight.
+template <class P>
+__device__ __forceinline__ void stage_hat_refs(const SpecArgs& a, float* ref, float* inv) {
+  const int n = a.sm_n;
+  if ((int)threadIdx.x < n) {
+    const int i = threadIdx.x;
+    ref[i] = a.sm_ref[i];
+    inv[i] = i + 1 < n ? 1.f / (a.sm_ref[i + 1] - a.sm_ref[i]) : 0.f;
+  }
+}
+// Fractional reference index g of slowness s: the hat weights are 1 - (g - j) on
+// reference j and g - j on j + 1, j = min(floor g, n - 2); g = 0 and g = n - 1 are
+// the clamped ends (weight 1 on the end reference, derivative 0).  Same
+// bracketing as hat_weight.
+__device__ __forceinline__ float hat_index(const float* ref, const float* inv, int n, float s) {
+  if (n == 1 || s <= ref[0]) return 0.f;
+  if (s >= ref[n - 1]) return (float)(n - 1);
+  int j = 0;
+  while (j < n - 2 && s >= ref[j + 1]) ++j;
+  return (float)j + (s - ref[j]) * inv[j];
+}
+__device__ __forceinline__ unsigned hat_index_support(int n, float g) {
+  if (n == 1 || g <= 0.f) return 1u;
+  if (g >= (float)(n - 1)) return 1u << (n - 1);
+  return 3u << min((int)g, n - 2);
+}
+// Hat weight (x) and its slowness derivative (y) of reference t at index g.
+__device__ __forceinline__ float2 hat_at(const float* inv, int n, int t, float g) {
+  if (n == 1 || g <= 0.f) return make_float2(t == 0 ? 1.f : 0.f, 0.f);
+  if (g >= (float)(n - 1)) return make_float2(t == n - 1 ? 1.f : 0.f, 0.f);
+  const int j = min((int)g, n - 2);
+  const float u = g - (float)j;
+  if (t == j) return make_float2(1.f - u, -inv[j]);
+  if (t == j + 1) return make_float2(u, inv[j]);
+  return make_float2(0.f, 0.f);
+}
+// Reference part of the smooth weight from the hat: w C (W_SMOOTH), w conj(C)
+// (W_SMOOTH_CONJ), (w' - i w dz w) C (W_SMOOTH_DERIV).
+template <int W>
+__device__ __forceinline__ float2 hat_ref_weight(float2 h, float wdz, float2 C) {
+  if (W == W_SMOOTH) return cscale(C, h.x);
+  if (W == W_SMOOTH_CONJ) return cscale(cconj(C), h.x);
+  return cmul(make_float2(h.y, -wdz * h.x), C);
+}
 
 // Per-thread view of a row pass: which row, which lane of the line, its smem line.
 template <class P>
@@ -278,6 +327,9 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(PRE) && (P::E == 16 ||
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
+  if (PRE == W_SMOOTH_CONJ && a.sm_n <= kMaxHatRefs)
+    stage_hat_refs<P>(a, reinterpret_cast<float*>(c.tw + tw_size<P>()),
+                      reinterpret_cast<float*>(c.tw + tw_size<P>()) + kMaxHatRefs);
   __syncthreads();
   float2 raw[P::E];
   const long long roff = (c.b * a.d.NY + (c.live ? c.y : 0)) * P::N;
@@ -296,14 +348,27 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(PRE) && (P::E == 16 ||
 #pragma unroll
     for (int e = 0; e < P::E; ++e) lab.set(e, c.live ? lrow[pos_first<P>(c.t, e)] : 255u);
   }
-  // smooth weights: terms that no sample of the warp's rows supports are zero rows
+  // smooth weights (references staged in shared memory): each cell's fractional
+  // reference index and the cell part conj(B(s)) of every reference's weight,
+  // once per cell; terms that no sample of the warp's rows supports are zero rows
+  constexpr bool kSmooth = PRE == W_SMOOTH_CONJ;
   unsigned used = 0xffffffffu;
-  if (PRE == W_SMOOTH_CONJ && a.sm_n <= 32) {
-    unsigned mine = 0;
+  float g[kSmooth ? P::E : 1];
+  const float* href = reinterpret_cast<const float*>(c.tw + tw_size<P>());
+  const float* hinv = href + kMaxHatRefs;
+  const bool hat_smem = kSmooth && a.sm_n <= kMaxHatRefs;
+  if (hat_smem) {
     const float* srow = a.sm_s + (long long)(c.live ? c.y : 0) * P::N;
+    unsigned mine = 0;
 #pragma unroll
-    for (int e = 0; e < P::E; ++e)
-      if (c.live) mine |= hat_support(a.sm_ref, a.sm_n, srow[pos_first<P>(c.t, e)]);
+    for (int e = 0; e < P::E; ++e) {
+      const float sv = c.live ? srow[pos_first<P>(c.t, e)] : 0.f;
+      g[e] = hat_index(href, hinv, a.sm_n, sv);
+      if (c.live) {
+        mine |= hat_index_support(a.sm_n, g[e]);
+        raw[e] = cmul_conj(raw[e], smooth_cell_phase(a, c.iw, sv));
+      }
+    }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
     used = mine;
@@ -318,12 +383,21 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(PRE) && (P::E == 16 ||
       }
       continue;
     }
+    if (hat_smem) {
+      const float2 C = smooth_ref_phase(a, c.iw, term);
+      const float wdz = a.w[c.iw] * a.dz;
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) {
-      if (PRE == W_MASK)
-        v[e] = lab.get(e) == term ? raw[e] : make_float2(0.f, 0.f);
-      else
-        v[e] = c.live ? row_weight<PRE>(a, term, c.iw, c.y, pos_first<P>(c.t, e), raw[e]) : make_float2(0.f, 0.f);
+      for (int e = 0; e < P::E; ++e)
+        v[e] = c.live ? cmul(raw[e], hat_ref_weight<PRE>(hat_at(hinv, a.sm_n, term, g[e]), wdz, C))
+                      : make_float2(0.f, 0.f);
+    } else {
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) {
+        if (PRE == W_MASK)
+          v[e] = lab.get(e) == term ? raw[e] : make_float2(0.f, 0.f);
+        else
+          v[e] = c.live ? row_weight<PRE>(a, term, c.iw, c.y, pos_first<P>(c.t, e), raw[e]) : make_float2(0.f, 0.f);
+      }
     }
     fft_fwd<P>(v, c.t, c.tw, c.line);
     if (c.live) {
@@ -342,8 +416,14 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
+  constexpr bool kSmooth = POST == W_SMOOTH || POST == W_SMOOTH_DERIV;
+  const bool hat_smem = kSmooth && a.sm_n <= kMaxHatRefs;
+  const float* href = reinterpret_cast<const float*>(c.tw + tw_size<P>());
+  const float* hinv = href + kMaxHatRefs;
+  if (hat_smem) stage_hat_refs<P>(a, const_cast<float*>(href), const_cast<float*>(hinv));
   __syncthreads();
   const int nterm = multi_term(POST) ? a.nterm : 1;
+  float g[kSmooth ? P::E : 1];
   float2 acc[P::E];
 #pragma unroll
   for (int e = 0; e < P::E; ++e) acc[e] = make_float2(0.f, 0.f);
@@ -362,12 +442,14 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
     used = nterm > 32 ? 0xffffffffu : mine;
-  } else if ((POST == W_SMOOTH || POST == W_SMOOTH_DERIV) && a.sm_n <= 32) {
+  } else if (hat_smem) {
     unsigned mine = 0;
     const float* srow = a.sm_s + (long long)(c.live ? c.y : 0) * P::N;
 #pragma unroll
-    for (int e = 0; e < P::E; ++e)
-      if (c.live) mine |= hat_support(a.sm_ref, a.sm_n, srow[pos_first<P>(c.t, e)]);
+    for (int e = 0; e < P::E; ++e) {
+      g[e] = hat_index(href, hinv, a.sm_n, c.live ? srow[pos_first<P>(c.t, e)] : 0.f);
+      if (c.live) mine |= hat_index_support(a.sm_n, g[e]);
+    }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
     used = mine;
@@ -396,12 +478,21 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
       for (int e = 0; e < P::E; ++e) pre[e] = c.live ? src[pos_last<P>(c.t, e)] : make_float2(0.f, 0.f);
     }
     fft_inv<P>(v, c.t, c.tw, c.line);
+    if (hat_smem) {
+      // reference part of the weights here, the cell part B(s) once after the sum
+      const float2 C = smooth_ref_phase(a, c.iw, term);
+      const float wdz = a.w[c.iw] * a.dz;
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) {
-      if (POST == W_MASK) {
-        if (lab.get(e) == term) acc[e] = v[e];
-      } else if (c.live) {
-        acc[e] = cadd(acc[e], row_weight<POST>(a, term, c.iw, c.y, pos_first<P>(c.t, e), v[e]));
+      for (int e = 0; e < P::E; ++e)
+        if (c.live) acc[e] = cadd(acc[e], cmul(v[e], hat_ref_weight<POST>(hat_at(hinv, a.sm_n, term, g[e]), wdz, C)));
+    } else {
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) {
+        if (POST == W_MASK) {
+          if (lab.get(e) == term) acc[e] = v[e];
+        } else if (c.live) {
+          acc[e] = cadd(acc[e], row_weight<POST>(a, term, c.iw, c.y, pos_first<P>(c.t, e), v[e]));
+        }
       }
     }
     term = nxt;
@@ -409,10 +500,12 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   if (!c.live) return;
   float2* dst = a.out + (c.b * a.d.NY + c.y) * P::N;
   const float ty = post_taper ? a.tapy[c.y] : 1.f;
+  const float* srow_out = kSmooth ? a.sm_s + (long long)c.y * P::N : nullptr;
 #pragma unroll
   for (int e = 0; e < P::E; ++e) {
     const int x = pos_first<P>(c.t, e);
     float2 v = acc[e];
+    if (hat_smem) v = cmul(v, smooth_cell_phase(a, c.iw, srow_out[x]));
     if (post_taper) v = cscale(v, a.tapx[x] * ty);
     if (a.add) v = cadd(dst[x], v);
     dst[x] = v;

@@ -79,6 +79,32 @@ __device__ __forceinline__ unsigned hat_support(const float* ref, int n, float s
   return 3u << j;
 }
 
+// The split-step factor of the smooth step factors into a cell part and a
+// reference part: SS_r = exp(-i w (s - s_r) dz) = B(s) C_r with B(s) =
+// exp(-i w s dz) and C_r = exp(i w s_r dz).  The register-resident row passes use
+// it to take one sine / cosine per cell (B, applied once to the sum over
+// references, or once to the input of the adjoint) and one per reference and
+// line (C_r) instead of one per cell and reference.
+__device__ __forceinline__ float2 smooth_cell_phase(const SpecArgs& a, int iw, float s) {  // B(s)
+  float sn, cs;
+  sincosf(a.w[iw] * a.dz * s, &sn, &cs);
+  return make_float2(cs, -sn);
+}
+__device__ __forceinline__ float2 smooth_ref_phase(const SpecArgs& a, int iw, int t) {  // C_t
+  float sn, cs;
+  sincosf(a.w[iw] * a.dz * a.sm_ref[t], &sn, &cs);
+  return make_float2(cs, sn);
+}
+// Reference part of the weight of term t at slowness s: w_t C_t (W_SMOOTH),
+// w_t conj(C_t) (W_SMOOTH_CONJ) or (w_t' - i w dz w_t) C_t (W_SMOOTH_DERIV).
+template <int W>
+__device__ __forceinline__ float2 smooth_ref_weight(const SpecArgs& a, int t, int iw, float s, float2 C) {
+  const Hat h = hat_weight(a.sm_ref, a.sm_n, t, s);
+  if (W == W_SMOOTH) return cscale(C, h.w);
+  if (W == W_SMOOTH_CONJ) return cscale(cconj(C), h.w);
+  return cmul(make_float2(h.dw, -a.w[iw] * a.dz * h.w), C);
+}
+
 // w_r SS_r (W_SMOOTH), w_r conj(SS_r) (W_SMOOTH_CONJ) or (w_r' - i w dz w_r) SS_r
 // (W_SMOOTH_DERIV) for reference t at cell (y, x) of frequency iw.
 template <int W>
