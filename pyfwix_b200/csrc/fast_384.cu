@@ -3,7 +3,7 @@
 // transform, so the first stage needs no twiddles and the line is exchanged
 // through shared memory once less than with radix-4 stages throughout).
 // The exchange placements (XSw) are the ones with the fewest shared-memory
-// bank conflicts for this plan's strides, per exchange.
+// bank conflicts for this plan's strides, per exchange (pyfwix_b200/tune_fft.py).
 #include "fast.cuh"
 
 using FwixPlan384 = fwix::fast::Plan<384, 12, fwix::fast::Radices<12, 4, 4, 2>, 0,
