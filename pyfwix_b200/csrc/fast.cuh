@@ -525,7 +525,7 @@ struct ColGeo {
   // Resident CTAs per SM the register allocation is held to: four for plans of
   // at most 8 samples per lane (64 registers; the few spills stay in L1 and the
   // extra warps hide more latency than they cost), else what fits.
-  static constexpr int kMinBlocks = P::E <= 8 ? 4 : P::E <= 12 ? 2 : 1;
+  static constexpr int kMinBlocks = P::E <= 8 ? 4 : P::E <= 16 ? 2 : 1;
   static size_t smem2() { return ((size_t)2 * LX * LINE + tw_size<P>()) * sizeof(float2); }  // tile, tw, tile
 };
 

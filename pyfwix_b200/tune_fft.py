@@ -18,7 +18,6 @@ csrc/fast_<N>.cu; tests/test_fft_tuning.py checks that they agree.
 """
 from __future__ import annotations
 
-import itertools
 import sys
 
 
@@ -142,9 +141,10 @@ def code_text(c):
     return f"fwix::fast::xs({c & 15}, {(c >> 4) & 15}, {c >> 8})"
 
 
-# (N, E, radices) of the plans with their own exchange placements (csrc/fast_<N>.cu)
+# (N, E, radices) of the plans with their own exchange placements (csrc/fast_<N>.cu;
+# for 256 the column plan: the rows place samples at p + (p >> 4) instead)
 PLANS = {96: (12, (12, 4, 2)), 128: (8, (8, 4, 4)), 160: (20, (20, 4, 2)), 192: (12, (12, 4, 4)),
-         256: (8, (8, 8, 4)), 320: (20, (20, 4, 4)), 384: (12, (12, 4, 4, 2)), 512: (16, (8, 8, 8)),
+         256: (16, (16, 16)), 320: (20, (20, 4, 4)), 384: (12, (12, 4, 4, 2)), 512: (16, (8, 8, 8)),
          640: (20, (20, 4, 4, 2)), 64: (8, (8, 8))}
 
 
