@@ -612,13 +612,24 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_a(co
   for (int e = 0; e < P::E; ++e) psi[e] = c.line[swz(pos_first<P>(c.t, e))];
   fft_fwd<P>(psi, c.t, c.tw, c.line);
   const int xq = c.x < a.d.NX ? c.x : 0;
-  float2 q[P::E];
-  col_factors<P, QM>(a, 0, c.iw, xq, c.t, q);
+  // Up to 12 samples per lane the next term's factors are fetched while the
+  // current term is transformed; with 16 the spectrum, the term and the factors
+  // do not fit the two-CTA register budget together, so each term's factors are
+  // fetched as they are applied.
+  constexpr bool kPrefetch = P::E <= 12;
+  float2 q[kPrefetch ? P::E : 1];
+  if constexpr (kPrefetch) col_factors<P, QM>(a, 0, c.iw, xq, c.t, q);
   for (int term = 0; term < a.nterm; ++term) {
     float2 v[P::E];
+    if constexpr (kPrefetch) {
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) v[e] = cmul(psi[e], q[e]);
-    if (term + 1 < a.nterm) col_factors<P, QM>(a, term + 1, c.iw, xq, c.t, q);
+      for (int e = 0; e < P::E; ++e) v[e] = cmul(psi[e], q[e]);
+      if (term + 1 < a.nterm) col_factors<P, QM>(a, term + 1, c.iw, xq, c.t, q);
+    } else {
+      col_factors<P, QM>(a, term, c.iw, xq, c.t, v);
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) v[e] = cmul(psi[e], v[e]);
+    }
     __syncthreads();  // the previous term's tile has been stored
     fft_inv<P>(v, c.t, c.tw, c.line);
     __syncwarp();
