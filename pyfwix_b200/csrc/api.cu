@@ -352,6 +352,17 @@ fwix_status do_scatter(fwix_plan* p, int iz, int adjoint, const float2* in, floa
     FWIX_TRY(cu(fwix::launch_scat_table(a0, p->scat_tab, s), "scatter weights"));
     a0.scat_tab = p->scat_tab;
   }
+  if (adjoint && p->desc.taylor >= 1 && fwix::fast_length(p->d.NX) && fwix::fast_length(p->d.NY)) {
+    // the zeroth term's filter is the identity: conj(W_0) d is added by the inverse
+    // row pass, and only orders 1 .. taylor go through the transforms.  (The
+    // forward keeps the zeroth term in the transforms: measured on B200, adding
+    // W_0 u in its inverse row pass, which then also reads the background and the
+    // image, was slower than transforming the term.)
+    a0.term0 = 1;
+    a0.nterm = p->desc.taylor;
+    a0.direct = in;
+    a0.direct_mode = 2;
+  }
   return for_chunks(p, a0, [&](const SpecArgs& a) { return scatter_chunk(adjoint, image, img_w, a, s); });
 }
 

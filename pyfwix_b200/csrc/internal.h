@@ -90,6 +90,14 @@ struct SpecArgs {
   float coef[5];
   float norm;          // scale folded into the column multiplier
   int nterm;           // references (W_MASK) or Taylor terms (W_SCAT)
+  // Born scattering with the zeroth Taylor term applied directly: its filter
+  // (|k| / w)^0 is the identity, so W_0 u needs no transform.  The transformed
+  // terms are then orders term0 .. term0 + nterm - 1 (term0 = 1), and the inverse
+  // row pass adds W_0 u (direct_mode 1: u = direct, times the W_IC image when
+  // `image` is set) or conj(W_0) d (direct_mode 2: d = direct) to its sum.
+  int term0;
+  int direct_mode;
+  const float2* direct;
   // buffers.  A launch covers the slices (shot, frequency) b0 .. b0 + nb - 1: in / out
   // (and the labels, images and tables) are indexed by the global slice b0 + bl,
   // the intermediates t1 / t2 by the launch-local slice bl, term after term tstride

@@ -35,6 +35,20 @@ __device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, 
   return rot90<false>(cscale(p, f));
 }
 
+// Zeroth Born term applied directly (SpecArgs::direct_mode): W_0 u for the
+// forward (u times the W_IC image when one is bound), conj(W_0) d for the adjoint,
+// at cell (y, x) of global slice b.
+__device__ __forceinline__ float2 scat_direct(const SpecArgs& a, long long b, int iw, int y, int x) {
+  float2 u = a.direct[(b * a.d.NY + y) * a.d.NX + x];
+  const float2 w0 = scat_weight(a, 0, iw, y, x);
+  if (a.direct_mode == 2) return cmul_conj(u, w0);
+  if (a.image) {
+    if (y >= a.d.ny || x >= a.d.nx) return make_float2(0.f, 0.f);
+    u = cmul(u, a.image[(long long)iw * a.img_w + (long long)y * a.d.nx + x]);
+  }
+  return cmul(u, w0);
+}
+
 // Hat-function interpolation weight of reference t at slowness s and its
 // derivative, on references sorted ascending (clamped to the end references
 // outside their range, where the derivative is 0).
@@ -130,8 +144,8 @@ __device__ __forceinline__ float2 row_weight(const SpecArgs& a, int t, int iw, i
     const uint8_t l = a.lab[(long long)iw * a.lab_w + (long long)y * a.d.NX + x];
     return (int)l == t ? v : make_float2(0.f, 0.f);
   }
-  if (W == W_SCAT) return cmul(v, scat_weight(a, t, iw, y, x));
-  if (W == W_SCAT_CONJ) return cmul_conj(v, scat_weight(a, t, iw, y, x));
+  if (W == W_SCAT) return cmul(v, scat_weight(a, t + a.term0, iw, y, x));
+  if (W == W_SCAT_CONJ) return cmul_conj(v, scat_weight(a, t + a.term0, iw, y, x));
   // W_IC
   if (y < a.d.ny && x < a.d.nx)
     return cmul(v, a.image[(long long)iw * a.img_w + (long long)y * a.d.nx + x]);
@@ -144,11 +158,12 @@ __device__ __forceinline__ float2 qmult(const SpecArgs& a, int t, int iw, int x,
   if (QM == Q_ONE) return make_float2(a.norm, 0.f);
   if (QM == Q_KPOW) {
     // (|k| / w)^(2t) (scatter.cu:49-50), the power by products
-    if (t == 0) return make_float2(a.norm, 0.f);
+    const int n = t + a.term0;
+    if (n == 0) return make_float2(a.norm, 0.f);
     const float kx = a.kx[x], ky = a.ky[y];
     const float r2 = (kx * kx + ky * ky) / a.w2[iw];  // (|k| / w)^2
     float p = r2;
-    for (int k = 1; k < t; ++k) p *= r2;
+    for (int k = 1; k < n; ++k) p *= r2;
     return make_float2(p * a.norm, 0.f);
   }
   const float2 sr = a.sref[t * a.d.nw + iw];
