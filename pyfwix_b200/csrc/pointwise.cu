@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
   }
   if (!c.ok) return;
   float2 r = mw == 0 ? rs[threadIdx.x] : make_float2(0.f, 0.f);
+#pragma unroll 4
   for (int iw = threadIdx.y; iw < d.nw; iw += kGroups) {
     if (mw != 0) {
       const long long m = iw * mw + c.yx;
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
              float2* __restrict__ wfld) {
   const Cell c = this_cell(d);
   if (!c.ok) return;
+#pragma unroll 4
   for (int iw = threadIdx.y; iw < d.nw; iw += kGroups) {
     const float2 im = image[iw * img_w + c.yx];
     for (int s = 0; s < d.ns; ++s) {
@@ -121,6 +123,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
              int add, int wsum) {
   const Cell c = this_cell(d);
   float2 acc[1] = {make_float2(0.f, 0.f)};
+#pragma unroll 4
   for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups) {
     float2 t = make_float2(0.f, 0.f);
     for (int s = 0; s < d.ns; ++s) {
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
     k_lin_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
                   const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw, float2* dm0,
                   float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr, int add,
-                  const float2* __restrict__ bg, float2* wf) {
+                  const float2* __restrict__ bg, float2* __restrict__ wf) {
   const Cell c = this_cell(d);
   const long long plane = (long long)d.ny * d.nx;
   const int wsum = adjoint && dm_w == 0;
@@ -184,6 +187,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
     cf = cs[threadIdx.x];
   }
   float2 g[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll 4
   for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups) {
     if (mw != 0) {
       const long long m = iw * mw + c.yx;
@@ -243,6 +247,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
                 int add) {
   const Cell c = this_cell(d);
   float2 acc[1] = {make_float2(0.f, 0.f)};
+#pragma unroll 4
   for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups)
     for (int s = 0; s < d.ns; ++s) {
       const long long k = wf_index(d, s, iw, c);
