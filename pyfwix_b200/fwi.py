@@ -117,6 +117,9 @@ class SmoothFWI:
         p = self.plan
         wb = p.ns * p.nw * p.NY * p.NX * 8
         free, _ = torch.cuda.mem_get_info(self.device)
+        # memory torch's allocator holds but does not use (fields of an earlier shot)
+        # is free for this shot's fields as well
+        free += torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
         budget = 0.6 * free
         if 3 * p.nz * wb + 4 * wb <= budget:
             return None
