@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
     const int x = pos_first<P>(c.t, e);
     float2 v = acc[e];
     if (hat_smem) v = cmul(v, smooth_cell_phase(a, c.iw, srow_out[x]));
-    if constexpr (POST == W_SCAT || POST == W_ONE)
+    if constexpr (POST == W_ONE)  // the Born scattering adjoint's zeroth term
       if (a.direct_mode) v = cadd(v, scat_direct(a, c.b, c.iw, c.y, x));
     if (post_taper) v = cscale(v, a.tapx[x] * ty);
     if (a.add) v = cadd(dst[x], v);
