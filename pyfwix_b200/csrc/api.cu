@@ -339,7 +339,8 @@ fwix_status scatter_chunk(int adjoint, const float2* image, long long img_w, Spe
   } else {
     FWIX_TRY(cu(fwix::row_forward(a, fwix::W_SCAT_CONJ, s), "scatter adjoint row pass"));
     FWIX_TRY(cu(fwix::col_type_b(a, fwix::Q_KPOW, s), "scatter adjoint column pass"));
-    FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_ONE, 0, s), "scatter adjoint inverse row pass"));
+    FWIX_TRY(cu(fwix::row_inverse(a, a.direct_mode ? fwix::W_ONE_DIRECT : fwix::W_ONE, 0, s),
+                "scatter adjoint inverse row pass"));
   }
   return FWIX_OK;
 }

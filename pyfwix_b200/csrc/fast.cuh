@@ -506,8 +506,7 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
     const int x = pos_first<P>(c.t, e);
     float2 v = acc[e];
     if (hat_smem) v = cmul(v, smooth_cell_phase(a, c.iw, srow_out[x]));
-    if constexpr (POST == W_ONE)  // the Born scattering adjoint's zeroth term
-      if (a.direct_mode) v = cadd(v, scat_direct(a, c.b, c.iw, c.y, x));
+    if constexpr (POST == W_ONE_DIRECT) v = cadd(v, scat_direct(a, c.b, c.iw, c.y, x));
     if (post_taper) v = cscale(v, a.tapx[x] * ty);
     if (a.add) v = cadd(dst[x], v);
     dst[x] = v;
@@ -790,6 +789,7 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
     break;
   switch (post) {
     FWIX_FAST_RI(W_ONE)
+    FWIX_FAST_RI(W_ONE_DIRECT)
     FWIX_FAST_RI(W_MASK)
     FWIX_FAST_RI(W_SCAT)
     FWIX_FAST_RI(W_SMOOTH)

@@ -27,7 +27,8 @@ enum RowWeight {
   // reference slownesses, times the split-step factor SS_r = exp(-i w (s - s_r) dz)
   W_SMOOTH = 6,       // w_r SS_r
   W_SMOOTH_CONJ = 7,  // w_r conj(SS_r)
-  W_SMOOTH_DERIV = 8  // d(w_r SS_r)/ds = (w_r' - i w dz w_r) SS_r
+  W_SMOOTH_DERIV = 8, // d(w_r SS_r)/ds = (w_r' - i w dz w_r) SS_r
+  W_ONE_DIRECT = 9    // 1, plus the Born adjoint's zeroth term conj(W_0) d (inverse row pass only)
 };
 
 // Weights that run one pass per term (reference or Taylor term).

@@ -138,7 +138,7 @@ __device__ __forceinline__ float2 smooth_factor(const SpecArgs& a, int t, int iw
 template <int W>
 __device__ __forceinline__ float2 row_weight(const SpecArgs& a, int t, int iw, int y, int x, float2 v) {
   if (W == W_SMOOTH || W == W_SMOOTH_CONJ || W == W_SMOOTH_DERIV) return cmul(v, smooth_factor<W>(a, t, iw, y, x));
-  if (W == W_ONE) return v;
+  if (W == W_ONE || W == W_ONE_DIRECT) return v;
   if (W == W_TAPER) return cscale(v, a.tapx[x] * a.tapy[y]);
   if (W == W_MASK) {
     const uint8_t l = a.lab[(long long)iw * a.lab_w + (long long)y * a.d.NX + x];
