@@ -85,6 +85,8 @@ class Plan:
         if depths is not None:
             need = need // self.nz * max(1, min(int(depths), self.nz))
         free, _ = torch.cuda.mem_get_info(self.device)
+        # memory torch's allocator holds but does not use counts as free
+        free += torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
         if need == 0 or need > max_fraction * free:
             return False
         self._keep["pcache"] = torch.empty(need, dtype=torch.uint8, device=self.device)
