@@ -99,7 +99,8 @@ class Plan:
 
     def set_refs(self, sref, labels, phase_cache=True):
         """sref [nz][nref][nw] complex; labels [nz][nw or 1][NY][NX] integer.  With
-        ``phase_cache`` a phase-factor cache is bound when memory allows."""
+        ``phase_cache`` a phase-factor cache is bound: every depth when memory
+        allows, else four depths in rotation."""
         sref = _c64(sref, self.device)
         if tuple(sref.shape) != (self.nz, self.nref, self.nw):
             raise ValueError(f"sref shape {tuple(sref.shape)} != {(self.nz, self.nref, self.nw)}")
@@ -114,8 +115,10 @@ class Plan:
         zst = labels.shape[1] * self.NY * self.NX
         L.check(self.lib.fwix_plan_set_refs(self._h, _p(sref), _p(labels), zst, wst))
         self._keep["sref"], self._keep["labels"] = sref, labels
-        if phase_cache and "pcache" not in self._keep:
-            self.enable_phase_cache()
+        if phase_cache and "pcache" not in self._keep and not self.enable_phase_cache():
+            # no room for every depth: a few depths in rotation still spare the
+            # column passes the per-sample factors (a migration level reuses its table)
+            self.enable_phase_cache(depths=min(self.nz, 4))
         return sref, labels
 
     def set_model(self, slow, den):
