@@ -187,6 +187,40 @@ __global__ void __launch_bounds__(kCells * kGroups)
     cf = cs[threadIdx.x];
   }
   float2 g[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  // model and perturbation shared by every frequency (with the imaging condition):
+  // dr is one value per cell, and the adjoint's frequency sum commutes with the
+  // coefficients, so both are formed once per cell
+  if (IC && mw == 0 && dm_w == 0) {
+    const long long k = c.yx;
+    if (!adjoint) {
+      if (!c.ok) return;
+      float2 v = csub(cmul(cf.as, dm0[k]), cmul(cf.bs, dm1[k]));
+      v = cadd(v, csub(cmul(cf.ar, dm3[k]), cmul(cf.br, dm2[k])));
+#pragma unroll 4
+      for (int iw = threadIdx.y; iw < d.nw; iw += kGroups)
+        for (int sh = 0; sh < d.ns; ++sh) {
+          const long long q = wf_index(d, sh, iw, c);
+          wf[q] = cadd(wf[q], cmul(bg[q], v));
+        }
+      return;
+    }
+    float2 gi[1] = {make_float2(0.f, 0.f)};
+#pragma unroll 4
+    for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups)
+      for (int sh = 0; sh < d.ns; ++sh) {
+        const long long q = wf_index(d, sh, iw, c);
+        gi[0] = cadd(gi[0], cmul_conj(wf[q], bg[q]));
+      }
+    reduce_groups<1>(gi);  // every thread of the block
+    if (threadIdx.y != 0 || !c.ok) return;
+    const float2 t0 = cmul_conj(gi[0], cf.as), t1 = cscale(cmul_conj(gi[0], cf.bs), -1.f);
+    const float2 t3 = cmul_conj(gi[0], cf.ar), t2 = cscale(cmul_conj(gi[0], cf.br), -1.f);
+    dm0[k] = add ? cadd(dm0[k], t0) : t0;
+    dm1[k] = (add || dm1 == dm0) ? cadd(dm1[k], t1) : t1;
+    dm2[k] = add ? cadd(dm2[k], t2) : t2;
+    dm3[k] = (add || dm3 == dm2) ? cadd(dm3[k], t3) : t3;
+    return;
+  }
 #pragma unroll 4
   for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups) {
     if (mw != 0) {
