@@ -77,7 +77,7 @@ enum { FWIX_PS_FWD = 0, FWIX_PS_ADJ = 1, FWIX_PS_INV = 2 };
 enum { FWIX_SMOOTH_FWD = 0, FWIX_SMOOTH_ADJ = 1, FWIX_SMOOTH_DERIV = 2 };
 
 /* Workspace classes for fwix_plan_workspace_bytes. */
-enum { FWIX_WS_STEP = 0, FWIX_WS_SWEEP = 1, FWIX_WS_BORN = 2 };
+enum { FWIX_WS_STEP = 0, FWIX_WS_SWEEP = 1, FWIX_WS_BORN = 2, FWIX_WS_BORN_PACKED = 3 };
 
 typedef struct fwix_desc {
   int nx, ny;        /* model lateral size                                   */
@@ -213,6 +213,31 @@ fwix_status fwix_migrate(fwix_plan* plan, const fwix_traces* src, const fwix_tra
 fwix_status fwix_born(fwix_plan* plan, int adjoint, const fwix_traces* rec, const void* bg_down,
                       const void* bg_up, void* dslow, void* dden, int64_t model_w_stride,
                       void* data, int add, void* stream);
+
+/* ---- lossy background store ---------------------------------------------------
+ * Replaces the role of the reference's ZFP-compressed background wavefields
+ * (propagator/src/WavefieldPool.cpp:13-219, fixed rate "compress_rate" = 8 bits
+ * per value) with this library's own fixed-rate format, kept in device memory:
+ * blocks of 16 floats share an exponent byte and keep 8-bit mantissas (8.5 bits
+ * per value, 3.76 x smaller than complex64; error at most 2^-7 of the block's
+ * largest magnitude).  Not ZFP's bit stream.
+ *   fwix_plan_packed_bytes: bytes of one packed wavefield [ns][nw][NY][NX]; [nz]
+ *     packed wavefields are nz times that, depth iz at iz * packed_bytes.
+ *   fwix_pack_rate8 / fwix_unpack_rate8: one wavefield.
+ *   fwix_propagate_packed: fwix_propagate storing the down and up fields of every
+ *     depth packed (packed_up may be NULL); the up pass reflects the unpacked down
+ *     fields, as the reference's reflects its decompressed ones.
+ *   fwix_born_packed: fwix_born reading packed backgrounds, each depth unpacked
+ *     when first needed; workspace class FWIX_WS_BORN_PACKED. */
+size_t fwix_plan_packed_bytes(const fwix_plan* plan);
+fwix_status fwix_pack_rate8(fwix_plan* plan, const void* wfld, void* packed, void* stream);
+fwix_status fwix_unpack_rate8(fwix_plan* plan, const void* packed, void* wfld, void* stream);
+fwix_status fwix_propagate_packed(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
+                                  const void* wavelet, void* data, int add, void* packed_down, void* packed_up,
+                                  void* stream);
+fwix_status fwix_born_packed(fwix_plan* plan, int adjoint, const fwix_traces* rec, const void* packed_down,
+                             const void* packed_up, void* dslow, void* dden, int64_t model_w_stride, void* data,
+                             int add, void* stream);
 
 /* ---- one-call forms of the depth steps and the image --------------------------
  * fwix_pspi_step / fwix_nsps_step: PSPI::cu_forward / cu_adjoint

@@ -19,7 +19,7 @@ STEP_PSPI, STEP_NSPS = 0, 1
 FWD, ADJ_ADD, ADJ_INPL = 0, 1, 2
 PS_FWD, PS_ADJ, PS_INV = 0, 1, 2
 SMOOTH_FWD, SMOOTH_ADJ, SMOOTH_DERIV = 0, 1, 2
-WS_STEP, WS_SWEEP, WS_BORN = 0, 1, 2
+WS_STEP, WS_SWEEP, WS_BORN, WS_BORN_PACKED = 0, 1, 2, 3
 
 
 class FwixDesc(ctypes.Structure):
@@ -88,10 +88,15 @@ SIGNATURES = {
     "fwix_nsps_step": [P, I, P, P, I, P],
     "fwix_image_accumulate": [P, P, P, P, I, P],
     "fwix_sweep": [I, ctypes.POINTER(FwixInstance), I, ctypes.POINTER(P), I, P],
+    "fwix_plan_packed_bytes": [P],
+    "fwix_pack_rate8": [P, P, P, P],
+    "fwix_unpack_rate8": [P, P, P, P],
+    "fwix_propagate_packed": [P, P, P, P, P, I, P, P, P],
+    "fwix_born_packed": [P, I, P, P, P, P, P, I64, P, I, P],
 }
 SWEEP_DOWN, SWEEP_UP, SWEEP_MODEL, SWEEP_IMAGE, SWEEP_BORN_FWD, SWEEP_BORN_ADJ = range(6)
 _RET = {"fwix_last_error": ctypes.c_char_p, "fwix_version": I, "fwix_plan_workspace_bytes": ctypes.c_size_t,
-        "fwix_plan_phase_cache_bytes": ctypes.c_size_t,
+        "fwix_plan_phase_cache_bytes": ctypes.c_size_t, "fwix_plan_packed_bytes": ctypes.c_size_t,
         "fwix_launch_count": ctypes.c_uint64}
 
 _lib = None

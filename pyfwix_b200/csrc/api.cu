@@ -142,6 +142,7 @@ struct fwix_plan {
     size_t b = 2 * tbytes();  // t1, t2 for one chunk
     if (cls >= FWIX_WS_SWEEP) b += 3 * wbytes();  // A, B, SC
     if (cls >= FWIX_WS_BORN) b += (size_t)desc.nz * wbytes();  // per-level field store
+    if (cls >= FWIX_WS_BORN_PACKED) b += wbytes();               // second unpacked background
     return b;
   }
   float2* t1() const { return (float2*)ws; }
@@ -150,6 +151,7 @@ struct fwix_plan {
   float2* wB() const { return wA() + d.wfld; }
   float2* wSC() const { return wB() + d.wfld; }
   float2* store(int iz) const { return wSC() + d.wfld * (long long)(1 + iz); }
+  size_t packed_bytes() const { return fwix::packed_rate8_bytes(2 * d.wfld); }
 
   SpecArgs args(const float2* in, float2* out, int add) const {
     SpecArgs a;
@@ -398,9 +400,146 @@ fwix_status do_record(fwix_plan* p, const fwix_traces* tr, int iz, const float2*
 
 long long mslice(const fwix_plan* p) { return (long long)p->d.nw * p->d.ny * p->d.nx; }
 
+// =============================================================================
+// Background wavefields of fwix_born: [nz] full fields, or [nz] packed ones each
+// unpacked into `slot` when a depth other than the one it holds is asked for.
+struct BgSrc {
+  const float2* full = nullptr;
+  const unsigned char* packed = nullptr;
+  float2* slot = nullptr;
+  int held = -1;
+  fwix_status get(const fwix_plan* p, int iz, cudaStream_t s, const float2** out) {
+    if (full) {
+      *out = full + (long long)iz * p->d.wfld;
+      return FWIX_OK;
+    }
+    if (held != iz) {
+      FWIX_TRY(cu(fwix::launch_unpack_rate8(2 * p->d.wfld, packed + (size_t)iz * p->packed_bytes(), (float*)slot, s),
+                  "unpack background"));
+      held = iz;
+    }
+    *out = slot;
+    return FWIX_OK;
+  }
+};
+
+// ExtendedBorn::forward / adjoint (ExtendedBorn.cpp:80-453) on backgrounds D, U.
+fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& D, BgSrc& U, float2* ds,
+                      float2* dr, long long mw, float2* data, int add, cudaStream_t s) {
+  const int nz = p->desc.nz, k = p->desc.step_kind;
+  const long long plane = (long long)p->d.ny * p->d.nx;
+  const long long M = mw ? mslice(p) : plane;
+  float2* A = p->wA();
+  const size_t wb = p->wbytes();
+  // The reference runs four sweeps each way (ExtendedBorn.cpp:152-453), every
+  // scattered source propagated by a step of its own.  All operators are linear,
+  // so sources that feed the same recursion are summed before one step:
+  // step(A) + step(scat) = step(A + scat).  The forward keeps one downward and one
+  // upward recursion, the adjoint one downward and one upward; the results equal
+  // the four-sweep operators up to float rounding.
+  float2* SC = p->wSC();
+  const bool pspi = k == FWIX_STEP_PSPI;
+  if (!adjoint) {
+    if (!add) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
+    // down scattering (ExtendedBorn.cpp:152-178): store[iz] = dD_iz, the field
+    // recorded at iz; dD_iz+1 = S_iz(dD_iz + Scat_iz(bg_down_iz * ds_iz))
+    FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
+    for (int iz = 0; iz < nz; ++iz) {
+      FWIX_TRY(do_record(p, rec, iz, p->store(iz), data, s));
+      if (iz == nz - 1) break;
+      const float2* bd;
+      FWIX_TRY(D.get(p, iz, s, &bd));
+      FWIX_TRY(do_scatter(p, iz, 0, bd, SC, 0, ds + iz * M, mw, s));
+      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, p->store(iz), p->store(iz + 1), 0, s, SC));
+    }
+    // one upward recursion for the reflected down-scattered field (:210-238), the
+    // up scattering (:282-311) and the back scattering (:352-389):
+    //   Z_iz = S_iz(Z_iz+1 + Scat_iz(bg_up_iz+1 * ds_iz+1)) + R_iz dD_iz + bg_down_iz * dR_iz
+    FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+    for (int iz = nz - 1; iz >= 0; --iz) {
+      const int z1 = lower_iz(p, iz);
+      if (iz < nz - 1) {
+        const float2* bu;
+        FWIX_TRY(U.get(p, iz + 1, s, &bu));
+        FWIX_TRY(do_scatter(p, iz, 0, bu, SC, 0, ds + (iz + 1) * M, mw, s));
+        FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s, SC));
+      }
+      FWIX_TRY(do_reflect(p, iz, 0, p->store(iz), A, 1, s));
+      const float2* bd;
+      FWIX_TRY(D.get(p, iz, s, &bd));
+      FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                              p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
+                                              ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, A, 1, s),
+                  "linearised reflection"));
+      FWIX_TRY(do_record(p, rec, iz, A, data, s));
+    }
+    return FWIX_OK;
+  }
+  if (!add) {
+    FWIX_CU(cudaMemsetAsync(ds, 0, (size_t)nz * M * sizeof(float2), s));
+    FWIX_CU(cudaMemsetAsync(dr, 0, (size_t)nz * M * sizeof(float2), s));
+  }
+  // The scattering adjoints step with the add-version adjoint (no taper,
+  // Scattering.cpp:54-61), the recursions with the in-place adjoint (taper last,
+  // PSPI.cpp:85-103); for PSPI the second is the taper of the first, so one
+  // add-version step serves both.  (NSPS has no taper: the two coincide.)
+  SpecArgs ta = p->args(nullptr, nullptr, 0);
+  auto taper_into = [&](const float2* u, float2* out) {
+    return cu(fwix::launch_taper(ta, u, out, 0, s), "taper");
+  };
+  // downward: zeta_iz = Rec_iz^H d + S_iz-1^H zeta_iz-1 (the adjoint of the upward
+  // recursion), kept in store[iz]; it feeds the up-scattering adjoint (:313-349)
+  // and the back-scattering adjoint (:391-453), which needs no steps of its own
+  FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
+  for (int iz = 0; iz < nz; ++iz) {
+    const int z1 = lower_iz(p, iz);
+    float2* cur = p->store(iz);
+    if (iz > 0) {
+      if (pspi) {
+        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, p->store(iz - 1), SC, 0, s));
+        FWIX_TRY(taper_into(SC, cur));
+        FWIX_TRY(do_scatter(p, iz - 1, 1, SC, SC, 0, nullptr, 0, s));
+      } else {
+        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, p->store(iz - 1), cur, 0, s));
+        FWIX_TRY(do_scatter(p, iz - 1, 1, cur, SC, 0, nullptr, 0, s));
+      }
+      const float2* bu;
+      FWIX_TRY(U.get(p, iz, s, &bu));
+      FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bu, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
+    }
+    FWIX_TRY(do_inject(p, rec, iz, data, cur, s));
+    const float2* bd;
+    FWIX_TRY(D.get(p, iz, s, &bd));
+    FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                            p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
+                                            ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, cur, 1, s),
+                "linearised reflection adjoint"));
+  }
+  // upward: eta_iz = Rec_iz^H d + conj(R_iz) zeta_iz + S_iz^H eta_iz+1, the adjoint of
+  // the down-scattering recursion (reflected :240-280 and direct :180-208)
+  FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+  for (int iz = nz - 1; iz >= 0; --iz) {
+    if (iz < nz - 1) {
+      if (pspi) {
+        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, SC, 0, s));
+        FWIX_TRY(taper_into(SC, A));
+        FWIX_TRY(do_scatter(p, iz, 1, SC, SC, 0, nullptr, 0, s));
+      } else {
+        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, A, 0, s));
+        FWIX_TRY(do_scatter(p, iz, 1, A, SC, 0, nullptr, 0, s));
+      }
+      const float2* bd;
+      FWIX_TRY(D.get(p, iz, s, &bd));
+      FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bd, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
+    }
+    FWIX_TRY(do_reflect(p, iz, 1, p->store(iz), A, 1, s));
+    FWIX_TRY(do_inject(p, rec, iz, data, A, s));
+  }
+  return FWIX_OK;
+}
+
 }  // namespace
 
-// =============================================================================
 extern "C" {
 
 const char* fwix_last_error(void) { return g_err.c_str(); }
@@ -861,6 +1000,66 @@ fwix_status fwix_propagate(fwix_plan* p, const fwix_traces* src, const fwix_trac
   return FWIX_OK;
 }
 
+size_t fwix_plan_packed_bytes(const fwix_plan* p) { return p ? p->packed_bytes() : 0; }
+
+fwix_status fwix_pack_rate8(fwix_plan* p, const void* wfld, void* packed, void* stream) {
+  if (!p || !wfld || !packed) return fail(FWIX_ERR_INVALID, "null argument");
+  if (((uintptr_t)wfld) % 16 != 0 || ((uintptr_t)packed) % 16 != 0)
+    return fail(FWIX_ERR_INVALID, "wavefield and packed buffers must be 16-byte aligned");
+  return cu(fwix::launch_pack_rate8(2 * p->d.wfld, (const float*)wfld, packed, (cudaStream_t)stream), "pack");
+}
+
+fwix_status fwix_unpack_rate8(fwix_plan* p, const void* packed, void* wfld, void* stream) {
+  if (!p || !wfld || !packed) return fail(FWIX_ERR_INVALID, "null argument");
+  if (((uintptr_t)wfld) % 16 != 0 || ((uintptr_t)packed) % 16 != 0)
+    return fail(FWIX_ERR_INVALID, "wavefield and packed buffers must be 16-byte aligned");
+  return cu(fwix::launch_unpack_rate8(2 * p->d.wfld, packed, (float*)wfld, (cudaStream_t)stream), "unpack");
+}
+
+// Propagator::forward (Propagator.cpp:121-221) keeping the down and up fields of
+// every depth packed, as the reference keeps them ZFP-compressed in its
+// WavefieldPool: D in workspace A, each depth packed after its injection; the up
+// pass reflects the unpacked down field of each depth (workspace B).
+fwix_status fwix_propagate_packed(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec, const void* wavelet,
+                                  void* data, int add, void* packed_down, void* packed_up, void* stream) {
+  if (!p || !src || !rec || !wavelet || !data || !packed_down) return fail(FWIX_ERR_INVALID, "null argument");
+  if (((uintptr_t)packed_down) % 16 != 0 || ((uintptr_t)packed_up) % 16 != 0)
+    return fail(FWIX_ERR_INVALID, "packed buffers must be 16-byte aligned");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_SWEEP));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nz = p->desc.nz, k = p->desc.step_kind;
+  const long long nf = 2 * p->d.wfld;
+  const size_t pb = p->packed_bytes();
+  unsigned char* pd = (unsigned char*)packed_down;
+  unsigned char* pu = (unsigned char*)packed_up;
+  float2* dat = (float2*)data;
+  const float2* wav = (const float2*)wavelet;
+  float2* D = p->wA();
+  float2* R = p->wB();
+  if (!add) FWIX_CU(cudaMemsetAsync(dat, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
+  FWIX_CU(cudaMemsetAsync(D, 0, p->wbytes(), s));
+  for (int iz = 0; iz < nz; ++iz) {
+    FWIX_TRY(do_inject(p, src, iz, wav, D, s));
+    FWIX_TRY(do_record(p, rec, iz, D, dat, s));
+    FWIX_TRY(cu(fwix::launch_pack_rate8(nf, (const float*)D, pd + (size_t)iz * pb, s), "pack down field"));
+    if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, D, D, 0, s));
+  }
+  float2* U = p->wA();  // the down pass is done with it
+  for (int iz = nz - 1; iz >= 0; --iz) {
+    if (iz == nz - 1)
+      FWIX_CU(cudaMemsetAsync(U, 0, p->wbytes(), s));
+    else
+      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, U, U, 0, s));
+    FWIX_TRY(cu(fwix::launch_unpack_rate8(nf, pd + (size_t)iz * pb, (float*)R, s), "unpack down field"));
+    FWIX_TRY(do_reflect(p, iz, 0, R, U, 1, s));
+    FWIX_TRY(do_record(p, rec, iz, U, dat, s));
+    if (pu) FWIX_TRY(cu(fwix::launch_pack_rate8(nf, (const float*)U, pu + (size_t)iz * pb, s), "pack up field"));
+  }
+  return FWIX_OK;
+}
+
 // Lockstep migration: the source field (Propagator.cpp:155-180) and the receiver
 // field of the back-scattering adjoint (ExtendedBorn.cpp:396-408) move down
 // together and image[iz] accumulates sum_w Re sum_s conj(S) R
@@ -902,109 +1101,26 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
   FWIX_TRY(need_refs(p));
   FWIX_TRY(need_model(p));
   FWIX_TRY(need_ws(p, FWIX_WS_BORN));
-  cudaStream_t s = (cudaStream_t)stream;
-  const int nz = p->desc.nz, k = p->desc.step_kind;
-  const long long W = p->d.wfld, M = mw ? mslice(p) : plane;
-  const float2* bgd = (const float2*)bg_down_v;
-  const float2* bgu = (const float2*)bg_up_v;
-  float2* ds = (float2*)dslow_v;
-  float2* dr = (float2*)dden_v;
-  float2* data = (float2*)data_v;
-  float2* A = p->wA();
-  const size_t wb = p->wbytes();
-  // The reference runs four sweeps each way (ExtendedBorn.cpp:152-453), every
-  // scattered source propagated by a step of its own.  All operators are linear,
-  // so sources that feed the same recursion are summed before one step:
-  // step(A) + step(scat) = step(A + scat).  The forward keeps one downward and one
-  // upward recursion, the adjoint one downward and one upward; the results equal
-  // the four-sweep operators up to float rounding.
-  float2* SC = p->wSC();
-  const bool pspi = k == FWIX_STEP_PSPI;
-  if (!adjoint) {
-    if (!add) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
-    // down scattering (ExtendedBorn.cpp:152-178): store[iz] = dD_iz, the field
-    // recorded at iz; dD_iz+1 = S_iz(dD_iz + Scat_iz(bg_down_iz * ds_iz))
-    FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
-    for (int iz = 0; iz < nz; ++iz) {
-      FWIX_TRY(do_record(p, rec, iz, p->store(iz), data, s));
-      if (iz == nz - 1) break;
-      FWIX_TRY(do_scatter(p, iz, 0, bgd + iz * W, SC, 0, ds + iz * M, mw, s));
-      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, p->store(iz), p->store(iz + 1), 0, s, SC));
-    }
-    // one upward recursion for the reflected down-scattered field (:210-238), the
-    // up scattering (:282-311) and the back scattering (:352-389):
-    //   Z_iz = S_iz(Z_iz+1 + Scat_iz(bg_up_iz+1 * ds_iz+1)) + R_iz dD_iz + bg_down_iz * dR_iz
-    FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
-    for (int iz = nz - 1; iz >= 0; --iz) {
-      const int z1 = lower_iz(p, iz);
-      if (iz < nz - 1) {
-        FWIX_TRY(do_scatter(p, iz, 0, bgu + (iz + 1) * W, SC, 0, ds + (iz + 1) * M, mw, s));
-        FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s, SC));
-      }
-      FWIX_TRY(do_reflect(p, iz, 0, p->store(iz), A, 1, s));
-      FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
-                                              p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                              ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bgd + iz * W, A, 1, s),
-                  "linearised reflection"));
-      FWIX_TRY(do_record(p, rec, iz, A, data, s));
-    }
-    return FWIX_OK;
-  }
-  if (!add) {
-    FWIX_CU(cudaMemsetAsync(ds, 0, (size_t)nz * M * sizeof(float2), s));
-    FWIX_CU(cudaMemsetAsync(dr, 0, (size_t)nz * M * sizeof(float2), s));
-  }
-  // The scattering adjoints step with the add-version adjoint (no taper,
-  // Scattering.cpp:54-61), the recursions with the in-place adjoint (taper last,
-  // PSPI.cpp:85-103); for PSPI the second is the taper of the first, so one
-  // add-version step serves both.  (NSPS has no taper: the two coincide.)
-  SpecArgs ta = p->args(nullptr, nullptr, 0);
-  auto taper_into = [&](const float2* u, float2* out) {
-    return cu(fwix::launch_taper(ta, u, out, 0, s), "taper");
-  };
-  // downward: zeta_iz = Rec_iz^H d + S_iz-1^H zeta_iz-1 (the adjoint of the upward
-  // recursion), kept in store[iz]; it feeds the up-scattering adjoint (:313-349)
-  // and the back-scattering adjoint (:391-453), which needs no steps of its own
-  FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
-  for (int iz = 0; iz < nz; ++iz) {
-    const int z1 = lower_iz(p, iz);
-    float2* cur = p->store(iz);
-    if (iz > 0) {
-      if (pspi) {
-        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, p->store(iz - 1), SC, 0, s));
-        FWIX_TRY(taper_into(SC, cur));
-        FWIX_TRY(do_scatter(p, iz - 1, 1, SC, SC, 0, nullptr, 0, s));
-      } else {
-        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, p->store(iz - 1), cur, 0, s));
-        FWIX_TRY(do_scatter(p, iz - 1, 1, cur, SC, 0, nullptr, 0, s));
-      }
-      FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgu + iz * W, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
-    }
-    FWIX_TRY(do_inject(p, rec, iz, data, cur, s));
-    FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
-                                            p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                            ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bgd + iz * W, cur, 1, s),
-                "linearised reflection adjoint"));
-  }
-  // upward: eta_iz = Rec_iz^H d + conj(R_iz) zeta_iz + S_iz^H eta_iz+1, the adjoint of
-  // the down-scattering recursion (reflected :240-280 and direct :180-208)
-  FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
-  for (int iz = nz - 1; iz >= 0; --iz) {
-    if (iz < nz - 1) {
-      if (pspi) {
-        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, SC, 0, s));
-        FWIX_TRY(taper_into(SC, A));
-        FWIX_TRY(do_scatter(p, iz, 1, SC, SC, 0, nullptr, 0, s));
-      } else {
-        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, A, 0, s));
-        FWIX_TRY(do_scatter(p, iz, 1, A, SC, 0, nullptr, 0, s));
-      }
-      FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bgd + iz * W, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
-    }
-    FWIX_TRY(do_reflect(p, iz, 1, p->store(iz), A, 1, s));
-    FWIX_TRY(do_inject(p, rec, iz, data, A, s));
-  }
-  return FWIX_OK;
+  BgSrc D{(const float2*)bg_down_v}, U{(const float2*)bg_up_v};
+  return born_body(p, adjoint, rec, D, U, (float2*)dslow_v, (float2*)dden_v, mw, (float2*)data_v, add,
+                   (cudaStream_t)stream);
+}
+
+fwix_status fwix_born_packed(fwix_plan* p, int adjoint, const fwix_traces* rec, const void* packed_down,
+                             const void* packed_up, void* dslow_v, void* dden_v, int64_t model_w_stride,
+                             void* data_v, int add, void* stream) {
+  if (!p || !rec || !packed_down || !packed_up || !dslow_v || !dden_v || !data_v)
+    return fail(FWIX_ERR_INVALID, "null argument");
+  const long long plane = (long long)p->d.ny * p->d.nx;
+  if (model_w_stride != 0 && model_w_stride != plane)
+    return fail(FWIX_ERR_INVALID, "model_w_stride must be 0 or ny*nx");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_BORN_PACKED));
+  BgSrc D{nullptr, (const unsigned char*)packed_down, p->wB()};
+  BgSrc U{nullptr, (const unsigned char*)packed_up, p->store(p->desc.nz)};
+  return born_body(p, adjoint, rec, D, U, (float2*)dslow_v, (float2*)dden_v, model_w_stride, (float2*)data_v,
+                   add, (cudaStream_t)stream);
 }
 
 

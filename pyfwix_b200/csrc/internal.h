@@ -172,6 +172,11 @@ cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, fl
 cudaError_t launch_correlate_padded(const Dims& d, const float2* S, const float2* R, float* img, int add,
                                     cudaStream_t s);
 cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s);
+// Fixed-rate lossy wavefield store (pack.cu): bytes of one packed array of nfloat
+// floats, and the packing / unpacking launches.
+size_t packed_rate8_bytes(long long nfloat);
+cudaError_t launch_pack_rate8(long long nfloat, const float* in, void* packed, cudaStream_t s);
+cudaError_t launch_unpack_rate8(long long nfloat, const void* packed, float* out, cudaStream_t s);
 
 // Acquisition kernels (pointwise.cu).  A depth level's injection is a gather
 // list: for each target cell, the (trace, weight) pairs that land on it.

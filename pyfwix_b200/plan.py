@@ -233,6 +233,42 @@ class Plan:
                                       _stream()))
         return image
 
+    # -------------------------------------------------------------- packed store
+    @property
+    def packed_bytes(self):
+        """Bytes of one packed wavefield (fixed rate, 8.5 bits per value)."""
+        return int(self.lib.fwix_plan_packed_bytes(self._h))
+
+    def packed(self, nfields=1):
+        """Uninitialised storage for nfields packed wavefields (uint8 tensor)."""
+        return torch.empty((nfields, self.packed_bytes), dtype=torch.uint8, device=self.device)
+
+    def pack(self, wfld, packed):
+        L.check(self.lib.fwix_pack_rate8(self._h, _p(wfld), _p(packed), _stream()))
+        return packed
+
+    def unpack(self, packed, wfld):
+        L.check(self.lib.fwix_unpack_rate8(self._h, _p(packed), _p(wfld), _stream()))
+        return wfld
+
+    def propagate_packed(self, src, rec, wavelet, data, packed_down, packed_up=None, add=False):
+        """Modelling with the down / up fields of every depth stored packed
+        ([nz][packed_bytes] uint8 tensors)."""
+        self.ensure_workspace(L.WS_SWEEP)
+        L.check(self.lib.fwix_propagate_packed(self._h, src._h, rec._h, _p(wavelet), _p(data), int(add),
+                                               _p(packed_down), _p(packed_up), _stream()))
+        return data
+
+    def born_packed(self, rec, packed_down, packed_up, dslow, dden, data, adjoint=False, add=False):
+        """Extended Born on packed backgrounds (see born)."""
+        self.ensure_workspace(L.WS_BORN_PACKED)
+        nwm = dslow.shape[1] if dslow.dim() == 4 else self.nw
+        if tuple(dslow.shape) != tuple(dden.shape) or nwm not in (1, self.nw):
+            raise ValueError("dslow / dden must both be [nz][nw or 1][ny][nx]")
+        mw = 0 if (nwm == 1 and self.nw > 1) else self.ny * self.nx
+        L.check(self.lib.fwix_born_packed(self._h, int(adjoint), rec._h, _p(packed_down), _p(packed_up), _p(dslow),
+                                          _p(dden), mw, _p(data), int(add), _stream()))
+
     def born(self, rec, bg_down, bg_up, dslow, dden, data, adjoint=False, add=False):
         """Extended Born.  dslow / dden are [nz][nw][ny][nx] (per frequency) or
         [nz][1][ny][nx] (one perturbation per depth for every frequency)."""

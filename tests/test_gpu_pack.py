@@ -1,0 +1,90 @@
+"""Fixed-rate lossy store of wavefields on the device (pyfwix_b200/csrc/pack.cu):
+packed bytes and unpacked values bit-exact against the oracle's restatement
+(oracle/pack.py); modelling with packed down / up fields against modelling with
+full ones; Born on packed backgrounds equal, bit for bit, to Born on the
+unpacked backgrounds, and within the store's error of Born on the exact ones."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import pack as opack
+from tests.conftest import crandn
+from tests.gpu_helpers import make_case, make_plan, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nx,ny,nw,ns,pad", [(32, 24, 3, 1, 4), (60, 44, 5, 2, 4), (64, 64, 2, 1, 0)])
+def test_pack_bits_against_oracle(nx, ny, nw, ns, pad):
+    g, rng, sref, labels, slow, den = make_case(nx=nx, ny=ny, nw=nw, nz=2, nref=2, padx=pad, pady=pad)
+    p = make_plan(g, ns, sref, labels)
+    x = crandn(rng, p.wshape).astype(np.complex64)
+    x *= np.float32(10.0) ** rng.integers(-5, 5, size=x.shape)
+    x[0, 0, :2] = 0
+    xd = torch.as_tensor(x).cuda()
+    pk = p.packed(1)[0]
+    p.pack(xd, pk)
+    y = torch.empty_like(xd)
+    p.unpack(pk, y)
+    torch.cuda.synchronize()
+    want = opack.pack(x)
+    assert pk.numel() == want.size == p.packed_bytes
+    nblk = -(-2 * x.size // 16)
+    got = pk.cpu().numpy()
+    assert np.array_equal(got[:nblk * 17], want[:nblk * 17])
+    assert np.array_equal(y.cpu().numpy().view(np.float32), opack.unpack(want, x.shape).view(np.float32))
+
+
+def _acq(g, p):
+    geom = dict(sx=[80.0], sy=[96.0], sz=[0.0], s_ids=[0], rx=list(np.linspace(0, 300, 16)), ry=[100.0] * 16,
+                rz=[0.0] * 16, r_ids=[0] * 16)
+    src = p.traces(geom["sx"], geom["sy"], geom["sz"], [0])
+    rec = p.traces(geom["rx"], geom["ry"], geom["rz"], [0] * 16)
+    return src, rec
+
+
+@pytest.mark.parametrize("kind,nx,ny,pad", [("pspi", 32, 24, 4), ("nsps", 64, 64, 0)])
+def test_packed_modelling_and_born(kind, nx, ny, pad):
+    g, rng, sref, labels, slow, den = make_case(nx=nx, ny=ny, nw=4, nz=6, nref=3, padx=pad, pady=pad)
+    slow = slow.copy()
+    slow[g.nz - 2:] *= 1.8
+    p = make_plan(g, 1, sref, labels, slow, den, step=kind)
+    src, rec = _acq(g, p)
+    wav = torch.as_tensor(crandn(rng, (1, g.nw)).astype(np.complex64)).cuda()
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((16, g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, wav, d, bd, bu)
+    pd, pu = p.packed(g.nz), p.packed(g.nz)
+    dp = torch.empty_like(d)
+    p.propagate_packed(src, rec, wav, dp, pd, pu)
+    # the packed fields are the packed full fields, the up pass reflecting unpacked down fields
+    ud, uu = torch.empty_like(bd), torch.empty_like(bu)
+    for iz in range(g.nz):
+        p.unpack(pd[iz], ud[iz])
+        p.unpack(pu[iz], uu[iz])
+    torch.cuda.synchronize()
+    assert rel(ud.cpu().numpy(), bd.cpu().numpy()) < 1e-2
+    assert rel(uu.cpu().numpy(), bu.cpu().numpy()) < 2e-2
+    assert rel(dp.cpu().numpy(), d.cpu().numpy()) < 2e-2
+    ms = torch.as_tensor(crandn(rng, (g.nz, g.nw, g.ny, g.nx)).astype(np.complex64)).cuda()
+    mr = torch.as_tensor(crandn(rng, (g.nz, g.nw, g.ny, g.nx)).astype(np.complex64)).cuda()
+    r = torch.as_tensor(crandn(rng, d.shape).astype(np.complex64)).cuda()
+    for adjoint in (False, True):
+        if not adjoint:
+            o1, o2, o3 = (torch.empty_like(d) for _ in range(3))
+            p.born_packed(rec, pd, pu, ms, mr, o1)
+            p.born(rec, ud, uu, ms, mr, o2)
+            p.born(rec, bd, bu, ms, mr, o3)
+            outs = [(o1, o2, o3)]
+        else:
+            gp = [torch.empty_like(ms) for _ in range(6)]
+            p.born_packed(rec, pd, pu, gp[0], gp[1], r, adjoint=True)
+            p.born(rec, ud, uu, gp[2], gp[3], r, adjoint=True)
+            p.born(rec, bd, bu, gp[4], gp[5], r, adjoint=True)
+            outs = [(gp[0], gp[2], gp[4]), (gp[1], gp[3], gp[5])]
+        torch.cuda.synchronize()
+        for a, b, c in outs:
+            assert torch.equal(a, b)
+            assert rel(a.cpu().numpy(), c.cpu().numpy()) < 3e-2
+    assert p.packed_bytes * 3.7 < 8 * int(np.prod(p.wshape))
