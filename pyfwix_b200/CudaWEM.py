@@ -189,8 +189,10 @@ class WindowPropagator:
     of these per (shot group, frequency band) pair.
 
     The background down- and up-going wavefields of the last ``forward`` stay in
-    device memory (lossless, every depth) for :class:`ExtendedBorn`; the reference
-    keeps ZFP-compressed copies on disk (``propagator/src/WavefieldPool.cpp``).
+    device memory for :class:`ExtendedBorn`: lossless by default, or, with the
+    reference's ``compress_rate`` key set to 8, in this library's fixed-rate
+    lossy format (8.5 bits per value, 3.76 x smaller; the reference keeps
+    ZFP-compressed copies at that rate on disk, ``propagator/src/WavefieldPool.cpp``).
     ``nbatches`` is accepted for signature compatibility: every shot and
     frequency runs in one batch."""
 
@@ -213,6 +215,10 @@ class WindowPropagator:
             raise ValueError(f"wavelet must be [nsrc={self.src.ntrace}][nw={self.plan.nw}]")
         self.bg_down = self.bg_up = None
         self._bg_key = None
+        rate = _get(par, "compress_rate")
+        if rate is not None and float(rate) != 8.0:
+            raise ValueError(f"compress_rate {rate} is not supported: the packed store has one rate, 8")
+        self.packed = rate is not None
 
     def set_background_model(self, model):
         s2, den = _model_pair(model)
@@ -222,6 +228,10 @@ class WindowPropagator:
         _refs(self.plan, s2d, self.par)
 
     def _ensure_storage(self):
+        if self.packed:
+            if self.bg_down is None:
+                self.bg_down, self.bg_up = self.plan.packed(self.plan.nz), self.plan.packed(self.plan.nz)
+            return
         shape = (self.plan.nz,) + self.plan.wshape
         if self.bg_down is None or tuple(self.bg_down.shape) != shape:
             self.bg_down = torch.empty(shape, dtype=torch.complex64, device=self.device)
@@ -232,13 +242,25 @@ class WindowPropagator:
             self.set_background_model(model)
             self._ensure_storage()
             out = _dev(data, self.device) if add else _dev(data, self.device, zero=True)
-            self.plan.propagate(self.src, self.rec, self.wavelet, out, self.bg_down, self.bg_up, add=bool(add))
+            if self.packed:
+                self.plan.propagate_packed(self.src, self.rec, self.wavelet, out, self.bg_down, self.bg_up,
+                                           add=bool(add))
+            else:
+                self.plan.propagate(self.src, self.rec, self.wavelet, out, self.bg_down, self.bg_up, add=bool(add))
             self._bg_key = tuple(id(v) for v in _model_pair(model))
             _store(data, out)
 
+    def born(self, dslow, dden, data, adjoint, add):
+        """Extended Born on the stored backgrounds (packed or full)."""
+        fn = self.plan.born_packed if self.packed else self.plan.born
+        fn(self.rec, self.bg_down, self.bg_up, dslow, dden, data, adjoint=adjoint, add=add)
+
     def get_compression_ratio(self):
-        """Background wavefields are kept uncompressed: ratio 1."""
-        return 1.0
+        """Bytes of a complex64 background wavefield over its stored bytes: 1
+        uncompressed, 3.76 with compress_rate 8."""
+        if not self.packed:
+            return 1.0
+        return 8.0 * float(np.prod(self.plan.wshape)) / self.plan.packed_bytes
 
 
 class WindowExtendedBorn:
@@ -271,7 +293,7 @@ class WindowExtendedBorn:
             self._background()
             _, _, dsd, drd = self._model(model, zero=False)
             out = _dev(data, p.device) if add else _dev(data, p.device, zero=True)
-            p.plan.born(p.rec, p.bg_down, p.bg_up, dsd, drd, out, adjoint=False, add=bool(add))
+            p.born(dsd, drd, out, adjoint=False, add=bool(add))
             _store(data, out)
 
     def adjoint(self, add, model, data):
@@ -280,7 +302,7 @@ class WindowExtendedBorn:
             self._background()
             ds, dr, dsd, drd = self._model(model, zero=not add)
             d = _dev(data, p.device)
-            p.plan.born(p.rec, p.bg_down, p.bg_up, dsd, drd, d, adjoint=True, add=bool(add))
+            p.born(dsd, drd, d, adjoint=True, add=bool(add))
             _store(ds, dsd)
             _store(dr, drd)
 
