@@ -54,6 +54,7 @@ def args_():
     ap.add_argument("--no-fwi", action="store_true", help="skip the FWI-gradient timing")
     ap.add_argument("--fwi-nz", type=int, default=None, help="depth levels of the FWI workload (quick runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched forward+imaging timing")
+    ap.add_argument("--no-packed", action="store_true", help="skip the packed-background Born timing")
     ap.add_argument("--batched-nz", type=int, default=None, help="depth levels of the batched workload (quick runs)")
     ap.add_argument("--batched-shots", type=int, default=32)
     ap.add_argument("--batched-streams", type=int, default=8)
@@ -169,6 +170,31 @@ def born_step(st):
     p = st["plan"]
     p.born(st["rec"], st["bd"], st["bu"], st["dslow"], st["dden"], st["data"])
     p.born(st["rec"], st["bd"], st["bu"], st["gs"], st["gr"], st["data"], adjoint=True)
+
+
+def born_packed_timing(st, w, steps=2):
+    """The same Born forward + adjoint step on backgrounds kept in the packed
+    fixed-rate store (8.5 bits per value): Gcell-steps/s, the stored bytes of the
+    backgrounds against complex64, and the gradient's relative difference from
+    the lossless step's."""
+    import torch
+    p = st["plan"]
+    pd, pu = p.packed(w.nz), p.packed(w.nz)
+    for iz in range(w.nz):
+        p.pack(st["bd"][iz], pd[iz])
+        p.pack(st["bu"][iz], pu[iz])
+    gs_ref = st["gs"].clone()
+    fn = lambda: (p.born_packed(st["rec"], pd, pu, st["dslow"], st["dden"], st["data"]),
+                  p.born_packed(st["rec"], pd, pu, st["gs"], st["gr"], st["data"], adjoint=True))
+    fn()
+    t = time_steps(fn, steps, lambda: None)
+    nref = float(torch.linalg.vector_norm(gs_ref))
+    diff = float(torch.linalg.vector_norm(st["gs"] - gs_ref)) / nref if nref > 0 else None
+    out = {"value": 2 * w.nx * w.ny * w.nw * w.nz * steps / t / 1e9, "unit": "Gcell-steps/s",
+           "ms_per_step": t / steps * 1e3, "background_bytes_ratio": 8.0 * st["bd"][0].numel() / p.packed_bytes,
+           "gradient_rel_diff": diff}
+    del pd, pu
+    return out
 
 
 def born_step_e2e(st, host):
@@ -511,6 +537,7 @@ def main():
             "kernel": "NSPS depth step (row pass + column pass + row pass), 256x256x128",
             "step_ms": tstep * 1e3, "alg_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP}
     bg_gb = st["bd"].numel() * 8 / 1e9
+    packed = born_packed_timing(st, w) if not a.no_packed else None
     fwi = batched = None
     del st
     torch.cuda.empty_cache()
@@ -534,7 +561,7 @@ def main():
                            "l2": "inputs larger than L2 (background wavefields 2 x %.1f GB)"
                                  % bg_gb},
                 "gpu_launches": launches, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "fwi_grad": fwi, "batched": batched}
+                "fwi_grad": fwi, "batched": batched, "born_packed_backgrounds": packed}
         print(json.dumps(line), flush=True)
     if ws > 1:
         tdist.destroy_process_group()
