@@ -527,6 +527,9 @@ struct ColGeo {
   // at most 8 samples per lane (64 registers; the few spills stay in L1 and the
   // extra warps hide more latency than they cost), else what fits.
   static constexpr int kMinBlocks = P::E <= 8 ? 4 : P::E <= 16 ? 2 : 1;
+  // k_col_a holds one spectrum and one term in registers (k_col_b a running sum
+  // as well): with 16 samples per lane it fits three CTAs per SM
+  static constexpr int kMinBlocksA = P::E <= 8 ? 4 : P::E <= 12 ? 2 : P::E <= 16 ? 3 : 1;
   static size_t smem2() { return ((size_t)2 * LX * LINE + tw_size<P>()) * sizeof(float2); }  // tile, tw, tile
 };
 
@@ -602,7 +605,7 @@ __device__ __forceinline__ void col_factors(const SpecArgs& a, int t, int iw, in
 
 // t2[term] = F_y^-1(Q_term * F_y(t1[0])); the spectrum stays in registers.
 template <class P, int QM>
-__global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_a(const SpecArgs a, int nxt) {
+__global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocksA) k_col_a(const SpecArgs a, int nxt) {
   extern __shared__ float2 smem[];
   ColCtx<P> c(a, smem, nxt);
   load_stage_tw<P>(c.tw, a.twy);
