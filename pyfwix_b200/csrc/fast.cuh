@@ -321,9 +321,18 @@ struct RowCtx {
   }
 };
 
+// Resident CTAs per SM the forward row pass's registers are held to: the
+// multi-term passes of 12- and 16-sample lanes at two (the scattering adjoint's,
+// with one term's weights and no labels, at three), the rest unhinted.
+template <class P, int PRE>
+constexpr int row_fwd_min_blocks() {
+  if (PRE == W_SCAT_CONJ && P::E == 16) return 3;
+  return multi_term(PRE) && (P::E == 16 || P::E == 12) ? 2 : 0;
+}
+
 // t1[term] = F_x(pre_term * in) for each term.
 template <class P, int PRE>
-__global__ void __launch_bounds__(kWarps * 32, multi_term(PRE) && (P::E == 16 || P::E == 12) ? 2 : 0) k_row_fwd(const SpecArgs a, int nchunk) {
+__global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_row_fwd(const SpecArgs a, int nchunk) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
