@@ -620,6 +620,17 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocksA) k_col_a(c
   load_stage_tw<P>(c.tw, a.twy);
   cols_to_tile<P>(c.tile, a.t1, a, c.b, c.x0);
   __syncthreads();
+  // The zeroth Born order's filter (|k| / w)^0 is the identity: its output is the
+  // tile itself, scaled as the transform pair would (NY times the normalisation),
+  // written before the transform overwrites the tile; the loop starts at order 1.
+  int first = 0;
+  if constexpr (QM == Q_KPOW) {
+    if (a.term0 == 0 && a.nterm > 0) {
+      tile_to_cols<P>(c.tile, a.t2, a, c.b, c.x0, 0, a.norm * (float)P::N);
+      __syncthreads();
+      first = 1;
+    }
+  }
   float2 psi[P::E];
 #pragma unroll
   for (int e = 0; e < P::E; ++e) psi[e] = c.line[swz(pos_first<P>(c.t, e))];
@@ -631,8 +642,8 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocksA) k_col_a(c
   // fetched as they are applied.
   constexpr bool kPrefetch = P::E <= 12;
   float2 q[kPrefetch ? P::E : 1];
-  if constexpr (kPrefetch) col_factors<P, QM>(a, 0, c.iw, xq, c.t, q);
-  for (int term = 0; term < a.nterm; ++term) {
+  if constexpr (kPrefetch) col_factors<P, QM>(a, first, c.iw, xq, c.t, q);
+  for (int term = first; term < a.nterm; ++term) {
     float2 v[P::E];
     if constexpr (kPrefetch) {
 #pragma unroll
