@@ -91,11 +91,11 @@ struct SpecArgs {
   float coef[5];
   float norm;          // scale folded into the column multiplier
   int nterm;           // references (W_MASK) or Taylor terms (W_SCAT)
-  // Born scattering with the zeroth Taylor term applied directly: its filter
-  // (|k| / w)^0 is the identity, so W_0 u needs no transform.  The transformed
-  // terms are then orders term0 .. term0 + nterm - 1 (term0 = 1), and the inverse
-  // row pass adds W_0 u (direct_mode 1: u = direct, times the W_IC image when
-  // `image` is set) or conj(W_0) d (direct_mode 2: d = direct) to its sum.
+  // Born scattering adjoint with the zeroth Taylor term applied directly: its
+  // filter (|k| / w)^0 is the identity, so conj(W_0) d needs no transform.  The
+  // transformed terms are then orders term0 .. term0 + nterm - 1 (term0 = 1), and
+  // the inverse row pass (W_ONE_DIRECT) adds conj(W_0) d, d = direct, to its sum
+  // (direct_mode 2; 0 = no direct term).
   int term0;
   int direct_mode;
   const float2* direct;

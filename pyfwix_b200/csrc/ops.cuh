@@ -35,18 +35,10 @@ __device__ __forceinline__ float2 scat_weight(const SpecArgs& a, int n, int iw, 
   return rot90<false>(cscale(p, f));
 }
 
-// Zeroth Born term applied directly (SpecArgs::direct_mode): W_0 u for the
-// forward (u times the W_IC image when one is bound), conj(W_0) d for the adjoint,
-// at cell (y, x) of global slice b.
+// Zeroth Born term of the scattering adjoint applied directly
+// (SpecArgs::direct_mode): conj(W_0) d at cell (y, x) of global slice b.
 __device__ __forceinline__ float2 scat_direct(const SpecArgs& a, long long b, int iw, int y, int x) {
-  float2 u = a.direct[(b * a.d.NY + y) * a.d.NX + x];
-  const float2 w0 = scat_weight(a, 0, iw, y, x);
-  if (a.direct_mode == 2) return cmul_conj(u, w0);
-  if (a.image) {
-    if (y >= a.d.ny || x >= a.d.nx) return make_float2(0.f, 0.f);
-    u = cmul(u, a.image[(long long)iw * a.img_w + (long long)y * a.d.nx + x]);
-  }
-  return cmul(u, w0);
+  return cmul_conj(a.direct[(b * a.d.NY + y) * a.d.NX + x], scat_weight(a, 0, iw, y, x));
 }
 
 // Hat-function interpolation weight of reference t at slowness s and its
