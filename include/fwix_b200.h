@@ -223,7 +223,8 @@ fwix_status fwix_born(fwix_plan* plan, int adjoint, const fwix_traces* rec, cons
  * largest magnitude).  Not ZFP's bit stream.
  *   fwix_plan_packed_bytes: bytes of one packed wavefield [ns][nw][NY][NX]; [nz]
  *     packed wavefields are nz times that, depth iz at iz * packed_bytes.
- *   fwix_pack_rate8 / fwix_unpack_rate8: one wavefield.
+ *   fwix_pack_rate8 / fwix_unpack_rate8: one wavefield (buffers 4-byte aligned;
+ *     16-byte aligned ones take the vector path).
  *   fwix_propagate_packed: fwix_propagate storing the down and up fields of every
  *     depth packed (packed_up may be NULL); the up pass reflects the unpacked down
  *     fields, as the reference's reflects its decompressed ones.

@@ -141,8 +141,10 @@ struct fwix_plan {
   size_t ws_need(int cls) const {
     size_t b = 2 * tbytes();  // t1, t2 for one chunk
     if (cls >= FWIX_WS_SWEEP) b += 3 * wbytes();  // A, B, SC
-    if (cls >= FWIX_WS_BORN) b += (size_t)desc.nz * wbytes();  // per-level field store
-    if (cls >= FWIX_WS_BORN_PACKED) b += wbytes();               // second unpacked background
+    if (cls == FWIX_WS_BORN) b += (size_t)desc.nz * wbytes();  // per-level field store
+    // packed backgrounds: the second unpacked background and the working level
+    // field, then the per-level store packed (256-byte aligned)
+    if (cls == FWIX_WS_BORN_PACKED) b += 2 * wbytes() + 256 + (size_t)desc.nz * packed_bytes();
     return b;
   }
   float2* t1() const { return (float2*)ws; }
@@ -152,6 +154,14 @@ struct fwix_plan {
   float2* wSC() const { return wB() + d.wfld; }
   float2* store(int iz) const { return wSC() + d.wfld * (long long)(1 + iz); }
   size_t packed_bytes() const { return fwix::packed_rate8_bytes(2 * d.wfld); }
+  // FWIX_WS_BORN_PACKED layout after A, B, SC: U (second background), X (working
+  // level field), then the packed per-level store
+  float2* wU() const { return wSC() + d.wfld; }
+  float2* wX() const { return wSC() + 2 * d.wfld; }
+  unsigned char* pstore(int iz) const {
+    const uintptr_t base = ((uintptr_t)(wSC() + 3 * d.wfld) + 255) & ~(uintptr_t)255;
+    return (unsigned char*)base + (size_t)iz * packed_bytes();
+  }
 
   SpecArgs args(const float2* in, float2* out, int add) const {
     SpecArgs a;
@@ -423,9 +433,33 @@ struct BgSrc {
   }
 };
 
+// Per-level fields of the Born recursions (dD_iz forward, zeta_iz adjoint), read
+// back in the opposite sweep for the reflections: [nz] full fields in the
+// workspace, or, with packed backgrounds, one working field (the recursion runs
+// in place in it) whose every level is kept packed and unpacked when read back.
+struct LevelStore {
+  fwix_plan* p;
+  bool packed;
+  float2* field(int iz) const { return packed ? p->wX() : p->store(iz); }
+  fwix_status keep(int iz, cudaStream_t s) const {
+    if (!packed) return FWIX_OK;
+    return cu(fwix::launch_pack_rate8(2 * p->d.wfld, (const float*)p->wX(), p->pstore(iz), s), "pack level field");
+  }
+  fwix_status get(int iz, cudaStream_t s, const float2** out) const {
+    if (!packed) {
+      *out = p->store(iz);
+      return FWIX_OK;
+    }
+    FWIX_TRY(cu(fwix::launch_unpack_rate8(2 * p->d.wfld, p->pstore(iz), (float*)p->wX(), s), "unpack level field"));
+    *out = p->wX();
+    return FWIX_OK;
+  }
+};
+
 // ExtendedBorn::forward / adjoint (ExtendedBorn.cpp:80-453) on backgrounds D, U.
 fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& D, BgSrc& U, float2* ds,
-                      float2* dr, long long mw, float2* data, int add, cudaStream_t s) {
+                      float2* dr, long long mw, float2* data, int add, cudaStream_t s, bool packed = false) {
+  const LevelStore Lv{p, packed};
   const int nz = p->desc.nz, k = p->desc.step_kind;
   const long long plane = (long long)p->d.ny * p->d.nx;
   const long long M = mw ? mslice(p) : plane;
@@ -443,14 +477,15 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
     if (!add) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
     // down scattering (ExtendedBorn.cpp:152-178): store[iz] = dD_iz, the field
     // recorded at iz; dD_iz+1 = S_iz(dD_iz + Scat_iz(bg_down_iz * ds_iz))
-    FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
+    FWIX_CU(cudaMemsetAsync(Lv.field(0), 0, wb, s));
     for (int iz = 0; iz < nz; ++iz) {
-      FWIX_TRY(do_record(p, rec, iz, p->store(iz), data, s));
+      FWIX_TRY(do_record(p, rec, iz, Lv.field(iz), data, s));
+      FWIX_TRY(Lv.keep(iz, s));
       if (iz == nz - 1) break;
       const float2* bd;
       FWIX_TRY(D.get(p, iz, s, &bd));
       FWIX_TRY(do_scatter(p, iz, 0, bd, SC, 0, ds + iz * M, mw, s));
-      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, p->store(iz), p->store(iz + 1), 0, s, SC));
+      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, Lv.field(iz), Lv.field(iz + 1), 0, s, SC));
     }
     // one upward recursion for the reflected down-scattered field (:210-238), the
     // up scattering (:282-311) and the back scattering (:352-389):
@@ -464,7 +499,9 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
         FWIX_TRY(do_scatter(p, iz, 0, bu, SC, 0, ds + (iz + 1) * M, mw, s));
         FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s, SC));
       }
-      FWIX_TRY(do_reflect(p, iz, 0, p->store(iz), A, 1, s));
+      const float2* dz;
+      FWIX_TRY(Lv.get(iz, s, &dz));
+      FWIX_TRY(do_reflect(p, iz, 0, dz, A, 1, s));
       const float2* bd;
       FWIX_TRY(D.get(p, iz, s, &bd));
       FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
@@ -490,17 +527,19 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
   // downward: zeta_iz = Rec_iz^H d + S_iz-1^H zeta_iz-1 (the adjoint of the upward
   // recursion), kept in store[iz]; it feeds the up-scattering adjoint (:313-349)
   // and the back-scattering adjoint (:391-453), which needs no steps of its own
-  FWIX_CU(cudaMemsetAsync(p->store(0), 0, wb, s));
+  FWIX_CU(cudaMemsetAsync(Lv.field(0), 0, wb, s));
   for (int iz = 0; iz < nz; ++iz) {
     const int z1 = lower_iz(p, iz);
-    float2* cur = p->store(iz);
+    float2* cur = Lv.field(iz);
     if (iz > 0) {
+      // (with the packed store the previous level and this one are the same
+      // working field: the step reads it before the taper or the step writes it)
       if (pspi) {
-        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, p->store(iz - 1), SC, 0, s));
+        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, Lv.field(iz - 1), SC, 0, s));
         FWIX_TRY(taper_into(SC, cur));
         FWIX_TRY(do_scatter(p, iz - 1, 1, SC, SC, 0, nullptr, 0, s));
       } else {
-        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, p->store(iz - 1), cur, 0, s));
+        FWIX_TRY(do_step(p, k, iz - 1, FWIX_ADJ_ADD, Lv.field(iz - 1), cur, 0, s));
         FWIX_TRY(do_scatter(p, iz - 1, 1, cur, SC, 0, nullptr, 0, s));
       }
       const float2* bu;
@@ -514,6 +553,7 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
                                             p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
                                             ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, cur, 1, s),
                 "linearised reflection adjoint"));
+    FWIX_TRY(Lv.keep(iz, s));
   }
   // upward: eta_iz = Rec_iz^H d + conj(R_iz) zeta_iz + S_iz^H eta_iz+1, the adjoint of
   // the down-scattering recursion (reflected :240-280 and direct :180-208)
@@ -532,7 +572,9 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
       FWIX_TRY(D.get(p, iz, s, &bd));
       FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bd, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
     }
-    FWIX_TRY(do_reflect(p, iz, 1, p->store(iz), A, 1, s));
+    const float2* zz;
+    FWIX_TRY(Lv.get(iz, s, &zz));
+    FWIX_TRY(do_reflect(p, iz, 1, zz, A, 1, s));
     FWIX_TRY(do_inject(p, rec, iz, data, A, s));
   }
   return FWIX_OK;
@@ -1004,15 +1046,15 @@ size_t fwix_plan_packed_bytes(const fwix_plan* p) { return p ? p->packed_bytes()
 
 fwix_status fwix_pack_rate8(fwix_plan* p, const void* wfld, void* packed, void* stream) {
   if (!p || !wfld || !packed) return fail(FWIX_ERR_INVALID, "null argument");
-  if (((uintptr_t)wfld) % 16 != 0 || ((uintptr_t)packed) % 16 != 0)
-    return fail(FWIX_ERR_INVALID, "wavefield and packed buffers must be 16-byte aligned");
+  if (((uintptr_t)wfld) % 4 != 0 || ((uintptr_t)packed) % 4 != 0)
+    return fail(FWIX_ERR_INVALID, "wavefield and packed buffers must be 4-byte aligned");
   return cu(fwix::launch_pack_rate8(2 * p->d.wfld, (const float*)wfld, packed, (cudaStream_t)stream), "pack");
 }
 
 fwix_status fwix_unpack_rate8(fwix_plan* p, const void* packed, void* wfld, void* stream) {
   if (!p || !wfld || !packed) return fail(FWIX_ERR_INVALID, "null argument");
-  if (((uintptr_t)wfld) % 16 != 0 || ((uintptr_t)packed) % 16 != 0)
-    return fail(FWIX_ERR_INVALID, "wavefield and packed buffers must be 16-byte aligned");
+  if (((uintptr_t)wfld) % 4 != 0 || ((uintptr_t)packed) % 4 != 0)
+    return fail(FWIX_ERR_INVALID, "wavefield and packed buffers must be 4-byte aligned");
   return cu(fwix::launch_unpack_rate8(2 * p->d.wfld, packed, (float*)wfld, (cudaStream_t)stream), "unpack");
 }
 
@@ -1023,8 +1065,8 @@ fwix_status fwix_unpack_rate8(fwix_plan* p, const void* packed, void* wfld, void
 fwix_status fwix_propagate_packed(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec, const void* wavelet,
                                   void* data, int add, void* packed_down, void* packed_up, void* stream) {
   if (!p || !src || !rec || !wavelet || !data || !packed_down) return fail(FWIX_ERR_INVALID, "null argument");
-  if (((uintptr_t)packed_down) % 16 != 0 || ((uintptr_t)packed_up) % 16 != 0)
-    return fail(FWIX_ERR_INVALID, "packed buffers must be 16-byte aligned");
+  if (((uintptr_t)packed_down) % 4 != 0 || ((uintptr_t)packed_up) % 4 != 0 || p->packed_bytes() % 16 != 0)
+    return fail(FWIX_ERR_INVALID, "packed buffers must be 4-byte aligned");
   FWIX_TRY(need_refs(p));
   FWIX_TRY(need_model(p));
   FWIX_TRY(need_ws(p, FWIX_WS_SWEEP));
@@ -1118,9 +1160,9 @@ fwix_status fwix_born_packed(fwix_plan* p, int adjoint, const fwix_traces* rec, 
   FWIX_TRY(need_model(p));
   FWIX_TRY(need_ws(p, FWIX_WS_BORN_PACKED));
   BgSrc D{nullptr, (const unsigned char*)packed_down, p->wB()};
-  BgSrc U{nullptr, (const unsigned char*)packed_up, p->store(p->desc.nz)};
+  BgSrc U{nullptr, (const unsigned char*)packed_up, p->wU()};
   return born_body(p, adjoint, rec, D, U, (float2*)dslow_v, (float2*)dden_v, model_w_stride, (float2*)data_v,
-                   add, (cudaStream_t)stream);
+                   add, (cudaStream_t)stream, true);
 }
 
 

@@ -23,14 +23,17 @@ namespace {
 
 constexpr int kBlk = 16;  // floats per block
 
+// kVec: 16-byte vector loads / stores (both buffers 16-byte aligned), else
+// single floats and 4-byte mantissa words (buffers 8- and 4-byte aligned).
+template <bool kVec>
 __global__ void __launch_bounds__(256) k_pack_rate8(long long n, const float* __restrict__ in,
-                                                    int4* __restrict__ mant, uint8_t* __restrict__ exps) {
+                                                    uint32_t* __restrict__ mant, uint8_t* __restrict__ exps) {
   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nblk = (n + kBlk - 1) / kBlk;
   if (b >= nblk) return;
   float v[kBlk];
   const long long f0 = b * kBlk;
-  if (f0 + kBlk <= n) {
+  if (kVec && f0 + kBlk <= n) {
     const float4* src = reinterpret_cast<const float4*>(in + f0);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -63,26 +66,41 @@ __global__ void __launch_bounds__(256) k_pack_rate8(long long n, const float* __
     }
     w[k] = word;
   }
-  mant[b] = make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
+  if (kVec) {
+    reinterpret_cast<int4*>(mant)[b] = make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mant[4 * b + k] = w[k];
+  }
   exps[b] = zero ? (uint8_t)0 : (uint8_t)min(max(E + 128, 1), 255);
 }
 
-__global__ void __launch_bounds__(256) k_unpack_rate8(long long n, const int4* __restrict__ mant,
+template <bool kVec>
+__global__ void __launch_bounds__(256) k_unpack_rate8(long long n, const uint32_t* __restrict__ mant,
                                                       const uint8_t* __restrict__ exps, float* __restrict__ out) {
   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nblk = (n + kBlk - 1) / kBlk;
   if (b >= nblk) return;
-  const int4 q4 = mant[b];
+  uint32_t w[4];
+  if (kVec) {
+    const int4 q4 = reinterpret_cast<const int4*>(mant)[b];
+    w[0] = (uint32_t)q4.x;
+    w[1] = (uint32_t)q4.y;
+    w[2] = (uint32_t)q4.z;
+    w[3] = (uint32_t)q4.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) w[k] = mant[4 * b + k];
+  }
   const uint8_t e = exps[b];
   const float scale = e == 0 ? 0.f : ldexpf(1.f, (int)e - 128 - 7);
-  const uint32_t w[4] = {(uint32_t)q4.x, (uint32_t)q4.y, (uint32_t)q4.z, (uint32_t)q4.w};
   float v[kBlk];
 #pragma unroll
   for (int k = 0; k < 4; ++k)
 #pragma unroll
     for (int j = 0; j < 4; ++j) v[4 * k + j] = (float)(int8_t)(uint8_t)(w[k] >> (8 * j)) * scale;
   const long long f0 = b * kBlk;
-  if (f0 + kBlk <= n) {
+  if (kVec && f0 + kBlk <= n) {
     float4* dst = reinterpret_cast<float4*>(out + f0);
 #pragma unroll
     for (int k = 0; k < 4; ++k) dst[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
@@ -103,12 +121,18 @@ size_t packed_rate8_bytes(long long nfloat) {
   return (b + 255) / 256 * 256;
 }
 
+static bool aligned16(const void* a, const void* b) { return (((uintptr_t)a | (uintptr_t)b) & 15) == 0; }
+
 cudaError_t launch_pack_rate8(long long nfloat, const float* in, void* packed, cudaStream_t s) {
   const long long nblk = (nfloat + kBlk - 1) / kBlk;
   if (nblk == 0) return cudaSuccess;
-  int4* mant = reinterpret_cast<int4*>(packed);
+  if ((((uintptr_t)in) & 3) || (((uintptr_t)packed) & 3)) return cudaErrorMisalignedAddress;
+  uint32_t* mant = reinterpret_cast<uint32_t*>(packed);
   uint8_t* exps = reinterpret_cast<uint8_t*>(packed) + nblk * kBlk;
-  k_pack_rate8<<<blocks_for(nblk), 256, 0, s>>>(nfloat, in, mant, exps);
+  if (aligned16(in, packed))
+    k_pack_rate8<true><<<blocks_for(nblk), 256, 0, s>>>(nfloat, in, mant, exps);
+  else
+    k_pack_rate8<false><<<blocks_for(nblk), 256, 0, s>>>(nfloat, in, mant, exps);
   count_launch();
   return cudaGetLastError();
 }
@@ -116,9 +140,13 @@ cudaError_t launch_pack_rate8(long long nfloat, const float* in, void* packed, c
 cudaError_t launch_unpack_rate8(long long nfloat, const void* packed, float* out, cudaStream_t s) {
   const long long nblk = (nfloat + kBlk - 1) / kBlk;
   if (nblk == 0) return cudaSuccess;
-  const int4* mant = reinterpret_cast<const int4*>(packed);
+  if ((((uintptr_t)out) & 3) || (((uintptr_t)packed) & 3)) return cudaErrorMisalignedAddress;
+  const uint32_t* mant = reinterpret_cast<const uint32_t*>(packed);
   const uint8_t* exps = reinterpret_cast<const uint8_t*>(packed) + nblk * kBlk;
-  k_unpack_rate8<<<blocks_for(nblk), 256, 0, s>>>(nfloat, mant, exps, out);
+  if (aligned16(out, packed))
+    k_unpack_rate8<true><<<blocks_for(nblk), 256, 0, s>>>(nfloat, mant, exps, out);
+  else
+    k_unpack_rate8<false><<<blocks_for(nblk), 256, 0, s>>>(nfloat, mant, exps, out);
   count_launch();
   return cudaGetLastError();
 }

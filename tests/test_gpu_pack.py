@@ -1,8 +1,9 @@
 """Fixed-rate lossy store of wavefields on the device (pyfwix_b200/csrc/pack.cu):
 packed bytes and unpacked values bit-exact against the oracle's restatement
-(oracle/pack.py); modelling with packed down / up fields against modelling with
-full ones; Born on packed backgrounds equal, bit for bit, to Born on the
-unpacked backgrounds, and within the store's error of Born on the exact ones."""
+(oracle/pack.py), with 16-byte aligned and unaligned buffers; modelling with
+packed down / up fields against modelling with full ones; Born on packed
+backgrounds (which also keeps its per-level recursion fields packed) within the
+store's error of Born on the unpacked and on the exact backgrounds."""
 import numpy as np
 import pytest
 import torch
@@ -33,6 +34,21 @@ def test_pack_bits_against_oracle(nx, ny, nw, ns, pad):
     got = pk.cpu().numpy()
     assert np.array_equal(got[:nblk * 17], want[:nblk * 17])
     assert np.array_equal(y.cpu().numpy().view(np.float32), opack.unpack(want, x.shape).view(np.float32))
+    # buffers 8 bytes off a 16-byte boundary take the scalar path: same bytes
+    xo = torch.zeros(x.size + 1, dtype=torch.complex64, device="cuda")[1:]
+    xo.copy_(xd.ravel())
+    po = torch.zeros(p.packed_bytes + 16, dtype=torch.uint8, device="cuda")[4:4 + p.packed_bytes]
+    import ctypes
+    from pyfwix_b200 import _lib as L
+    from pyfwix_b200.plan import _stream
+    L.check(L.load().fwix_pack_rate8(p._h, ctypes.c_void_p(xo.data_ptr()), ctypes.c_void_p(po.data_ptr()),
+                                     _stream()))
+    yo = torch.zeros(x.size + 1, dtype=torch.complex64, device="cuda")[1:]
+    L.check(L.load().fwix_unpack_rate8(p._h, ctypes.c_void_p(po.data_ptr()), ctypes.c_void_p(yo.data_ptr()),
+                                       _stream()))
+    torch.cuda.synchronize()
+    assert np.array_equal(po.cpu().numpy()[:nblk * 17], want[:nblk * 17])
+    assert torch.equal(yo, y.ravel())
 
 
 def _acq(g, p):
@@ -43,9 +59,12 @@ def _acq(g, p):
     return src, rec
 
 
-@pytest.mark.parametrize("kind,nx,ny,pad", [("pspi", 32, 24, 4), ("nsps", 64, 64, 0)])
-def test_packed_modelling_and_born(kind, nx, ny, pad):
-    g, rng, sref, labels, slow, den = make_case(nx=nx, ny=ny, nw=4, nz=6, nref=3, padx=pad, pady=pad)
+@pytest.mark.parametrize("kind,nx,ny,pad,nw", [("pspi", 32, 24, 4, 4), ("nsps", 64, 64, 0, 4),
+                                               ("pspi", 27, 21, 0, 3)])
+def test_packed_modelling_and_born(kind, nx, ny, pad, nw):
+    """(27 x 21 x 3: an odd wavefield size, so the workspace fields sit 8 bytes off
+    a 16-byte boundary and the packing kernels take their scalar path.)"""
+    g, rng, sref, labels, slow, den = make_case(nx=nx, ny=ny, nw=nw, nz=6, nref=3, padx=pad, pady=pad)
     slow = slow.copy()
     slow[g.nz - 2:] *= 1.8
     p = make_plan(g, 1, sref, labels, slow, den, step=kind)
@@ -85,6 +104,8 @@ def test_packed_modelling_and_born(kind, nx, ny, pad):
             outs = [(gp[0], gp[2], gp[4]), (gp[1], gp[3], gp[5])]
         torch.cuda.synchronize()
         for a, b, c in outs:
-            assert torch.equal(a, b)
+            assert rel(a.cpu().numpy(), b.cpu().numpy()) < 2e-2
             assert rel(a.cpu().numpy(), c.cpu().numpy()) < 3e-2
-    assert p.packed_bytes * 3.7 < 8 * int(np.prod(p.wshape))
+    n = int(np.prod(p.wshape))
+    assert p.packed_bytes == opack.packed_bytes(2 * n)  # 17 bytes per 16 floats, padded to 256
+    assert p.packed_bytes * 3.7 < 8 * n or n < 4096
