@@ -55,6 +55,8 @@ def args_():
     ap.add_argument("--fwi-nz", type=int, default=None, help="depth levels of the FWI workload (quick runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched forward+imaging timing")
     ap.add_argument("--no-packed", action="store_true", help="skip the packed-background Born timing")
+    ap.add_argument("--large", action="store_true",
+                    help="run only the 512 x 512 x 400 x 200 Born on packed storage and print its own line")
     ap.add_argument("--batched-nz", type=int, default=None, help="depth levels of the batched workload (quick runs)")
     ap.add_argument("--batched-shots", type=int, default=32)
     ap.add_argument("--batched-streams", type=int, default=8)
@@ -470,8 +472,71 @@ def profile_step(a):
     print(json.dumps({"profile_step": a.profile_step, "workload": w.name, "ok": True}))
 
 
+def large_born(a):
+    """The fifth configuration's size on one GPU (512 x 512 x 400, 200 frequencies,
+    PSPI nref 8, one shot): modelling and one Born forward + adjoint with the
+    backgrounds and the per-level recursion fields in the packed store, which is
+    what makes the shot fit (lossless storage would take three times 400
+    wavefields of 419 MB).  Prints one JSON line with the times and the memory."""
+    import torch
+
+    from pyfwix_b200 import _lib as L
+    from pyfwix_b200 import refsampler, workloads
+    from pyfwix_b200.plan import Plan
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    w = workloads.config5(nz=a.nz)
+    t0 = time.perf_counter()
+    p = Plan(ns=1, device=dev, **w.plan_kwargs())
+    s2 = workloads.slow2_on(w, dev)[:, None]
+    sref, labels = refsampler.sample(s2, w.nref, w.padx, w.pady)
+    p.set_refs(refsampler.expand_refs(sref, w.nw), labels)
+    s2c = s2.to(torch.complex64)
+    p.set_model(s2c, torch.ones_like(s2c))
+    del s2, sref
+    p.ensure_workspace(L.WS_BORN_PACKED)
+    g = w.geom
+    src = p.traces(g["sx"], g["sy"], g["sz"], np.zeros(1, np.int32))
+    rec = p.traces(g["rx"], g["ry"], g["rz"], np.zeros(len(g["rx"]), np.int32))
+    wav = torch.as_tensor(w.wavelet).to(dev)
+    data = torch.empty((len(g["rx"]), w.nw), dtype=torch.complex64, device=dev)
+    pd, pu = p.packed(w.nz), p.packed(w.nz)
+    ds = torch.zeros((w.nz, 1, w.ny, w.nx), dtype=torch.complex64, device=dev)
+    rng = np.random.default_rng(1004)
+    levels = np.arange(min(10, w.nz // 4), max(w.nz - 10, w.nz // 4 + 1))
+    for iz in rng.choice(levels, size=min(8, len(levels)), replace=False):
+        ds[iz] = s2c[iz] * float(rng.uniform(-0.1, 0.1))
+    dr = torch.zeros_like(ds)
+    gs, gr = torch.empty_like(ds), torch.empty_like(ds)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    p.propagate_packed(src, rec, wav, data, pd, pu)
+    ev[1].record()
+    p.born_packed(rec, pd, pu, ds, dr, data)
+    ev[2].record()
+    p.born_packed(rec, pd, pu, gs, gr, data, adjoint=True)
+    ev[3].record()
+    torch.cuda.synchronize()
+    t = [ev[i].elapsed_time(ev[i + 1]) / 1e3 for i in range(3)]
+    cells = w.nx * w.ny * w.nw * w.nz
+    wb = 8 * w.nx * w.ny * w.nw
+    assert torch.isfinite(gs).all()
+    print(json.dumps({"large_born": {
+        "workload": w.name + ("" if a.nz is None else f" (nz={w.nz})"), "modelling_s": t[0], "born_forward_s": t[1],
+        "born_adjoint_s": t[2], "born_gcell_steps_per_s": 2 * cells / (t[1] + t[2]) / 1e9,
+        "modelling_gcell_steps_per_s": 2 * cells / t[0] / 1e9, "setup_s": setup_s,
+        "peak_device_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
+        "stored_fields_gb": (2 * pd.numel() + w.nz * p.packed_bytes) / 1e9,
+        "lossless_fields_gb": 3 * w.nz * wb / 1e9}}), flush=True)
+
+
 def main():
     a = args_()
+    if a.large:
+        large_born(a)
+        return
     if a.impl == "reference":
         run_reference(a)
         return

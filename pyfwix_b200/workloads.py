@@ -65,6 +65,7 @@ class Workload:
     oz: float = 0.0
     slow2: np.ndarray = None      # [nz][ny][nx] float32, s^2 = 1/v^2
     anomaly: tuple = None         # (cx, cy, cz) of the +10 % anomaly; slow2 then comes from slow2_on()
+    layers: tuple = None          # config5's layers and body; slow2 then comes from slow2_on()
     geom: dict = field(default_factory=dict)
     wavelet: np.ndarray = None    # [nsrc][nw] complex64
     dslow: np.ndarray = None      # Born perturbation [nz][ny][nx] float32 (or None)
@@ -190,6 +191,8 @@ def slow2_on(w, device):
     """s^2 [nz][ny][nx] (float32, on ``device``) of a config1-family workload:
     v = (1500 + 0.5 z) (1 + 0.10 exp(-|r - c|^2 / (2 150^2)))."""
     import torch
+    if getattr(w, "layers", None) is not None:
+        return _slow2_layers(w, device)
     if w.anomaly is None:
         return torch.as_tensor(w.slow2).to(device)
     cx, cy, cz = w.anomaly
@@ -198,6 +201,46 @@ def slow2_on(w, device):
     x = (w.ox + w.dx * torch.arange(w.nx, device=device, dtype=torch.float64))[None, None, :]
     v = (1500.0 + 0.5 * z) * (1 + 0.10 * torch.exp(-((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2)
                                                     / (2 * 150.0 ** 2)))
+    return (1.0 / v ** 2).float().contiguous()
+
+
+def config5(nz=None, seed=1004):
+    """Large migration with gradient, one shot of 64: 512 x 512 x 400, d = 12.5 m,
+    nw = 200 (2-50 Hz), PSPI with nref 8; 12 layers of 1500-4500 m/s whose
+    interfaces dip by seeded angles within +-10 degrees, and a Gaussian body of
+    4500 m/s; source at a seeded surface position, receivers on every surface node.
+    s^2 comes from ``slow2_on`` (``w.layers`` holds the layer parameters)."""
+    rng = np.random.default_rng(seed)
+    nz_full = 400
+    w = Workload(name="born-pspi-512x512x400-nw200", nx=512, ny=512, nz=nz or nz_full, dx=12.5, dy=12.5,
+                 dz=12.5, nw=200, ow=2.0, dw=48.0 / 199.0, nref=8, step="pspi", taperx=20, tapery=20)
+    depth = nz_full * w.dz
+    tops = np.sort(rng.uniform(0.05, 0.95, 11)) * depth
+    dips = np.deg2rad(rng.uniform(-10, 10, size=(11, 2)))
+    vel = np.linspace(1500.0, 4500.0, 12)
+    body = (float(rng.uniform(0.3, 0.7) * w.nx * w.dx), float(rng.uniform(0.3, 0.7) * w.ny * w.dy),
+            float(rng.uniform(0.4, 0.7) * depth), 400.0)
+    w.layers = (tops, dips, vel, body)
+    sx, sy = rng.uniform(0.2, 0.8, 2) * np.array([w.nx * w.dx, w.ny * w.dy])
+    w.geom = dict(sx=np.array([sx], np.float32), sy=np.array([sy], np.float32), sz=np.array([0.0], np.float32),
+                  s_ids=np.array([0], np.int32), **w.surface_receivers())
+    w.wavelet = ricker_spectrum(w.freqs)[None, :].astype(np.complex64)
+    return w
+
+
+def _slow2_layers(w, device):
+    import torch
+    tops, dips, vel, (bx, by, bz, br) = w.layers
+    z = (w.oz + w.dz * torch.arange(w.nz, device=device, dtype=torch.float64))[:, None, None]
+    y = (w.oy + w.dy * torch.arange(w.ny, device=device, dtype=torch.float64))[None, :, None]
+    x = (w.ox + w.dx * torch.arange(w.nx, device=device, dtype=torch.float64))[None, None, :]
+    cx, cy = w.nx * w.dx / 2, w.ny * w.dy / 2
+    v = torch.full((w.nz, w.ny, w.nx), float(vel[0]), dtype=torch.float64, device=device)
+    for i in range(len(tops)):
+        surf = tops[i] + np.tan(dips[i, 0]) * (x - cx) + np.tan(dips[i, 1]) * (y - cy)
+        v = torch.where(z >= surf, torch.full_like(v, float(vel[i + 1])), v)
+    g = torch.exp(-((x - bx) ** 2 + (y - by) ** 2 + (z - bz) ** 2) / (2 * br ** 2))
+    v = v + (4500.0 - v) * g
     return (1.0 / v ** 2).float().contiguous()
 
 
