@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import re
 import subprocess
@@ -601,6 +602,16 @@ def main():
             "traffic": traffic, "peak_source": peak_kind,
             "kernel": "NSPS depth step (row pass + column pass + row pass), 256x256x128",
             "step_ms": tstep * 1e3, "alg_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP}
+    # the FP32 arithmetic the same step needs (the bound that applies: nref + 1
+    # complex 2D transforms of 5 log2(NX NY) flop per sample, and a complex
+    # multiply-add of the phase factor per reference), against the FP32 issue rate
+    # of 148 SMs x 128 lanes x 2 flop at the sampled SM clock
+    flop = (w.nref + 1) * 5 * math.log2(w.nx * w.ny) + 8 * w.nref
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    fp32 = flop * cells_step / tstep / 1e12
+    roof["fp32"] = {"flop_per_cell_step": flop, "achieved_tflops": fp32, "peak_tflops": fp32_peak,
+                    "frac": fp32 / fp32_peak, "peak_source": f"nominal at the sampled {mhz:.0f} MHz"}
     bg_gb = st["bd"].numel() * 8 / 1e9
     packed = born_packed_timing(st, w) if not a.no_packed else None
     fwi = batched = None
