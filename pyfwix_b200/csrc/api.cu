@@ -204,6 +204,9 @@ struct fwix_traces {
 
 namespace {
 
+// A trace buffer ([ntrace][nw]) may be null only when its trace set is empty.
+bool no_traces(const fwix_traces* t, const void* buf) { return !t || (!buf && t->ntrace > 0); }
+
 fwix_status need_ws(const fwix_plan* p, int cls) {
   if (!p->ws) return fail(FWIX_ERR_STATE, "workspace not bound (fwix_plan_set_workspace)");
   if (p->ws_bytes < p->ws_need(cls))
@@ -474,7 +477,7 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
   float2* SC = p->wSC();
   const bool pspi = k == FWIX_STEP_PSPI;
   if (!adjoint) {
-    if (!add) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
+    if (!add && rec->ntrace > 0) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
     // down scattering (ExtendedBorn.cpp:152-178): store[iz] = dD_iz, the field
     // recorded at iz; dD_iz+1 = S_iz(dD_iz + Scat_iz(bg_down_iz * ds_iz))
     FWIX_CU(cudaMemsetAsync(Lv.field(0), 0, wb, s));
@@ -502,12 +505,17 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
       const float2* dz;
       FWIX_TRY(Lv.get(iz, s, &dz));
       FWIX_TRY(do_reflect(p, iz, 0, dz, A, 1, s));
-      const float2* bd;
-      FWIX_TRY(D.get(p, iz, s, &bd));
-      FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
-                                              p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                              ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, A, 1, s),
-                  "linearised reflection"));
+      // The bottom level reflects against a copy of itself (LinReflect.h:30-41):
+      // its linearised coefficients cancel exactly (FP32 would leave only their
+      // rounding), so nothing is added there, forward or adjoint.
+      if (z1 != iz) {
+        const float2* bd;
+        FWIX_TRY(D.get(p, iz, s, &bd));
+        FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                                p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
+                                                ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, A, 1, s),
+                    "linearised reflection"));
+      }
       FWIX_TRY(do_record(p, rec, iz, A, data, s));
     }
     return FWIX_OK;
@@ -547,12 +555,14 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
       FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bu, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
     }
     FWIX_TRY(do_inject(p, rec, iz, data, cur, s));
-    const float2* bd;
-    FWIX_TRY(D.get(p, iz, s, &bd));
-    FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
-                                            p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                            ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, cur, 1, s),
-                "linearised reflection adjoint"));
+    if (z1 != iz) {  // nothing at the bottom level (see the forward)
+      const float2* bd;
+      FWIX_TRY(D.get(p, iz, s, &bd));
+      FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                              p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
+                                              ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, cur, 1, s),
+                  "linearised reflection adjoint"));
+    }
     FWIX_TRY(Lv.keep(iz, s));
   }
   // upward: eta_iz = Rec_iz^H d + conj(R_iz) zeta_iz + S_iz^H eta_iz+1, the adjoint of
@@ -962,13 +972,13 @@ fwix_status fwix_traces_destroy(fwix_traces* tr) {
 
 fwix_status fwix_inject(fwix_plan* p, const fwix_traces* tr, int iz, int adjoint, void* traces, void* wfld,
                         int add, void* stream) {
-  if (!p || !tr || !traces || !wfld) return fail(FWIX_ERR_INVALID, "null argument");
+  if (!p || no_traces(tr, traces) || !wfld) return fail(FWIX_ERR_INVALID, "null argument");
   cudaStream_t s = (cudaStream_t)stream;
   if (!adjoint) {
     if (!add) FWIX_CU(cudaMemsetAsync(wfld, 0, p->wbytes(), s));
     return do_inject(p, tr, iz, (const float2*)traces, (float2*)wfld, s);
   }
-  if (!add) FWIX_CU(cudaMemsetAsync(traces, 0, (size_t)tr->ntrace * p->d.nw * sizeof(float2), s));
+  if (!add && tr->ntrace > 0) FWIX_CU(cudaMemsetAsync(traces, 0, (size_t)tr->ntrace * p->d.nw * sizeof(float2), s));
   return do_record(p, tr, iz, (const float2*)wfld, (float2*)traces, s);
 }
 
@@ -1008,7 +1018,7 @@ fwix_status fwix_upward(fwix_plan* p, int adjoint, void* wfld, void* stream) {
 // working buffers themselves: the step from iz writes straight into slot iz+1.
 fwix_status fwix_propagate(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec, const void* wavelet,
                            void* data, int add, void* bg_down, void* bg_up, void* stream) {
-  if (!p || !src || !rec || !wavelet || !data) return fail(FWIX_ERR_INVALID, "null argument");
+  if (!p || no_traces(src, wavelet) || no_traces(rec, data)) return fail(FWIX_ERR_INVALID, "null argument");
   if (!bg_down) return fail(FWIX_ERR_INVALID, "bg_down storage ([nz] wavefields) is required");
   FWIX_TRY(need_refs(p));
   FWIX_TRY(need_model(p));
@@ -1020,7 +1030,7 @@ fwix_status fwix_propagate(fwix_plan* p, const fwix_traces* src, const fwix_trac
   float2* up = (float2*)bg_up;
   float2* dat = (float2*)data;
   const float2* wav = (const float2*)wavelet;
-  if (!add) FWIX_CU(cudaMemsetAsync(dat, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
+  if (!add && rec->ntrace > 0) FWIX_CU(cudaMemsetAsync(dat, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
   FWIX_CU(cudaMemsetAsync(down, 0, p->wbytes(), s));
   for (int iz = 0; iz < nz; ++iz) {
     float2* cur = down + iz * W;
@@ -1064,7 +1074,8 @@ fwix_status fwix_unpack_rate8(fwix_plan* p, const void* packed, void* wfld, void
 // pass reflects the unpacked down field of each depth (workspace B).
 fwix_status fwix_propagate_packed(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec, const void* wavelet,
                                   void* data, int add, void* packed_down, void* packed_up, void* stream) {
-  if (!p || !src || !rec || !wavelet || !data || !packed_down) return fail(FWIX_ERR_INVALID, "null argument");
+  if (!p || no_traces(src, wavelet) || no_traces(rec, data) || !packed_down)
+    return fail(FWIX_ERR_INVALID, "null argument");
   if (((uintptr_t)packed_down) % 4 != 0 || ((uintptr_t)packed_up) % 4 != 0 || p->packed_bytes() % 16 != 0)
     return fail(FWIX_ERR_INVALID, "packed buffers must be 4-byte aligned");
   FWIX_TRY(need_refs(p));
@@ -1080,7 +1091,7 @@ fwix_status fwix_propagate_packed(fwix_plan* p, const fwix_traces* src, const fw
   const float2* wav = (const float2*)wavelet;
   float2* D = p->wA();
   float2* R = p->wB();
-  if (!add) FWIX_CU(cudaMemsetAsync(dat, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
+  if (!add && rec->ntrace > 0) FWIX_CU(cudaMemsetAsync(dat, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
   FWIX_CU(cudaMemsetAsync(D, 0, p->wbytes(), s));
   for (int iz = 0; iz < nz; ++iz) {
     FWIX_TRY(do_inject(p, src, iz, wav, D, s));
@@ -1108,7 +1119,7 @@ fwix_status fwix_propagate_packed(fwix_plan* p, const fwix_traces* src, const fw
 // (imaging_condition.cu:57-108 summed over frequency).
 fwix_status fwix_migrate(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec, const void* wavelet,
                          const void* data, float* image, int add, void* stream) {
-  if (!p || !src || !rec || !wavelet || !data || !image) return fail(FWIX_ERR_INVALID, "null argument");
+  if (!p || no_traces(src, wavelet) || no_traces(rec, data) || !image) return fail(FWIX_ERR_INVALID, "null argument");
   FWIX_TRY(need_refs(p));
   FWIX_TRY(need_ws(p, FWIX_WS_SWEEP));
   cudaStream_t s = (cudaStream_t)stream;
@@ -1134,7 +1145,7 @@ fwix_status fwix_migrate(fwix_plan* p, const fwix_traces* src, const fwix_traces
 fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const void* bg_down_v,
                       const void* bg_up_v, void* dslow_v, void* dden_v, int64_t model_w_stride, void* data_v,
                       int add, void* stream) {
-  if (!p || !rec || !bg_down_v || !bg_up_v || !dslow_v || !dden_v || !data_v)
+  if (!p || no_traces(rec, data_v) || !bg_down_v || !bg_up_v || !dslow_v || !dden_v)
     return fail(FWIX_ERR_INVALID, "null argument");
   const long long plane = (long long)p->d.ny * p->d.nx;
   if (model_w_stride != 0 && model_w_stride != plane)
@@ -1151,7 +1162,7 @@ fwix_status fwix_born(fwix_plan* p, int adjoint, const fwix_traces* rec, const v
 fwix_status fwix_born_packed(fwix_plan* p, int adjoint, const fwix_traces* rec, const void* packed_down,
                              const void* packed_up, void* dslow_v, void* dden_v, int64_t model_w_stride,
                              void* data_v, int add, void* stream) {
-  if (!p || !rec || !packed_down || !packed_up || !dslow_v || !dden_v || !data_v)
+  if (!p || no_traces(rec, data_v) || !packed_down || !packed_up || !dslow_v || !dden_v)
     return fail(FWIX_ERR_INVALID, "null argument");
   const long long plane = (long long)p->d.ny * p->d.nx;
   if (model_w_stride != 0 && model_w_stride != plane)

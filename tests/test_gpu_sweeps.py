@@ -181,3 +181,76 @@ def test_phase_cache_rotation(nx, ny, pad):
         assert p.enable_phase_cache(depths=depths)
         for a, b in zip(run(), full):
             assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("kind", ["pspi", "nsps"])
+def test_shallow_grids(kind):
+    """One and two depth levels: the bottom level reflects nothing and its
+    linearised reflection reads the same level twice (ExtendedBorn.cpp and
+    Reflect.h:20-38 take z + 1 = z there), receivers below the grid are skipped.
+    With one level the Born operators add nothing to what the output held."""
+    for nz in (1, 2):
+        g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind, nz=nz)
+        data, bgd, bgu = wem.propagate(g, st, acq, slow, den, wav)
+        bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+        bu = torch.empty_like(bd)
+        d = torch.empty((len(acq.rec.ix), g.nw), dtype=torch.complex64, device="cuda")
+        p.propagate(src, rec, to_dev(wav), d, bd, bu)
+        assert rel(to_host(d), data) < TOL
+        ms = crandn(rng, (g.nz, g.nw, g.ny, g.nx))
+        mr = crandn(rng, (g.nz, g.nw, g.ny, g.nx))
+        r = crandn(rng, d.shape)
+        ref = wem.born_forward(g, st, acq, slow, den, bgd, bgu, ms, mr)
+        gs_ref, gr_ref = wem.born_adjoint(g, st, acq, slow, den, bgd, bgu, r)
+        d0 = crandn(rng, d.shape)
+        g0 = crandn(rng, ms.shape)
+        out = to_dev(d0)
+        p.born(rec, bd, bu, to_dev(ms), to_dev(mr), out, add=True)
+        gs = to_dev(g0)
+        gr = to_dev(g0)
+        p.born(rec, bd, bu, gs, gr, to_dev(r), adjoint=True, add=True)
+        assert rel(to_host(out), d0 + ref) < TOL
+        assert rel(to_host(gs), g0 + gs_ref) < TOL
+        assert rel(to_host(gr), g0 + gr_ref) < TOL
+        if nz == 1:
+            assert np.linalg.norm(ref) == 0 and np.linalg.norm(gs_ref) == 0
+
+
+def test_receivers_all_dropped():
+    """Receivers on the last column of the padded grid are dropped
+    (propagator/src/injection.cu:46-48): the data are zero, Born forward records
+    nothing and its adjoint injects nothing."""
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case("nsps")
+    xs = [(g.NX - 1) * g.dx + 0.5] * 4
+    off = p.traces(xs, [100.0] * 4, [0.0, 0.0, 12.0, 12.0], [0, 1, 1, 0])
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = to_dev(crandn(rng, (4, g.nw)))
+    p.propagate(src, off, to_dev(wav), d, bd, bu)
+    assert not to_host(d).any()
+    ms = to_dev(crandn(rng, (g.nz, g.nw, g.ny, g.nx)))
+    p.born(off, bd, bu, ms, ms, d)
+    assert not to_host(d).any()
+    r = to_dev(crandn(rng, (4, g.nw)))
+    gs = to_dev(crandn(rng, (g.nz, g.nw, g.ny, g.nx)))
+    gr = torch.empty_like(gs)
+    p.born(off, bd, bu, gs, gr, r, adjoint=True)
+    assert not to_host(gs).any() and not to_host(gr).any()
+
+
+def test_no_receivers():
+    """An empty receiver set (null data buffer allowed): modelling still fills
+    the background wavefields, and the Born adjoint of no data is zero."""
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case("pspi")
+    _, bgd, bgu = wem.propagate(g, st, acq, slow, den, wav)
+    none = p.traces([], [], [], [])
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((0, g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, none, to_dev(wav), d, bd, bu)
+    assert rel(to_host(bd), np.stack(bgd)) < TOL
+    assert rel(to_host(bu), np.stack(bgu)) < TOL
+    gs = to_dev(crandn(rng, (g.nz, g.nw, g.ny, g.nx)))
+    gr = torch.empty_like(gs)
+    p.born(none, bd, bu, gs, gr, d, adjoint=True)
+    assert not to_host(gs).any() and not to_host(gr).any()
