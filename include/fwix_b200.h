@@ -181,7 +181,9 @@ fwix_status fwix_correlate(fwix_plan* plan, const void* a, const void* b, float*
                            void* stream);
 
 /* ---- acquisition ------------------------------------------------------------ */
-/* Host coordinate arrays; ids are dense shot indices in [0, ns). */
+/* Host coordinate arrays; ids are dense shot indices in [0, ns).  ntrace may be 0
+ * (the arrays may then be NULL); a [ntrace][nw] trace buffer of an empty trace set
+ * (wavelet, data) may be NULL in every call that takes one. */
 fwix_status fwix_traces_create(fwix_plan* plan, int ntrace, const float* cx, const float* cy,
                                const float* cz, const int32_t* ids, fwix_traces** out);
 fwix_status fwix_traces_destroy(fwix_traces* tr);
