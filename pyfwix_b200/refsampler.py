@@ -9,8 +9,9 @@ choice is deterministic:
 * ``method="quantile"`` (default): reference slownesses are the quantiles
   (2k+1)/(2 nref) of the depth slice's slowness sqrt(Re s^2); the reference s^2
   is their square.
-* ``method="kmeans"``: Lloyd iterations on Re s^2 started from those quantiles
-  (the same objective as cv::kmeans, without the random seeding).
+* ``method="kmeans"``: Lloyd iterations on s^2 started from those quantiles
+  (the same objective as cv::kmeans, without the random seeding), stopped per
+  chunk of (depth, frequency) rows.
 
 Labels are the index of the nearest reference in s^2 (complex distance), padded
 by edge replication.  Runs on the model's device with torch.
@@ -25,12 +26,60 @@ def _quantile_levels(nref, device):
     return (torch.arange(nref, device=device, dtype=torch.float64) * 2 + 1) / (2 * nref)
 
 
-def sample(slow2, nref, padx=0, pady=0, method="quantile", iters=100, tol=1e-3):
+# Bytes of the [rows][ny*nx][nref] complex128 distance array one chunk of
+# (depth, frequency) rows may take: a per-frequency model of 256 x 256 x 128
+# frequencies x 200 depths would need 107 GB at once.
+_CHUNK_BYTES = 1 << 28
+
+
+def _nearest(x, centers):
+    """Index of the nearest center (complex distance) per sample: [rows][npix]."""
+    return torch.argmin(torch.abs(x[:, :, None] - centers[:, None, :]), dim=2)
+
+
+def _quantile_centers(x, nref):
+    """s^2 of the quantiles (2k+1)/(2 nref) of sqrt(Re s^2) per row (numpy's
+    default linear interpolation)."""
+    npix = x.shape[1]
+    s = torch.sqrt(torch.clamp(x.real, min=0.0))
+    q = _quantile_levels(nref, x.device)
+    srt, _ = torch.sort(s, dim=1)
+    pos = q * (npix - 1)
+    lo = torch.floor(pos).long()
+    hi = torch.clamp(lo + 1, max=npix - 1)
+    frac = (pos - lo.to(pos.dtype))[None, :]
+    sq = srt[:, lo] * (1 - frac) + srt[:, hi] * frac          # [rows, nref]
+    return (sq ** 2).to(torch.complex128)
+
+
+def _lloyd(x, centers, iters, tol):
+    """Lloyd iterations on the rows of x from the given centers; stops when no
+    center of the chunk moves by more than tol times the largest one."""
+    nref = centers.shape[1]
+    for _ in range(iters):
+        lab = _nearest(x, centers)
+        new = centers.clone()
+        for r in range(nref):
+            m = (lab == r)
+            cnt = m.sum(dim=1)
+            ssum = torch.where(m, x, torch.zeros_like(x)).sum(dim=1)
+            new[:, r] = torch.where(cnt > 0, ssum / torch.clamp(cnt, min=1), centers[:, r])
+        shift = torch.max(torch.abs(new - centers))
+        centers = new
+        if float(shift) <= tol * float(torch.max(torch.abs(centers))):
+            break
+    return centers
+
+
+def sample(slow2, nref, padx=0, pady=0, method="quantile", iters=100, tol=1e-3, chunk_bytes=_CHUNK_BYTES):
     """slow2: complex or real s^2, [nz][nw or 1][ny][nx] (torch or numpy).
 
     Returns (sref [nz][nref][nw'] complex64, labels [nz][nw'][NY][NX] uint8) on
     slow2's device (CUDA if slow2 is numpy and a GPU is present), nw' = slow2's
-    frequency extent."""
+    frequency extent.  The (depth, frequency) rows are independent and are
+    processed in chunks of about ``chunk_bytes`` of distances each."""
+    if method not in ("quantile", "kmeans"):
+        raise ValueError(f"unknown reference method {method!r}")
     t = torch.as_tensor(slow2)
     if t.device.type == "cpu" and torch.cuda.is_available():
         t = t.to("cuda")
@@ -39,36 +88,18 @@ def sample(slow2, nref, padx=0, pady=0, method="quantile", iters=100, tol=1e-3):
     else:
         t = t.to(torch.complex128)
     nz, nw, ny, nx = t.shape
-    dev = t.device
     flat = t.reshape(nz * nw, ny * nx)
-    s = torch.sqrt(torch.clamp(flat.real, min=0.0))
-    q = _quantile_levels(nref, dev)
-    srt, _ = torch.sort(s, dim=1)
-    # linear-interpolated quantiles (numpy's default "linear" method)
-    pos = q * (ny * nx - 1)
-    lo = torch.floor(pos).long()
-    hi = torch.clamp(lo + 1, max=ny * nx - 1)
-    frac = (pos - lo.to(pos.dtype))[None, :]
-    sq = srt[:, lo] * (1 - frac) + srt[:, hi] * frac          # [nz*nw, nref]
-    centers = (sq ** 2).to(torch.complex128)                  # reference s^2
-    if method == "kmeans":
-        x = flat
-        for _ in range(iters):
-            lab = torch.argmin(torch.abs(x[:, :, None] - centers[:, None, :]), dim=2)
-            new = centers.clone()
-            for r in range(nref):
-                m = (lab == r)
-                cnt = m.sum(dim=1)
-                ssum = torch.where(m, x, torch.zeros_like(x)).sum(dim=1)
-                new[:, r] = torch.where(cnt > 0, ssum / torch.clamp(cnt, min=1), centers[:, r])
-            shift = torch.max(torch.abs(new - centers))
-            centers = new
-            if float(shift) <= tol * float(torch.max(torch.abs(centers))):
-                break
-    elif method != "quantile":
-        raise ValueError(f"unknown reference method {method!r}")
-    lab = torch.argmin(torch.abs(flat[:, :, None] - centers[:, None, :]), dim=2)
-    lab = lab.reshape(nz, nw, ny, nx).to(torch.uint8)
+    rows = max(1, min(nz * nw, int(chunk_bytes) // max(1, ny * nx * nref * 16)))
+    cs, ls = [], []
+    for i in range(0, nz * nw, rows):
+        x = flat[i:i + rows]
+        c = _quantile_centers(x, nref)
+        if method == "kmeans":
+            c = _lloyd(x, c, iters, tol)
+        cs.append(c)
+        ls.append(_nearest(x, c).to(torch.uint8))
+    centers = torch.cat(cs)
+    lab = torch.cat(ls).reshape(nz, nw, ny, nx)
     if padx or pady:
         lab = torch.nn.functional.pad(lab.to(torch.float32), (0, padx, 0, pady), mode="replicate").to(torch.uint8)
     sref = centers.reshape(nz, nw, nref).permute(0, 2, 1).contiguous().to(torch.complex64)

@@ -99,3 +99,28 @@ def test_next_fft_length_and_even_split():
     assert split_even(10, 3) == [4, 3, 3]
     assert split_even(2, 5) == [1, 1]
     assert sum(split_even(128, 7)) == 128
+
+
+@pytest.mark.parametrize("method", ["quantile", "kmeans"])
+def test_refsampler_chunks_rows_independently(method):
+    """The (depth, frequency) rows of the reference sampler are independent: any
+    chunking gives the same references and labels (Lloyd run to its fixed
+    point, tol = 0), labels are the nearest reference and the pads replicate the
+    last row / column (propagator/src/RefSampler.cpp:75-86)."""
+    from pyfwix_b200 import refsampler
+    rng = np.random.default_rng(3)
+    shape = (3, 5, 20, 24)
+    s2 = (1 / 1800.0) ** 2 * (1 + 0.5 * rng.random(shape)) + 1j * 1e-9 * rng.standard_normal(shape)
+    whole = refsampler.sample(s2, 4, 3, 2, method=method, tol=0.0)
+    for chunk in (20 * 24 * 4 * 16 * 2, 1):
+        part = refsampler.sample(s2, 4, 3, 2, method=method, tol=0.0, chunk_bytes=chunk)
+        assert torch.equal(part[0], whole[0]) and torch.equal(part[1], whole[1])
+    sref, lab = whole
+    assert sref.shape == (3, 4, 5) and lab.shape == (3, 5, 22, 27) and lab.dtype == torch.uint8
+    refs = sref.numpy().astype(np.complex128)                        # [nz][nref][nw]
+    near = np.argmin(np.abs(s2[:, None] - refs[:, :, :, None, None]), axis=1)
+    assert np.mean(lab.numpy()[:, :, :20, :24] == near) > 0.999
+    assert torch.equal(lab[:, :, 20:, :24], lab[:, :, 19:20, :24].expand(-1, -1, 2, -1))
+    assert torch.equal(lab[:, :, :, 24:], lab[:, :, :, 23:24].expand(-1, -1, -1, 3))
+    with pytest.raises(ValueError):
+        refsampler.sample(s2, 4, method="median")
