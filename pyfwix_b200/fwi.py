@@ -74,6 +74,15 @@ def _get(par, key, default=None):
     return default if v is None else v
 
 
+def _checkpoint_key(par):
+    """``checkpoint`` of par: absent -> "auto"; None, 0 or 1 -> every depth
+    stored; k -> every k-th level.  (A parameter object other than a dict cannot
+    tell an absent key from None, and gives "auto" for both.)"""
+    if isinstance(par, dict):
+        return par.get("checkpoint", "auto")
+    return _get(par, "checkpoint", "auto")
+
+
 class SmoothFWI:
     """One shot batch: plan, acquisition and stored fields.
 
@@ -103,7 +112,7 @@ class SmoothFWI:
         self.rec = p.traces(geometry["rx"], geometry["ry"], geometry["rz"], r_ids)
         self.wavelet = wav.to(self.device, torch.complex64).contiguous()
         self.ntrace = len(np.asarray(geometry["rx"]))
-        self.k = self._storage(_get(par, "checkpoint", "auto"))
+        self.k = self._storage(_checkpoint_key(par))
         self.refs_fixed = _get(par, "refs", None)
         p.ensure_workspace(L.WS_STEP)
 

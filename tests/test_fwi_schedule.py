@@ -1,0 +1,156 @@
+"""Sequencing of the FWI gradient driver (``pyfwix_b200.fwi.SmoothFWI``) on the
+CPU.  The device plan is replaced by a stand-in that applies the oracle's
+operators (smooth step, its adjoint and derivative, injection / recording,
+reflection, correlation) to the same torch fields, rounded to complex64 as the
+device stores them.  That checks the driver's storage modes -- every depth
+stored, or checkpoints every k levels with segments recomputed -- against each
+other and against the oracle's adjoint-state gradient without a GPU; the
+device operators themselves are checked in ``test_gpu_fwi.py``."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import wem
+from pyfwix_b200 import _lib as L
+from pyfwix_b200 import fwi
+from tests.conftest import crandn
+
+
+def _np(t):
+    return t.detach().cpu().numpy().astype(np.complex128)
+
+
+def _put(t, a):
+    t.copy_(torch.from_numpy(np.ascontiguousarray(a).astype(np.complex64)))
+    return t
+
+
+class OraclePlan:
+    """The part of ``pyfwix_b200.plan.Plan`` that SmoothFWI calls, on the oracle."""
+
+    def __init__(self, nx, ny, nw, ns, nz, dx, dy, dz, ox, oy, oz, ow, dw, padx, pady, nref, eps, taperx,
+                 tapery, step, device):
+        assert step == "pspi" and torch.device(device).type == "cpu"
+        self.g = wem.Grid(nx=nx, ny=ny, nw=nw, nz=nz, dx=dx, dy=dy, dz=dz, ox=ox, oy=oy, oz=oz, ow=ow, dw=dw,
+                          padx=padx, pady=pady, nref=nref, eps=eps, taperx=taperx, tapery=tapery)
+        self.nx, self.ny, self.nw, self.ns, self.nz, self.nref = nx, ny, nw, ns, nz, nref
+        self.NX, self.NY = nx + padx, ny + pady
+        self.wshape = (ns, nw, self.NY, self.NX)
+        self.calls = {"step": 0}
+
+    def traces(self, cx, cy, cz, ids):
+        g = self.g
+        return wem.make_traces(cx, cy, cz, ids, g.ox, g.oy, g.dx, g.dy, g.oz, g.dz, self.NX, self.NY)
+
+    def ensure_workspace(self, cls=None):
+        return None
+
+    def set_smooth(self, slow_pad, sref_real):
+        self.sp = slow_pad.double().numpy()
+        self.refs = sref_real.double().numpy()
+
+    def set_model(self, slow, den):
+        self.s2 = np.repeat(slow.numpy().astype(np.complex128), self.nw, axis=1)
+        self.den = np.repeat(den.numpy().astype(np.complex128), self.nw, axis=1)
+
+    def inject(self, tr, iz, traces, wfld, adjoint=False, add=True):
+        assert add
+        if adjoint:
+            _put(traces, wem.record(tr, _np(wfld), _np(traces), iz))
+        else:
+            _put(wfld, wem.inject(tr, _np(traces), _np(wfld), iz))
+
+    def smooth_step(self, iz, inp, out, mode=L.SMOOTH_FWD, add=False):
+        assert not add
+        self.calls["step"] += 1
+        f = {L.SMOOTH_FWD: wem.smooth_forward, L.SMOOTH_ADJ: wem.smooth_adjoint,
+             L.SMOOTH_DERIV: wem.smooth_deriv}[mode]
+        return _put(out, f(self.g, self.refs[iz], self.sp[iz], _np(inp)))
+
+    def reflect(self, iz, inp, out, adjoint=False, add=False):
+        assert add
+        f = wem.reflect_adjoint if adjoint else wem.reflect_forward
+        return _put(out, f(self.g, self.s2, self.den, iz, _np(inp), _np(out)))
+
+    def correlate(self, a, b, out, add=False, padded=True):
+        a, b = _np(a), _np(b)
+        if not padded:
+            a, b = a[:, :, :self.ny, :self.nx], b[:, :, :self.ny, :self.nx]
+        c = torch.from_numpy(np.real(np.sum(np.conj(a) * b, axis=(0, 1))).astype(np.float32))
+        if add:
+            out += c
+        else:
+            out.copy_(c)
+        return out
+
+
+def _problem(nz=7):
+    rng = np.random.default_rng(5)
+    nx, ny, nw, nref = 24, 20, 4, 3
+    g = wem.Grid(nx=nx, ny=ny, nw=nw, nz=nz, dx=10.0, dy=12.0, dz=10.0, ox=0.0, oy=0.0, oz=0.0, ow=3.0, dw=2.5,
+                 padx=4, pady=2, nref=nref, eps=0.0, taperx=3, tapery=2)
+    s = (1.0 / 1800.0) * (1 + 0.2 * rng.random((nz, ny, nx)))
+    s[nz // 2:] *= 1.3
+    s = s.astype(np.float32).astype(np.float64)
+    refs = wem.smooth_refs(s, nref).astype(np.float32).astype(np.float64)
+    geom = dict(sx=[60.0, 150.0], sy=[96.0, 120.0], sz=[0.0, 5.0], s_ids=[3, 8],
+                rx=list(np.linspace(0, 230, 10)), ry=[100.0] * 10, rz=[0.0] * 5 + [12.0] * 5, r_ids=[3, 8] * 5)
+    wav = crandn(rng, (2, nw))
+    par = dict(dx=g.dx, dy=g.dy, dz=g.dz, ox=g.ox, oy=g.oy, oz=g.oz, ow=g.ow, dw=g.dw, nref=nref, padx=g.padx,
+               pady=g.pady, eps=0.0, taperx=g.taperx, tapery=g.tapery, refs=torch.from_numpy(refs))
+    acq = wem.make_acquisition(g, geom)
+    d_obs = crandn(rng, (len(geom["rx"]), nw)) * 1e-3
+    return g, s, refs, geom, wav, par, acq, d_obs
+
+
+def _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, checkpoint):
+    monkeypatch.setattr(fwi, "Plan", OraclePlan)
+    prob = fwi.SmoothFWI(s.shape, geom, torch.from_numpy(wav), dict(par, checkpoint=checkpoint), device="cpu")
+    data = prob.model(torch.from_numpy(s), keep=True)
+    res = data - torch.from_numpy(d_obs).to(torch.complex64)
+    g = prob.gradient(res)
+    return _np(data), g.double().numpy(), prob
+
+
+def _rel(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def test_every_depth_matches_oracle_gradient(monkeypatch):
+    g, s, refs, geom, wav, par, acq, d_obs = _problem()
+    data, grad, prob = _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, None)
+    assert prob.k is None
+    ref_data, _, _ = wem.smooth_propagate(g, refs, s, acq, wav)
+    _, ref_grad = wem.smooth_gradient(g, refs, s, acq, wav, d_obs)
+    assert _rel(data, ref_data) < 1e-5
+    assert _rel(grad, ref_grad) < 1e-4
+
+
+@pytest.mark.parametrize("k", [2, 3, 7, 16])
+def test_checkpoints_match_every_depth(monkeypatch, k):
+    """k = 3 leaves a short last segment (7 levels), k = 7 makes one segment and
+    k = 16 is deeper than the grid.  With every depth stored the driver takes
+    6 nz - 3 steps (down and up modelling, mu and its derivative steps, nu and
+    its derivative steps); checkpoints add the recomputed segments."""
+    g, s, refs, geom, wav, par, acq, d_obs = _problem()
+    data0, grad0, full = _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, None)
+    data, grad, prob = _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, k)
+    assert prob.k == k
+    assert _rel(data, data0) < 1e-6
+    assert _rel(grad, grad0) < 1e-5
+    nz = g.nz
+    assert full.plan.calls["step"] == 6 * nz - 3
+    assert prob.plan.calls["step"] > full.plan.calls["step"]
+
+
+def test_checkpoint_key():
+    """An absent key means "auto"; None (and 0, 1) every depth stored."""
+    assert fwi._checkpoint_key({}) == "auto"
+    assert fwi._checkpoint_key({"checkpoint": None}) is None
+    assert fwi._checkpoint_key({"checkpoint": 8}) == 8
+
+    class Params:
+        checkpoint = 4
+
+    assert fwi._checkpoint_key(Params()) == 4
+    assert fwi._checkpoint_key(object()) == "auto"
