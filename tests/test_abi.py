@@ -81,3 +81,27 @@ def test_sweep_argument_checks_without_gpu():
     assert lib.fwix_sweep(_lib.SWEEP_IMAGE, None, -1, None, 0, None) == -1
     assert b"instance" in lib.fwix_last_error()
     assert lib.fwix_sweep(_lib.SWEEP_IMAGE, None, 0, None, 0, None) == 0
+
+
+def test_null_plan_is_rejected_by_every_entry_point():
+    """Every entry point that takes a plan (or trace set) first rejects a null one
+    with FWIX_ERR_INVALID and a message, before any CUDA call; the destroy
+    functions accept null like free()."""
+    from pyfwix_b200 import _lib
+    lib = _lib.load()
+    sized = {"fwix_plan_workspace_bytes", "fwix_plan_phase_cache_bytes", "fwix_plan_packed_bytes"}
+    for name, args in sorted(_lib.SIGNATURES.items()):
+        if not args or args[0] is not _lib.P:
+            continue
+        zeros = [0 if a in (_lib.I, _lib.I64, ctypes.c_size_t) else None for a in args]
+        st = getattr(lib, name)(*zeros)
+        if name in sized:
+            assert st == 0, name
+        elif name in ("fwix_plan_destroy", "fwix_traces_destroy"):
+            assert st == 0, name
+        else:
+            assert st == -1, (name, st)  # FWIX_ERR_INVALID
+            assert lib.fwix_last_error(), name
+    assert lib.fwix_plan_create(None, None) == -1
+    st = lib.fwix_step_noalloc(None, 0, 0, 0, None, None, 0, 0, None, None, 0, None)
+    assert st == -1 and lib.fwix_last_error()
