@@ -7,6 +7,7 @@ replaces that with its own block format, restated here: the wavefield's floats i
 blocks of 16; per block the largest magnitude m = f 2^E (f in [0.5, 1)), mantissas
 q = rint(v 2^(7 - E)) clamped to [-127, 127] (int8), exponent byte E + 128
 (clamped to 1..255); blocks with m < 2^-100 are zeros with exponent byte 0.
+Blocks with m >= 2^127 and non-finite values are outside the format.
 Packed layout: all mantissas (16 bytes per block), then the exponent bytes, padded
 to a multiple of 256 bytes.  Parity with the device is bit-exact (powers-of-two
 scaling and round-half-even on both sides).  There is no reference code to pin

@@ -11,6 +11,8 @@
 // v = q 2^(E - 7), so |v - v'| <= 2^(E - 8) <= m 2^-7.  The scaling is by powers
 // of two and rint rounds to nearest even, so the packed bytes are exact functions
 // of the input (the oracle restates the rule in numpy and the tests compare bytes).
+// The exponent byte covers blocks up to m < 2^127; larger (and non-finite) values
+// are outside the format (a NaN block reads back as zeros).
 //
 // Layout of one packed wavefield of n floats, nblk = ceil(n / 16): nblk x 16
 // mantissa bytes, then nblk exponent bytes, the whole rounded up to 256 bytes.
