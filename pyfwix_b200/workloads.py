@@ -21,6 +21,9 @@ config4: FWI gradient, PSPI smooth step, 384 x 384 x 300, nw = 96 (3-30 Hz), nre
          sigma 150 m, at seeded centres), starting model the background; 8 sources
          at seeded surface positions (shot s uses source s), receivers on every
          surface node, depth checkpoints every 16 levels.
+config5: large migration with gradient, one shot, 512 x 512 x 400, d = 12.5 m,
+         nw = 200 (2-50 Hz), PSPI nref 8; 12 dipping layers of 1500-4500 m/s and a
+         Gaussian body of 4500 m/s.
 
 Seeds are ``numpy.random.default_rng(1000 + config_index)``.
 """
