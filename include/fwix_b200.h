@@ -311,6 +311,8 @@ fwix_status fwix_sweep(int kind, const fwix_instance* insts, int ninst, void* co
  * calls that overlap on the GPU (other streams, other host threads) race: order
  * them on one stream.  The first call on each device looks up the array's device
  * address (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The address is kept for the life of the process: do not call this entry point
+ * on a device after a cudaDeviceReset of it (the array may then have moved).
  * sref / labels / strides are as in fwix_plan_set_refs; in may equal out. */
 #define FWIX_NOALLOC_SCRATCH_BYTES (64ull * 1024ull * 1024ull)
 fwix_status fwix_step_noalloc(const fwix_desc* desc, int kind, int iz, int dir, const void* sref,

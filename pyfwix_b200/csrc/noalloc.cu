@@ -27,7 +27,10 @@ namespace {
 
 // Device address of g_noalloc_scratch for the current device, looked up once per
 // device with that device current (cudaGetSymbolAddress).  The host-side symbol
-// itself is not a device address and is never passed to a kernel.
+// itself is not a device address and is never passed to a kernel.  The cached
+// address belongs to the device's context as it was at the first call: after a
+// cudaDeviceReset the module is loaded again and the array may move, so the
+// entry point must not be called on a device after it has been reset.
 cudaError_t scratch_address(unsigned char** out) {
   static std::mutex mu;
   static unsigned char* addr[64] = {nullptr};
@@ -121,11 +124,14 @@ extern "C" fwix_status fwix_step_noalloc(const fwix_desc* desc, int kind, int iz
   if (q.nx < 1 || q.ny < 1 || q.nw < 1 || q.ns < 1 || q.nz < 1 || q.padx < 0 || q.pady < 0)
     return fail(FWIX_ERR_INVALID, "sizes must be positive and pads non-negative");
   if (q.nref < 1 || q.nref > 255) return fail(FWIX_ERR_INVALID, "nref must be in [1, 255]");
+  if (q.taperx < 0 || q.tapery < 0) return fail(FWIX_ERR_INVALID, "taper widths must be non-negative");
   if (!(q.dx > 0) || !(q.dy > 0) || !(q.dz > 0)) return fail(FWIX_ERR_INVALID, "sampling must be positive");
   if (kind != FWIX_STEP_PSPI && kind != FWIX_STEP_NSPS) return fail(FWIX_ERR_INVALID, "unknown step kind");
   if (dir != FWIX_FWD && dir != FWIX_ADJ_ADD && dir != FWIX_ADJ_INPL)
     return fail(FWIX_ERR_INVALID, "unknown step direction");
   if (iz < 0 || iz >= q.nz) return fail(FWIX_ERR_INVALID, "depth index out of range");
+  if ((long long)q.nx + q.padx > FWIX_MAX_N || (long long)q.ny + q.pady > FWIX_MAX_N)
+    return fail(FWIX_ERR_UNSUPPORTED, "wavefield sizes must be 2^a 3^b 5^c 7^d and at most 1024");
   fwix::Dims d;
   d.nx = q.nx;
   d.ny = q.ny;
@@ -134,21 +140,30 @@ extern "C" fwix_status fwix_step_noalloc(const fwix_desc* desc, int kind, int iz
   d.nw = q.nw;
   d.ns = q.ns;
   d.slice = (long long)d.NX * d.NY;
-  d.wfld = d.slice * q.nw * q.ns;
   Fft1D px, py;
   if (!radix_plan(d.NX, &px) || !radix_plan(d.NY, &py))
     return fail(FWIX_ERR_UNSUPPORTED, "wavefield sizes must be 2^a 3^b 5^c 7^d and at most 1024");
   // scratch layout: tables, then the row-pass output (t1) and the column-pass output (t2)
+  const size_t cap = (size_t)FWIX_NOALLOC_SCRATCH_BYTES;
   const size_t tab = align256(8 * (size_t)(d.NX + d.NY)) + align256(4 * (size_t)(2 * d.NX + 2 * d.NY + 2 * q.nw));
+  // (nref + 1) wavefields of ns * nw slices follow the tables.  The factors are
+  // checked one at a time against what is left, so no product below can wrap: a
+  // slice is at most 1024^2 * 8 bytes, and nw, ns and nref + 1 each at most the
+  // number of such units that fit.
+  const size_t slice_b = (size_t)d.slice * sizeof(float2);
+  const size_t room = tab < cap ? cap - tab : 0;
+  const size_t units = room / slice_b;  // slices that fit after the tables
+  const bool fits = (size_t)q.nw <= units && (size_t)q.ns <= units / (size_t)q.nw &&
+                    (size_t)(q.nref + 1) <= units / ((size_t)q.nw * (size_t)q.ns);
+  if (!fits) {
+    const double need = (double)tab + (double)(q.nref + 1) * (double)q.ns * (double)q.nw * (double)slice_b;
+    return fail(FWIX_ERR_UNSUPPORTED, "fwix_step_noalloc needs " + std::to_string((unsigned long long)need) +
+                                          " bytes of scratch; the static scratch holds " + std::to_string(cap) +
+                                          " bytes ((nref + 1) wavefields plus tables)");
+  }
+  d.wfld = d.slice * q.nw * q.ns;
   // one side of the step carries a single wavefield, the other nref of them
   const bool one_in = (kind == FWIX_STEP_PSPI) == (dir == FWIX_FWD);
-  const size_t wb = (size_t)d.wfld * sizeof(float2);
-  const size_t need = tab + (size_t)(q.nref + 1) * wb;
-  if (need > (size_t)FWIX_NOALLOC_SCRATCH_BYTES)
-    return fail(FWIX_ERR_UNSUPPORTED, "fwix_step_noalloc needs " + std::to_string(need) +
-                                          " bytes of scratch; the static scratch holds " +
-                                          std::to_string((size_t)FWIX_NOALLOC_SCRATCH_BYTES) +
-                                          " bytes ((nref + 1) wavefields plus tables)");
   unsigned char* base = nullptr;
   cudaError_t e = scratch_address(&base);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");

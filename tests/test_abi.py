@@ -105,3 +105,22 @@ def test_null_plan_is_rejected_by_every_entry_point():
     assert lib.fwix_plan_create(None, None) == -1
     st = lib.fwix_step_noalloc(None, 0, 0, 0, None, None, 0, 0, None, None, 0, None)
     assert st == -1 and lib.fwix_last_error()
+
+
+def test_noalloc_descriptor_checks_without_gpu():
+    """fwix_step_noalloc refuses, before any CUDA call, the descriptors that
+    fwix_plan_create refuses (negative taper widths) and problems whose scratch
+    size would wrap a 64-bit byte count.  The buffer pointers are never read on
+    these paths."""
+    from pyfwix_b200 import _lib
+    lib = _lib.load()
+    fake = ctypes.c_void_p(256)
+    call = lambda d: lib.fwix_step_noalloc(ctypes.byref(d), 0, 0, 0, fake, fake, 0, 0, fake, fake, 0, None)
+    d = _lib.FwixDesc(nx=64, ny=64, nw=1, ns=1, nz=1, dx=1, dy=1, dz=1, nref=1, taperx=-1)
+    assert call(d) == -1 and b"taper" in lib.fwix_last_error()
+    h = ctypes.c_void_p()
+    assert lib.fwix_plan_create(ctypes.byref(d), ctypes.byref(h)) == -1
+    big = _lib.FwixDesc(nx=1024, ny=1024, nw=2 ** 30, ns=2 ** 30, nz=1, dx=1, dy=1, dz=1, nref=255)
+    assert call(big) == -2 and b"static scratch holds" in lib.fwix_last_error()
+    wide = _lib.FwixDesc(nx=1000, ny=64, padx=100, nw=1, ns=1, nz=1, dx=1, dy=1, dz=1, nref=1)
+    assert call(wide) == -2 and b"at most 1024" in lib.fwix_last_error()

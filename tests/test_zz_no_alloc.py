@@ -32,18 +32,27 @@ def _noalloc(lib, plan, kind, iz, direction, sref, labels, inp, out, add):
     return out
 
 
-@pytest.mark.parametrize("kind,direction", [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1)])
-def test_noalloc_step_matches_workspace_step(kind, direction):
+# (nx, ny, pad, nw): a padded 48 x 40 grid takes the generic passes; 64 x 64 and
+# 256 x 256 take the size-specialised register-resident passes that production
+# grids use (256 x 256 x 16 frequencies: five wavefields of 8 MiB in the scratch).
+SIZES = [(40, 36, (8, 4), 4), (56, 60, (8, 4), 4), (256, 256, (0, 0), 16)]
+
+
+@pytest.mark.parametrize("size", SIZES, ids=["48x40", "64x64", "256x256"])
+@pytest.mark.parametrize("kind,direction", [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2)])
+def test_noalloc_step_matches_workspace_step(kind, direction, size):
     from pyfwix_b200 import _lib
     lib = _lib.load()
     step = "pspi" if kind == 0 else "nsps"
-    g, rng, sref, labels, _, _ = make_case(nx=40, ny=36, nw=4, nz=3, nref=4, padx=8, pady=4, eps=0.01,
+    nx, ny, (padx, pady), nw = size
+    ns = 2 if nx < 256 else 1
+    g, rng, sref, labels, _, _ = make_case(nx=nx, ny=ny, nw=nw, nz=3, nref=4, padx=padx, pady=pady, eps=0.01,
                                            complex_refs=True, labels_per_w=False)
-    p = make_plan(g, 2, sref, labels, step=step)
+    p = make_plan(g, ns, sref, labels, step=step)
     sref_d = p._keep["sref"]
     for call in range(2):  # two calls in a row on the shared scratch
-        x = wavefield(rng, 2, g)
-        d0 = wavefield(rng, 2, g)
+        x = wavefield(rng, ns, g)
+        d0 = wavefield(rng, ns, g)
         iz = call + 1
         ref = to_host(p.step(iz, to_dev(x), to_dev(d0), direction=direction, add=True))
         got = to_host(_noalloc(lib, p, kind, iz, direction, sref_d, labels, to_dev(x), to_dev(d0), True))
@@ -65,4 +74,12 @@ def test_noalloc_rejects_oversize_problem():
                                ctypes.c_void_p(lab.data_ptr()), 0, 0, ctypes.c_void_p(x.data_ptr()),
                                ctypes.c_void_p(x.data_ptr()), 0, None)
     assert st == -2  # FWIX_ERR_UNSUPPORTED
+    assert b"static scratch holds" in lib.fwix_last_error()
+    # frequency and shot counts whose product with the slice size would wrap a
+    # 64-bit byte count are refused the same way, before anything is launched
+    big = _lib.FwixDesc(nx=1024, ny=1024, nw=2 ** 30, ns=2 ** 30, nz=1, dx=10, dy=10, dz=10, ow=1, dw=1, nref=255)
+    st = lib.fwix_step_noalloc(ctypes.byref(big), 0, 0, 0, ctypes.c_void_p(x.data_ptr()),
+                               ctypes.c_void_p(lab.data_ptr()), 0, 0, ctypes.c_void_p(x.data_ptr()),
+                               ctypes.c_void_p(x.data_ptr()), 0, None)
+    assert st == -2
     assert b"static scratch holds" in lib.fwix_last_error()
