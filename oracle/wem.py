@@ -211,30 +211,39 @@ def select(labels, value, x):
     return np.where(labels[None] == value, x, 0)
 
 
-def pspi_forward(g, sref_z, labels_z, m, d=None, taper=True):
+def _factors(g, sref_z, fn, factors, dtype):
+    """Phase factors of every reference at one depth: the precomputed list when
+    given (``Stepper`` keeps one per depth), else evaluated here."""
+    if factors is not None:
+        return [f.astype(dtype, copy=False) for f in factors]
+    kx, ky, w2 = g.kx(), g.ky(), g.w2()
+    return [fn(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(dtype) for r in range(g.nref)]
+
+
+def pspi_forward(g, sref_z, labels_z, m, d=None, taper=True, factors=None):
     """PSPI forward, add version (``propagator/src/PSPI.cpp:6-24``):
     d (+)= sum_r mask_r * F^-1( P_r * F(taper * m) ).  The in-place overload
     (``propagator/src/PSPI.cpp:66-83``) is the same map with d = 0."""
-    kx, ky, w2 = g.kx(), g.ky(), g.w2()
+    Ps = _factors(g, sref_z, phase_forward_factor, factors, m.dtype)
     tap = g.taper().astype(m.real.dtype) if taper else 1.0
     mk = fft2(tap * m)
     out = np.zeros_like(m) if d is None else d.copy()
     for r in range(g.nref):
-        P = phase_forward_factor(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(m.dtype)
+        P = Ps[r]
         ref = ifft2(mk * P[None])
         out += select(labels_z, r, ref)
     return out.astype(m.dtype, copy=False)
 
 
-def pspi_adjoint(g, sref_z, labels_z, d, m=None, taper=False):
+def pspi_adjoint(g, sref_z, labels_z, d, m=None, taper=False, factors=None):
     """PSPI adjoint.  Add version (``propagator/src/PSPI.cpp:26-44``):
     m (+)= F^-1( sum_r P_r^adj * F(mask_r * d) ) with NO taper; the in-place
     overload (``propagator/src/PSPI.cpp:85-103``) multiplies by the taper at the
     end (``taper=True``)."""
-    kx, ky, w2 = g.kx(), g.ky(), g.w2()
+    Qs = _factors(g, sref_z, phase_adjoint_factor, factors, d.dtype)
     mk = np.zeros_like(d)
     for r in range(g.nref):
-        Q = phase_adjoint_factor(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(d.dtype)
+        Q = Qs[r]
         mk = mk + Q[None] * fft2(select(labels_z, r, d))
     x = ifft2(mk)
     if taper:
@@ -243,27 +252,27 @@ def pspi_adjoint(g, sref_z, labels_z, d, m=None, taper=False):
     return out.astype(d.dtype, copy=False)
 
 
-def nsps_forward(g, sref_z, labels_z, m, d=None):
+def nsps_forward(g, sref_z, labels_z, m, d=None, factors=None):
     """NSPS forward (``propagator/src/NSPS.cpp:27-45``):
     d (+)= F^-1( sum_r P_r * F(mask_r * m) )."""
-    kx, ky, w2 = g.kx(), g.ky(), g.w2()
+    Ps = _factors(g, sref_z, phase_forward_factor, factors, m.dtype)
     mk = np.zeros_like(m)
     for r in range(g.nref):
-        P = phase_forward_factor(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(m.dtype)
+        P = Ps[r]
         mk = mk + P[None] * fft2(select(labels_z, r, m))
     x = ifft2(mk)
     out = x if d is None else d + x
     return out.astype(m.dtype, copy=False)
 
 
-def nsps_adjoint(g, sref_z, labels_z, d, m=None):
+def nsps_adjoint(g, sref_z, labels_z, d, m=None, factors=None):
     """NSPS adjoint (``propagator/src/NSPS.cpp:6-25``):
     m (+)= sum_r mask_r * F^-1( P_r^adj * F(d) )."""
-    kx, ky, w2 = g.kx(), g.ky(), g.w2()
+    Qs = _factors(g, sref_z, phase_adjoint_factor, factors, d.dtype)
     dk = fft2(d)
     out = np.zeros_like(d) if m is None else m.copy()
     for r in range(g.nref):
-        Q = phase_adjoint_factor(w2, kx, ky, sref_z[r], g.dz, g.eps).astype(d.dtype)
+        Q = Qs[r]
         out += select(labels_z, r, ifft2(Q[None] * dk))
     return out.astype(d.dtype, copy=False)
 
@@ -274,30 +283,44 @@ class Stepper:
     reference hard-wires PSPI there (``propagator/src/OneWay.h:24-25,39-40``);
     ``kind='nsps'`` swaps in NSPS for the NSPS-driven sweeps."""
 
-    def __init__(self, g, sref, labels, kind="pspi"):
+    def __init__(self, g, sref, labels, kind="pspi", cache_factors=True):
         self.g, self.sref, self.labels, self.kind = g, sref, labels, kind
+        # the factors of a depth depend only on its references: evaluated once per
+        # depth and direction and reused by every later step there (same values)
+        self._cache = {} if cache_factors else None
+
+    def _f(self, iz, adjoint):
+        if self._cache is None:
+            return None
+        key = (iz, adjoint)
+        if key not in self._cache:
+            g = self.g
+            fn = phase_adjoint_factor if adjoint else phase_forward_factor
+            self._cache[key] = [fn(g.w2(), g.kx(), g.ky(), self.sref[iz][r], g.dz, g.eps) for r in range(g.nref)]
+        return self._cache[key]
 
     def fwd(self, iz, psi):
         if self.kind == "pspi":
-            return pspi_forward(self.g, self.sref[iz], self.labels[iz], psi, taper=True)
-        return nsps_forward(self.g, self.sref[iz], self.labels[iz], psi)
+            return pspi_forward(self.g, self.sref[iz], self.labels[iz], psi, taper=True, factors=self._f(iz, False))
+        return nsps_forward(self.g, self.sref[iz], self.labels[iz], psi, factors=self._f(iz, False))
 
     def adj(self, iz, psi):
         if self.kind == "pspi":
-            return pspi_adjoint(self.g, self.sref[iz], self.labels[iz], psi, taper=True)
-        return nsps_adjoint(self.g, self.sref[iz], self.labels[iz], psi)
+            return pspi_adjoint(self.g, self.sref[iz], self.labels[iz], psi, taper=True, factors=self._f(iz, True))
+        return nsps_adjoint(self.g, self.sref[iz], self.labels[iz], psi, factors=self._f(iz, True))
 
     def fwd_add(self, iz, m, d):
         """``prop->cu_forward(true, m, d)`` (``propagator/src/Scattering.cpp:50``)."""
         if self.kind == "pspi":
-            return pspi_forward(self.g, self.sref[iz], self.labels[iz], m, d, taper=True)
-        return nsps_forward(self.g, self.sref[iz], self.labels[iz], m, d)
+            return pspi_forward(self.g, self.sref[iz], self.labels[iz], m, d, taper=True, factors=self._f(iz, False))
+        return nsps_forward(self.g, self.sref[iz], self.labels[iz], m, d, factors=self._f(iz, False))
 
     def adj_set(self, iz, d):
         """``prop->cu_adjoint(false, m, d)`` (``propagator/src/Scattering.cpp:58``)."""
         if self.kind == "pspi":
-            return pspi_adjoint(self.g, self.sref[iz], self.labels[iz], d, None, taper=False)
-        return nsps_adjoint(self.g, self.sref[iz], self.labels[iz], d)
+            return pspi_adjoint(self.g, self.sref[iz], self.labels[iz], d, None, taper=False,
+                                factors=self._f(iz, True))
+        return nsps_adjoint(self.g, self.sref[iz], self.labels[iz], d, factors=self._f(iz, True))
 
 
 def downward(stepper, nz, psi):

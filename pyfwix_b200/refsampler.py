@@ -10,8 +10,8 @@ choice is deterministic:
   (2k+1)/(2 nref) of the depth slice's slowness sqrt(Re s^2); the reference s^2
   is their square.
 * ``method="kmeans"``: Lloyd iterations on s^2 started from those quantiles
-  (the same objective as cv::kmeans, without the random seeding), stopped per
-  chunk of (depth, frequency) rows.
+  (the same objective as cv::kmeans, without the random seeding), each
+  (depth, frequency) row stopped on its own.
 
 Labels are the index of the nearest reference in s^2 (complex distance), padded
 by edge replication.  Runs on the model's device with torch.
@@ -53,9 +53,13 @@ def _quantile_centers(x, nref):
 
 
 def _lloyd(x, centers, iters, tol):
-    """Lloyd iterations on the rows of x from the given centers; stops when no
-    center of the chunk moves by more than tol times the largest one."""
+    """Lloyd iterations on each row of x from the given centers.  Rows are
+    independent, as the reference's one cv::kmeans call per (depth, frequency)
+    row: a row stops, keeping the update that got it there, once none of its
+    centers moved by more than tol times its largest center; an empty cluster
+    keeps its center."""
     nref = centers.shape[1]
+    active = torch.ones(centers.shape[0], dtype=torch.bool, device=x.device)
     for _ in range(iters):
         lab = _nearest(x, centers)
         new = centers.clone()
@@ -64,9 +68,10 @@ def _lloyd(x, centers, iters, tol):
             cnt = m.sum(dim=1)
             ssum = torch.where(m, x, torch.zeros_like(x)).sum(dim=1)
             new[:, r] = torch.where(cnt > 0, ssum / torch.clamp(cnt, min=1), centers[:, r])
-        shift = torch.max(torch.abs(new - centers))
-        centers = new
-        if float(shift) <= tol * float(torch.max(torch.abs(centers))):
+        shift = torch.abs(new - centers).amax(dim=1)
+        centers = torch.where(active[:, None], new, centers)
+        active = active & ~(shift <= tol * torch.abs(centers).amax(dim=1))
+        if not bool(active.any()):
             break
     return centers
 
