@@ -22,7 +22,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
 OUT_DIR = os.path.join(ORACLE, "_ref")
 LIB = os.path.join(OUT_DIR, "librefshim.so")
-REF = os.environ.get("FWIX_REFERENCE_TREE", "/root/reference")
+# the reference tree: FWIX_REFERENCE_TREE, else a "reference" directory beside this repository
+REF = os.environ.get("FWIX_REFERENCE_TREE",
+                     os.path.normpath(os.path.join(os.path.dirname(ORACLE), os.pardir, "reference")))
 KERNELS = ["phase_shift", "selector", "taper", "injection", "reflect", "scatter", "imaging_condition",
            "lin_reflect"]
 
