@@ -283,11 +283,14 @@ class Stepper:
     reference hard-wires PSPI there (``propagator/src/OneWay.h:24-25,39-40``);
     ``kind='nsps'`` swaps in NSPS for the NSPS-driven sweeps."""
 
-    def __init__(self, g, sref, labels, kind="pspi", cache_factors=True):
+    def __init__(self, g, sref, labels, kind="pspi", cache_factors=True, cache_bytes=4 << 30):
         self.g, self.sref, self.labels, self.kind = g, sref, labels, kind
         # the factors of a depth depend only on its references: evaluated once per
-        # depth and direction and reused by every later step there (same values)
+        # depth and direction and reused by later steps there (same values); the
+        # most recent (depth, direction) pairs that fit in cache_bytes are kept
         self._cache = {} if cache_factors else None
+        entry = 16 * g.nref * g.nw * g.NX * g.NY
+        self._entries = max(1, int(cache_bytes) // max(entry, 1))
 
     def _f(self, iz, adjoint):
         if self._cache is None:
@@ -296,6 +299,8 @@ class Stepper:
         if key not in self._cache:
             g = self.g
             fn = phase_adjoint_factor if adjoint else phase_forward_factor
+            while len(self._cache) >= self._entries:
+                self._cache.pop(next(iter(self._cache)))
             self._cache[key] = [fn(g.w2(), g.kx(), g.ky(), self.sref[iz][r], g.dz, g.eps) for r in range(g.nref)]
         return self._cache[key]
 

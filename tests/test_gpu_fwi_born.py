@@ -1,0 +1,147 @@
+"""The FWI gradient (``pyfwix_b200.fwi``) tied to the reference's gradient
+operator, ExtendedBorn::adjoint (``propagator/src/ExtendedBorn.cpp:122-150``,
+called as the gradient in ``fwix/workers.py:62-76``), and checked by central
+finite differences on the device.
+
+How the two operators relate.  ExtendedBorn linearises the PSPI modelling in
+s^2 per frequency; its gradient with respect to a real, frequency-independent
+slowness s is g_s = 2 s sum_w Re g_{s^2}[w].  FWIGradient differentiates the
+smooth step's modelling in s.  Both linearise the same Propagator
+(``propagator/src/Propagator.cpp:121-221``), but discretise the scattering
+differently:
+
+* ExtendedBorn scatters before the step, S(W u ds^2) (``Scattering.cpp:43-52``);
+  the smooth step's derivative multiplies after it, -i w dz ds S(u);
+* its up scattering takes the perturbation of the level a step leaves
+  (``ExtendedBorn.cpp:282-311``), the smooth model that of the level it reaches;
+* its linearised reflection carries a factor sqrt(s0 / s1) that the derivative
+  of r = (s0 - s1) / (s0 + s1) does not (``lin_reflect.cu:48-92``);
+* its Taylor terms beyond the first and eps_scat are not in the split-step
+  derivative.
+
+All four differences vanish in a homogeneous background with one reference
+(the smooth step is then the PSPI step; no reflection, so no up-going
+background), Taylor order 0, eps_scat 0, no taper (the reference's scattering
+adjoint omits the taper, ``PSPI.cpp:26-44``), and for perturbations constant
+over each depth level (multiplying before or after the step is then the same).
+There the two gradients' sums over each depth level must agree for any data
+residual: the first test below.  The fields themselves differ by where the
+scattering sits inside the step.
+"""
+import numpy as np
+import pytest
+import torch
+
+from tests.conftest import crandn
+from tests.gpu_helpers import rel, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+def _homogeneous(nz=6, n=64, nw=8):
+    s = np.float32(1 / 2000.0)
+    dx = dz = 10.0
+    gx, gy = np.meshgrid(np.arange(4, n - 4, 6) * dx, np.arange(4, n - 4, 6) * dx)
+    nr = gx.size
+    geom = dict(sx=np.array([n // 2 * dx], np.float32), sy=np.array([n // 2 * dx], np.float32),
+                sz=np.array([0.0], np.float32), s_ids=np.array([0], np.int32),
+                # receivers on the surface and on level 3 (all on grid nodes)
+                rx=np.concatenate([gx.ravel(), gx.ravel()]).astype(np.float32),
+                ry=np.concatenate([gy.ravel(), gy.ravel()]).astype(np.float32),
+                rz=np.concatenate([np.zeros(nr), np.full(nr, 3 * dz)]).astype(np.float32),
+                r_ids=np.zeros(2 * nr, np.int32))
+    par = dict(nref=1, padx=0, pady=0, taperx=0, tapery=0, eps=0.0, ox=0.0, oy=0.0, oz=0.0, dx=dx, dy=dx,
+               dz=dz, ow=4.0, dw=3.0, checkpoint=None)
+    return s, geom, par, (nz, n, n), nw
+
+
+def test_fwi_gradient_ties_to_born_adjoint():
+    from pyfwix_b200.fwi import SmoothFWI
+    from pyfwix_b200.plan import Plan
+    s, geom, par, shape, nw = _homogeneous()
+    nz, ny, nx = shape
+    rng = np.random.default_rng(77)
+    wav = torch.as_tensor(crandn(rng, (1, nw)).astype(np.complex64)).cuda()
+    sfield = torch.full(shape, float(s), dtype=torch.float32)
+    refs = torch.full((nz, 1), float(s), dtype=torch.float32)
+    prob = SmoothFWI(shape, geom, wav, dict(par, refs=refs))
+    d_smooth = prob.model(sfield, keep=True)
+    ntr = len(geom["rx"])
+    r = torch.as_tensor(crandn(rng, (ntr, nw)).astype(np.complex64)).cuda()
+    g_fwi = prob.gradient(r).double().cpu().numpy()
+
+    # the reference's Born on the same modelling: PSPI, one reference per depth
+    p = Plan(nx=nx, ny=ny, nw=nw, ns=1, nz=nz, dx=par["dx"], dy=par["dy"], dz=par["dz"], ow=par["ow"],
+             dw=par["dw"], nref=1, taperx=0, tapery=0, eps_scat=0.0, taylor=0, step="pspi")
+    s2 = (torch.full((nz, 1, ny, nx), float(s), dtype=torch.float64) ** 2).to(torch.complex64)
+    p.set_refs(s2[:, :, :1, :1].reshape(nz, 1, 1).expand(nz, 1, nw), torch.zeros((nz, 1, ny, nx), dtype=torch.uint8))
+    p.set_model(s2, torch.ones_like(s2))
+    src = p.traces(geom["sx"], geom["sy"], geom["sz"], geom["s_ids"])
+    rec = p.traces(geom["rx"], geom["ry"], geom["rz"], geom["r_ids"])
+    bd = torch.empty((nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d_pspi = torch.empty((ntr, nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, wav, d_pspi, bd, bu)
+    # one reference at the local slowness: the smooth step is the PSPI step
+    assert float(torch.abs(d_smooth).max()) > 0
+    assert rel(to_host(d_smooth), to_host(d_pspi)) < 1e-5
+    gs2 = torch.empty((nz, 1, ny, nx), dtype=torch.complex64, device="cuda")
+    gr = torch.empty_like(gs2)
+    p.born(rec, bd, bu, gs2, gr, r, adjoint=True)
+    g_born = (2 * float(s) * to_host(gs2)[:, 0].real)
+    sums_fwi = g_fwi.sum(axis=(1, 2))
+    sums_born = g_born.sum(axis=(1, 2))
+    assert np.abs(sums_born).max() > 0
+    assert rel(sums_fwi, sums_born) < 1e-4, (sums_fwi, sums_born)
+    # the linearisations agree, the fields do not: scattering before the step
+    # (Born) and after it (smooth) put the same sum at different places
+    assert rel(g_fwi, g_born) > 1e-3
+
+
+def test_fwi_gradient_central_differences_on_device():
+    """The central finite-difference check of the FWI configuration, on the
+    device: 384 x 384 x 96 frequencies, three levels through the first anomaly,
+    h = 1e-3 relative.  A single cell moves the FP32 objective by less than its
+    rounding, so each of the 16 random cells is the centre of a Gaussian
+    perturbation (sigma 8 cells on its level); (J(s + h ds) - J(s - h ds)) / 2h
+    must equal <dJ/ds, ds> from the adjoint-state gradient."""
+    from pyfwix_b200 import workloads
+    from pyfwix_b200.fwi import SmoothFWI
+    w, s_true, s0 = workloads.config4()
+    z0 = int(np.argmax(np.abs(s_true - s0).sum(axis=(1, 2)))) - 1
+    s_true = np.ascontiguousarray(s_true[z0:z0 + 3])
+    s0 = np.ascontiguousarray(s0[z0:z0 + 3])
+    w.oz, w.nz = z0 * w.dz, 3
+    geom = dict(w.geom, sz=np.full(1, w.oz, np.float32), rz=np.full(len(w.geom["rz"]), w.oz, np.float32))
+    par = dict(nref=w.nref, padx=0, pady=0, taperx=w.taperx, tapery=w.tapery, eps=0.0, ox=w.ox, oy=w.oy,
+               oz=w.oz, dx=w.dx, dy=w.dy, dz=w.dz, ow=w.ow, dw=w.dw, checkpoint=None)
+    wav = torch.as_tensor(w.wavelet).cuda()
+    prob = SmoothFWI(s_true.shape, geom, wav, par)
+    prob.set_slowness(torch.as_tensor(s_true))
+    prob = SmoothFWI(s_true.shape, geom, wav, dict(par, refs=prob.refs.clone()))
+    d_obs = prob.model(torch.as_tensor(s_true), keep=False).to(torch.complex128)
+    s0t = torch.as_tensor(s0, dtype=torch.float64)
+    data = prob.model(s0t.float(), keep=True)
+    grad = prob.gradient(data - d_obs.to(torch.complex64)).double().cpu()
+
+    def objective(s):
+        res = prob.model(s.float(), keep=False).to(torch.complex128) - d_obs
+        return 0.5 * float(torch.sum(res.real ** 2 + res.imag ** 2))
+
+    rng = np.random.default_rng(1003)
+    ny, nx = s0.shape[1:]
+    yy, xx = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    h = 1e-3
+    fd, ad = [], []
+    for _ in range(16):
+        iz, iy, ix = int(rng.integers(0, 2)), int(rng.integers(20, ny - 20)), int(rng.integers(20, nx - 20))
+        bump = np.zeros(s0.shape)
+        bump[iz] = np.exp(-((yy - iy) ** 2 + (xx - ix) ** 2) / (2 * 8.0 ** 2))
+        ds = s0t * torch.as_tensor(bump)
+        fd.append((objective(s0t + h * ds) - objective(s0t - h * ds)) / (2 * h))
+        ad.append(float(torch.sum(grad * ds)))
+    fd, ad = np.array(fd), np.array(ad)
+    err = np.abs(fd - ad) / np.abs(ad).max()
+    assert np.abs(ad).max() > 0
+    assert err.max() < 1e-2, (fd, ad)
+    assert rel(fd, ad) < 1e-2, (fd, ad)
