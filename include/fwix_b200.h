@@ -175,6 +175,12 @@ fwix_status fwix_lin_reflect(fwix_plan* plan, int iz, int adjoint, void* dmodel,
 fwix_status fwix_plan_set_smooth(fwix_plan* plan, const float* slow_pad, const float* sref_real);
 fwix_status fwix_smooth_step(fwix_plan* plan, int iz, int mode, const void* in, void* out, int add,
                              void* stream);
+/* FWD into out and DERIV into deriv (different buffers; in may be either) from
+ * one set of transforms: the forward step and its slowness derivative share the
+ * forward row and column passes and each inverse row transform, which the
+ * gradient's segment recomputations need together. */
+fwix_status fwix_smooth_step_pair(fwix_plan* plan, int iz, const void* in, void* out, void* deriv, int add,
+                                  void* stream);
 /* out[y][x] (+)= Re sum_{shots, w} conj(a) b over the padded slice (padded != 0,
  * out is [NY][NX]) or the model window (out is [ny][nx]). */
 fwix_status fwix_correlate(fwix_plan* plan, const void* a, const void* b, float* out, int add, int padded,

@@ -70,6 +70,7 @@ SIGNATURES = {
     "fwix_step": [P, I, I, I, P, P, I, P],
     "fwix_plan_set_smooth": [P, P, P],
     "fwix_smooth_step": [P, I, I, P, P, I, P],
+    "fwix_smooth_step_pair": [P, I, P, P, P, I, P],
     "fwix_correlate": [P, P, P, P, I, I, P],
     "fwix_scatter": [P, I, I, P, P, I, P],
     "fwix_reflect": [P, I, I, P, P, I, P],

@@ -316,6 +316,11 @@ fwix_status need_smooth(const fwix_plan* p) {
 //   out (+)= sum_r w_r(s) SS_r F^-1(P_r F(taper in)),
 // its exact transpose, and the derivative with respect to the local slowness
 //   out (+)= sum_r (w_r' - i w dz w_r) SS_r F^-1(P_r F(taper in)).
+// mode kSmoothPair: FWD into a.out and DERIV into a.out2 from one forward row pass
+// and one column pass (the inverse row pass of the register-resident plans sums
+// each term with both weights; other lengths run two inverse row passes).
+constexpr int kSmoothPair = -1;
+
 fwix_status smooth_chunk(fwix_plan* p, int iz, int mode, SpecArgs a, cudaStream_t s) {
   a.sref = p->sref + (long long)iz * p->desc.nref * p->d.nw;
   a.sm_s = p->sm_s + (long long)iz * p->d.slice;
@@ -329,6 +334,13 @@ fwix_status smooth_chunk(fwix_plan* p, int iz, int mode, SpecArgs a, cudaStream_
   }
   FWIX_TRY(cu(fwix::row_forward(a, fwix::W_TAPER, s), "smooth row pass"));
   FWIX_TRY(cu(fwix::col_type_a(a, fwix::Q_PS_FWD, s), "smooth column pass"));
+  if (mode == kSmoothPair) {
+    if (fwix::fast_length(p->d.NX))
+      return cu(fwix::row_inverse(a, fwix::W_SMOOTH_PAIR, 0, s), "smooth pair inverse row pass");
+    FWIX_TRY(cu(fwix::row_inverse(a, fwix::W_SMOOTH, 0, s), "smooth inverse row pass"));
+    a.out = a.out2;
+    return cu(fwix::row_inverse(a, fwix::W_SMOOTH_DERIV, 0, s), "smooth derivative inverse row pass");
+  }
   return cu(fwix::row_inverse(a, mode == FWIX_SMOOTH_DERIV ? fwix::W_SMOOTH_DERIV : fwix::W_SMOOTH, 0, s),
             "smooth inverse row pass");
 }
@@ -800,6 +812,22 @@ fwix_status fwix_smooth_step(fwix_plan* p, int iz, int mode, const void* in, voi
   SpecArgs a0 = p->args((const float2*)in, (float2*)out, add);
   FWIX_TRY(phase_factors(p, iz, a0, s));
   return for_chunks(p, a0, [&](const SpecArgs& a) { return smooth_chunk(p, iz, mode, a, s); });
+}
+
+fwix_status fwix_smooth_step_pair(fwix_plan* p, int iz, const void* in, void* out, void* deriv, int add,
+                                  void* stream) {
+  if (!p || !in || !out || !deriv) return fail(FWIX_ERR_INVALID, "null argument");
+  if (out == deriv) return fail(FWIX_ERR_INVALID, "out and deriv must be different buffers");
+  FWIX_TRY(need_smooth(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  FWIX_TRY(check_iz(p, iz));
+  cudaStream_t s = (cudaStream_t)stream;
+  SpecArgs a0 = p->args((const float2*)in, (float2*)out, add);
+  FWIX_TRY(phase_factors(p, iz, a0, s));
+  return for_chunks(p, a0, [&](SpecArgs a) {
+    a.out2 = (float2*)deriv;
+    return smooth_chunk(p, iz, kSmoothPair, a, s);
+  });
 }
 
 fwix_status fwix_correlate(fwix_plan* p, const void* a, const void* b, float* out, int add, int padded,

@@ -419,13 +419,16 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
 
 // out (+)= post * sum_term W_term * F_x^-1(t2[term]); the next term's row is
 // prefetched while the current one is transformed, and with labels the terms
-// that no sample of the warp's rows selects are skipped.
+// that no sample of the warp's rows selects are skipped.  W_SMOOTH_PAIR sums each
+// transformed term twice, with the smooth weights into out and with their
+// slowness derivatives into out2.
 template <class P, int POST>
 __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 || P::E == 12) ? 2 : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
-  constexpr bool kSmooth = POST == W_SMOOTH || POST == W_SMOOTH_DERIV;
+  constexpr bool kPair = POST == W_SMOOTH_PAIR;
+  constexpr bool kSmooth = POST == W_SMOOTH || POST == W_SMOOTH_DERIV || kPair;
   const bool hat_smem = kSmooth && a.sm_n <= kMaxHatRefs;
   const float* href = reinterpret_cast<const float*>(c.tw + tw_size<P>());
   const float* hinv = href + kMaxHatRefs;
@@ -434,8 +437,13 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   const int nterm = multi_term(POST) ? a.nterm : 1;
   float g[kSmooth ? P::E : 1];
   float2 acc[P::E];
+  float2 acc2[kPair ? P::E : 1];
 #pragma unroll
   for (int e = 0; e < P::E; ++e) acc[e] = make_float2(0.f, 0.f);
+  if constexpr (kPair) {
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) acc2[e] = make_float2(0.f, 0.f);
+  }
   Labels<P::E> lab;
   unsigned used = 0xffffffffu;
   if (POST == W_MASK) {
@@ -492,15 +500,28 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
       const float2 C = smooth_ref_phase(a, c.iw, term);
       const float wdz = a.w[c.iw] * a.dz;
 #pragma unroll
-      for (int e = 0; e < P::E; ++e)
-        if (c.live) acc[e] = cadd(acc[e], cmul(v[e], hat_ref_weight<POST>(hat_at(hinv, a.sm_n, term, g[e]), wdz, C)));
+      for (int e = 0; e < P::E; ++e) {
+        if (!c.live) continue;
+        const float2 h = hat_at(hinv, a.sm_n, term, g[e]);
+        if constexpr (kPair) {
+          acc[e] = cadd(acc[e], cmul(v[e], hat_ref_weight<W_SMOOTH>(h, wdz, C)));
+          acc2[e] = cadd(acc2[e], cmul(v[e], hat_ref_weight<W_SMOOTH_DERIV>(h, wdz, C)));
+        } else {
+          acc[e] = cadd(acc[e], cmul(v[e], hat_ref_weight<POST>(h, wdz, C)));
+        }
+      }
     } else {
 #pragma unroll
       for (int e = 0; e < P::E; ++e) {
         if (POST == W_MASK) {
           if (lab.get(e) == term) acc[e] = v[e];
         } else if (c.live) {
-          acc[e] = cadd(acc[e], row_weight<POST>(a, term, c.iw, c.y, pos_first<P>(c.t, e), v[e]));
+          if constexpr (kPair) {
+            acc[e] = cadd(acc[e], row_weight<W_SMOOTH>(a, term, c.iw, c.y, pos_first<P>(c.t, e), v[e]));
+            acc2[e] = cadd(acc2[e], row_weight<W_SMOOTH_DERIV>(a, term, c.iw, c.y, pos_first<P>(c.t, e), v[e]));
+          } else {
+            acc[e] = cadd(acc[e], row_weight<POST>(a, term, c.iw, c.y, pos_first<P>(c.t, e), v[e]));
+          }
         }
       }
     }
@@ -508,17 +529,28 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   }
   if (!c.live) return;
   float2* dst = a.out + (c.b * a.d.NY + c.y) * P::N;
+  float2* dst2 = kPair ? a.out2 + (c.b * a.d.NY + c.y) * P::N : nullptr;
   const float ty = post_taper ? a.tapy[c.y] : 1.f;
   const float* srow_out = kSmooth ? a.sm_s + (long long)c.y * P::N : nullptr;
 #pragma unroll
   for (int e = 0; e < P::E; ++e) {
     const int x = pos_first<P>(c.t, e);
     float2 v = acc[e];
-    if (hat_smem) v = cmul(v, smooth_cell_phase(a, c.iw, srow_out[x]));
+    float2 cell = make_float2(1.f, 0.f);
+    if (hat_smem) {
+      cell = smooth_cell_phase(a, c.iw, srow_out[x]);
+      v = cmul(v, cell);
+    }
     if constexpr (POST == W_ONE_DIRECT) v = cadd(v, scat_direct(a, c.b, c.iw, c.y, x));
     if (post_taper) v = cscale(v, a.tapx[x] * ty);
     if (a.add) v = cadd(dst[x], v);
     dst[x] = v;
+    if constexpr (kPair) {
+      float2 u = hat_smem ? cmul(acc2[e], cell) : acc2[e];
+      if (post_taper) u = cscale(u, a.tapx[x] * ty);
+      if (a.add) u = cadd(dst2[x], u);
+      dst2[x] = u;
+    }
   }
 }
 
@@ -817,6 +849,7 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
     FWIX_FAST_RI(W_SCAT)
     FWIX_FAST_RI(W_SMOOTH)
     FWIX_FAST_RI(W_SMOOTH_DERIV)
+    FWIX_FAST_RI(W_SMOOTH_PAIR)
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_FAST_RI

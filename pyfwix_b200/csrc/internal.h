@@ -28,13 +28,15 @@ enum RowWeight {
   W_SMOOTH = 6,       // w_r SS_r
   W_SMOOTH_CONJ = 7,  // w_r conj(SS_r)
   W_SMOOTH_DERIV = 8, // d(w_r SS_r)/ds = (w_r' - i w dz w_r) SS_r
-  W_ONE_DIRECT = 9    // 1, plus the Born adjoint's zeroth term conj(W_0) d (inverse row pass only)
+  W_ONE_DIRECT = 9,   // 1, plus the Born adjoint's zeroth term conj(W_0) d (inverse row pass only)
+  W_SMOOTH_PAIR = 10  // W_SMOOTH into out and W_SMOOTH_DERIV into out2 from the same
+                      // inverse transforms (register-resident inverse row pass only)
 };
 
 // Weights that run one pass per term (reference or Taylor term).
 __host__ __device__ constexpr bool multi_term(int w) {
   return w == W_MASK || w == W_SCAT || w == W_SCAT_CONJ || w == W_SMOOTH || w == W_SMOOTH_CONJ ||
-         w == W_SMOOTH_DERIV;
+         w == W_SMOOTH_DERIV || w == W_SMOOTH_PAIR;
 }
 
 // Spectral multipliers applied between the column FFTs.
@@ -106,6 +108,7 @@ struct SpecArgs {
   const float2* in;    // row-pass input (W_IC: the background wavefield)
   const float2* in2;   // optional second row-pass input added to `in` (NULL: none)
   float2* out;         // row-pass output
+  float2* out2;        // second inverse-row-pass output (W_SMOOTH_PAIR: the derivative)
   int add;
   float2* t1;
   float2* t2;

@@ -30,6 +30,15 @@ only every k-th down / up / mu field is kept and each k-level segment is
 recomputed from its checkpoint when the backward sweeps reach it;
 ``checkpoint="auto"`` (the default) stores everything when it fits in device
 memory and picks the interval otherwise.
+
+With checkpoints the backward runs the mu recursion alone first (one adjoint
+step per level, keeping mu at every segment start), then the nu recursion
+segment by segment from the bottom, recomputing the segment's down fields, up
+fields and mu fields and taking every gradient term there.  The down and up
+recomputations use the paired step (``fwix_smooth_step_pair``: the step and its
+slowness derivative from one set of transforms), so the derivative terms cost
+little beyond the recomputation itself: about five steps per level for the
+backward against three for the checkpointed forward.
 """
 from __future__ import annotations
 
@@ -133,9 +142,16 @@ class SmoothFWI:
         if 3 * p.nz * wb + 4 * wb <= budget:
             return None
         for k in (4, 8, 16, 32, 64, 128, 256):
-            if (3 * (-(-p.nz // k)) + 2 * k + 4) * wb <= budget:
+            if self.checkpoint_fields(p.nz, k) * wb <= budget:
                 return k
         return 256
+
+    @staticmethod
+    def checkpoint_fields(nz, k):
+        """Wavefields held at once with checkpoints every k levels: the down, up
+        and mu checkpoints, and one segment's down fields, their derivatives, the
+        up derivatives and mu fields, plus working fields."""
+        return 3 * (-(-nz // k)) + 4 * k + 6
 
     # ---------------------------------------------------------------- state
     def set_slowness(self, s):
@@ -203,28 +219,72 @@ class SmoothFWI:
             self.Uck[a] = U.clone()
         return data
 
-    def _segment_D(self, a):
-        """Down fields D_a .. D_{a+k-1} (after injection) recomputed from the
-        checkpoint at a, without recording."""
-        p, nz = self.plan, self.plan.nz
-        D = self.Dck[a].clone()
-        out = []
-        for iz in range(a, min(a + self.k, nz)):
-            p.inject(self.src, iz, self.wavelet, D)
-            out.append(D.clone())
-            p.smooth_step(iz, D, D)
-        return out
+    def _empty(self):
+        return torch.empty(self.plan.wshape, dtype=torch.complex64, device=self.device)
 
-    def _segment_U(self, a, Dseg):
-        """Up fields U_a .. U_{a+k} of a segment, from the checkpoint at a+k."""
+    def _segment_D(self, a, derivs=False):
+        """Down fields D_a .. D_{a+k-1} (after injection) recomputed from the
+        checkpoint at a, without recording; with ``derivs`` also dS_iz(D_iz) for
+        every level of the segment above the bottom of the model.  Each step
+        writes the next level's field (no copies)."""
         p, nz = self.plan, self.plan.nz
         top = min(a + self.k, nz)
-        U = self.Uck[top].clone()
-        out = {top: U.clone()}
+        D = self.Dck[a].clone()
+        out, der = [], []
+        for iz in range(a, top):
+            p.inject(self.src, iz, self.wavelet, D)
+            out.append(D)
+            last = iz + 1 == top
+            if derivs and iz + 1 < nz:
+                d = self._empty()
+                if last:
+                    p.smooth_step(iz, D, d, mode=L.SMOOTH_DERIV)
+                else:
+                    nxt = self._empty()
+                    p.smooth_step_pair(iz, D, nxt, d)
+                    D = nxt
+                der.append(d)
+            elif not last:
+                nxt = self._empty()
+                p.smooth_step(iz, D, nxt)
+                D = nxt
+        return (out, der) if derivs else out
+
+    def _segment_U_derivs(self, a, Dseg):
+        """dS_iz(U_{iz+1}) for the levels iz of the segment above the bottom of the
+        model, walking the up fields from the checkpoint U_{a+k} (which stays
+        untouched) with the paired step; index iz - a."""
+        p, nz = self.plan, self.plan.nz
+        top = min(a + self.k, nz)
+        der = [None] * (top - a)
+        U = self.Uck[top]
         for iz in range(top - 1, a - 1, -1):
-            p.smooth_step(iz, U, U)
-            p.reflect(iz, Dseg[iz - a], U, add=True)
-            out[iz] = U.clone()
+            nxt = self._empty()
+            if iz + 1 < nz:
+                d = self._empty()
+                p.smooth_step_pair(iz, U, nxt, d)
+                der[iz - a] = d
+            else:
+                nxt.zero_()   # the step of the zero field below the model
+            if iz > a:
+                p.reflect(iz, Dseg[iz - a], nxt, add=True)
+                U = nxt
+        return der
+
+    def _segment_mu(self, a):
+        """mu_a .. mu_{a+k-1} recomputed from mu_{a-1} (kept at a)."""
+        p, nz = self.plan, self.plan.nz
+        out = []
+        m = self.Mck[a]
+        for iz in range(a, min(a + self.k, nz)):
+            nxt = self._empty()
+            if iz > 0:
+                p.smooth_step(iz - 1, m, nxt, mode=L.SMOOTH_ADJ)
+            else:
+                nxt.zero_()
+            p.inject(self.rec, iz, self._res, nxt)
+            out.append(nxt)
+            m = nxt
         return out
 
     # ---------------------------------------------------------------- gradient
@@ -249,27 +309,34 @@ class SmoothFWI:
                 self._nu_level(iz, nu, res, Dget(iz), mus[iz], gpad, G)
         else:
             k = self.k
+            self._res = res
+            # mu recursion alone, keeping mu_{a-1} at every segment start a
             mu = self._field()
             self.Mck = {}
-            for a in range(0, nz, k):
-                self.Mck[a] = mu.clone()  # mu_{a-1} (zero for a = 0)
-                Dseg = self._segment_D(a)
-                Useg = self._segment_U(a, Dseg)
-                for iz in range(a, min(a + k, nz)):
-                    self._mu_level(iz, mu, res, Dseg[iz - a], Useg[iz + 1] if iz + 1 < nz else None,
-                                   gpad, crefl, G)
+            for iz in range(nz):
+                if iz % k == 0:
+                    self.Mck[iz] = mu.clone()
+                if iz > 0:
+                    p.smooth_step(iz - 1, mu, mu, mode=L.SMOOTH_ADJ)
+                p.inject(self.rec, iz, res, mu)
+            del mu
+            # nu recursion segment by segment from the bottom, with every gradient term
             nu = self._field()
             for a in reversed(range(0, nz, k)):
-                Dseg = self._segment_D(a)
-                mseg = []
-                m = self.Mck[a].clone()
-                for iz in range(a, min(a + k, nz)):
-                    if iz > 0:
-                        p.smooth_step(iz - 1, m, m, mode=L.SMOOTH_ADJ)
-                    p.inject(self.rec, iz, res, m)
-                    mseg.append(m.clone())
+                Dseg, dSD = self._segment_D(a, derivs=True)
+                dSU = self._segment_U_derivs(a, Dseg)
+                mseg = self._segment_mu(a)
                 for iz in range(min(a + k, nz) - 1, a - 1, -1):
-                    self._nu_level(iz, nu, res, Dseg[iz - a], mseg[iz - a], gpad, G)
+                    j = iz - a
+                    if iz + 1 < nz:
+                        p.correlate(mseg[j], dSU[j], gpad[iz], add=True, padded=True)
+                        p.correlate(mseg[j], Dseg[j], crefl[iz], add=True, padded=False)
+                        p.correlate(nu, dSD[j], gpad[iz], add=True, padded=True)
+                    p.smooth_step(iz, nu, nu, mode=L.SMOOTH_ADJ)
+                    p.reflect(iz, mseg[j], nu, adjoint=True, add=True)
+                    p.inject(self.rec, iz, res, nu)
+                del Dseg, dSD, dSU, mseg
+            self._res = None
         # reflection coefficients r_iz = (s_iz - s_iz+1) / (s_iz + s_iz+1)
         s = self.s
         grefl = torch.zeros_like(crefl)
@@ -321,3 +388,70 @@ class FWIGradient(torch.autograd.Function):
         g = ctx.prob.gradient(ctx.res)
         ctx.prob = ctx.res = None
         return (gJ * g).to(gJ.dtype), None, None, None, None
+
+
+def shot_objective_and_gradient(s, shot_list, par, group=None, device=None):
+    """J = 1/2 sum_i |d_i(s) - d_obs_i|^2 and dJ/ds over a list of shots, each
+    rank of the process group running its share of the shots.
+
+    This replaces the reference's shot loop and reduction: Dask workers each run
+    a partition of the shots in micro-batches, accumulating the misfit and the
+    ExtendedBorn adjoint of the residual (``fwix/workers.py:14-83``,
+    ``_obj_grad_worker``), and the per-worker gradients are summed by a streaming
+    Zarr reduction (``fwix/workers.py:154-177``, ``_reduce_vector``).  Here the
+    shots are partitioned across the ranks by cost (longest first,
+    ``pyfwix_b200.shots.partition``), each rank models and differentiates its
+    own shots with no communication (the smooth-step modelling and
+    adjoint-state gradient of ``SmoothFWI``), and one all-reduce sums J and the
+    gradient (NCCL over NVLink between GPUs).  Without a process group it is the
+    plain sum over all shots.
+
+    ``s``: slowness [nz][ny][nx] (float32; its device is the one used unless
+    ``device`` is given).  ``shot_list``: dicts with ``geometry`` (the
+    reference's geometry dict), ``wavelet`` [nsrc][nw] and ``d_obs`` [ntrace][nw];
+    a rank reads ``d_obs`` only for its own shots, so the other entries may hold
+    None.  ``par`` as for ``SmoothFWI``; its ``refs`` (fixed reference slownesses)
+    default to ``smooth_refs(s)`` on every rank alike.  Returns (J, gradient)
+    identical on every rank."""
+    from . import shots as _shots
+    s = torch.as_tensor(s)
+    dev = torch.device(device) if device is not None else s.device
+    s = s.to(dev, torch.float32)
+    nz, ny, nx = s.shape
+    par = dict(par) if isinstance(par, dict) else {k: _get(par, k) for k in (
+        "ox", "dx", "oy", "dy", "oz", "dz", "ow", "dw", "nref", "padx", "pady", "eps", "taperx", "tapery",
+        "checkpoint", "refs") if _get(par, k) is not None}
+    if par.get("refs") is None:
+        par["refs"] = smooth_refs(s, int(par.get("nref", 2))).to(torch.float32)
+    costs = [_shots.shot_cost(nx, ny, torch.as_tensor(sh["wavelet"]).shape[1], nz) for sh in shot_list]
+
+    def work(i):
+        sh = shot_list[i]
+        prob = SmoothFWI(tuple(s.shape), sh["geometry"], torch.as_tensor(sh["wavelet"]).to(dev), par, device=dev)
+        data = prob.model(s, keep=True)
+        res = data - torch.as_tensor(sh["d_obs"]).to(dev, torch.complex64)
+        J = 0.5 * float(torch.sum(res.real.double() ** 2 + res.imag.double() ** 2))
+        return J, prob.gradient(res)
+
+    return _shots.objective_and_gradient(costs, work, s, group)
+
+
+class FWIShotsGradient(torch.autograd.Function):
+    """J over many shots spread across the ranks of the process group
+    (``shot_objective_and_gradient``); backward returns the summed dJ/ds.
+    ``FWIShotsGradient.apply(s, shot_list, par)``.  The gradient is computed with
+    the objective (each shot's stored fields are released before the next shot
+    runs) and handed out by backward."""
+
+    @staticmethod
+    def forward(ctx, s, shot_list, par, group=None):
+        J, g = shot_objective_and_gradient(s.detach(), shot_list, par, group=group)
+        ctx.g = g
+        out = torch.tensor(J, dtype=torch.float64, device=s.device)
+        return out.to(s.dtype) if s.is_floating_point() else out
+
+    @staticmethod
+    def backward(ctx, gJ):
+        g = ctx.g
+        ctx.g = None
+        return (gJ * g).to(gJ.dtype), None, None, None

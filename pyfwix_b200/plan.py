@@ -160,6 +160,13 @@ class Plan:
         L.check(self.lib.fwix_smooth_step(self._h, iz, mode, _p(inp), _p(out), int(add), _stream()))
         return out
 
+    def smooth_step_pair(self, iz, inp, out, deriv, add=False):
+        """out (+)= the smooth forward step of inp and deriv (+)= its slowness
+        derivative, from one set of transforms."""
+        self.ensure_workspace(L.WS_STEP)
+        L.check(self.lib.fwix_smooth_step_pair(self._h, iz, _p(inp), _p(out), _p(deriv), int(add), _stream()))
+        return out, deriv
+
     def correlate(self, a, b, out, add=False, padded=True):
         """out (+)= Re sum_{shots, w} conj(a) b, [NY][NX] (padded) or [ny][nx]."""
         L.check(self.lib.fwix_correlate(self._h, _p(a), _p(b), _p(out), int(add), int(padded), _stream()))

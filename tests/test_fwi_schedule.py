@@ -36,7 +36,7 @@ class OraclePlan:
         self.nx, self.ny, self.nw, self.ns, self.nz, self.nref = nx, ny, nw, ns, nz, nref
         self.NX, self.NY = nx + padx, ny + pady
         self.wshape = (ns, nw, self.NY, self.NX)
-        self.calls = {"step": 0}
+        self.calls = {"step": 0, "pair": 0}
 
     def traces(self, cx, cy, cz, ids):
         g = self.g
@@ -66,6 +66,13 @@ class OraclePlan:
         f = {L.SMOOTH_FWD: wem.smooth_forward, L.SMOOTH_ADJ: wem.smooth_adjoint,
              L.SMOOTH_DERIV: wem.smooth_deriv}[mode]
         return _put(out, f(self.g, self.refs[iz], self.sp[iz], _np(inp)))
+
+    def smooth_step_pair(self, iz, inp, out, deriv, add=False):
+        assert not add and out is not deriv
+        self.calls["pair"] += 1
+        x = _np(inp)
+        _put(deriv, wem.smooth_deriv(self.g, self.refs[iz], self.sp[iz], x))
+        return _put(out, wem.smooth_forward(self.g, self.refs[iz], self.sp[iz], x)), deriv
 
     def reflect(self, iz, inp, out, adjoint=False, add=False):
         assert add
@@ -139,8 +146,25 @@ def test_checkpoints_match_every_depth(monkeypatch, k):
     assert _rel(data, data0) < 1e-6
     assert _rel(grad, grad0) < 1e-5
     nz = g.nz
-    assert full.plan.calls["step"] == 6 * nz - 3
-    assert prob.plan.calls["step"] > full.plan.calls["step"]
+    assert full.plan.calls["step"] == 6 * nz - 3 and full.plan.calls["pair"] == 0
+    assert prob.plan.calls["step"] + prob.plan.calls["pair"] > full.plan.calls["step"]
+
+
+def test_checkpointed_step_count(monkeypatch):
+    """With checkpoints every k levels the forward takes about 3 nz steps (down
+    pass, and the up pass recomputing each down segment) and the backward about
+    5 nz: mu alone, then per segment the down fields with their derivatives and
+    the up derivatives as paired steps, the mu fields, and nu."""
+    g, s, refs, geom, wav, par, acq, d_obs = _problem(nz=12)
+    monkeypatch.setattr(fwi, "Plan", OraclePlan)
+    prob = fwi.SmoothFWI(s.shape, geom, torch.from_numpy(wav), dict(par, checkpoint=4), device="cpu")
+    data = prob.model(torch.from_numpy(s), keep=True)
+    fwd = dict(prob.plan.calls)
+    prob.gradient(data - torch.from_numpy(d_obs).to(torch.complex64))
+    bwd = {k: prob.plan.calls[k] - fwd[k] for k in fwd}
+    nz = g.nz
+    assert fwd["pair"] == 0 and fwd["step"] <= 3 * nz
+    assert bwd["step"] + bwd["pair"] <= 5 * nz
 
 
 def test_checkpoint_key():

@@ -56,6 +56,32 @@ def test_smooth_step_modes(nx, ny):
         assert abs(np.vdot(y, fx) / np.vdot(ay, x) - 1) < 1e-5
 
 
+@pytest.mark.parametrize("nx,ny,pad", [(56, 60, 4), (32, 24, 4), (384, 384, 0)])
+def test_smooth_step_pair(nx, ny, pad):
+    """fwix_smooth_step_pair: the forward step into one buffer and its slowness
+    derivative into another from one set of transforms, equal to the two separate
+    steps (register-resident lengths 64 and 384 sum both weightings in one inverse
+    row pass; 36 x 28 runs two generic inverse passes), in and add included."""
+    from pyfwix_b200 import _lib as L
+    from pyfwix_b200.fwi import SmoothFWI
+    g, rng, s, geom, wav, par = _case(nx=nx, ny=ny, nw=3, padx=pad, pady=pad, nz=3)
+    prob = SmoothFWI(s.shape, geom, wav, par)
+    prob.set_slowness(torch.as_tensor(s, dtype=torch.float32))
+    p = prob.plan
+    x = to_dev(crandn(rng, (1, g.nw, g.NY, g.NX)))
+    fwd = p.smooth_step(1, x, torch.empty_like(x))
+    der = p.smooth_step(1, x, torch.empty_like(x), mode=L.SMOOTH_DERIV)
+    out, d = torch.empty_like(x), torch.empty_like(x)
+    p.smooth_step_pair(1, x, out, d)
+    assert rel(to_host(out), to_host(fwd)) < 1e-6 and rel(to_host(d), to_host(der)) < 1e-6
+    y = x.clone()
+    p.smooth_step_pair(1, y, y, d)            # in place on the forward output
+    assert rel(to_host(y), to_host(fwd)) < 1e-6
+    out2, d2 = fwd.clone(), der.clone()
+    p.smooth_step_pair(1, x, out2, d2, add=True)
+    assert rel(to_host(out2), 2 * to_host(fwd)) < 1e-6 and rel(to_host(d2), 2 * to_host(der)) < 1e-6
+
+
 @pytest.mark.parametrize("checkpoint", [None, 2])
 def test_gradient_matches_oracle(checkpoint):
     from pyfwix_b200.fwi import SmoothFWI
