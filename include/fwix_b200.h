@@ -108,6 +108,10 @@ uint64_t fwix_launch_count(void);
 fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** plan);
 fwix_status fwix_plan_destroy(fwix_plan* plan);
 size_t fwix_plan_workspace_bytes(const fwix_plan* plan, int ws_class);
+/* Bounded device-side waits of this plan's kernels that ran out of tries (the
+ * kernel then skipped its work); 0 in normal operation.  Reads device memory
+ * (synchronous). */
+uint64_t fwix_plan_wait_timeouts(const fwix_plan* plan);
 fwix_status fwix_plan_set_workspace(fwix_plan* plan, void* dev_ptr, size_t bytes);
 /* sref: [nz][nref][nw] complex; labels: uint8 label of (iz, iw, y, x) at
  * labels[iz*z_stride + iw*w_stride + y*NX + x] (RefSampler.cpp:27-28, 126-133). */

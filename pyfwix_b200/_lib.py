@@ -58,6 +58,7 @@ SIGNATURES = {
     "fwix_plan_create": [ctypes.POINTER(FwixDesc), ctypes.POINTER(P)],
     "fwix_plan_destroy": [P],
     "fwix_plan_workspace_bytes": [P, I],
+    "fwix_plan_wait_timeouts": [P],
     "fwix_plan_set_workspace": [P, P, ctypes.c_size_t],
     "fwix_plan_set_refs": [P, P, P, I64, I64],
     "fwix_plan_phase_cache_bytes": [P],
@@ -98,7 +99,7 @@ SIGNATURES = {
 SWEEP_DOWN, SWEEP_UP, SWEEP_MODEL, SWEEP_IMAGE, SWEEP_BORN_FWD, SWEEP_BORN_ADJ = range(6)
 _RET = {"fwix_last_error": ctypes.c_char_p, "fwix_version": I, "fwix_plan_workspace_bytes": ctypes.c_size_t,
         "fwix_plan_phase_cache_bytes": ctypes.c_size_t, "fwix_plan_packed_bytes": ctypes.c_size_t,
-        "fwix_launch_count": ctypes.c_uint64}
+        "fwix_launch_count": ctypes.c_uint64, "fwix_plan_wait_timeouts": ctypes.c_uint64}
 
 _lib = None
 

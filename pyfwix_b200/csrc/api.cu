@@ -125,6 +125,8 @@ struct fwix_plan {
   int nterm_max = 1;
   long long chunk = 1;  // slices per launch: the intermediates of one chunk fit in L2
   bool fused = false;   // 256 x 256 slices: one-launch cluster step (fused256.cu), opt-in
+  bool col_tma = false; // column passes with TMA tiles where the plan allows (FWIX_COL_TMA)
+  unsigned* err = nullptr;  // device word: bounded waits of the TMA passes that ran out
   float2* scat_tab = nullptr;     // scatter weights of one depth, [taylor+1][NY][NX]
   const float* sm_s = nullptr;    // smooth step: padded slowness [nz][NY][NX]
   const float* sm_ref = nullptr;  // smooth step: sorted real reference slownesses [nz][nref]
@@ -191,6 +193,8 @@ struct fwix_plan {
     a.b0 = 0;
     a.nb = (long long)d.ns * d.nw;
     a.tstride = chunk * d.slice;
+    a.tma = col_tma ? 1 : 0;
+    a.err = err;
     return a;
   }
 };
@@ -651,6 +655,8 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
     // is slower than the three-launch step at these sizes.
     const char* env = getenv("FWIX_FUSED");
     p->fused = p->d.NX == 256 && p->d.NY == 256 && env && env[0] == '1';
+    const char* tma = getenv("FWIX_COL_TMA");
+    p->col_tma = tma && tma[0] == '1';
   }
   std::vector<float> w2(q.nw), w(q.nw);
   for (int i = 0; i < q.nw; ++i) {
@@ -671,6 +677,8 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
   if (e == cudaSuccess) e = upload(&p->tapy, taper_table(p->d.NY, q.tapery));
   if (e == cudaSuccess)
     e = cudaMalloc((void**)&p->scat_tab, (size_t)(q.taylor + 1) * p->d.slice * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&p->err, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(p->err, 0, sizeof(unsigned));
   if (e != cudaSuccess) {
     fwix_plan_destroy(p);
     return fail(FWIX_ERR_CUDA, std::string("plan tables: ") + cudaGetErrorString(e));
@@ -681,7 +689,7 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
 
 fwix_status fwix_plan_destroy(fwix_plan* p) {
   if (!p) return FWIX_OK;
-  void* ptrs[] = {p->twx, p->twy, p->kx, p->ky, p->w2, p->w, p->tapx, p->tapy, p->scat_tab};
+  void* ptrs[] = {p->twx, p->twy, p->kx, p->ky, p->w2, p->w, p->tapx, p->tapy, p->scat_tab, p->err};
   for (void* v : ptrs)
     if (v) cudaFree(v);
   delete p;
@@ -689,6 +697,13 @@ fwix_status fwix_plan_destroy(fwix_plan* p) {
 }
 
 size_t fwix_plan_workspace_bytes(const fwix_plan* p, int cls) { return p ? p->ws_need(cls) : 0; }
+
+uint64_t fwix_plan_wait_timeouts(const fwix_plan* p) {
+  if (!p || !p->err) return 0;
+  unsigned v = 0;
+  if (cudaMemcpy(&v, p->err, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+  return v;
+}
 
 fwix_status fwix_plan_set_workspace(fwix_plan* p, void* ptr, size_t bytes) {
   if (!p) return fail(FWIX_ERR_INVALID, "null plan");

@@ -25,6 +25,7 @@
 #include <utility>
 
 #include "ops.cuh"
+#include "tma.cuh"
 
 namespace fwix {
 namespace fast {
@@ -754,6 +755,98 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks) k_col_b(co
   tile_to_cols<P>(c.tile, a.t2, a, c.b, c.x0, 0, 1.f);
 }
 
+// t2[0] = F_y^-1(sum_term Q_term * F_y(t1[term])) with the tiles moved by TMA
+// (plans of 16 columns per CTA, 128 bytes per tile row).  Each term's tile
+// arrives in one of two row-major swizzled buffers while the previous term is
+// transformed; once every lane holds its column in registers the buffer serves
+// as the line-exchange scratch (lines of N samples, column-major); the result
+// leaves through a swizzled staging tile and one TMA store per box.  A load
+// that does not complete within the bounded wait counts in *a.err and the CTA
+// leaves without writing.
+template <class P>
+struct ColTma {
+  static constexpr int LX = ColGeo<P>::LX;
+  static constexpr int TILE = P::N * LX;  // samples per tile
+  static constexpr int NBOX = P::N <= 256 ? 1 : (P::N % 2 == 0 && P::N / 2 <= 256 ? 2 : 4);
+  static constexpr int ROWS = P::N / NBOX;  // rows per box (<= 256)
+  static_assert(ROWS * NBOX == P::N && ROWS <= 256, "a tile is a whole number of boxes of at most 256 rows");
+  // two tiles, the twiddles, two mbarriers, and room to align the tiles to 1024 bytes
+  static size_t smem() { return (size_t)2 * TILE * sizeof(float2) + tw_size<P>() * sizeof(float2) + 16 + 1024; }
+};
+
+template <class P, int QM>
+__global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
+    k_col_b_tma(const SpecArgs a, int nxt, const __grid_constant__ CUtensorMap tin,
+                const __grid_constant__ CUtensorMap tout) {
+  using C = ColTma<P>;
+  static_assert(C::LX == 16, "TMA column tiles are 16 columns (128 bytes) wide");
+  extern __shared__ unsigned char smem_raw[];
+  float2* base = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  float2* tiles[2] = {base, base + C::TILE};
+  float2* tw = base + 2 * C::TILE;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + tw_size<P>());
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane / P::T, t = lane % P::T, col = warp * P::G + g;
+  const long long b = blockIdx.x / nxt;  // launch-local slice
+  const int x0 = (int)(blockIdx.x - b * nxt) * C::LX;
+  const int iw = (int)((a.b0 + b) % a.d.nw);
+  const int x = x0 + col;
+  const int xq = x < a.d.NX ? x : 0;
+  const int zstride = (int)(a.tstride / a.d.slice);  // slices per term in t1
+  if (threadIdx.x == 0) {
+    tma::mbar_init(&bar[0], 1);
+    tma::mbar_init(&bar[1], 1);
+    tma::fence_mbar_init();
+  }
+  load_stage_tw<P>(tw, a.twy);
+  __syncthreads();
+  auto issue = [&](int term, int buf) {
+    tma::mbar_expect_tx(&bar[buf], (unsigned)(C::TILE * sizeof(float2)));
+#pragma unroll
+    for (int k = 0; k < C::NBOX; ++k)
+      tma::load_3d(tiles[buf] + k * C::ROWS * C::LX, &tin, x0, k * C::ROWS, term * zstride + (int)b, &bar[buf]);
+  };
+  if (threadIdx.x == 0) issue(0, 0);
+  float2 acc[P::E];
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) acc[e] = make_float2(0.f, 0.f);
+  for (int term = 0; term < a.nterm; ++term) {
+    const int buf = term & 1;
+    if (threadIdx.x == 0 && term + 1 < a.nterm) issue(term + 1, buf ^ 1);
+    float2 q[P::E];
+    col_factors<P, QM>(a, term, iw, xq, t, q);
+    const bool ok = tma::mbar_wait(&bar[buf], (unsigned)(term >> 1) & 1u);
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) {
+        atomicAdd(a.err, 1u);
+        if (term + 1 < a.nterm) tma::mbar_wait(&bar[buf ^ 1], (unsigned)((term + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    float2 v[P::E];
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) v[e] = tiles[buf][tma::sw128(pos_first<P>(t, e), col)];
+    __syncthreads();  // the tile is in registers: its buffer is free for the exchanges
+    fft_fwd<P>(v, t, tw, tiles[buf] + col * P::N);
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) acc[e] = cadd(acc[e], cmul(v[e], q[e]));
+    tma::fence_proxy_async();  // the exchanges precede the next load into this buffer
+    __syncthreads();
+  }
+  // no load is pending: buffer 0 holds the inverse transform's exchanges, buffer 1 the result
+  fft_inv<P>(acc, t, tw, tiles[0] + col * P::N);
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) tiles[1][tma::sw128(pos_first<P>(t, e), col)] = acc[e];
+  tma::fence_proxy_async();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < C::NBOX; ++k) tma::store_3d(&tout, x0, k * C::ROWS, (int)b, tiles[1] + k * C::ROWS * C::LX);
+    tma::store_commit();
+    tma::store_wait_read();
+  }
+}
+
 // out (+)= scale * F_y^{-+1}(in): the column half of a plain 2D transform.
 template <class P, bool INV>
 __global__ void __launch_bounds__(kWarps * 32) k_col_fft(const SpecArgs a, int nxt, const float2* in, float2* out,
@@ -880,8 +973,40 @@ cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+// The TMA form of k_col_b: plans of 16 columns per CTA, an even row pitch (the
+// tensor map's pitch is a multiple of 16 bytes) and a plan whose error word is set.
+template <class P>
+cudaError_t col_type_b_tma(const SpecArgs& a, int qmode, cudaStream_t s) {
+  using C = ColTma<P>;
+  const int nxt = (a.d.NX + C::LX - 1) / C::LX;
+  const unsigned grid = (unsigned)(a.nb * nxt);
+  const size_t sm = C::smem();
+  CUtensorMap tin, tout;
+  cudaError_t e = tile_map(&tin, a.t1, a.d.NX, a.d.NY, (a.tstride / a.d.slice) * a.nterm, C::ROWS);
+  if (e == cudaSuccess) e = tile_map(&tout, a.t2, a.d.NX, a.d.NY, a.nb, C::ROWS);
+  if (e != cudaSuccess) return e;
+#define FWIX_FAST_CBT(Q)                                                                  \
+  case Q:                                                                                 \
+    e = opt_in_smem(k_col_b_tma<P, Q>, sm);                                               \
+    if (e == cudaSuccess) k_col_b_tma<P, Q><<<grid, kWarps * 32, sm, s>>>(a, nxt, tin, tout); \
+    break;
+  switch (qmode) {
+    FWIX_FAST_CBT(Q_PS_FWD)
+    FWIX_FAST_CBT(Q_PS_ADJ)
+    FWIX_FAST_CBT(Q_KPOW)
+    FWIX_FAST_CBT(Q_ONE)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_FAST_CBT
+  if (e == cudaSuccess) count_launch();
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 template <class P>
 cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s) {
+  if constexpr (ColGeo<P>::LX == 16) {
+    if (a.tma && a.err && a.d.NX % 2 == 0) return col_type_b_tma<P>(a, qmode, s);
+  }
   const int nxt = (a.d.NX + ColGeo<P>::LX - 1) / ColGeo<P>::LX;
   const unsigned grid = (unsigned)(a.nb * nxt);
   const size_t sm = ColGeo<P>::smem2();

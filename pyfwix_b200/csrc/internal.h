@@ -113,6 +113,10 @@ struct SpecArgs {
   float2* t1;
   float2* t2;
   long long b0, nb, tstride;
+  // column passes: move the tiles with TMA where the plan allows (tma != 0); a
+  // bounded wait that runs out adds one to *err (the plan's error word)
+  int tma;
+  unsigned* err;
 };
 
 // Spectral passes (dispatch.cu: register-resident passes for lengths with a

@@ -89,7 +89,8 @@ def test_null_plan_is_rejected_by_every_entry_point():
     functions accept null like free()."""
     from pyfwix_b200 import _lib
     lib = _lib.load()
-    sized = {"fwix_plan_workspace_bytes", "fwix_plan_phase_cache_bytes", "fwix_plan_packed_bytes"}
+    sized = {"fwix_plan_workspace_bytes", "fwix_plan_phase_cache_bytes", "fwix_plan_packed_bytes",
+             "fwix_plan_wait_timeouts"}
     for name, args in sorted(_lib.SIGNATURES.items()):
         if not args or args[0] is not _lib.P:
             continue
