@@ -51,10 +51,13 @@ def args_():
     ap.add_argument("--config", default="config2")
     ap.add_argument("--nz", type=int, default=None, help="override depth count (quick runs only)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-per-w", type=int, default=1,
+                    help="also time e2e with the per-frequency model domain when host memory allows (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fwi", action="store_true", help="skip the FWI-gradient timing")
     ap.add_argument("--fwi-nz", type=int, default=None, help="depth levels of the FWI workload (quick runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched forward+imaging timing")
+    ap.add_argument("--no-config1", action="store_true", help="skip the plain modelling + imaging timing")
     ap.add_argument("--no-packed", action="store_true", help="skip the packed-background Born timing")
     ap.add_argument("--large", action="store_true",
                     help="run only the 512 x 512 x 400 x 200 Born on packed storage and print its own line")
@@ -200,19 +203,68 @@ def born_packed_timing(st, w, steps=2):
     return out
 
 
-def born_step_e2e(st, host):
-    """Same step through the public API with host buffers: the perturbation goes in
-    from pinned host memory, the data comes back, goes in again for the adjoint,
-    and the gradient comes back."""
-    p = st["plan"]
-    st["dslow"].copy_(host["dslow"], non_blocking=True)
-    st["dden"].copy_(host["dden"], non_blocking=True)
-    p.born(st["rec"], st["bd"], st["bu"], st["dslow"], st["dden"], st["data"])
-    host["data"].copy_(st["data"], non_blocking=True)
-    st["data"].copy_(host["data"], non_blocking=True)
-    p.born(st["rec"], st["bd"], st["bu"], st["gs"], st["gr"], st["data"], adjoint=True)
-    host["gs"].copy_(st["gs"], non_blocking=True)
-    host["gr"].copy_(st["gr"], non_blocking=True)
+def setup_surface(w, device, per_w=False, pinned=True):
+    """The Born workload through the drop-in surface: ``pyfwix_b200.CudaWEM``'s
+    ``Propagator`` and ``ExtendedBorn``, the classes and calls of
+    ``fwix/workers.py:62-76`` (``prop.forward(False, model, res)``,
+    ``born.forward / adjoint(False, model, data)``), with every caller array a
+    numpy array in host memory (pinned, or pageable with ``pinned=False``).  The
+    background model is frequency-independent ([nz][1][ny][nx], one value per
+    cell for every frequency, as the configuration's model is); the Born model
+    domain is that too, or with ``per_w`` the reference's per-frequency domain
+    [nz][nw][ny][nx].  The backgrounds are modelled here, untimed."""
+    import torch
+
+    from pyfwix_b200 import CudaWEM
+
+    def host(shape):
+        if pinned:
+            return torch.empty(shape, dtype=torch.complex64, pin_memory=True).numpy()
+        return np.empty(shape, np.complex64)
+
+    s2 = host((w.nz, 1, w.ny, w.nx))
+    s2[...] = w.slow2[:, None]
+    den = host(s2.shape)
+    den[...] = 1.0
+    g = w.geom
+    ntr = len(g["rx"])
+    data = host((ntr, w.nw))
+    par = dict(nref=w.nref, padx=w.padx, pady=w.pady, taperx=w.taperx, tapery=w.tapery, eps=w.eps,
+               eps_scat=w.eps_scat, taylor=w.taylor, step=w.step, ox=w.ox, dx=w.dx, oy=w.oy, dy=w.dy, oz=w.oz,
+               dz=w.dz, ow=w.ow, dw=w.dw)
+    model = [s2, den]
+    prop = CudaWEM.Propagator(model, data, w.wavelet, par, g)
+    prop.forward(False, model, data)
+    nwm = w.nw if per_w else 1
+    ds, dr = host((w.nz, nwm, w.ny, w.nx)), host((w.nz, nwm, w.ny, w.nx))
+    ds[...] = w.dslow[:, None]
+    dr[...] = 0.0
+    gs, gr = host(ds.shape), host(ds.shape)
+    born = CudaWEM.ExtendedBorn([ds, dr], data, model, prop)
+    torch.cuda.synchronize()
+    return dict(prop=prop, born=born, dm=[ds, dr], g=[gs, gr], data=data)
+
+
+def born_step_e2e(su):
+    """One Born forward + adjoint step through the surface with host arrays: the
+    perturbation goes in, the Born data come back, go in again for the adjoint,
+    and the gradient comes back (``fwix/workers.py:66-76``)."""
+    su["born"].forward(False, su["dm"], su["data"])
+    su["born"].adjoint(False, su["g"], su["data"])
+
+
+def e2e_bytes(su):
+    nb = lambda a: a.size * a.itemsize
+    return {"h2d_bytes_per_step": nb(su["dm"][0]) + nb(su["dm"][1]) + nb(su["data"]),
+            "d2h_bytes_per_step": nb(su["data"]) + nb(su["g"][0]) + nb(su["g"][1])}
+
+
+def _host_available():
+    try:
+        import psutil
+        return psutil.virtual_memory().available
+    except Exception:
+        return 0
 
 
 def time_steps(fn, k, barrier):
@@ -289,6 +341,75 @@ def fwi_gradient_timing(device, nz=None, checkpoint="auto"):
             "s_per_shot": t_fwd + t_bwd, "forward_s_per_shot": t_fwd, "gradient_s_per_shot": t_bwd,
             "grad_over_forward": (t_fwd + t_bwd) / t_fwd, "checkpoint": FWIGradient.last_storage,
             "forward_gcell_steps_per_s": 2 * cells / t_fwd / 1e9, "objective": float(J.detach())}
+
+
+def fwi_shots_timing(device, ws, rank, barrier, nz=None):
+    """The FWI objective and gradient over ``ws`` shots of the 384 x 384 x 300
+    workload, one shot per rank, through the product's multi-shot entry point
+    (``fwi.shot_objective_and_gradient``: shots partitioned across the ranks,
+    each rank modelling and differentiating its own, one all-reduce of J and the
+    gradient); each rank's observed data are modelled first in the true model
+    (untimed).  Seconds for the whole call, max over ranks."""
+    import torch
+
+    from pyfwix_b200 import workloads
+    from pyfwix_b200.fwi import SmoothFWI, shot_objective_and_gradient
+    w, s_true, s0 = workloads.config4(nz=nz)
+    par = dict(nref=w.nref, padx=0, pady=0, taperx=w.taperx, tapery=w.tapery, eps=0.0, ox=w.ox, oy=w.oy,
+               oz=w.oz, dx=w.dx, dy=w.dy, dz=w.dz, ow=w.ow, dw=w.dw, checkpoint="auto")
+    wav = torch.as_tensor(w.wavelet).to(device)
+    shot_list = [dict(geometry=workloads.config4_geometry(w, r % 8), wavelet=wav, d_obs=None) for r in range(ws)]
+    prob = SmoothFWI(s_true.shape, shot_list[rank]["geometry"], wav, dict(par, checkpoint=None), device=device)
+    shot_list[rank]["d_obs"] = prob.model(torch.as_tensor(s_true), keep=False)
+    par["refs"] = prob.refs.clone()
+    del prob
+    torch.cuda.empty_cache()
+    s = torch.as_tensor(s0, device=device)
+    shot_objective_and_gradient(s, shot_list, par)      # warm-up (allocator, plan tables)
+    t = time_steps(lambda: shot_objective_and_gradient(s, shot_list, par), 1, barrier)
+    return {"workload": w.name + ("" if nz is None else f" (nz={w.nz})") + f", {ws} shots, one per rank",
+            "api": "pyfwix_b200.fwi.shot_objective_and_gradient (one all-reduce of J and dJ/ds)",
+            "shots": ws, "s": t}
+
+
+def config1_timing(device, reps=10):
+    """Plain PSPI forward modelling + imaging of the first configuration (one shot,
+    128 x 128 x 100, 64 frequencies 2-30 Hz, nref 4 quantile references, taper 20,
+    15 Hz Ricker at the surface centre, receivers on every surface node):
+    ``fwix_propagate`` (down pass with injection and recording, reflection, up
+    pass with recording) and then ``fwix_migrate`` of the modelled data (source
+    and receiver fields continued in lockstep, image summed over frequency at
+    every level), each timed with CUDA events over ``reps`` runs after a warm-up
+    run.  Cell-steps count both continued wavefields of each sweep."""
+    import torch
+
+    from pyfwix_b200 import refsampler, workloads
+    from pyfwix_b200.plan import Plan
+    w = workloads.config1()
+    plan = Plan(ns=1, device=device, **w.plan_kwargs())
+    s2 = torch.as_tensor(w.slow2)[:, None].to(device)
+    sref, labels = refsampler.sample(s2, w.nref, w.padx, w.pady)
+    plan.set_refs(refsampler.expand_refs(sref, w.nw), labels)
+    s2c = s2.to(torch.complex64)
+    plan.set_model(s2c, torch.ones_like(s2c))
+    g = w.geom
+    src = plan.traces(g["sx"], g["sy"], g["sz"], np.zeros(len(g["sx"]), np.int32))
+    rec = plan.traces(g["rx"], g["ry"], g["rz"], np.zeros(len(g["rx"]), np.int32))
+    wav = torch.as_tensor(w.wavelet).to(device)
+    bd = torch.empty((w.nz,) + plan.wshape, dtype=torch.complex64, device=device)
+    data = torch.empty((len(g["rx"]), w.nw), dtype=torch.complex64, device=device)
+    img = torch.zeros((w.nz, w.ny, w.nx), dtype=torch.float32, device=device)
+    model = lambda: plan.propagate(src, rec, wav, data, bd, None)
+    image = lambda: plan.migrate(src, rec, wav, data, img)
+    model()
+    image()
+    t_model = time_steps(model, reps, lambda: None) / reps
+    t_image = time_steps(image, reps, lambda: None) / reps
+    cells = w.nx * w.ny * w.nw * w.nz
+    return {"workload": w.name, "modelling_ms": t_model * 1e3, "imaging_ms": t_image * 1e3,
+            "modelling_gcell_steps_per_s": 2 * cells / t_model / 1e9,
+            "imaging_gcell_steps_per_s": 2 * cells / t_image / 1e9,
+            "modelling_plus_imaging_gcell_steps_per_s": 4 * cells / (t_model + t_image) / 1e9}
 
 
 def batched_timing(device, nshots=32, nz=None, nstreams=8):
@@ -575,23 +696,6 @@ def main():
         t = float(tt.item())
     cells = 2 * w.nx * w.ny * w.nw * w.nz
     value = ws * cells * a.steps / t / 1e9
-    # end to end through the host buffers
-    e2e = None
-    if not a.no_e2e:
-        host = {k: torch.empty(st[k].shape, dtype=st[k].dtype, pin_memory=True)
-                for k in ("dslow", "dden", "gs", "gr", "data")}
-        host["dslow"].copy_(st["dslow"].cpu())
-        host["dden"].zero_()
-        born_step_e2e(st, host)
-        te = time_steps(lambda: born_step_e2e(st, host), a.steps, barrier)
-        if ws > 1:
-            tt = torch.tensor([te], device=device)
-            tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
-            te = float(tt.item())
-        nb = lambda k: host[k].numel() * host[k].element_size()
-        e2e = {"value": ws * cells * a.steps / te / 1e9, "unit": "Gcell-steps/s",
-               "h2d_bytes_per_step": nb("dslow") + nb("dden") + nb("data"),
-               "d2h_bytes_per_step": nb("data") + nb("gs") + nb("gr")}
     # roofline of the depth step
     tstep = step_roofline(st, w)
     cells_step = w.nx * w.ny * w.nw
@@ -617,12 +721,56 @@ def main():
     fwi = batched = None
     del st
     torch.cuda.empty_cache()
+    # end to end through the drop-in surface with host arrays
+    e2e = None
+    if not a.no_e2e:
+        def reduce_max(te):
+            if ws > 1:
+                tt = torch.tensor([te], device=device)
+                tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+                te = float(tt.item())
+            return te
+        su = setup_surface(w, device)
+        born_step_e2e(su)
+        te = reduce_max(time_steps(lambda: born_step_e2e(su), a.steps, barrier))
+        e2e = {"value": ws * cells * a.steps / te / 1e9, "unit": "Gcell-steps/s", **e2e_bytes(su),
+               "api": "pyfwix_b200.CudaWEM.ExtendedBorn forward + adjoint (False, model, data), numpy arrays "
+                      "in pinned host memory",
+               "model_layout": "[nz][1][ny][nx]: one perturbation per cell for every frequency (the "
+                               "configuration's reflectivity is frequency-independent)"}
+        del su
+        torch.cuda.empty_cache()
+        # the reference's per-frequency model domain [nz][nw][ny][nx] (13.4 GB per
+        # component at this size), pageable numpy arrays as a caller passes them;
+        # two steps, and only where the host has the memory for the four arrays
+        need = 4 * w.nz * w.nw * w.ny * w.nx * 8
+        if a.e2e_per_w and _host_available() > 2.5 * need:
+            su = setup_surface(w, device, per_w=True, pinned=False)
+            born_step_e2e(su)
+            k = 2
+            te = reduce_max(time_steps(lambda: born_step_e2e(su), k, barrier))
+            e2e["per_frequency_model"] = {
+                "value": ws * cells * k / te / 1e9, "unit": "Gcell-steps/s", "steps": k, **e2e_bytes(su),
+                "model_layout": "[nz][nw][ny][nx] (the reference's ExtendedBorn domain), pageable numpy arrays"}
+            del su
+            torch.cuda.empty_cache()
+        elif a.e2e_per_w:
+            e2e["per_frequency_model"] = {"skipped": f"host memory: {_host_available() / 1e9:.0f} GB available, "
+                                                     f"{2.5 * need / 1e9:.0f} GB wanted"}
     if not a.no_fwi:
         fwi = fwi_gradient_timing(device, nz=a.fwi_nz)
         # the configuration's depth checkpoints (every 16th level, segments recomputed)
         k16 = fwi_gradient_timing(device, nz=a.fwi_nz, checkpoint=16)
         fwi["checkpoint_16"] = {k: k16[k] for k in ("s_per_shot", "forward_s_per_shot", "gradient_s_per_shot",
                                                     "grad_over_forward", "checkpoint")}
+        sh = fwi_shots_timing(device, ws, rank, barrier, nz=a.fwi_nz)
+        if ws > 1:
+            tt = torch.tensor([sh["s"]], device=device)
+            tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+            sh["s"] = float(tt.item())
+        sh["shots_per_s"] = ws / sh["s"]
+        fwi["shots_across_ranks"] = sh
+    config1 = config1_timing(device) if not a.no_config1 else None
     if ws == 1 and not a.no_batched:
         batched = batched_timing(device, nshots=a.batched_shots, nz=a.batched_nz, nstreams=a.batched_streams)
     cpu = None
@@ -637,7 +785,7 @@ def main():
                            "l2": "inputs larger than L2 (background wavefields 2 x %.1f GB)"
                                  % bg_gb},
                 "gpu_launches": launches, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "fwi_grad": fwi, "batched": batched, "born_packed_backgrounds": packed}
+                "fwi_grad": fwi, "batched": batched, "born_packed_backgrounds": packed, "config1": config1}
         print(json.dumps(line), flush=True)
     if ws > 1:
         tdist.destroy_process_group()

@@ -212,4 +212,231 @@ int refshim_pspi_forward_timed(int NX, int NY, int nw, int ns, int nref, const f
   return done();
 }
 
+// ---------------------------------------------------------------------------
+// Whole-shot sweeps with the reference's kernels and cuFFT, composed as the
+// reference composes them, for the "plain per-shot GPU path" comparison:
+//   PSPI in-place forward  (propagator/src/PSPI.cpp:66-83): taper -> FFT -> per
+//     reference: phase shift into a zeroed buffer -> inverse FFT -> select-add;
+//   PSPI in-place adjoint  (propagator/src/PSPI.cpp:85-103): per reference:
+//     select into a zeroed buffer -> FFT -> adjoint phase shift added -> then
+//     inverse FFT -> taper;
+//   modelling (propagator/src/Propagator.cpp:121-221): down pass inject source,
+//     record, keep the field, step; up pass step, reflect the kept down field,
+//     record;
+//   migration: the source field of the down pass and the receiver field of the
+//     back-scattering adjoint (propagator/src/ExtendedBorn.cpp:391-453: inject
+//     the data, imaging condition ic_adj, adjoint step) continued in lockstep.
+// Launch shapes are the reference operators' (grid {32,4,4} x block {16,16,4}
+// for taper / phase shift / imaging, Reflect's grid over (x, y, w*s) with
+// 16x16x4 blocks, Injection's (nw/16, ntrace/16) x 16x16, Selector's 256-thread
+// blocks over every sample).  Differences, stated: the kept down fields stay
+// in device memory (the reference ZFP-compresses and copies them to the host,
+// propagator/src/WavefieldPool.cpp); the per-depth host-to-device copies of
+// labels and reference slownesses (Selector.h set_labels, PhaseShift.h
+// set_slow) are replaced by a device expansion of one depth's labels to every
+// frequency; the plans have no store callback, so the 1/(NX NY) of the unitary
+// transform pair (operator/src/fft_callback.cu:7-12) is one scaling pass over
+// the step's output; the migration sums its per-frequency image over
+// frequency into the float image once per level (k_sum_w).  All but the last
+// two make the reference path faster than it is; the scaling pass and the sum
+// are one read and write of a wavefield and of an image per level.
+}  // extern "C"
+
+namespace {
+
+__global__ void k_scale(cuFloatComplex* x, long long n, float s) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = make_cuFloatComplex(cuCrealf(x[i]) * s, cuCimagf(x[i]) * s);
+}
+
+__global__ void k_expand_labels(const int* lab, int* out, long long plane, int nw) {
+  const long long n = plane * nw;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = lab[i % plane];
+}
+
+// img[y][x] += sum_w Re img_w[w][y][x]
+__global__ void k_sum_w(const cuFloatComplex* img_w, float* img, int nw, long long plane) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+    float acc = 0.f;
+    for (int w = 0; w < nw; ++w) acc += cuCrealf(img_w[(long long)w * plane + i]);
+    img[i] += acc;
+  }
+}
+
+struct Shot {
+  int NX, NY, nx, ny, nw, nref, nz, tapx, tapy;
+  float dz, eps;
+  const float *w2, *kx, *ky;
+  const cuFloatComplex* sref;  // [nz][nref][nw]
+  const int* labels;           // [nz][NY][NX]
+  int* labw;                   // [nw][NY][NX] scratch
+  long long n;                 // NX NY nw
+  size_t bytes;
+  cufftHandle plan = 0;
+  dim3 g{32, 4, 4}, b{16, 16, 4};
+  unsigned sel_grid = 1;
+  Header *K = nullptr, *W = nullptr;
+
+  int init(void* model_k, void* wfld_ref) {
+    n = (long long)NX * NY * nw;
+    bytes = (size_t)n * sizeof(cuFloatComplex);
+    int dims[2] = {NY, NX};
+    if (cufftPlanMany(&plan, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nw) != CUFFT_SUCCESS) return -1;
+    sel_grid = (unsigned)((n + 255) / 256);
+    K = new Header(model_k, {NX, NY, nw, 1});
+    W = new Header(wfld_ref, {NX, NY, nw, 1});
+    return 0;
+  }
+  ~Shot() {
+    delete K;
+    delete W;
+    if (plan) cufftDestroy(plan);
+  }
+  void labels_at(int iz) {
+    k_expand_labels<<<1184, 256>>>(labels + (long long)iz * NX * NY, labw, (long long)NX * NY, nw);
+  }
+  const cuFloatComplex* refs(int iz, int r) const { return sref + ((long long)iz * nref + r) * nw; }
+  void scale(Header& X) { k_scale<<<1184, 256>>>(X.v->mat, n, 1.f / ((float)NX * (float)NY)); }
+  // PSPI::cu_forward(model) in place on X
+  void fwd(int iz, Header& X) {
+    labels_at(iz);
+    cudaMemsetAsync(K->v->mat, 0, bytes);
+    taper_forward<<<g, b>>>(X.v, K->v, tapx, tapy);
+    cufftExecC2C(plan, K->v->mat, K->v->mat, CUFFT_FORWARD);
+    cudaMemsetAsync(X.v->mat, 0, bytes);
+    for (int r = 0; r < nref; ++r) {
+      cudaMemsetAsync(W->v->mat, 0, bytes);
+      ps_forward<<<g, b>>>(K->v, W->v, w2, kx, ky, refs(iz, r), dz, eps);
+      cufftExecC2C(plan, W->v->mat, W->v->mat, CUFFT_INVERSE);
+      select_forward<<<sel_grid, 256>>>(W->v, X.v, r, labw);
+    }
+    scale(X);
+  }
+  // PSPI::cu_adjoint(data) in place on X
+  void adj(int iz, Header& X) {
+    labels_at(iz);
+    cudaMemsetAsync(K->v->mat, 0, bytes);
+    for (int r = 0; r < nref; ++r) {
+      cudaMemsetAsync(W->v->mat, 0, bytes);
+      select_forward<<<sel_grid, 256>>>(X.v, W->v, r, labw);
+      cufftExecC2C(plan, W->v->mat, W->v->mat, CUFFT_FORWARD);
+      ps_adjoint<<<g, b>>>(K->v, W->v, w2, kx, ky, refs(iz, r), dz, eps);
+    }
+    cufftExecC2C(plan, K->v->mat, K->v->mat, CUFFT_INVERSE);
+    cudaMemsetAsync(X.v->mat, 0, bytes);
+    taper_forward<<<g, b>>>(K->v, X.v, tapx, tapy);
+    scale(X);
+  }
+};
+
+struct Traces {
+  int n;
+  const float *cx, *cy, *cz;
+  const int* ids;
+  Header* h;
+};
+
+template <class F>
+int timed(F run, int reps, float* ms) {
+  run();
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaDeviceSynchronize();
+  cudaEventRecord(e0);
+  for (int i = 0; i < reps; ++i) run();
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  *ms = t / (float)(reps > 0 ? reps : 1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return done();
+}
+
+}  // namespace
+
+extern "C" {
+
+// One shot (ns = 1, no padding: NX = nx, NY = ny).  task 0: modelling, data
+// [ntrace][nw] recorded, the down field of every level kept in keep [nz][nw][NY][NX];
+// slow2 / den2 are the per-frequency model with one level more,
+// [nz + 1][nw][ny][nx], level nz a copy of level nz - 1 (the reference's bottom
+// reflection pairs the last level with itself, propagator/src/Reflect.h:20-38),
+// so that levels (iz, iz + 1) are the pair each reflection reads.  task 1:
+// lockstep migration of `data`, image [nz][ny][nx] (float); img_w [nw][ny][nx]
+// scratch.  S, R, model_k, wfld_ref: wavefield
+// scratch [nw][NY][NX].  One warm-up run, then `reps` runs between CUDA events
+// (the image / data are zeroed before each run); *ms receives the mean time.
+int refshim_shot_timed(int task, int NX, int NY, int nw, int nz, int nref, const float* w2, const float* kx,
+                       const float* ky, const void* sref, const int* labels, int* labw, float dz, float eps, int tapx,
+                       int tapy, float ox, float oy, float oz, float dx, float dy, int nsrc, const float* scx,
+                       const float* scy, const float* scz, const int* sids, const void* wavelet, int ntrace,
+                       const float* rcx, const float* rcy, const float* rcz, const int* rids, void* data,
+                       const void* slow2, const void* den2, void* keep, float* image, void* img_w, void* S,
+                       void* R, void* model_k, void* wfld_ref, int reps, float* ms) {
+  Shot sh;
+  sh.NX = NX, sh.NY = NY, sh.nx = NX, sh.ny = NY, sh.nw = nw, sh.nref = nref, sh.nz = nz, sh.tapx = tapx;
+  sh.tapy = tapy, sh.dz = dz, sh.eps = eps, sh.w2 = w2, sh.kx = kx, sh.ky = ky;
+  sh.sref = (const cuFloatComplex*)sref, sh.labels = labels, sh.labw = labw;
+  if (sh.init(model_k, wfld_ref) != 0) return -1;
+  const std::vector<float> o4 = {ox, oy, 0.f, 0.f}, d4 = {dx, dy, 1.f, 1.f};
+  Header hS(S, {NX, NY, nw, 1}, o4, d4), hR(R, {NX, NY, nw, 1}, o4, d4);
+  Header wav(wavelet, {nw, nsrc}), dat(data, {nw, ntrace});
+  const dim3 gs((nw + 15) / 16, (nsrc + 15) / 16), gr((nw + 15) / 16, (ntrace + 15) / 16), b2(16, 16);
+  const size_t fb = sh.bytes;
+  const long long plane = (long long)NX * NY;
+  if (task == 0) {
+    // per-level views of the kept fields and of the model's level pairs
+    std::vector<Header*> kept, sl, dn;
+    for (int iz = 0; iz < nz; ++iz) {
+      kept.push_back(new Header((char*)keep + (size_t)iz * fb, {NX, NY, nw, 1}));
+      sl.push_back(new Header((const char*)slow2 + (size_t)iz * fb, {NX, NY, nw, 2}));
+      dn.push_back(new Header((const char*)den2 + (size_t)iz * fb, {NX, NY, nw, 2}));
+    }
+    const dim3 rg((NX + 15) / 16, (NY + 15) / 16, (nw + 3) / 4), rb(16, 16, 4);
+    auto run = [&]() {
+      cudaMemsetAsync(data, 0, (size_t)ntrace * nw * sizeof(cuFloatComplex));
+      cudaMemsetAsync(S, 0, fb);
+      for (int iz = 0; iz < nz; ++iz) {
+        inj_forward<<<gs, b2>>>(wav.v, hS.v, scx, scy, scz, sids, oz, dz, iz);
+        inj_adjoint<<<gr, b2>>>(dat.v, hS.v, rcx, rcy, rcz, rids, oz, dz, iz);
+        cudaMemcpyAsync(kept[iz]->v->mat, S, fb, cudaMemcpyDeviceToDevice);
+        sh.fwd(iz, hS);
+      }
+      cudaMemsetAsync(R, 0, fb);
+      for (int iz = nz - 1; iz >= 0; --iz) {
+        sh.fwd(iz, hR);
+        refl_forward<<<rg, rb>>>(kept[iz]->v, hR.v, sl[iz]->v, dn[iz]->v);
+        inj_adjoint<<<gr, b2>>>(dat.v, hR.v, rcx, rcy, rcz, rids, oz, dz, iz);
+      }
+    };
+    const int st = timed(run, reps, ms);
+    for (auto* h : kept) delete h;
+    for (auto* h : sl) delete h;
+    for (auto* h : dn) delete h;
+    return st;
+  }
+  Header img(img_w, {NX, NY, nw});
+  auto run = [&]() {
+    cudaMemsetAsync(image, 0, (size_t)nz * plane * sizeof(float));
+    cudaMemsetAsync(S, 0, fb);
+    cudaMemsetAsync(R, 0, fb);
+    for (int iz = 0; iz < nz; ++iz) {
+      inj_forward<<<gs, b2>>>(wav.v, hS.v, scx, scy, scz, sids, oz, dz, iz);
+      inj_forward<<<gr, b2>>>(dat.v, hR.v, rcx, rcy, rcz, rids, oz, dz, iz);
+      cudaMemsetAsync(img_w, 0, (size_t)plane * nw * sizeof(cuFloatComplex));
+      ic_adj<<<sh.g, sh.b>>>(img.v, hR.v, hS.v);
+      k_sum_w<<<(unsigned)((plane + 255) / 256), 256>>>((const cuFloatComplex*)img_w, image + iz * plane, nw, plane);
+      if (iz < nz - 1) {
+        sh.fwd(iz, hS);
+        sh.adj(iz, hR);
+      }
+    }
+  };
+  return timed(run, reps, ms);
+}
+
 }  // extern "C"

@@ -116,7 +116,11 @@ def _store(dst, t):
         if raw.data_ptr() != t.data_ptr() or raw.device != t.device:
             raw.copy_(t.reshape(raw.shape))
     elif isinstance(raw, np.ndarray):
-        np.copyto(raw, t.reshape(raw.shape).cpu().numpy().astype(raw.dtype, copy=False))
+        src = t.reshape(raw.shape)
+        if raw.dtype == np.complex64 and raw.flags.c_contiguous and raw.flags.writeable:
+            torch.from_numpy(raw).copy_(src)   # one device-to-host copy into the caller's array
+        else:
+            np.copyto(raw, src.cpu().numpy().astype(raw.dtype, copy=False))
     else:
         raise TypeError(f"cannot write a result into {type(dst).__name__}")
 

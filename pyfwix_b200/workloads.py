@@ -159,12 +159,19 @@ def config4(nz=None, shot=0, seed=1003):
     s_true = (1.0 / (v0 * (1 + pert))).astype(np.float32)
     s0 = (1.0 / v0).astype(np.float32)
     src = rng.uniform(0.1, 0.9, size=(8, 2)) * np.array([w.nx * w.dx, w.ny * w.dy])
-    sx, sy = src[shot]
-    w.geom = dict(sx=np.array([sx], np.float32), sy=np.array([sy], np.float32), sz=np.array([0.0], np.float32),
-                  s_ids=np.array([0], np.int32), **w.surface_receivers())
+    w.sources = src                      # the eight seeded source positions (x, y)
+    w.geom = config4_geometry(w, shot)
     w.wavelet = ricker_spectrum(w.freqs)[None, :].astype(np.complex64)
     w.slow2 = s0 ** 2
     return w, s_true, s0
+
+
+def config4_geometry(w, shot):
+    """Geometry of shot ``shot`` (0-7) of the FWI workload: its source on the
+    surface, receivers on every surface node."""
+    sx, sy = w.sources[shot]
+    return dict(sx=np.array([sx], np.float32), sy=np.array([sy], np.float32), sz=np.array([w.oz], np.float32),
+                s_ids=np.array([0], np.int32), **w.surface_receivers())
 
 
 def config3(nshots=32, nz=None, seed=1002):
