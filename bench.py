@@ -40,6 +40,7 @@ sys.path.insert(0, ROOT)
 METRIC = "Gcell-steps/s (x*y*w*z), Born forward + adjoint"
 HBM_FALLBACK_GBS = 6650.0
 ALG_BYTES_PER_CELL_STEP = 16  # one wavefield read + written once per depth step
+TRAFFIC_PROFILE = "nsps_step_256x256x128.txt"  # DRAM bytes per step of the timed step's kernels (ncu)
 
 
 def args_():
@@ -155,6 +156,7 @@ def setup_born(w, device):
     plan.set_refs(refsampler.expand_refs(sref, w.nw), labels)
     s2c = s2.to(torch.complex64)
     plan.set_model(s2c, torch.ones_like(s2c))
+    tuning = plan.autotune()      # the fastest equivalent form of this plan's depth step
     g = w.geom
     src = plan.traces(g["sx"], g["sy"], g["sz"], np.zeros(len(g["sx"]), np.int32))
     rec = plan.traces(g["rx"], g["ry"], g["rz"], np.zeros(len(g["rx"]), np.int32))
@@ -169,7 +171,7 @@ def setup_born(w, device):
     gr = torch.empty_like(dslow)
     plan.ensure_workspace(2)
     torch.cuda.synchronize()
-    return dict(plan=plan, rec=rec, bd=bd, bu=bu, data=data, dslow=dslow, dden=dden, gs=gs, gr=gr)
+    return dict(plan=plan, rec=rec, bd=bd, bu=bu, data=data, dslow=dslow, dden=dden, gs=gs, gr=gr, tuning=tuning)
 
 
 def born_step(st):
@@ -392,6 +394,7 @@ def config1_timing(device, reps=10):
     plan.set_refs(refsampler.expand_refs(sref, w.nw), labels)
     s2c = s2.to(torch.complex64)
     plan.set_model(s2c, torch.ones_like(s2c))
+    tuning = plan.autotune()      # the fastest equivalent form of this plan's depth step
     g = w.geom
     src = plan.traces(g["sx"], g["sy"], g["sz"], np.zeros(len(g["sx"]), np.int32))
     rec = plan.traces(g["rx"], g["ry"], g["rz"], np.zeros(len(g["rx"]), np.int32))
@@ -701,9 +704,12 @@ def main():
     cells_step = w.nx * w.ny * w.nw
     peak, peak_kind = measured_peak()
     achieved = ALG_BYTES_PER_CELL_STEP * cells_step / tstep / 1e9
-    traffic = profiled_traffic("nsps_step_256x256x128.txt") if (w.nx, w.nw) == (256, 128) else None
+    traffic = profiled_traffic(TRAFFIC_PROFILE) if (w.nx, w.nw) == (256, 128) else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": peak_kind,
+            "traffic_source": ("profiles/" + TRAFFIC_PROFILE + ": ncu DRAM bytes of the same step's launches, "
+                               "captured separately (a profiler cannot run inside the timed bench)")
+            if traffic is not None else None,
             "kernel": "NSPS depth step (row pass + column pass + row pass), 256x256x128",
             "step_ms": tstep * 1e3, "alg_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP}
     # the FP32 arithmetic the same step needs (the bound that applies: nref + 1
@@ -717,6 +723,7 @@ def main():
     roof["fp32"] = {"flop_per_cell_step": flop, "achieved_tflops": fp32, "peak_tflops": fp32_peak,
                     "frac": fp32 / fp32_peak, "peak_source": f"nominal at the sampled {mhz:.0f} MHz"}
     bg_gb = st["bd"].numel() * 8 / 1e9
+    tuning = st["tuning"]
     packed = born_packed_timing(st, w) if not a.no_packed else None
     fwi = batched = None
     del st
@@ -785,7 +792,8 @@ def main():
                            "l2": "inputs larger than L2 (background wavefields 2 x %.1f GB)"
                                  % bg_gb},
                 "gpu_launches": launches, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "fwi_grad": fwi, "batched": batched, "born_packed_backgrounds": packed, "config1": config1}
+                "fwi_grad": fwi, "batched": batched, "born_packed_backgrounds": packed, "config1": config1,
+                "tuning": tuning}
         print(json.dumps(line), flush=True)
     if ws > 1:
         tdist.destroy_process_group()

@@ -307,6 +307,25 @@ typedef struct fwix_instance {
 fwix_status fwix_sweep(int kind, const fwix_instance* insts, int ninst, void* const* streams, int nstreams,
                        void* stream);
 
+/* ---- runtime tuning ----------------------------------------------------------
+ * fwix_plan_autotune times the equivalent implementations of one depth step of
+ * kind `kind` at level iz on the caller's wavefield (in -> out, distinct buffers;
+ * refs and a FWIX_WS_STEP workspace bound) and keeps the fastest for every later
+ * call of the plan: column tiles moved per thread (cp.async) or by TMA; all
+ * slices (shot, frequency) in one launch, or halves / quarters of them; for
+ * 256 x 256 slices the one-launch cluster step.  Each candidate runs once untimed,
+ * then `reps` steps between CUDA events on `stream`.  It synchronises `stream`:
+ * call it before any stream capture.  `result` (may be NULL) receives the choice. */
+typedef struct fwix_tuning {
+  int col_tma;                /* 1: TMA column tiles                               */
+  int fused;                  /* 1: one-launch cluster step                        */
+  int64_t slices_per_launch;  /* slices of one launch of each pass                 */
+  float ms;                   /* time per step of the choice                       */
+  int candidates;             /* candidates timed                                  */
+} fwix_tuning;
+fwix_status fwix_plan_autotune(fwix_plan* plan, int kind, int iz, const void* in, void* out, int reps, void* stream,
+                               fwix_tuning* result);
+
 /* ---- allocation-free depth step ----------------------------------------------
  * fwix_step_noalloc has no counterpart in the reference.  It is fwix_step for
  * callers that cannot call cudaMalloc -- for example a host application or

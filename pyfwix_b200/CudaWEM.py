@@ -30,8 +30,9 @@ current device otherwise); there is no CPU path.
 Extensions over the reference, all opt-in through ``par``:
 ``step`` ("pspi" as in the reference's ``OneWay``, or "nsps"),
 ``ref_method`` ("quantile" or "kmeans"; the reference runs a randomised
-OpenCV k-means), and a model whose frequency axis has length 1 (one s^2 for
-every frequency).
+OpenCV k-means), ``autotune`` (time the equivalent forms of the depth step
+once per propagator and keep the fastest, ``fwix_plan_autotune``), and a model
+whose frequency axis has length 1 (one s^2 for every frequency).
 """
 from __future__ import annotations
 
@@ -232,6 +233,10 @@ class WindowPropagator:
             raise RuntimeError("Error: model hypercube does not match the slow_hyper")
         s2d, dend = self.plan.set_model(_raw(s2), _raw(den))
         _refs(self.plan, s2d, self.par)
+        if bool(_get(self.par, "autotune", False)) and not getattr(self, "tuning", None):
+            # par["autotune"]: time the equivalent forms of the depth step once
+            # (synchronises the current stream) and keep the fastest
+            self.tuning = self.plan.autotune()
 
     def _ensure_storage(self):
         if self.packed:

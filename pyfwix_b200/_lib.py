@@ -50,6 +50,12 @@ class FwixInstance(ctypes.Structure):
         ("adjoint", I), ("add", I),
     ]
 
+class FwixTuning(ctypes.Structure):
+    """fwix_tuning: the choice of fwix_plan_autotune."""
+    _fields_ = [("col_tma", ctypes.c_int), ("fused", ctypes.c_int), ("slices_per_launch", ctypes.c_int64),
+                ("ms", ctypes.c_float), ("candidates", ctypes.c_int)]
+
+
 # name -> argtypes (all return fwix_status as int unless listed in _RET)
 SIGNATURES = {
     "fwix_last_error": [],
@@ -85,6 +91,7 @@ SIGNATURES = {
     "fwix_propagate": [P, P, P, P, P, I, P, P, P],
     "fwix_migrate": [P, P, P, P, P, P, I, P],
     "fwix_born": [P, I, P, P, P, P, P, I64, P, I, P],
+    "fwix_plan_autotune": [P, I, I, P, P, I, P, ctypes.POINTER(FwixTuning)],
     "fwix_step_noalloc": [ctypes.POINTER(FwixDesc), I, I, I, P, P, I64, I64, P, P, I, P],
     "fwix_pspi_step": [P, I, P, P, I, P],
     "fwix_nsps_step": [P, I, P, P, I, P],

@@ -33,7 +33,7 @@ from .plan import Plan, sweep
 class Instance:
     """One shot: plan, traces, wavelet, recorded data and image."""
 
-    def __init__(self, w, device, slow2):
+    def __init__(self, w, device, slow2, autotune=True):
         self.w = w
         self.plan = Plan(ns=1, device=device, **w.plan_kwargs())
         p = self.plan
@@ -51,6 +51,9 @@ class Instance:
         self.data = torch.zeros((len(g["rx"]), w.nw), dtype=torch.complex64, device=device)
         self.image = torch.zeros((w.nz, w.ny, w.nx), dtype=torch.float32, device=device)
         p.ensure_workspace(L.WS_SWEEP)
+        # per instance, the fastest equivalent form of its depth step (column tile
+        # movement, slices per launch) for its own grid and band
+        self.tuning = p.autotune() if autotune else None
 
     @property
     def cells(self):

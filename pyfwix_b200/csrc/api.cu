@@ -1220,6 +1220,92 @@ fwix_status fwix_born_packed(fwix_plan* p, int adjoint, const fwix_traces* rec, 
 }
 
 
+// ---------------------------------------------------------------- runtime tuning
+// Times the equivalent implementations of one depth step of this plan on the
+// caller's wavefield and keeps the fastest: column tiles moved by per-thread
+// cp.async or by TMA; every slice in one launch, or halves / quarters of them
+// (the intermediates of a smaller launch stay in L2); for 256 x 256 slices the
+// one-launch cluster step.  Each candidate runs once untimed (it builds its
+// tables), then `reps` steps between CUDA events on `stream`.  Synchronises the
+// stream: call it before any capture.
+fwix_status fwix_plan_autotune(fwix_plan* p, int kind, int iz, const void* in, void* out, int reps, void* stream,
+                               fwix_tuning* result) {
+  if (!p || !in || !out) return fail(FWIX_ERR_INVALID, "null argument");
+  if (kind != FWIX_STEP_PSPI && kind != FWIX_STEP_NSPS) return fail(FWIX_ERR_INVALID, "unknown step kind");
+  FWIX_TRY(need_refs(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  FWIX_TRY(check_iz(p, iz));
+  if (in == out) return fail(FWIX_ERR_INVALID, "autotune needs distinct in and out buffers");
+  cudaStream_t s = (cudaStream_t)stream;
+  reps = std::max(1, reps);
+  struct Cand {
+    bool tma;
+    long long chunk;
+    bool fused;
+  };
+  std::vector<Cand> cands;
+  const long long c0 = p->chunk;  // the workspace is sized for this many slices per launch
+  for (long long c : {c0, c0 / 2, c0 / 4}) {
+    if (c < 8 && c != c0) continue;
+    bool dup = false;
+    for (const Cand& k : cands) dup = dup || k.chunk == c;
+    if (dup) continue;
+    cands.push_back({false, c, false});
+    cands.push_back({true, c, false});
+  }
+  if (p->d.NX == 256 && p->d.NY == 256 && fwix::fused_step_available()) cands.push_back({false, c0, true});
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  FWIX_CU(cudaEventCreate(&e0));
+  FWIX_CU(cudaEventCreate(&e1));
+  const bool tma0 = p->col_tma, fused0 = p->fused;
+  float best = -1.f;
+  Cand pick{tma0, c0, fused0};
+  int tried = 0;
+  for (const Cand& k : cands) {
+    p->col_tma = k.tma;
+    p->chunk = k.chunk;
+    p->fused = k.fused;
+    if (do_step(p, kind, iz, FWIX_FWD, (const float2*)in, (float2*)out, 0, s) != FWIX_OK) {
+      cudaGetLastError();  // a candidate this device or size does not run (launch error, not sticky)
+      continue;
+    }
+    fwix_status st = FWIX_OK;
+    cudaError_t ce = cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && st == FWIX_OK; ++r)
+      st = do_step(p, kind, iz, FWIX_FWD, (const float2*)in, (float2*)out, 0, s);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e1, s);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    if (st != FWIX_OK || ce != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      p->col_tma = tma0, p->chunk = c0, p->fused = fused0;
+      return st != FWIX_OK ? st : fail(FWIX_ERR_CUDA, std::string("autotune timing: ") + cudaGetErrorString(ce));
+    }
+    ++tried;
+    ms /= (float)reps;
+    if (best < 0.f || ms < best) {
+      best = ms;
+      pick = k;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  p->col_tma = pick.tma;
+  p->chunk = pick.chunk;
+  p->fused = pick.fused;
+  if (tried == 0) return fail(FWIX_ERR_UNSUPPORTED, "autotune: no candidate ran");
+  if (result) {
+    result->col_tma = pick.tma ? 1 : 0;
+    result->fused = pick.fused ? 1 : 0;
+    result->slices_per_launch = pick.chunk;
+    result->ms = best;
+    result->candidates = tried;
+  }
+  return FWIX_OK;
+}
+
 // ---------------------------------------------------------------- one-call forms
 fwix_status fwix_pspi_step(fwix_plan* p, int iz, const void* in, void* out, int adjoint, void* stream) {
   return fwix_step(p, FWIX_STEP_PSPI, iz, adjoint, in, out, 0, stream);

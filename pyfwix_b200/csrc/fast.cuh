@@ -847,6 +847,99 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
   }
 }
 
+// t2[term] = F_y^-1(Q_term * F_y(t1[0])) with the tiles moved by TMA (plans of 16
+// columns per CTA): the input tile arrives once; every term's result goes
+// through one swizzled staging tile and a TMA store, the staging tile being
+// rewritten only after the previous term's store has read it.  The zeroth Born
+// order (Q_KPOW with term0 0, the identity filter) is the input tile scaled,
+// stored from the staging tile before the transforms.
+template <class P>
+struct ColTmaA {
+  static constexpr int LX = ColTma<P>::LX, TILE = ColTma<P>::TILE, NBOX = ColTma<P>::NBOX, ROWS = ColTma<P>::ROWS;
+  // input tile (then the exchange lines), staging tile, twiddles, one mbarrier, alignment room
+  static size_t smem() { return (size_t)2 * TILE * sizeof(float2) + tw_size<P>() * sizeof(float2) + 16 + 1024; }
+};
+
+template <class P, int QM>
+__global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocksA)
+    k_col_a_tma(const SpecArgs a, int nxt, const __grid_constant__ CUtensorMap tin,
+                const __grid_constant__ CUtensorMap tout) {
+  using C = ColTmaA<P>;
+  static_assert(C::LX == 16, "TMA column tiles are 16 columns (128 bytes) wide");
+  extern __shared__ unsigned char smem_raw[];
+  float2* in = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  float2* stage = in + C::TILE;
+  float2* tw = stage + C::TILE;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + tw_size<P>());
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane / P::T, t = lane % P::T, col = warp * P::G + g;
+  const long long b = blockIdx.x / nxt;
+  const int x0 = (int)(blockIdx.x - b * nxt) * C::LX;
+  const int iw = (int)((a.b0 + b) % a.d.nw);
+  const int x = x0 + col;
+  const int xq = x < a.d.NX ? x : 0;
+  const int zstride = (int)(a.tstride / a.d.slice);
+  if (threadIdx.x == 0) {
+    tma::mbar_init(bar, 1);
+    tma::fence_mbar_init();
+  }
+  load_stage_tw<P>(tw, a.twy);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tma::mbar_expect_tx(bar, (unsigned)(C::TILE * sizeof(float2)));
+#pragma unroll
+    for (int k = 0; k < C::NBOX; ++k) tma::load_3d(in + k * C::ROWS * C::LX, &tin, x0, k * C::ROWS, (int)b, bar);
+  }
+  const bool ok = tma::mbar_wait(bar, 0u);
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) atomicAdd(a.err, 1u);
+    return;
+  }
+  float2 psi[P::E];
+#pragma unroll
+  for (int e = 0; e < P::E; ++e) psi[e] = in[tma::sw128(pos_first<P>(t, e), col)];
+  int first = 0;
+  auto store = [&](int term) {  // staging tile -> t2[term]
+    tma::fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < C::NBOX; ++k)
+        tma::store_3d(&tout, x0, k * C::ROWS, term * zstride + (int)b, stage + k * C::ROWS * C::LX);
+      tma::store_commit();
+    }
+  };
+  auto stage_free = [&]() {  // the previous store has read the staging tile
+    if (threadIdx.x == 0) tma::store_wait_read();
+    __syncthreads();
+  };
+  if constexpr (QM == Q_KPOW) {
+    if (a.term0 == 0 && a.nterm > 0) {
+      const float sc = a.norm * (float)P::N;
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) stage[tma::sw128(pos_first<P>(t, e), col)] = cscale(psi[e], sc);
+      store(0);
+      first = 1;
+    }
+  }
+  __syncthreads();  // every lane holds its column: the input tile becomes the exchange lines
+  float2* line = in + col * P::N;
+  fft_fwd<P>(psi, t, tw, line);
+  const int nterm = a.nterm;
+  for (int term = first; term < nterm; ++term) {
+    float2 v[P::E];
+    col_factors<P, QM>(a, term, iw, xq, t, v);
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) v[e] = cmul(psi[e], v[e]);
+    fft_inv<P>(v, t, tw, line);
+    stage_free();
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) stage[tma::sw128(pos_first<P>(t, e), col)] = v[e];
+    store(term);
+  }
+  if (threadIdx.x == 0) tma::store_wait_read();
+}
+
 // out (+)= scale * F_y^{-+1}(in): the column half of a plain 2D transform.
 template <class P, bool INV>
 __global__ void __launch_bounds__(kWarps * 32) k_col_fft(const SpecArgs a, int nxt, const float2* in, float2* out,
@@ -951,7 +1044,37 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
 }
 
 template <class P>
+cudaError_t col_type_a_tma(const SpecArgs& a, int qmode, cudaStream_t s) {
+  using C = ColTmaA<P>;
+  const int nxt = (a.d.NX + C::LX - 1) / C::LX;
+  const unsigned grid = (unsigned)(a.nb * nxt);
+  const size_t sm = C::smem();
+  CUtensorMap tin, tout;
+  cudaError_t e = tile_map(&tin, a.t1, a.d.NX, a.d.NY, a.nb, C::ROWS);
+  if (e == cudaSuccess) e = tile_map(&tout, a.t2, a.d.NX, a.d.NY, (a.tstride / a.d.slice) * (a.term0 + a.nterm), C::ROWS);
+  if (e != cudaSuccess) return e;
+#define FWIX_FAST_CAT(Q)                                                                  \
+  case Q:                                                                                 \
+    e = opt_in_smem(k_col_a_tma<P, Q>, sm);                                               \
+    if (e == cudaSuccess) k_col_a_tma<P, Q><<<grid, kWarps * 32, sm, s>>>(a, nxt, tin, tout); \
+    break;
+  switch (qmode) {
+    FWIX_FAST_CAT(Q_PS_FWD)
+    FWIX_FAST_CAT(Q_PS_ADJ)
+    FWIX_FAST_CAT(Q_KPOW)
+    FWIX_FAST_CAT(Q_ONE)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FWIX_FAST_CAT
+  if (e == cudaSuccess) count_launch();
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <class P>
 cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
+  if constexpr (ColGeo<P>::LX == 16) {
+    if (a.tma && a.err && a.d.NX % 2 == 0) return col_type_a_tma<P>(a, qmode, s);
+  }
   const int nxt = (a.d.NX + ColGeo<P>::LX - 1) / ColGeo<P>::LX;
   const unsigned grid = (unsigned)(a.nb * nxt);
   const size_t sm = ColGeo<P>::smem();

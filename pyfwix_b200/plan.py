@@ -160,6 +160,23 @@ class Plan:
         L.check(self.lib.fwix_smooth_step(self._h, iz, mode, _p(inp), _p(out), int(add), _stream()))
         return out
 
+    def autotune(self, iz=None, reps=3, kind=None):
+        """Times the equivalent implementations of this plan's depth step (column
+        tiles by cp.async or TMA, slices per launch, the one-launch cluster step at
+        256 x 256) on a random wavefield at level ``iz`` (the middle one by
+        default) and keeps the fastest (fwix_plan_autotune).  Synchronises the
+        current stream.  Returns the choice as a dict."""
+        self.ensure_workspace(L.WS_STEP)
+        k = self.step_kind if kind is None else STEP_KINDS.get(kind, kind)
+        iz = self.nz // 2 if iz is None else int(iz)
+        x = torch.randn(self.wshape, dtype=torch.complex64, device=self.device)
+        y = torch.empty_like(x)
+        res = L.FwixTuning()
+        L.check(self.lib.fwix_plan_autotune(self._h, k, iz, _p(x), _p(y), int(reps), _stream(), ctypes.byref(res)))
+        return {"col_tma": bool(res.col_tma), "fused_cluster_step": bool(res.fused),
+                "slices_per_launch": int(res.slices_per_launch), "step_ms": float(res.ms),
+                "candidates": int(res.candidates)}
+
     def smooth_step_pair(self, iz, inp, out, deriv, add=False):
         """out (+)= the smooth forward step of inp and deriv (+)= its slowness
         derivative, from one set of transforms."""
