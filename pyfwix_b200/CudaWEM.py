@@ -31,8 +31,14 @@ Extensions over the reference, all opt-in through ``par``:
 ``step`` ("pspi" as in the reference's ``OneWay``, or "nsps"),
 ``ref_method`` ("quantile" or "kmeans"; the reference runs a randomised
 OpenCV k-means), ``autotune`` (time the equivalent forms of the depth step
-once per propagator and keep the fastest, ``fwix_plan_autotune``), and a model
-whose frequency axis has length 1 (one s^2 for every frequency).
+once per propagator and keep the fastest, ``fwix_plan_autotune``),
+``background_store = "host"`` (with ``compress_rate = 8``: the packed
+backgrounds in pinned host memory, read by the kernels over the host link, for
+runs whose backgrounds do not fit in device memory), ``wfld_path`` / ``run_id``
+(every forward also writes its stored backgrounds into the reference's
+checkpoint-file layout, ``pyfwix_b200.pool``; ``load_backgrounds`` reads them
+back), and a model whose frequency axis has length 1 (one s^2 for every
+frequency).
 """
 from __future__ import annotations
 
@@ -226,6 +232,13 @@ class WindowPropagator:
         if rate is not None and float(rate) != 8.0:
             raise ValueError(f"compress_rate {rate} is not supported: the packed store has one rate, 8")
         self.packed = rate is not None
+        where = str(_get(par, "background_store", "device"))
+        if where not in ("device", "host"):
+            raise ValueError(f"background_store must be 'device' or 'host', got {where!r}")
+        if where == "host" and not self.packed:
+            raise ValueError("background_store 'host' keeps the packed backgrounds: set compress_rate = 8")
+        self.host_store = where == "host"
+        self.pool = None
 
     def set_background_model(self, model):
         s2, den = _model_pair(model)
@@ -241,7 +254,8 @@ class WindowPropagator:
     def _ensure_storage(self):
         if self.packed:
             if self.bg_down is None:
-                self.bg_down, self.bg_up = self.plan.packed(self.plan.nz), self.plan.packed(self.plan.nz)
+                self.bg_down = self.plan.packed(self.plan.nz, host=self.host_store)
+                self.bg_up = self.plan.packed(self.plan.nz, host=self.host_store)
             return
         shape = (self.plan.nz,) + self.plan.wshape
         if self.bg_down is None or tuple(self.bg_down.shape) != shape:
@@ -260,6 +274,39 @@ class WindowPropagator:
                 self.plan.propagate(self.src, self.rec, self.wavelet, out, self.bg_down, self.bg_up, add=bool(add))
             self._bg_key = tuple(id(v) for v in _model_pair(model))
             _store(data, out)
+            if _get(self.par, "wfld_path") is not None:
+                self._checkpoint()
+
+    def _pool(self):
+        if self.pool is None:
+            from .pool import WavefieldPool
+            import uuid
+            run_id = str(_get(self.par, "run_id", "run_" + uuid.uuid4().hex[:12]))
+            self.pool = WavefieldPool(self.plan, self.par, run_id, self.plan.nz)
+        return self.pool
+
+    def _checkpoint(self):
+        """The stored backgrounds of the last forward, every depth, into the
+        reference's checkpoint files (tags "down" and "up",
+        ``propagator/src/OneWay.h:195-239``; file layout of
+        ``propagator/src/WavefieldPool.cpp:78-100``)."""
+        pool = self._pool()
+        pool.store(self.bg_down, "down")
+        pool.store(self.bg_up, "up")
+        pool.wait_to_finish()
+
+    def load_backgrounds(self, model):
+        """Backgrounds of ``model`` read back from the checkpoint files of this
+        propagator's pool (``par`` keys ``wfld_path`` and ``run_id`` name them),
+        instead of modelling them again: the restart of a run whose forward was
+        done earlier, with the same geometry."""
+        with torch.cuda.device(self.device):
+            self.set_background_model(model)
+            pool = self._pool()
+            self._ensure_storage()
+            self.bg_down = pool.load("down", out=self.bg_down)
+            self.bg_up = pool.load("up", out=self.bg_up)
+            self._bg_key = tuple(id(v) for v in _model_pair(model))
 
     def born(self, dslow, dden, data, adjoint, add):
         """Extended Born on the stored backgrounds (packed or full)."""

@@ -263,8 +263,14 @@ class Plan:
         """Bytes of one packed wavefield (fixed rate, 8.5 bits per value)."""
         return int(self.lib.fwix_plan_packed_bytes(self._h))
 
-    def packed(self, nfields=1):
-        """Uninitialised storage for nfields packed wavefields (uint8 tensor)."""
+    def packed(self, nfields=1, host=False):
+        """Uninitialised storage for nfields packed wavefields (uint8 tensor), in
+        device memory or, with ``host``, in pinned host memory: the packing and
+        unpacking kernels then write and read it directly over the host link
+        (pinned host memory is addressable from the device with the same
+        pointer), which keeps the stored backgrounds out of device memory."""
+        if host:
+            return torch.empty((nfields, self.packed_bytes), dtype=torch.uint8, pin_memory=True)
         return torch.empty((nfields, self.packed_bytes), dtype=torch.uint8, device=self.device)
 
     def pack(self, wfld, packed):

@@ -192,6 +192,9 @@ class StreamingPropagator:
             nxw, nyw = x1 - x0 + 1, y1 - y0 + 1
             par["padx"] = next_fft_length(nxw + int(_get(par, "padx", 0))) - nxw
             par["pady"] = next_fft_length(nyw + int(_get(par, "pady", 0))) - nyw
+            if len(self.pairs) > 1 and _get(par, "run_id") is not None:
+                # every pair keeps its checkpoint files in a run directory of its own
+                par["run_id"] = f"{par['run_id']}_pair{self.pairs.index(p)}"
             p.prop = _w.WindowPropagator(wmodel, data, wav, par, self._pair_geometry(p))
             p.stream = torch.cuda.Stream(device=self.device)
         return p.prop
@@ -215,6 +218,17 @@ class StreamingPropagator:
             out[rows, p.f0:p.f0 + p.nf] += d
         self._model_key = tuple(id(v) for v in _model_pair(model))
         _store(data, out)
+
+    def load_backgrounds(self, model):
+        """The backgrounds of ``model`` read back, for every (shot group, band)
+        pair, from the checkpoint files of an earlier forward with the same
+        geometry (``par`` keys ``wfld_path`` and ``run_id`` name them,
+        ``pyfwix_b200.pool``) instead of modelling them again: a restart."""
+        for p in self.pairs:
+            wm = self._window_model(p, model)
+            p.wm = wm
+            self._build(p, wm).load_backgrounds(wm)
+        self._model_key = tuple(id(v) for v in _model_pair(model))
 
     def get_compression_ratio(self):
         """Stored bytes ratio of the background wavefields (1 lossless; with
