@@ -59,6 +59,8 @@ def args_():
     ap.add_argument("--fwi-nz", type=int, default=None, help="depth levels of the FWI workload (quick runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched forward+imaging timing")
     ap.add_argument("--no-config1", action="store_true", help="skip the plain modelling + imaging timing")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="time the plan's default form of the depth step instead of the tuned one")
     ap.add_argument("--no-packed", action="store_true", help="skip the packed-background Born timing")
     ap.add_argument("--large", action="store_true",
                     help="run only the 512 x 512 x 400 x 200 Born on packed storage and print its own line")
@@ -144,7 +146,7 @@ def dist():
 
 # ----------------------------------------------------------------------------- B200 arm
 
-def setup_born(w, device):
+def setup_born(w, device, autotune=True):
     import torch
 
     from pyfwix_b200 import refsampler
@@ -156,7 +158,8 @@ def setup_born(w, device):
     plan.set_refs(refsampler.expand_refs(sref, w.nw), labels)
     s2c = s2.to(torch.complex64)
     plan.set_model(s2c, torch.ones_like(s2c))
-    tuning = plan.autotune()      # the fastest equivalent form of this plan's depth step
+    # the fastest equivalent form of this plan's depth step (else the plan's defaults)
+    tuning = plan.autotune() if autotune else None
     g = w.geom
     src = plan.traces(g["sx"], g["sy"], g["sz"], np.zeros(len(g["sx"]), np.int32))
     rec = plan.traces(g["rx"], g["ry"], g["rz"], np.zeros(len(g["rx"]), np.int32))
@@ -394,7 +397,8 @@ def config1_timing(device, reps=10):
     plan.set_refs(refsampler.expand_refs(sref, w.nw), labels)
     s2c = s2.to(torch.complex64)
     plan.set_model(s2c, torch.ones_like(s2c))
-    tuning = plan.autotune()      # the fastest equivalent form of this plan's depth step
+    # the fastest equivalent form of this plan's depth step (else the plan's defaults)
+    tuning = plan.autotune() if autotune else None
     g = w.geom
     src = plan.traces(g["sx"], g["sy"], g["sz"], np.zeros(len(g["sx"]), np.int32))
     rec = plan.traces(g["rx"], g["ry"], g["rz"], np.zeros(len(g["rx"]), np.int32))
@@ -682,7 +686,7 @@ def main():
     device = torch.device("cuda", torch.cuda.current_device())
     from pyfwix_b200 import workloads
     w = workloads.CONFIGS[a.config](nz=a.nz)
-    st = setup_born(w, device)
+    st = setup_born(w, device, autotune=not a.no_autotune)
     for _ in range(a.warmup):
         born_step(st)
     torch.cuda.synchronize()

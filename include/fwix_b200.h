@@ -312,8 +312,10 @@ fwix_status fwix_sweep(int kind, const fwix_instance* insts, int ninst, void* co
  * kind `kind` at level iz on the caller's wavefield (in -> out, distinct buffers;
  * refs and a FWIX_WS_STEP workspace bound) and keeps the fastest for every later
  * call of the plan: column tiles moved per thread (cp.async) or by TMA; all
- * slices (shot, frequency) in one launch, or halves / quarters of them; for
- * 256 x 256 slices the one-launch cluster step.  Each candidate runs once untimed,
+ * slices (shot, frequency) in one launch, or halves / quarters of them, on the
+ * caller's stream or alternating between it and a second stream of the plan
+ * (forked and joined with events, so calls stay ordered on `stream` and can be
+ * captured); for 256 x 256 slices the one-launch cluster step.  Each candidate runs once untimed,
  * then `reps` steps between CUDA events on `stream`.  It synchronises `stream`:
  * call it before any stream capture.  `result` (may be NULL) receives the choice. */
 typedef struct fwix_tuning {
@@ -322,6 +324,7 @@ typedef struct fwix_tuning {
   int64_t slices_per_launch;  /* slices of one launch of each pass                 */
   float ms;                   /* time per step of the choice                       */
   int candidates;             /* candidates timed                                  */
+  int streams;                /* 1, or 2: chunks alternate between two streams     */
 } fwix_tuning;
 fwix_status fwix_plan_autotune(fwix_plan* plan, int kind, int iz, const void* in, void* out, int reps, void* stream,
                                fwix_tuning* result);

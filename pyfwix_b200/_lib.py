@@ -53,7 +53,7 @@ class FwixInstance(ctypes.Structure):
 class FwixTuning(ctypes.Structure):
     """fwix_tuning: the choice of fwix_plan_autotune."""
     _fields_ = [("col_tma", ctypes.c_int), ("fused", ctypes.c_int), ("slices_per_launch", ctypes.c_int64),
-                ("ms", ctypes.c_float), ("candidates", ctypes.c_int)]
+                ("ms", ctypes.c_float), ("candidates", ctypes.c_int), ("streams", ctypes.c_int)]
 
 
 # name -> argtypes (all return fwix_status as int unless listed in _RET)

@@ -126,6 +126,11 @@ struct fwix_plan {
   long long chunk = 1;  // slices per launch: the intermediates of one chunk fit in L2
   bool fused = false;   // 256 x 256 slices: one-launch cluster step (fused256.cu), opt-in
   bool col_tma = false; // column passes with TMA tiles where the plan allows (FWIX_COL_TMA)
+  // depth steps in chunks alternating between the caller's stream and lane_s
+  // (lanes = 2, set by fwix_plan_autotune), each lane with its own intermediates
+  int lanes = 1;
+  cudaStream_t lane_s = nullptr;
+  cudaEvent_t lane_fork = nullptr, lane_join = nullptr;
   unsigned* err = nullptr;  // device word: bounded waits of the TMA passes that ran out
   float2* scat_tab = nullptr;     // scatter weights of one depth, [taylor+1][NY][NX]
   const float* sm_s = nullptr;    // smooth step: padded slowness [nz][NY][NX]
@@ -139,7 +144,8 @@ struct fwix_plan {
   float coef[5] = {1.f, 1.f / 2.f, 3.f / 8.f, 5.f / 16.f, 35.f / 128.f};  // Scatter.h:526
 
   size_t wbytes() const { return (size_t)d.wfld * sizeof(float2); }
-  size_t tbytes() const { return (size_t)nterm_max * chunk * d.slice * sizeof(float2); }
+  long long lane_span() const { return (long long)nterm_max * chunk * d.slice; }  // samples of one lane's t1 (or t2)
+  size_t tbytes() const { return (size_t)lane_span() * lanes * sizeof(float2); }
   size_t ws_need(int cls) const {
     size_t b = 2 * tbytes();  // t1, t2 for one chunk
     if (cls >= FWIX_WS_SWEEP) b += 3 * wbytes();  // A, B, SC
@@ -307,7 +313,31 @@ fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, f
   SpecArgs a0 = p->args(in, out, add);
   a0.in2 = in2;  // the step of in + in2 (linear: one step instead of two)
   FWIX_TRY(phase_factors(p, iz, a0, s));
-  return for_chunks(p, a0, [&](const SpecArgs& a) { return step_chunk(p, kind, iz, dir, a, s); });
+  if (p->lanes < 2 || p->fused)
+    return for_chunks(p, a0, [&](const SpecArgs& a) { return step_chunk(p, kind, iz, dir, a, s); });
+  // Two lanes: chunks alternate between `s` and the plan's lane stream, forked
+  // from and joined back into `s` with events, each lane with its own half of the
+  // intermediates; one chunk's column pass overlaps the next chunk's row pass.
+  FWIX_CU(cudaEventRecord(p->lane_fork, s));
+  FWIX_CU(cudaStreamWaitEvent(p->lane_s, p->lane_fork, 0));
+  const long long B = (long long)p->d.ns * p->d.nw;
+  fwix_status st = FWIX_OK;
+  int k = 0;
+  for (long long b0 = 0; b0 < B && st == FWIX_OK; b0 += p->chunk, ++k) {
+    SpecArgs a = a0;
+    a.b0 = b0;
+    a.nb = std::min(p->chunk, B - b0);
+    a.tstride = p->chunk * p->d.slice;
+    const int lane = k & 1;
+    a.t1 = p->t1() + lane * p->lane_span();
+    a.t2 = p->t2() + lane * p->lane_span();
+    st = step_chunk(p, kind, iz, dir, a, lane ? p->lane_s : s);
+  }
+  // `s` waits for the lane also after a failure
+  const cudaError_t e1 = cudaEventRecord(p->lane_join, p->lane_s);
+  const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(s, p->lane_join, 0) : e1;
+  if (st != FWIX_OK) return st;
+  return cu(e2, "lane join");
 }
 
 fwix_status need_smooth(const fwix_plan* p) {
@@ -692,6 +722,9 @@ fwix_status fwix_plan_destroy(fwix_plan* p) {
   void* ptrs[] = {p->twx, p->twy, p->kx, p->ky, p->w2, p->w, p->tapx, p->tapy, p->scat_tab, p->err};
   for (void* v : ptrs)
     if (v) cudaFree(v);
+  if (p->lane_fork) cudaEventDestroy(p->lane_fork);
+  if (p->lane_join) cudaEventDestroy(p->lane_join);
+  if (p->lane_s) cudaStreamDestroy(p->lane_s);
   delete p;
   return FWIX_OK;
 }
@@ -1224,8 +1257,9 @@ fwix_status fwix_born_packed(fwix_plan* p, int adjoint, const fwix_traces* rec, 
 // Times the equivalent implementations of one depth step of this plan on the
 // caller's wavefield and keeps the fastest: column tiles moved by per-thread
 // cp.async or by TMA; every slice in one launch, or halves / quarters of them
-// (the intermediates of a smaller launch stay in L2); for 256 x 256 slices the
-// one-launch cluster step.  Each candidate runs once untimed (it builds its
+// (the intermediates of a smaller launch stay in L2), also alternating between
+// two streams; for 256 x 256 slices the one-launch cluster step.  Each
+// candidate runs once untimed (it builds its
 // tables), then `reps` steps between CUDA events on `stream`.  Synchronises the
 // stream: call it before any capture.
 fwix_status fwix_plan_autotune(fwix_plan* p, int kind, int iz, const void* in, void* out, int reps, void* stream,
@@ -1242,29 +1276,46 @@ fwix_status fwix_plan_autotune(fwix_plan* p, int kind, int iz, const void* in, v
     bool tma;
     long long chunk;
     bool fused;
+    int lanes;
   };
   std::vector<Cand> cands;
-  const long long c0 = p->chunk;  // the workspace is sized for this many slices per launch
+  // the workspace holds the intermediates of this many slices (one lane)
+  const long long c0 = p->chunk * p->lanes;
   for (long long c : {c0, c0 / 2, c0 / 4}) {
     if (c < 8 && c != c0) continue;
     bool dup = false;
     for (const Cand& k : cands) dup = dup || k.chunk == c;
     if (dup) continue;
-    cands.push_back({false, c, false});
-    cands.push_back({true, c, false});
+    cands.push_back({false, c, false, 1});
+    cands.push_back({true, c, false, 1});
   }
-  if (p->d.NX == 256 && p->d.NY == 256 && fwix::fused_step_available()) cands.push_back({false, c0, true});
+  for (long long c : {c0 / 2, c0 / 4, c0 / 8}) {  // two lanes of c slices each
+    if (c < 8) continue;
+    cands.push_back({false, c, false, 2});
+    cands.push_back({true, c, false, 2});
+  }
+  if (p->d.NX == 256 && p->d.NY == 256 && fwix::fused_step_available()) cands.push_back({false, c0, true, 1});
+  bool have_lanes = false;
+  for (const Cand& k : cands) have_lanes = have_lanes || k.lanes == 2;
+  if (have_lanes && !p->lane_s) {
+    FWIX_CU(cudaStreamCreateWithFlags(&p->lane_s, cudaStreamNonBlocking));
+    FWIX_CU(cudaEventCreateWithFlags(&p->lane_fork, cudaEventDisableTiming));
+    FWIX_CU(cudaEventCreateWithFlags(&p->lane_join, cudaEventDisableTiming));
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   FWIX_CU(cudaEventCreate(&e0));
   FWIX_CU(cudaEventCreate(&e1));
   const bool tma0 = p->col_tma, fused0 = p->fused;
+  const long long chunk0 = p->chunk;
+  const int lanes0 = p->lanes;
   float best = -1.f;
-  Cand pick{tma0, c0, fused0};
+  Cand pick{tma0, chunk0, fused0, lanes0};
   int tried = 0;
   for (const Cand& k : cands) {
     p->col_tma = k.tma;
     p->chunk = k.chunk;
     p->fused = k.fused;
+    p->lanes = k.lanes;
     if (do_step(p, kind, iz, FWIX_FWD, (const float2*)in, (float2*)out, 0, s) != FWIX_OK) {
       cudaGetLastError();  // a candidate this device or size does not run (launch error, not sticky)
       continue;
@@ -1280,7 +1331,7 @@ fwix_status fwix_plan_autotune(fwix_plan* p, int kind, int iz, const void* in, v
     if (st != FWIX_OK || ce != cudaSuccess) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
-      p->col_tma = tma0, p->chunk = c0, p->fused = fused0;
+      p->col_tma = tma0, p->chunk = chunk0, p->fused = fused0, p->lanes = lanes0;
       return st != FWIX_OK ? st : fail(FWIX_ERR_CUDA, std::string("autotune timing: ") + cudaGetErrorString(ce));
     }
     ++tried;
@@ -1295,6 +1346,7 @@ fwix_status fwix_plan_autotune(fwix_plan* p, int kind, int iz, const void* in, v
   p->col_tma = pick.tma;
   p->chunk = pick.chunk;
   p->fused = pick.fused;
+  p->lanes = pick.lanes;
   if (tried == 0) return fail(FWIX_ERR_UNSUPPORTED, "autotune: no candidate ran");
   if (result) {
     result->col_tma = pick.tma ? 1 : 0;
@@ -1302,6 +1354,7 @@ fwix_status fwix_plan_autotune(fwix_plan* p, int kind, int iz, const void* in, v
     result->slices_per_launch = pick.chunk;
     result->ms = best;
     result->candidates = tried;
+    result->streams = pick.lanes;
   }
   return FWIX_OK;
 }

@@ -174,8 +174,8 @@ class Plan:
         res = L.FwixTuning()
         L.check(self.lib.fwix_plan_autotune(self._h, k, iz, _p(x), _p(y), int(reps), _stream(), ctypes.byref(res)))
         return {"col_tma": bool(res.col_tma), "fused_cluster_step": bool(res.fused),
-                "slices_per_launch": int(res.slices_per_launch), "step_ms": float(res.ms),
-                "candidates": int(res.candidates)}
+                "slices_per_launch": int(res.slices_per_launch), "streams": int(res.streams),
+                "step_ms": float(res.ms), "candidates": int(res.candidates)}
 
     def smooth_step_pair(self, iz, inp, out, deriv, add=False):
         """out (+)= the smooth forward step of inp and deriv (+)= its slowness

@@ -125,3 +125,25 @@ def test_noalloc_descriptor_checks_without_gpu():
     assert call(big) == -2 and b"static scratch holds" in lib.fwix_last_error()
     wide = _lib.FwixDesc(nx=1000, ny=64, padx=100, nw=1, ns=1, nz=1, dx=1, dy=1, dz=1, nref=1)
     assert call(wide) == -2 and b"at most 1024" in lib.fwix_last_error()
+
+
+def test_tuning_struct_layout_matches_header(tmp_path):
+    """The ctypes mirror of fwix_tuning (fwix_plan_autotune's result) has the C
+    struct's size and field offsets."""
+    import shutil
+    import subprocess
+    from pyfwix_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    fields = [f for f, _ in _lib.FwixTuning._fields_]
+    src = tmp_path / "tuning.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "fwix_b200.h"\nint main(void) {\n'
+                   '  printf("%zu", sizeof(fwix_tuning));\n'
+                   + "".join(f'  printf(" %zu", offsetof(fwix_tuning, {f}));\n' for f in fields)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "tuning"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [ctypes.sizeof(_lib.FwixTuning)] + [getattr(_lib.FwixTuning, f).offset for f in fields]
+    assert got == want
