@@ -233,16 +233,25 @@ fwix_status fwix_born(fwix_plan* plan, int adjoint, const fwix_traces* rec, cons
  * blocks of 16 floats share an exponent byte and keep 8-bit mantissas (8.5 bits
  * per value, 3.76 x smaller than complex64; error at most 2^-7 of the block's
  * largest magnitude).  Not ZFP's bit stream.
- *   fwix_plan_packed_bytes: bytes of one packed wavefield [ns][nw][NY][NX]; [nz]
- *     packed wavefields are nz times that, depth iz at iz * packed_bytes.
- *   fwix_pack_rate8 / fwix_unpack_rate8: one wavefield (buffers 4-byte aligned;
- *     16-byte aligned ones take the vector path).
+ *   fwix_plan_set_pack_rate: 8 (default) or 16 mantissa bits per value for the
+ *     plan's packed store (16.5 bits per value, 1.94 x smaller than complex64,
+ *     error at most 2^-15 of a block's largest magnitude), used by everything
+ *     below except the explicitly 8-bit fwix_pack_rate8 / fwix_unpack_rate8.
+ *   fwix_plan_packed_bytes: bytes of one packed wavefield [ns][nw][NY][NX] at the
+ *     plan's rate; [nz] packed wavefields are nz times that, depth iz at
+ *     iz * packed_bytes.
+ *   fwix_pack_wavefield / fwix_unpack_wavefield: one wavefield at the plan's rate;
+ *   fwix_pack_rate8 / fwix_unpack_rate8: one wavefield at 8 bits (buffers 4-byte
+ *     aligned; 16-byte aligned ones take the vector path).
  *   fwix_propagate_packed: fwix_propagate storing the down and up fields of every
  *     depth packed (packed_up may be NULL); the up pass reflects the unpacked down
  *     fields, as the reference's reflects its decompressed ones.
  *   fwix_born_packed: fwix_born reading packed backgrounds, each depth unpacked
  *     when first needed; workspace class FWIX_WS_BORN_PACKED. */
 size_t fwix_plan_packed_bytes(const fwix_plan* plan);
+fwix_status fwix_plan_set_pack_rate(fwix_plan* plan, int bits);
+fwix_status fwix_pack_wavefield(fwix_plan* plan, const void* wfld, void* packed, void* stream);
+fwix_status fwix_unpack_wavefield(fwix_plan* plan, const void* packed, void* wfld, void* stream);
 fwix_status fwix_pack_rate8(fwix_plan* plan, const void* wfld, void* packed, void* stream);
 fwix_status fwix_unpack_rate8(fwix_plan* plan, const void* packed, void* wfld, void* stream);
 fwix_status fwix_propagate_packed(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,

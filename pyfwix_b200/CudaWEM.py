@@ -32,7 +32,7 @@ Extensions over the reference, all opt-in through ``par``:
 ``ref_method`` ("quantile" or "kmeans"; the reference runs a randomised
 OpenCV k-means), ``autotune`` (time the equivalent forms of the depth step
 once per propagator and keep the fastest, ``fwix_plan_autotune``),
-``background_store = "host"`` (with ``compress_rate = 8``: the packed
+``background_store = "host"`` (with ``compress_rate`` 8 or 16: the packed
 backgrounds in pinned host memory, read by the kernels over the host link, for
 runs whose backgrounds do not fit in device memory), ``wfld_path`` / ``run_id``
 (every forward also writes its stored backgrounds into the reference's
@@ -229,14 +229,17 @@ class WindowPropagator:
         self.bg_down = self.bg_up = None
         self._bg_key = None
         rate = _get(par, "compress_rate")
-        if rate is not None and float(rate) != 8.0:
-            raise ValueError(f"compress_rate {rate} is not supported: the packed store has one rate, 8")
+        if rate is not None and float(rate) not in (8.0, 16.0):
+            raise ValueError(f"compress_rate {rate} is not supported: the packed store has rates 8 and 16")
         self.packed = rate is not None
+        self.rate = int(float(rate)) if self.packed else None
+        if self.packed:
+            self.plan.set_pack_rate(self.rate)
         where = str(_get(par, "background_store", "device"))
         if where not in ("device", "host"):
             raise ValueError(f"background_store must be 'device' or 'host', got {where!r}")
         if where == "host" and not self.packed:
-            raise ValueError("background_store 'host' keeps the packed backgrounds: set compress_rate = 8")
+            raise ValueError("background_store 'host' keeps the packed backgrounds: set compress_rate = 8 or 16")
         self.host_store = where == "host"
         self.pool = None
 
@@ -315,7 +318,7 @@ class WindowPropagator:
 
     def get_compression_ratio(self):
         """Bytes of a complex64 background wavefield over its stored bytes: 1
-        uncompressed, 3.76 with compress_rate 8."""
+        uncompressed, 3.76 with compress_rate 8, 1.94 with compress_rate 16."""
         if not self.packed:
             return 1.0
         return 8.0 * float(np.prod(self.plan.wshape)) / self.plan.packed_bytes
@@ -328,8 +331,8 @@ class PackedGradientWarning(UserWarning):
 PACKED_GRADIENT_WARNING = (
     "compress_rate=8 keeps the background wavefields in the 8.5-bit packed store; the Born adjoint (the FWI "
     "gradient) on them differs from the lossless one by about 5e-3 relative L2 (measured on the 256 x 256 x 128 "
-    "frequency workload), which is above the 1e-3 gradient tolerance of the lossless path.  Leave compress_rate "
-    "unset for gradients that must meet it.")
+    "frequency workload), which is above the 1e-3 gradient tolerance of the lossless path.  Use compress_rate=16 "
+    "(16.5 bits per value) or leave compress_rate unset for gradients that must meet it.")
 
 
 class WindowExtendedBorn:
@@ -367,7 +370,7 @@ class WindowExtendedBorn:
 
     def adjoint(self, add, model, data):
         p = self.prop
-        if p.packed:
+        if p.packed and p.rate == 8:
             warnings.warn(PACKED_GRADIENT_WARNING, PackedGradientWarning, stacklevel=3)
         with torch.cuda.device(p.device):
             self._background()

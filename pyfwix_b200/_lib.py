@@ -98,6 +98,9 @@ SIGNATURES = {
     "fwix_image_accumulate": [P, P, P, P, I, P],
     "fwix_sweep": [I, ctypes.POINTER(FwixInstance), I, ctypes.POINTER(P), I, P],
     "fwix_plan_packed_bytes": [P],
+    "fwix_plan_set_pack_rate": [P, I],
+    "fwix_pack_wavefield": [P, P, P, P],
+    "fwix_unpack_wavefield": [P, P, P, P],
     "fwix_pack_rate8": [P, P, P, P],
     "fwix_unpack_rate8": [P, P, P, P],
     "fwix_propagate_packed": [P, P, P, P, P, I, P, P, P],

@@ -161,7 +161,8 @@ struct fwix_plan {
   float2* wB() const { return wA() + d.wfld; }
   float2* wSC() const { return wB() + d.wfld; }
   float2* store(int iz) const { return wSC() + d.wfld * (long long)(1 + iz); }
-  size_t packed_bytes() const { return fwix::packed_rate8_bytes(2 * d.wfld); }
+  int pack_bits = 8;  // mantissa bits of the packed store (fwix_plan_set_pack_rate)
+  size_t packed_bytes() const { return fwix::packed_bytes(2 * d.wfld, pack_bits); }
   // FWIX_WS_BORN_PACKED layout after A, B, SC: U (second background), X (working
   // level field), then the packed per-level store
   float2* wU() const { return wSC() + d.wfld; }
@@ -473,7 +474,8 @@ struct BgSrc {
       return FWIX_OK;
     }
     if (held != iz) {
-      FWIX_TRY(cu(fwix::launch_unpack_rate8(2 * p->d.wfld, packed + (size_t)iz * p->packed_bytes(), (float*)slot, s),
+      FWIX_TRY(cu(fwix::launch_unpack(p->pack_bits, 2 * p->d.wfld, packed + (size_t)iz * p->packed_bytes(),
+                                      (float*)slot, s),
                   "unpack background"));
       held = iz;
     }
@@ -492,14 +494,16 @@ struct LevelStore {
   float2* field(int iz) const { return packed ? p->wX() : p->store(iz); }
   fwix_status keep(int iz, cudaStream_t s) const {
     if (!packed) return FWIX_OK;
-    return cu(fwix::launch_pack_rate8(2 * p->d.wfld, (const float*)p->wX(), p->pstore(iz), s), "pack level field");
+    return cu(fwix::launch_pack(p->pack_bits, 2 * p->d.wfld, (const float*)p->wX(), p->pstore(iz), s),
+              "pack level field");
   }
   fwix_status get(int iz, cudaStream_t s, const float2** out) const {
     if (!packed) {
       *out = p->store(iz);
       return FWIX_OK;
     }
-    FWIX_TRY(cu(fwix::launch_unpack_rate8(2 * p->d.wfld, p->pstore(iz), (float*)p->wX(), s), "unpack level field"));
+    FWIX_TRY(cu(fwix::launch_unpack(p->pack_bits, 2 * p->d.wfld, p->pstore(iz), (float*)p->wX(), s),
+                "unpack level field"));
     *out = p->wX();
     return FWIX_OK;
   }
@@ -1130,6 +1134,28 @@ fwix_status fwix_propagate(fwix_plan* p, const fwix_traces* src, const fwix_trac
 
 size_t fwix_plan_packed_bytes(const fwix_plan* p) { return p ? p->packed_bytes() : 0; }
 
+fwix_status fwix_plan_set_pack_rate(fwix_plan* p, int bits) {
+  if (!p) return fail(FWIX_ERR_INVALID, "null plan");
+  if (bits != 8 && bits != 16) return fail(FWIX_ERR_UNSUPPORTED, "pack rate must be 8 or 16 bits per value");
+  p->pack_bits = bits;
+  return FWIX_OK;
+}
+
+fwix_status fwix_pack_wavefield(fwix_plan* p, const void* wfld, void* packed, void* stream) {
+  if (!p || !wfld || !packed) return fail(FWIX_ERR_INVALID, "null argument");
+  if (((uintptr_t)wfld) % 4 != 0 || ((uintptr_t)packed) % 4 != 0)
+    return fail(FWIX_ERR_INVALID, "wavefield and packed buffers must be 4-byte aligned");
+  return cu(fwix::launch_pack(p->pack_bits, 2 * p->d.wfld, (const float*)wfld, packed, (cudaStream_t)stream), "pack");
+}
+
+fwix_status fwix_unpack_wavefield(fwix_plan* p, const void* packed, void* wfld, void* stream) {
+  if (!p || !wfld || !packed) return fail(FWIX_ERR_INVALID, "null argument");
+  if (((uintptr_t)wfld) % 4 != 0 || ((uintptr_t)packed) % 4 != 0)
+    return fail(FWIX_ERR_INVALID, "wavefield and packed buffers must be 4-byte aligned");
+  return cu(fwix::launch_unpack(p->pack_bits, 2 * p->d.wfld, packed, (float*)wfld, (cudaStream_t)stream),
+            "unpack");
+}
+
 fwix_status fwix_pack_rate8(fwix_plan* p, const void* wfld, void* packed, void* stream) {
   if (!p || !wfld || !packed) return fail(FWIX_ERR_INVALID, "null argument");
   if (((uintptr_t)wfld) % 4 != 0 || ((uintptr_t)packed) % 4 != 0)
@@ -1172,7 +1198,7 @@ fwix_status fwix_propagate_packed(fwix_plan* p, const fwix_traces* src, const fw
   for (int iz = 0; iz < nz; ++iz) {
     FWIX_TRY(do_inject(p, src, iz, wav, D, s));
     FWIX_TRY(do_record(p, rec, iz, D, dat, s));
-    FWIX_TRY(cu(fwix::launch_pack_rate8(nf, (const float*)D, pd + (size_t)iz * pb, s), "pack down field"));
+    FWIX_TRY(cu(fwix::launch_pack(p->pack_bits, nf, (const float*)D, pd + (size_t)iz * pb, s), "pack down field"));
     if (iz < nz - 1) FWIX_TRY(do_step(p, k, iz, FWIX_FWD, D, D, 0, s));
   }
   float2* U = p->wA();  // the down pass is done with it
@@ -1181,10 +1207,11 @@ fwix_status fwix_propagate_packed(fwix_plan* p, const fwix_traces* src, const fw
       FWIX_CU(cudaMemsetAsync(U, 0, p->wbytes(), s));
     else
       FWIX_TRY(do_step(p, k, iz, FWIX_FWD, U, U, 0, s));
-    FWIX_TRY(cu(fwix::launch_unpack_rate8(nf, pd + (size_t)iz * pb, (float*)R, s), "unpack down field"));
+    FWIX_TRY(cu(fwix::launch_unpack(p->pack_bits, nf, pd + (size_t)iz * pb, (float*)R, s), "unpack down field"));
     FWIX_TRY(do_reflect(p, iz, 0, R, U, 1, s));
     FWIX_TRY(do_record(p, rec, iz, U, dat, s));
-    if (pu) FWIX_TRY(cu(fwix::launch_pack_rate8(nf, (const float*)U, pu + (size_t)iz * pb, s), "pack up field"));
+    if (pu)
+      FWIX_TRY(cu(fwix::launch_pack(p->pack_bits, nf, (const float*)U, pu + (size_t)iz * pb, s), "pack up field"));
   }
   return FWIX_OK;
 }

@@ -184,6 +184,10 @@ cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s)
 size_t packed_rate8_bytes(long long nfloat);
 cudaError_t launch_pack_rate8(long long nfloat, const float* in, void* packed, cudaStream_t s);
 cudaError_t launch_unpack_rate8(long long nfloat, const void* packed, float* out, cudaStream_t s);
+// The same at 8 or 16 mantissa bits.
+size_t packed_bytes(long long nfloat, int bits);
+cudaError_t launch_pack(int bits, long long nfloat, const float* in, void* packed, cudaStream_t s);
+cudaError_t launch_unpack(int bits, long long nfloat, const void* packed, float* out, cudaStream_t s);
 
 // Acquisition kernels (pointwise.cu).  A depth level's injection is a gather
 // list: for each target cell, the (trace, weight) pairs that land on it.

@@ -48,6 +48,7 @@ class Plan:
         self.nx, self.ny, self.nw, self.ns, self.nz = nx, ny, nw, ns, nz
         self.NX, self.NY = nx + padx, ny + pady
         self.nref, self.taylor, self.step_kind = nref, taylor, STEP_KINDS[step]
+        self.pack_bits = 8
         self._h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             L.check(self.lib.fwix_plan_create(ctypes.byref(self.desc), ctypes.byref(self._h)))
@@ -260,8 +261,13 @@ class Plan:
     # -------------------------------------------------------------- packed store
     @property
     def packed_bytes(self):
-        """Bytes of one packed wavefield (fixed rate, 8.5 bits per value)."""
+        """Bytes of one packed wavefield at the plan's rate (8.5 or 16.5 bits per value)."""
         return int(self.lib.fwix_plan_packed_bytes(self._h))
+
+    def set_pack_rate(self, bits):
+        """Mantissa bits of the packed store, 8 (default) or 16."""
+        L.check(self.lib.fwix_plan_set_pack_rate(self._h, int(bits)))
+        self.pack_bits = int(bits)
 
     def packed(self, nfields=1, host=False):
         """Uninitialised storage for nfields packed wavefields (uint8 tensor), in
@@ -274,11 +280,12 @@ class Plan:
         return torch.empty((nfields, self.packed_bytes), dtype=torch.uint8, device=self.device)
 
     def pack(self, wfld, packed):
-        L.check(self.lib.fwix_pack_rate8(self._h, _p(wfld), _p(packed), _stream()))
+        """One wavefield into packed storage at the plan's rate."""
+        L.check(self.lib.fwix_pack_wavefield(self._h, _p(wfld), _p(packed), _stream()))
         return packed
 
     def unpack(self, packed, wfld):
-        L.check(self.lib.fwix_unpack_rate8(self._h, _p(packed), _p(wfld), _stream()))
+        L.check(self.lib.fwix_unpack_wavefield(self._h, _p(packed), _p(wfld), _stream()))
         return wfld
 
     def propagate_packed(self, src, rec, wavelet, data, packed_down, packed_up=None, add=False):

@@ -11,9 +11,10 @@ decompressed (``decompress_slice_async``).  This store keeps the same file
 layout and keys (``wfld_path``, ``compress_rate``, ``wflds_to_store``) with
 this library's codecs in place of ZFP, which is not available to reproduce:
 
-* ``compress_rate = 8``: the fixed-rate packed format of ``fwix_pack_rate8``
-  (8.5 bits per value; chunk = ``fwix_plan_packed_bytes``), packed on the device
-  straight into a pinned host buffer;
+* ``compress_rate = 8`` or ``16``: the fixed-rate packed format of
+  ``fwix_pack_wavefield`` (8.5 or 16.5 bits per value; chunk =
+  ``fwix_plan_packed_bytes``), packed on the device straight into a pinned host
+  buffer;
 * no ``compress_rate``: complex64 as is (chunk = the wavefield's bytes).
 
 Writes run on a host thread pool after the device-to-host copy of their slice
@@ -48,9 +49,11 @@ class WavefieldPool:
     def __init__(self, plan, par, run_id, max_depth):
         self.plan = plan
         rate = _get(par, "compress_rate")
-        if rate is not None and float(rate) != 8.0:
-            raise ValueError(f"compress_rate {rate} is not supported: the packed store has one rate, 8")
+        if rate is not None and float(rate) not in (8.0, 16.0):
+            raise ValueError(f"compress_rate {rate} is not supported: the packed store has rates 8 and 16")
         self.packed = rate is not None
+        if self.packed and int(float(rate)) != getattr(plan, "pack_bits", 8):
+            plan.set_pack_rate(int(float(rate)))
         self.wbytes = int(torch.Size(plan.wshape).numel()) * 8
         self.chunk = plan.packed_bytes if self.packed else self.wbytes
         self.max_depth = int(max_depth)
@@ -96,7 +99,7 @@ class WavefieldPool:
         i = self._free_buffer()
         buf = self.buffers[i]
         if self.packed:
-            L.check(self.plan.lib.fwix_pack_rate8(self.plan._h, _p(wfld), _p(buf), _stream()))
+            L.check(self.plan.lib.fwix_pack_wavefield(self.plan._h, _p(wfld), _p(buf), _stream()))
         else:
             buf.copy_(wfld.reshape(-1).view(torch.uint8), non_blocking=True)
         ev = torch.cuda.Event()
@@ -137,7 +140,7 @@ class WavefieldPool:
             if own:
                 os.close(fd)
         if self.packed:
-            L.check(self.plan.lib.fwix_unpack_rate8(self.plan._h, _p(buf), _p(out), _stream()))
+            L.check(self.plan.lib.fwix_unpack_wavefield(self.plan._h, _p(buf), _p(out), _stream()))
         else:
             out.reshape(-1).view(torch.uint8).copy_(buf, non_blocking=True)
         # the buffer is reused only after this stream's work on it has finished

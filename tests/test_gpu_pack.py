@@ -15,10 +15,12 @@ from tests.gpu_helpers import make_case, make_plan, rel
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("bits", [8, 16])
 @pytest.mark.parametrize("nx,ny,nw,ns,pad", [(32, 24, 3, 1, 4), (60, 44, 5, 2, 4), (64, 64, 2, 1, 0)])
-def test_pack_bits_against_oracle(nx, ny, nw, ns, pad):
+def test_pack_bits_against_oracle(nx, ny, nw, ns, pad, bits):
     g, rng, sref, labels, slow, den = make_case(nx=nx, ny=ny, nw=nw, nz=2, nref=2, padx=pad, pady=pad)
     p = make_plan(g, ns, sref, labels)
+    p.set_pack_rate(bits)
     x = crandn(rng, p.wshape).astype(np.complex64)
     x *= np.float32(10.0) ** rng.integers(-5, 5, size=x.shape)
     x[0, 0, :2] = 0
@@ -28,12 +30,13 @@ def test_pack_bits_against_oracle(nx, ny, nw, ns, pad):
     y = torch.empty_like(xd)
     p.unpack(pk, y)
     torch.cuda.synchronize()
-    want = opack.pack(x)
+    want = opack.pack(x, bits)
     assert pk.numel() == want.size == p.packed_bytes
     nblk = -(-2 * x.size // 16)
+    used = nblk * (16 * bits // 8 + 1)
     got = pk.cpu().numpy()
-    assert np.array_equal(got[:nblk * 17], want[:nblk * 17])
-    assert np.array_equal(y.cpu().numpy().view(np.float32), opack.unpack(want, x.shape).view(np.float32))
+    assert np.array_equal(got[:used], want[:used])
+    assert np.array_equal(y.cpu().numpy().view(np.float32), opack.unpack(want, x.shape, bits).view(np.float32))
     # buffers 8 bytes off a 16-byte boundary take the scalar path: same bytes
     xo = torch.zeros(x.size + 1, dtype=torch.complex64, device="cuda")[1:]
     xo.copy_(xd.ravel())
@@ -41,13 +44,13 @@ def test_pack_bits_against_oracle(nx, ny, nw, ns, pad):
     import ctypes
     from pyfwix_b200 import _lib as L
     from pyfwix_b200.plan import _stream
-    L.check(L.load().fwix_pack_rate8(p._h, ctypes.c_void_p(xo.data_ptr()), ctypes.c_void_p(po.data_ptr()),
-                                     _stream()))
+    pack, unpack = ((L.load().fwix_pack_rate8, L.load().fwix_unpack_rate8) if bits == 8 else
+                    (L.load().fwix_pack_wavefield, L.load().fwix_unpack_wavefield))
+    L.check(pack(p._h, ctypes.c_void_p(xo.data_ptr()), ctypes.c_void_p(po.data_ptr()), _stream()))
     yo = torch.zeros(x.size + 1, dtype=torch.complex64, device="cuda")[1:]
-    L.check(L.load().fwix_unpack_rate8(p._h, ctypes.c_void_p(po.data_ptr()), ctypes.c_void_p(yo.data_ptr()),
-                                       _stream()))
+    L.check(unpack(p._h, ctypes.c_void_p(po.data_ptr()), ctypes.c_void_p(yo.data_ptr()), _stream()))
     torch.cuda.synchronize()
-    assert np.array_equal(po.cpu().numpy()[:nblk * 17], want[:nblk * 17])
+    assert np.array_equal(po.cpu().numpy()[:used], want[:used])
     assert torch.equal(yo, y.ravel())
 
 
@@ -109,3 +112,36 @@ def test_packed_modelling_and_born(kind, nx, ny, pad, nw):
     n = int(np.prod(p.wshape))
     assert p.packed_bytes == opack.packed_bytes(2 * n)  # 17 bytes per 16 floats, padded to 256
     assert p.packed_bytes * 3.7 < 8 * n or n < 4096
+
+
+@pytest.mark.parametrize("kind", ["pspi", "nsps"])
+def test_rate16_born_within_gradient_tolerance(kind):
+    """At 16 mantissa bits per value the packed backgrounds (and the packed
+    per-level recursion fields) keep ExtendedBorn forward and adjoint within the
+    1e-3 gradient bar of the lossless operator, where rate 8 does not."""
+    g, rng, sref, labels, slow, den = make_case(nx=32, ny=24, nw=4, nz=6, nref=3, padx=4, pady=4)
+    slow = slow.copy()
+    slow[g.nz - 2:] *= 1.8
+    p = make_plan(g, 1, sref, labels, slow, den, step=kind)
+    src, rec = _acq(g, p)
+    wav = torch.as_tensor(crandn(rng, (1, g.nw)).astype(np.complex64)).cuda()
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((16, g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, wav, d, bd, bu)
+    r = torch.as_tensor(crandn(rng, d.shape).astype(np.complex64)).cuda()
+    g_ref = [torch.empty((g.nz, g.nw, g.ny, g.nx), dtype=torch.complex64, device="cuda") for _ in range(2)]
+    p.born(rec, bd, bu, g_ref[0], g_ref[1], r, adjoint=True)
+    errs = {}
+    for bits in (8, 16):
+        p.set_pack_rate(bits)
+        pd, pu = p.packed(g.nz), p.packed(g.nz)
+        dp = torch.empty_like(d)
+        p.propagate_packed(src, rec, wav, dp, pd, pu)
+        gp = [torch.empty_like(g_ref[0]) for _ in range(2)]
+        p.born_packed(rec, pd, pu, gp[0], gp[1], r, adjoint=True)
+        torch.cuda.synchronize()
+        errs[bits] = max(rel(gp[k].cpu().numpy(), g_ref[k].cpu().numpy()) for k in range(2))
+        if bits == 16:
+            assert rel(dp.cpu().numpy(), d.cpu().numpy()) < 1e-4
+    assert errs[16] < 1e-3 < errs[8] * 10 and errs[16] < errs[8] / 50, errs
