@@ -479,18 +479,27 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   };
   const long long roff = (c.bl * a.d.NY + (c.live ? c.y : 0)) * P::N;
   int term = next_term(0);
-  float2 pre[P::E];
-  if (term < nterm) {
+  // the next term's row is prefetched, except where the paired sums of 16-sample
+  // lanes leave no registers for it (two accumulators, the term and the hat indices)
+  constexpr bool kPrefetch = !(kPair && P::E >= 16);
+  float2 pre[kPrefetch ? P::E : 1];
+  if (kPrefetch && term < nterm) {
     const float2* src = a.t2 + (long long)term * a.tstride + roff;
 #pragma unroll
     for (int e = 0; e < P::E; ++e) pre[e] = c.live ? src[pos_last<P>(c.t, e)] : make_float2(0.f, 0.f);
   }
   while (term < nterm) {
     float2 v[P::E];
+    if constexpr (kPrefetch) {
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) v[e] = pre[e];
+      for (int e = 0; e < P::E; ++e) v[e] = pre[e];
+    } else {
+      const float2* src = a.t2 + (long long)term * a.tstride + roff;
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) v[e] = c.live ? src[pos_last<P>(c.t, e)] : make_float2(0.f, 0.f);
+    }
     const int nxt = next_term(term + 1);
-    if (nxt < nterm) {
+    if (kPrefetch && nxt < nterm) {
       const float2* src = a.t2 + (long long)nxt * a.tstride + roff;
 #pragma unroll
       for (int e = 0; e < P::E; ++e) pre[e] = c.live ? src[pos_last<P>(c.t, e)] : make_float2(0.f, 0.f);
