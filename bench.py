@@ -385,7 +385,7 @@ def fwi_shots_timing(device, ws, rank, barrier, nz=None):
             "shots": ws, "s": t}
 
 
-def config1_timing(device, reps=10):
+def config1_timing(device, reps=10, autotune=True):
     """Plain PSPI forward modelling + imaging of the first configuration (one shot,
     128 x 128 x 100, 64 frequencies 2-30 Hz, nref 4 quantile references, taper 20,
     15 Hz Ricker at the surface centre, receivers on every surface node):
@@ -424,7 +424,8 @@ def config1_timing(device, reps=10):
     return {"workload": w.name, "modelling_ms": t_model * 1e3, "imaging_ms": t_image * 1e3,
             "modelling_gcell_steps_per_s": 2 * cells / t_model / 1e9,
             "imaging_gcell_steps_per_s": 2 * cells / t_image / 1e9,
-            "modelling_plus_imaging_gcell_steps_per_s": 4 * cells / (t_model + t_image) / 1e9}
+            "modelling_plus_imaging_gcell_steps_per_s": 4 * cells / (t_model + t_image) / 1e9,
+            "tuning": tuning}
 
 
 def batched_timing(device, nshots=32, nz=None, nstreams=8):
@@ -789,7 +790,7 @@ def main():
             sh["s"] = float(tt.item())
         sh["shots_per_s"] = ws / sh["s"]
         fwi["shots_across_ranks"] = sh
-    config1 = config1_timing(device) if not a.no_config1 else None
+    config1 = config1_timing(device, autotune=not a.no_autotune) if not a.no_config1 else None
     if ws == 1 and not a.no_batched:
         batched = batched_timing(device, nshots=a.batched_shots, nz=a.batched_nz, nstreams=a.batched_streams)
     cpu = None

@@ -360,6 +360,26 @@ int timed(F run, int reps, float* ms) {
 
 extern "C" {
 
+// One in-place PSPI step of X [nw][NY][NX] at one level, as the sweeps below
+// take it: PSPI::cu_forward(model) (adjoint 0) or PSPI::cu_adjoint(data)
+// (adjoint 1), propagator/src/PSPI.cpp:64-102; sref [nref][nw] and labels
+// [NY][NX] of that level.  model_k, wfld_ref: wavefield scratch.
+int refshim_pspi_step(int adjoint, int NX, int NY, int nw, int nref, const float* w2, const float* kx,
+                      const float* ky, const void* sref, const int* labels, int* labw, float dz, float eps, int tapx,
+                      int tapy, void* X, void* model_k, void* wfld_ref) {
+  Shot sh;
+  sh.NX = NX, sh.NY = NY, sh.nx = NX, sh.ny = NY, sh.nw = nw, sh.nref = nref, sh.nz = 1, sh.tapx = tapx;
+  sh.tapy = tapy, sh.dz = dz, sh.eps = eps, sh.w2 = w2, sh.kx = kx, sh.ky = ky;
+  sh.sref = (const cuFloatComplex*)sref, sh.labels = labels, sh.labw = labw;
+  if (sh.init(model_k, wfld_ref) != 0) return -1;
+  Header hX(X, {NX, NY, nw, 1});
+  if (adjoint)
+    sh.adj(0, hX);
+  else
+    sh.fwd(0, hX);
+  return done();
+}
+
 // One shot (ns = 1, no padding: NX = nx, NY = ny).  task 0: modelling, data
 // [ntrace][nw] recorded, the down field of every level kept in keep [nz][nw][NY][NX];
 // slow2 / den2 are the per-frequency model with one level more,

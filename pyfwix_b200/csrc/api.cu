@@ -125,7 +125,7 @@ struct fwix_plan {
   int nterm_max = 1;
   long long chunk = 1;  // slices per launch: the intermediates of one chunk fit in L2
   bool fused = false;   // 256 x 256 slices: one-launch cluster step (fused256.cu), opt-in
-  bool col_tma = false; // column passes with TMA tiles where the plan allows (FWIX_COL_TMA)
+  bool col_tma = true;  // column passes with TMA tiles where the plan allows (FWIX_COL_TMA=0: copies)
   // depth steps in chunks alternating between the caller's stream and lane_s
   // (lanes = 2, set by fwix_plan_autotune), each lane with its own intermediates
   int lanes = 1;
@@ -690,7 +690,7 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
     const char* env = getenv("FWIX_FUSED");
     p->fused = p->d.NX == 256 && p->d.NY == 256 && env && env[0] == '1';
     const char* tma = getenv("FWIX_COL_TMA");
-    p->col_tma = tma && tma[0] == '1';
+    p->col_tma = !(tma && tma[0] == '0');
   }
   std::vector<float> w2(q.nw), w(q.nw);
   for (int i = 0; i < q.nw; ++i) {

@@ -39,6 +39,13 @@ __global__ void __launch_bounds__(256) k_pack(long long n, const float* __restri
   constexpr float LIM = (float)((1 << B) - 1);
   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nblk = (n + kBlk - 1) / kBlk;
+  {
+    // The bytes after the exponents, up to the 256-byte rounded size, are
+    // written as zeros, so that a packed field's bytes depend on its values
+    // alone (fewer than 256 of them; the grid has at least 256 threads).
+    const long long used = nblk * (kBlk * BITS / 8 + 1);
+    if (b < (used + 255) / 256 * 256 - used) exps[nblk + b] = 0;
+  }
   if (b >= nblk) return;
   float v[kBlk];
   const long long f0 = b * kBlk;

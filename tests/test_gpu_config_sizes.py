@@ -67,7 +67,18 @@ def refs_on_device(w, s2):
     sref, labels = refsampler.sample(s2, w.nref, w.padx, w.pady)
     sref_o, lab_o = oracle_refs.sample(s2.double().cpu().numpy(), w.nref, w.padx, w.pady)
     assert np.allclose(sref.cpu().numpy(), sref_o, rtol=1e-6, atol=0)
-    assert np.array_equal(labels.cpu().numpy().astype(np.int64), lab_o)
+    # Labels: the nearest reference.  A cell that lies (to float32 rounding)
+    # halfway between two references may take either; any other must agree.
+    lab = labels.cpu().numpy().astype(np.int64)
+    ny, nx = s2.shape[-2:]
+    x = s2.double().cpu().numpy()                                        # [nz][1][ny][nx]
+    c = np.asarray(sref_o).real[:, :, 0]                                 # [nz][nref]
+    pick = lambda l: np.take_along_axis(c[:, None, None, None, :], l[..., None], axis=-1)[..., 0]
+    dev, ora = lab[..., :ny, :nx], lab_o[..., :ny, :nx]
+    gap = np.abs(x - pick(dev)) - np.abs(x - pick(ora))
+    assert np.all(gap <= 1e-6 * np.abs(x)), gap.max()
+    assert np.mean(dev != ora) < 1e-3
+    assert np.array_equal(lab[..., ny:, :], lab[..., ny - 1:ny, :].repeat(lab.shape[-2] - ny, axis=-2))
     return refsampler.expand_refs(sref, w.nw), labels
 
 

@@ -42,8 +42,11 @@ def test_host_packed_backgrounds_equal_device_packed():
         p.born_packed(rec, pd, pu, ms, mr, out)
         gs, gr = torch.empty_like(ms), torch.empty_like(ms)
         p.born_packed(rec, pd, pu, gs, gr, out, adjoint=True)
+        # the stored bytes (each field's zero tail up to 256 bytes included) and the fields they unpack to
+        fields = torch.stack([p.unpack(pd[iz].cuda(), torch.empty(p.wshape, dtype=torch.complex64, device="cuda"))
+                              for iz in range(g.nz)])
         torch.cuda.synchronize()
-        res.append((d.clone(), pd.cpu(), out.clone(), gs.clone(), gr.clone()))
+        res.append((d.clone(), pd.cpu(), fields, out.clone(), gs.clone(), gr.clone()))
     for a, b in zip(*res):
         assert torch.equal(a.cpu(), b.cpu())
 
