@@ -61,6 +61,9 @@ def args_():
     ap.add_argument("--no-config1", action="store_true", help="skip the plain modelling + imaging timing")
     ap.add_argument("--no-autotune", action="store_true",
                     help="time the plan's default form of the depth step instead of the tuned one")
+    ap.add_argument("--tuning", default=None,
+                    help="apply this tuner choice instead of timing candidates: col_tma,slices_per_launch,streams"
+                         "[,fused] (profiling runs, where the tuner would time under the profiler)")
     ap.add_argument("--no-packed", action="store_true", help="skip the packed-background Born timing")
     ap.add_argument("--large", action="store_true",
                     help="run only the 512 x 512 x 400 x 200 Born on packed storage and print its own line")
@@ -146,7 +149,14 @@ def dist():
 
 # ----------------------------------------------------------------------------- B200 arm
 
-def setup_born(w, device, autotune=True):
+def parse_tuning(text):
+    """"col_tma,slices_per_launch,streams[,fused]" -> the dict Plan.set_tuning takes."""
+    f = [int(v) for v in text.split(",")]
+    return {"col_tma": bool(f[0]), "slices_per_launch": f[1], "streams": f[2],
+            "fused_cluster_step": bool(f[3]) if len(f) > 3 else False}
+
+
+def setup_born(w, device, autotune=True, tuning=None):
     import torch
 
     from pyfwix_b200 import refsampler
@@ -158,8 +168,13 @@ def setup_born(w, device, autotune=True):
     plan.set_refs(refsampler.expand_refs(sref, w.nw), labels)
     s2c = s2.to(torch.complex64)
     plan.set_model(s2c, torch.ones_like(s2c))
-    # the fastest equivalent form of this plan's depth step (else the plan's defaults)
-    tuning = plan.autotune() if autotune else None
+    # the fastest equivalent form of this plan's depth step (else the plan's
+    # defaults, or a choice given by the caller)
+    if tuning is not None:
+        plan.set_tuning(tuning)
+        tuning = dict(tuning, applied_without_timing=True)
+    else:
+        tuning = plan.autotune() if autotune else None
     g = w.geom
     src = plan.traces(g["sx"], g["sy"], g["sz"], np.zeros(len(g["sx"]), np.int32))
     rec = plan.traces(g["rx"], g["ry"], g["rz"], np.zeros(len(g["rx"]), np.int32))
@@ -695,7 +710,8 @@ def main():
     device = torch.device("cuda", torch.cuda.current_device())
     from pyfwix_b200 import workloads
     w = workloads.CONFIGS[a.config](nz=a.nz)
-    st = setup_born(w, device, autotune=not a.no_autotune)
+    st = setup_born(w, device, autotune=not a.no_autotune,
+                    tuning=parse_tuning(a.tuning) if a.tuning else None)
     for _ in range(a.warmup):
         born_step(st)
     torch.cuda.synchronize()

@@ -337,6 +337,12 @@ typedef struct fwix_tuning {
 } fwix_tuning;
 fwix_status fwix_plan_autotune(fwix_plan* plan, int kind, int iz, const void* in, void* out, int reps, void* stream,
                                fwix_tuning* result);
+/* fwix_plan_set_tuning applies a choice fwix_plan_autotune returned earlier (for a
+ * plan of the same sizes) without timing anything: col_tma, fused,
+ * slices_per_launch (1 .. ns * nw) and streams (1 or 2) are read, ms and
+ * candidates ignored.  A later call whose workspace is too small for the
+ * chosen slices per launch fails with FWIX_ERR_WORKSPACE. */
+fwix_status fwix_plan_set_tuning(fwix_plan* plan, const fwix_tuning* tuning);
 
 /* ---- allocation-free depth step ----------------------------------------------
  * fwix_step_noalloc has no counterpart in the reference.  It is fwix_step for

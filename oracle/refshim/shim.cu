@@ -387,7 +387,8 @@ int refshim_pspi_step(int adjoint, int NX, int NY, int nw, int nref, const float
 // reflection pairs the last level with itself, propagator/src/Reflect.h:20-38),
 // so that levels (iz, iz + 1) are the pair each reflection reads.  task 1:
 // lockstep migration of `data`, image [nz][ny][nx] (float); img_w [nw][ny][nx]
-// scratch.  S, R, model_k, wfld_ref: wavefield
+// scratch; task 2: the same with the receivers injected without the race of
+// Injection's launch shape (below).  S, R, model_k, wfld_ref: wavefield
 // scratch [nw][NY][NX].  One warm-up run, then `reps` runs between CUDA events
 // (the image / data are zeroed before each run); *ms receives the mean time.
 int refshim_shot_timed(int task, int NX, int NY, int nw, int nz, int nref, const float* w2, const float* kx,
@@ -440,13 +441,20 @@ int refshim_shot_timed(int task, int NX, int NY, int nw, int nz, int nref, const
     return st;
   }
   Header img(img_w, {NX, NY, nw});
+  // Task 2 launches the receivers' injection with one thread per frequency, each
+  // looping over every trace: inj_forward adds into the wavefield without atomics
+  // (injection.cu:89-92), so under Injection's launch shape the traces whose
+  // bilinear footprints share a cell (receivers on adjacent nodes) race and some
+  // additions are lost.  Same kernel, same arithmetic, no race; slower, so only
+  // for parity.
+  const dim3 gri = task == 2 ? dim3((nw + 15) / 16, 1) : gr, bri = task == 2 ? dim3(16, 1) : b2;
   auto run = [&]() {
     cudaMemsetAsync(image, 0, (size_t)nz * plane * sizeof(float));
     cudaMemsetAsync(S, 0, fb);
     cudaMemsetAsync(R, 0, fb);
     for (int iz = 0; iz < nz; ++iz) {
       inj_forward<<<gs, b2>>>(wav.v, hS.v, scx, scy, scz, sids, oz, dz, iz);
-      inj_forward<<<gr, b2>>>(dat.v, hR.v, rcx, rcy, rcz, rids, oz, dz, iz);
+      inj_forward<<<gri, bri>>>(dat.v, hR.v, rcx, rcy, rcz, rids, oz, dz, iz);
       cudaMemsetAsync(img_w, 0, (size_t)plane * nw * sizeof(cuFloatComplex));
       ic_adj<<<sh.g, sh.b>>>(img.v, hR.v, hS.v);
       k_sum_w<<<(unsigned)((plane + 255) / 256), 256>>>((const cuFloatComplex*)img_w, image + iz * plane, nw, plane);

@@ -92,6 +92,7 @@ SIGNATURES = {
     "fwix_migrate": [P, P, P, P, P, P, I, P],
     "fwix_born": [P, I, P, P, P, P, P, I64, P, I, P],
     "fwix_plan_autotune": [P, I, I, P, P, I, P, ctypes.POINTER(FwixTuning)],
+    "fwix_plan_set_tuning": [P, ctypes.POINTER(FwixTuning)],
     "fwix_step_noalloc": [ctypes.POINTER(FwixDesc), I, I, I, P, P, I64, I64, P, P, I, P],
     "fwix_pspi_step": [P, I, P, P, I, P],
     "fwix_nsps_step": [P, I, P, P, I, P],

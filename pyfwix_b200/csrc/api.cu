@@ -310,9 +310,13 @@ fwix_status step_chunk(fwix_plan* p, int kind, int iz, int dir, SpecArgs a, cuda
 }
 
 fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, float2* out, int add,
-                    cudaStream_t s, const float2* in2 = nullptr) {
+                    cudaStream_t s, const float2* in2 = nullptr, const float2* ic_bg = nullptr,
+                    float* ic_img = nullptr) {
   SpecArgs a0 = p->args(in, out, add);
   a0.in2 = in2;  // the step of in + in2 (linear: one step instead of two)
+  // image epilogue of the last (inverse row) pass: ic_img += Re sum conj(ic_bg) out
+  a0.ic_bg = ic_bg;
+  a0.ic_img = ic_img;
   FWIX_TRY(phase_factors(p, iz, a0, s));
   if (p->lanes < 2 || p->fused)
     return for_chunks(p, a0, [&](const SpecArgs& a) { return step_chunk(p, kind, iz, dir, a, s); });
@@ -1232,13 +1236,27 @@ fwix_status fwix_migrate(fwix_plan* p, const fwix_traces* src, const fwix_traces
   FWIX_CU(cudaMemsetAsync(S, 0, p->wbytes(), s));
   FWIX_CU(cudaMemsetAsync(R, 0, p->wbytes(), s));
   const long long plane = (long long)p->d.ny * p->d.nx;
-  for (int iz = 0; iz < nz; ++iz) {
-    FWIX_TRY(do_inject(p, src, iz, (const float2*)wavelet, S, s));
-    FWIX_TRY(do_inject(p, rec, iz, (const float2*)data, R, s));
-    FWIX_TRY(cu(fwix::launch_image_acc(p->d, S, R, image + iz * plane, add, s), "image"));
-    if (iz < nz - 1) {
-      FWIX_TRY(do_step(p, k, iz, FWIX_FWD, S, S, 0, s));
+  // The image of a level is summed by the receiver step that reaches it (the
+  // epilogue of its inverse row pass, reading S of that level), except at the
+  // first level and at levels where receivers inject: there the field is only
+  // complete after the injection, and one correlation pass sums the image.
+  // The one-launch cluster step has no such epilogue.
+  const bool fuse = !p->fused;
+  if (!add) FWIX_CU(cudaMemsetAsync(image, 0, (size_t)nz * plane * sizeof(float), s));
+  FWIX_TRY(do_inject(p, src, 0, (const float2*)wavelet, S, s));
+  FWIX_TRY(do_inject(p, rec, 0, (const float2*)data, R, s));
+  FWIX_TRY(cu(fwix::launch_image_acc(p->d, S, R, image, 1, s), "image"));
+  for (int iz = 0; iz + 1 < nz; ++iz) {
+    float* img = image + (iz + 1) * plane;
+    FWIX_TRY(do_step(p, k, iz, FWIX_FWD, S, S, 0, s));
+    FWIX_TRY(do_inject(p, src, iz + 1, (const float2*)wavelet, S, s));
+    const fwix::InjectLevel* L = level_of(rec, iz + 1);
+    if (fuse && !(L && L->ncell > 0)) {
+      FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, R, R, 0, s, nullptr, S, img));
+    } else {
       FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_INPL, R, R, 0, s));
+      FWIX_TRY(do_inject(p, rec, iz + 1, (const float2*)data, R, s));
+      FWIX_TRY(cu(fwix::launch_image_acc(p->d, S, R, img, 1, s), "image"));
     }
   }
   return FWIX_OK;
@@ -1383,6 +1401,28 @@ fwix_status fwix_plan_autotune(fwix_plan* p, int kind, int iz, const void* in, v
     result->candidates = tried;
     result->streams = pick.lanes;
   }
+  return FWIX_OK;
+}
+
+// A choice fwix_plan_autotune made earlier (for a plan of the same sizes),
+// applied without timing: tile movement, slices per launch, lanes, cluster step.
+fwix_status fwix_plan_set_tuning(fwix_plan* p, const fwix_tuning* t) {
+  if (!p || !t) return fail(FWIX_ERR_INVALID, "null argument");
+  const long long slices = (long long)p->d.ns * p->d.nw;
+  if (t->slices_per_launch < 1 || t->slices_per_launch > slices)
+    return fail(FWIX_ERR_INVALID, "slices_per_launch must be in [1, ns * nw]");
+  if (t->streams != 1 && t->streams != 2) return fail(FWIX_ERR_INVALID, "streams must be 1 or 2");
+  if (t->fused && !(p->d.NX == 256 && p->d.NY == 256 && fwix::fused_step_available()))
+    return fail(FWIX_ERR_UNSUPPORTED, "the one-launch cluster step needs 256 x 256 slices");
+  if (t->streams == 2 && !p->lane_s) {
+    FWIX_CU(cudaStreamCreateWithFlags(&p->lane_s, cudaStreamNonBlocking));
+    FWIX_CU(cudaEventCreateWithFlags(&p->lane_fork, cudaEventDisableTiming));
+    FWIX_CU(cudaEventCreateWithFlags(&p->lane_join, cudaEventDisableTiming));
+  }
+  p->col_tma = t->col_tma != 0;
+  p->chunk = t->slices_per_launch;
+  p->fused = t->fused != 0;
+  p->lanes = t->streams;
   return FWIX_OK;
 }
 

@@ -555,6 +555,11 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
     if (post_taper) v = cscale(v, a.tapx[x] * ty);
     if (a.add) v = cadd(dst[x], v);
     dst[x] = v;
+    if (a.ic_img && c.y < a.d.ny && x < a.d.nx) {
+      // a warp's lanes hold consecutive x for each e: coalesced reductions
+      const float2 bg = a.ic_bg[(c.b * a.d.NY + c.y) * P::N + x];
+      atomicAdd(a.ic_img + (long long)c.y * a.d.nx + x, bg.x * v.x + bg.y * v.y);
+    }
     if constexpr (kPair) {
       float2 u = hat_smem ? cmul(acc2[e], cell) : acc2[e];
       if (post_taper) u = cscale(u, a.tapx[x] * ty);

@@ -117,6 +117,11 @@ struct SpecArgs {
   // bounded wait that runs out adds one to *err (the plan's error word)
   int tma;
   unsigned* err;
+  // inverse row pass image epilogue (the lockstep migration): for every output
+  // sample of the unpadded window, ic_img[y][x] += Re(conj(ic_bg[b][y][x]) out)
+  // by float atomics (ic_img NULL: none)
+  const float2* ic_bg;
+  float* ic_img;
 };
 
 // Spectral passes (dispatch.cu: register-resident passes for lengths with a

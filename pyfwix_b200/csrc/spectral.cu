@@ -117,6 +117,10 @@ __global__ void __launch_bounds__(256) k_row_inverse(const SpecArgs a, int nchun
       if (post_taper) v = cscale(v, a.tapx[x] * ty);
       if (a.add) v = cadd(a.out[roff + x], v);
       a.out[roff + x] = v;
+      if (a.ic_img && y < a.d.ny && x < a.d.nx) {
+        const float2 bg = a.ic_bg[roff + x];
+        atomicAdd(a.ic_img + (long long)y * a.d.nx + x, bg.x * v.x + bg.y * v.y);
+      }
     }
     __syncwarp();
   }

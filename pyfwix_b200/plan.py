@@ -178,6 +178,16 @@ class Plan:
                 "slices_per_launch": int(res.slices_per_launch), "streams": int(res.streams),
                 "step_ms": float(res.ms), "candidates": int(res.candidates)}
 
+    def set_tuning(self, choice):
+        """Applies a choice ``autotune`` returned (the dict, for a plan of the same
+        sizes) without timing anything (fwix_plan_set_tuning)."""
+        t = L.FwixTuning()
+        t.col_tma = int(bool(choice["col_tma"]))
+        t.fused = int(bool(choice.get("fused_cluster_step", False)))
+        t.slices_per_launch = int(choice["slices_per_launch"])
+        t.streams = int(choice.get("streams", 1))
+        L.check(self.lib.fwix_plan_set_tuning(self._h, ctypes.byref(t)))
+
     def smooth_step_pair(self, iz, inp, out, deriv, add=False):
         """out (+)= the smooth forward step of inp and deriv (+)= its slowness
         derivative, from one set of transforms."""

@@ -83,7 +83,8 @@ def _job(task, g, i0, i1, a):
         wav = a["wavelet"]
         d_obs = wem.smooth_propagate(gb, a["refs"], a["s_true"], acq, wav)[0]
         J, grad = wem.smooth_gradient(gb, a["refs"], a["s0"], acq, wav, d_obs)
-        return d_obs, J, grad
+        data0 = wem.smooth_propagate(gb, a["refs"], a["s0"], acq, wav)[0]
+        return d_obs, J, grad, data0
     slow, den, st = _model(gb, a["s2"], a["labels"], a["sref"], a["kind"])
     wav = a["wavelet"]
     data, bgd, bgu = wem.propagate(gb, st, acq, slow, den, wav)
@@ -114,12 +115,14 @@ def run(task, g, args, nband=None):
       per depth and cell for every frequency) and adjoint of ``args["r"]`` ->
       {"data", "born" [ntr][nw], "gs", "gr" [nz][ny][nx] summed over frequency};
     * "smooth": smooth-step modelling of s_true (d_obs) and the adjoint-state
-      gradient at s0 -> (d_obs [ntr][nw], J, gradient [nz][ny][nx])."""
+      gradient at s0 -> (d_obs [ntr][nw], J, gradient [nz][ny][nx], data at s0
+      [ntr][nw])."""
     parts = bands(g.nw, nband)
     futs = [pool().submit(_job, task, g, i0, i1, _band_args(args, i0, i1)) for i0, i1 in parts]
     res = [f.result() for f in futs]
     if task == "smooth":
-        return (np.concatenate([r[0] for r in res], axis=1), sum(r[1] for r in res), sum(r[2] for r in res))
+        return (np.concatenate([r[0] for r in res], axis=1), sum(r[1] for r in res), sum(r[2] for r in res),
+                np.concatenate([r[3] for r in res], axis=1))
     out = {"data": np.concatenate([r["data"] for r in res], axis=1)}
     if task == "migrate":
         out["image"] = sum(r["image"] for r in res)

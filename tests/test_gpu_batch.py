@@ -2,7 +2,8 @@
 (pyfwix_b200/batch.py): every instance's data and image against the FP64
 oracle (Propagator.cpp:121-221 modelling, lockstep migration image), and the
 three execution modes -- shot after shot, over CUDA streams, replayed from one
-captured CUDA graph -- giving identical images."""
+captured CUDA graph -- giving the same images (to the rounding of their
+frequency sums, which float atomics add in no fixed order)."""
 import numpy as np
 import pytest
 import torch
@@ -63,7 +64,8 @@ def test_batch_modes_and_oracle():
         run()
         torch.cuda.synchronize()
         for im, ref in zip(b.images(), plain):
-            assert torch.equal(im, ref)
+            # images are summed over frequency by float atomics: order-dependent rounding
+            assert rel(im.cpu().numpy(), ref.cpu().numpy()) < 1e-6
 
 
 def _acq_plan(seed, nx, ny, nw, nz, kind, pad=4):

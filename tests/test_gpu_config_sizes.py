@@ -68,7 +68,8 @@ def refs_on_device(w, s2):
     sref_o, lab_o = oracle_refs.sample(s2.double().cpu().numpy(), w.nref, w.padx, w.pady)
     assert np.allclose(sref.cpu().numpy(), sref_o, rtol=1e-6, atol=0)
     # Labels: the nearest reference.  A cell that lies (to float32 rounding)
-    # halfway between two references may take either; any other must agree.
+    # halfway between two references, or at two equal references (the quantiles
+    # of a layered level repeat), may take either; any other must agree.
     lab = labels.cpu().numpy().astype(np.int64)
     ny, nx = s2.shape[-2:]
     x = s2.double().cpu().numpy()                                        # [nz][1][ny][nx]
@@ -77,7 +78,6 @@ def refs_on_device(w, s2):
     dev, ora = lab[..., :ny, :nx], lab_o[..., :ny, :nx]
     gap = np.abs(x - pick(dev)) - np.abs(x - pick(ora))
     assert np.all(gap <= 1e-6 * np.abs(x)), gap.max()
-    assert np.mean(dev != ora) < 1e-3
     assert np.array_equal(lab[..., ny:, :], lab[..., ny - 1:ny, :].repeat(lab.shape[-2] - ny, axis=-2))
     return refsampler.expand_refs(sref, w.nw), labels
 
@@ -228,15 +228,23 @@ def test_config4_fwi_gradient():
     prob = SmoothFWI(s_true.shape, w.geom, wav, dict(par, checkpoint=None))
     prob.set_slowness(torch.as_tensor(s_true))
     refs = prob.refs.clone()
-    d_obs_o, _, grad_o = oracle_bands.run("smooth", grid(w), dict(
+    d_obs_o, _, grad_o, data_o = oracle_bands.run("smooth", grid(w), dict(
         geom=w.geom, refs=refs.cpu().numpy().astype(np.float64), s_true=s_true.astype(np.float64),
         s0=s0.astype(np.float64), wavelet=w.wavelet.astype(np.complex128)))
+    # Over three levels the data of both models are the same direct arrival up to
+    # small reflections, so d(s0) - d_obs keeps only a few of the FP32 digits of
+    # either.  The residual is therefore checked on the data's scale, and the
+    # gradient (linear in the residual) is taken of the oracle's FP64 residual.
+    res_o = data_o - d_obs_o
+    res_dev = torch.as_tensor(res_o.astype(np.complex64)).cuda()
     for checkpoint in (None, 2):
         prob = SmoothFWI(s_true.shape, w.geom, wav, dict(par, refs=refs, checkpoint=checkpoint))
         d_obs = prob.model(torch.as_tensor(s_true), keep=False)
         assert rel(to_host(d_obs), d_obs_o) < TOL
         data = prob.model(torch.as_tensor(s0), keep=True)
-        grad = prob.gradient(data - d_obs).cpu().numpy()
+        assert rel(to_host(data), data_o) < TOL
+        assert np.linalg.norm(to_host(data - d_obs) - res_o) < TOL * np.linalg.norm(d_obs_o)
+        grad = prob.gradient(res_dev).cpu().numpy()
         assert rel(grad, grad_o) < GTOL, (checkpoint, rel(grad, grad_o))
 
 

@@ -112,7 +112,14 @@ def test_fwi_gradient_central_differences_on_device():
     s_true = np.ascontiguousarray(s_true[z0:z0 + 3])
     s0 = np.ascontiguousarray(s0[z0:z0 + 3])
     w.oz, w.nz = z0 * w.dz, 3
-    geom = dict(w.geom, sz=np.full(1, w.oz, np.float32), rz=np.full(len(w.geom["rz"]), w.oz, np.float32))
+    # the receivers off the source's cells: there the data are the reflections
+    # alone, whose change with s stands far above the FP32 rounding of the data
+    # (with the direct arrival recorded, d(s + h ds) - d(s - h ds) would keep few
+    # of its digits)
+    g0 = w.geom
+    far = (g0["rx"] - g0["sx"][0]) ** 2 + (g0["ry"] - g0["sy"][0]) ** 2 > (4 * w.dx) ** 2
+    geom = dict(g0, sz=np.full(1, w.oz, np.float32), rx=g0["rx"][far], ry=g0["ry"][far],
+                rz=np.full(int(far.sum()), w.oz, np.float32), r_ids=g0["r_ids"][far])
     par = dict(nref=w.nref, padx=0, pady=0, taperx=w.taperx, tapery=w.tapery, eps=0.0, ox=w.ox, oy=w.oy,
                oz=w.oz, dx=w.dx, dy=w.dy, dz=w.dz, ow=w.ow, dw=w.dw, checkpoint=None)
     wav = torch.as_tensor(w.wavelet).cuda()

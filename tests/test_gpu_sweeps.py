@@ -65,14 +65,24 @@ def test_propagate(kind, nx, ny, pad):
     assert rel(to_host(d2), 2 * data) < TOL
 
 
-def test_migrate():
-    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case()
+@pytest.mark.parametrize("kind,nx,ny,pad", [("pspi", 32, 24, 4), ("nsps", 32, 24, 4), ("pspi", 64, 64, 0),
+                                             ("nsps", 60, 60, 4)])
+def test_migrate(kind, nx, ny, pad):
+    """Lockstep migration of two shots with receivers at two depths (levels 0-2):
+    the image of the levels without receiver injection is summed in the receiver
+    step's last pass, the others by a separate correlation; generic and
+    register-resident lengths; add semantics."""
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind, nx=nx, ny=ny, pad=pad)
     data = crandn(rng, (len(acq.rec.ix), g.nw))
     img = wem.migrate(g, st, acq, wav, data)
     out = torch.empty((g.nz, g.ny, g.nx), dtype=torch.float32, device="cuda")
     p.migrate(src, rec, to_dev(wav), to_dev(data), out)
     torch.cuda.synchronize()
     assert rel(out.cpu().numpy(), img) < TOL
+    base = torch.ones((g.nz, g.ny, g.nx), dtype=torch.float32, device="cuda")
+    p.migrate(src, rec, to_dev(wav), to_dev(data), base, add=True)
+    torch.cuda.synchronize()
+    assert rel(base.cpu().numpy() - 1, img) < TOL
 
 
 @pytest.mark.parametrize("kind,taper,nx,ny,pad", [("pspi", 3, 32, 24, 4), ("nsps", 0, 32, 24, 4),

@@ -85,3 +85,24 @@ def test_autotune_keeps_the_step(n, step):
     torch.cuda.synchronize()
     assert rel(to_host(after), to_host(before)) < 1e-6
     assert int(p.lib.fwix_plan_wait_timeouts(p._h)) == 0
+
+
+def test_set_tuning_applies_a_saved_choice():
+    """fwix_plan_set_tuning: a second plan of the same sizes takes the first one's
+    tuned choice without timing; its step equals the untuned step; out-of-range
+    choices are refused."""
+    from pyfwix_b200 import _lib as L
+    g, rng, sref, labels, slow, den = make_case(nx=256, ny=256, nw=8, nz=3, nref=4)
+    p = make_plan(g, 1, sref, labels, slow, den, step="nsps")
+    q = make_plan(g, 1, sref, labels, slow, den, step="nsps")
+    x = to_dev(wavefield(rng, 1, g))
+    before = q.step(1, x, torch.empty_like(x))
+    choice = p.autotune(iz=1, reps=2)
+    q.set_tuning(choice)
+    after = q.step(1, x, torch.empty_like(x))
+    torch.cuda.synchronize()
+    assert rel(to_host(after), to_host(before)) < 1e-6
+    for bad in (dict(choice, slices_per_launch=0), dict(choice, streams=3),
+                dict(choice, slices_per_launch=g.nw + 1)):
+        with pytest.raises(RuntimeError):
+            q.set_tuning(bad)

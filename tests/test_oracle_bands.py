@@ -54,8 +54,8 @@ def test_banded_smooth_gradient_equals_one_run():
     s = np.sqrt(a["s2"])
     refs = wem.smooth_refs(s, g.nref)
     b = dict(geom=a["geom"], refs=refs, s_true=s * 1.01, s0=s, wavelet=a["wavelet"])
-    d1, J1, g1 = _serial("smooth", g, b)
-    d2, J2, g2 = oracle_bands.run("smooth", g, b, nband=3)
-    assert np.allclose(d2, d1, rtol=1e-12, atol=1e-14)
+    d1, J1, g1, m1 = _serial("smooth", g, b)
+    d2, J2, g2, m2 = oracle_bands.run("smooth", g, b, nband=3)
+    assert np.allclose(d2, d1, rtol=1e-12, atol=1e-14) and np.allclose(m2, m1, rtol=1e-12, atol=1e-14)
     assert abs(J2 / J1 - 1) < 1e-12
     assert np.allclose(g2, g1, rtol=1e-10, atol=1e-12 * np.abs(g1).max())
