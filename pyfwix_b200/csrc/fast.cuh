@@ -325,10 +325,23 @@ struct RowCtx {
 // Resident CTAs per SM the forward row pass's registers are held to: the
 // multi-term passes of 12- and 16-sample lanes at two (the scattering adjoint's,
 // with one term's weights and no labels, at three), the rest unhinted.
+// Compile-time occupancy knobs (defaults as measured best): resident CTAs of the
+// multi-term forward and inverse row passes and of the multi-input column pass
+// with 16-sample lanes, and whether the multi-term inverse row pass prefetches
+// the next term's row.
+#ifndef FWIX_ROW_MULTI_MINB
+#define FWIX_ROW_MULTI_MINB 2
+#endif
+#ifndef FWIX_ROWINV_PREFETCH
+#define FWIX_ROWINV_PREFETCH 1
+#endif
+#ifndef FWIX_COLB_MINB16
+#define FWIX_COLB_MINB16 2
+#endif
 template <class P, int PRE>
 constexpr int row_fwd_min_blocks() {
   if (PRE == W_SCAT_CONJ && P::E == 16) return 3;
-  return multi_term(PRE) && (P::E == 16 || P::E == 12) ? 2 : 0;
+  return multi_term(PRE) && (P::E == 16 || P::E == 12) ? FWIX_ROW_MULTI_MINB : 0;
 }
 
 // t1[term] = F_x(pre_term * in) for each term.
@@ -424,7 +437,7 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
 // transformed term twice, with the smooth weights into out and with their
 // slowness derivatives into out2.
 template <class P, int POST>
-__global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 || P::E == 12) ? 2 : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
+__global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 || P::E == 12) ? FWIX_ROW_MULTI_MINB : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   load_stage_tw<P>(c.tw, a.twx);
@@ -481,7 +494,7 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   int term = next_term(0);
   // the next term's row is prefetched, except where the paired sums of 16-sample
   // lanes leave no registers for it (two accumulators, the term and the hat indices)
-  constexpr bool kPrefetch = !(kPair && P::E >= 16);
+  constexpr bool kPrefetch = FWIX_ROWINV_PREFETCH && !(kPair && P::E >= 16);
   float2 pre[kPrefetch ? P::E : 1];
   if (kPrefetch && term < nterm) {
     const float2* src = a.t2 + (long long)term * a.tstride + roff;
@@ -582,7 +595,7 @@ struct ColGeo {
   // Resident CTAs per SM the register allocation is held to: four for plans of
   // at most 8 samples per lane (64 registers; the few spills stay in L1 and the
   // extra warps hide more latency than they cost), else what fits.
-  static constexpr int kMinBlocks = P::E <= 8 ? 4 : P::E <= 16 ? 2 : 1;
+  static constexpr int kMinBlocks = P::E <= 8 ? 4 : P::E <= 16 ? FWIX_COLB_MINB16 : 1;
   // k_col_a holds one spectrum and one term in registers (k_col_b a running sum
   // as well): with 16 samples per lane it fits three CTAs per SM
   static constexpr int kMinBlocksA = P::E <= 8 ? 4 : P::E <= 12 ? 2 : P::E <= 16 ? 3 : 1;

@@ -123,9 +123,17 @@ def test_fwi_gradient_central_differences_on_device():
     par = dict(nref=w.nref, padx=0, pady=0, taperx=w.taperx, tapery=w.tapery, eps=0.0, ox=w.ox, oy=w.oy,
                oz=w.oz, dx=w.dx, dy=w.dy, dz=w.dz, ow=w.ow, dw=w.dw, checkpoint=None)
     wav = torch.as_tensor(w.wavelet).cuda()
-    prob = SmoothFWI(s_true.shape, geom, wav, par)
-    prob.set_slowness(torch.as_tensor(s_true))
-    prob = SmoothFWI(s_true.shape, geom, wav, dict(par, refs=prob.refs.clone()))
+    # Fixed references with the starting slowness inside one interval, 2 % from
+    # either end: the smooth step is piecewise linear in s between references,
+    # so J has kinks at the reference values, and a central difference across
+    # one averages two slopes.  The starting model is laterally constant on a
+    # level and is an end of the true model's range (the references
+    # smooth_refs would take), so every cell would sit on a kink.
+    lev = s0.mean(axis=(1, 2)).astype(np.float64)
+    refs = torch.as_tensor(lev[:, None] * (1 + np.array([-0.06, -0.02, 0.02, 0.06]))[None, :],
+                           dtype=torch.float32).cuda()
+    assert w.nref == refs.shape[1] and np.allclose(s0, lev[:, None, None])
+    prob = SmoothFWI(s_true.shape, geom, wav, dict(par, refs=refs))
     d_obs = prob.model(torch.as_tensor(s_true), keep=False).to(torch.complex128)
     s0t = torch.as_tensor(s0, dtype=torch.float64)
     data = prob.model(s0t.float(), keep=True)
