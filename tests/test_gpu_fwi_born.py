@@ -101,9 +101,9 @@ def test_fwi_gradient_ties_to_born_adjoint():
 def test_fwi_gradient_central_differences_on_device():
     """The central finite-difference check of the FWI configuration, on the
     device: 384 x 384 x 96 frequencies, three levels through the first anomaly,
-    h = 1e-3 relative.  A single cell moves the FP32 objective by less than its
+    h = 1e-2 relative.  A single cell moves the FP32 objective by less than its
     rounding, so each of the 16 random cells is the centre of a Gaussian
-    perturbation (sigma 8 cells on its level); (J(s + h ds) - J(s - h ds)) / 2h
+    perturbation (sigma 16 cells on its level); (J(s + h ds) - J(s - h ds)) / 2h
     must equal <dJ/ds, ds> from the adjoint-state gradient."""
     from pyfwix_b200 import workloads
     from pyfwix_b200.fwi import SmoothFWI
@@ -146,17 +146,22 @@ def test_fwi_gradient_central_differences_on_device():
     rng = np.random.default_rng(1003)
     ny, nx = s0.shape[1:]
     yy, xx = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
-    h = 1e-3
-    fd, ad = [], []
+    # h = 1e-2 of s at the bump's centre (the slowness stays inside its reference
+    # interval): the data are FP32, so J carries a rounding of about 1e-7 of
+    # itself, and for h = 1e-3 the change h <dJ/ds, ds> of some bumps is no larger
+    h = 1e-2
+    fd, ad, at = [], [], []
     for _ in range(16):
-        iz, iy, ix = int(rng.integers(0, 2)), int(rng.integers(20, ny - 20)), int(rng.integers(20, nx - 20))
+        iz, iy, ix = int(rng.integers(0, 2)), int(rng.integers(24, ny - 24)), int(rng.integers(24, nx - 24))
         bump = np.zeros(s0.shape)
-        bump[iz] = np.exp(-((yy - iy) ** 2 + (xx - ix) ** 2) / (2 * 8.0 ** 2))
+        bump[iz] = np.exp(-((yy - iy) ** 2 + (xx - ix) ** 2) / (2 * 16.0 ** 2))
         ds = s0t * torch.as_tensor(bump)
         fd.append((objective(s0t + h * ds) - objective(s0t - h * ds)) / (2 * h))
         ad.append(float(torch.sum(grad * ds)))
+        at.append((iz, iy, ix))
     fd, ad = np.array(fd), np.array(ad)
     err = np.abs(fd - ad) / np.abs(ad).max()
+    k = int(np.argmax(err))
     assert np.abs(ad).max() > 0
-    assert err.max() < 1e-2, (fd, ad)
+    assert err.max() < 1e-2, ("worst", at[k], fd[k], ad[k], err[k], "source", g0["sx"][0] / w.dx, g0["sy"][0] / w.dy)
     assert rel(fd, ad) < 1e-2, (fd, ad)
