@@ -213,7 +213,9 @@ fwix_status fwix_upward(fwix_plan* plan, int adjoint, void* wfld, void* stream);
 fwix_status fwix_propagate(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
                            const void* wavelet, void* data, int add, void* bg_down, void* bg_up,
                            void* stream);
-/* Lockstep migration image[nz][ny][nx] (float) (+)= sum_w Re sum_s conj(S) R. */
+/* Lockstep migration image[nz][ny][nx] (float) (+)= sum_w Re sum_s conj(S) R.  The
+ * sum over frequencies and shots is taken with float atomics in no fixed order:
+ * repeated calls agree to rounding, not bit for bit. */
 fwix_status fwix_migrate(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
                          const void* wavelet, const void* data, float* image, int add,
                          void* stream);

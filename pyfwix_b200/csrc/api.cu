@@ -126,6 +126,7 @@ struct fwix_plan {
   long long chunk = 1;  // slices per launch: the intermediates of one chunk fit in L2
   bool fused = false;   // 256 x 256 slices: one-launch cluster step (fused256.cu), opt-in
   bool col_tma = true;  // column passes with TMA tiles where the plan allows (FWIX_COL_TMA=0: copies)
+  int qtile = 1;        // SpecArgs::qtile bits (FWIX_QTILE)
   // depth steps in chunks alternating between the caller's stream and lane_s
   // (lanes = 2, set by fwix_plan_autotune), each lane with its own intermediates
   int lanes = 1;
@@ -139,7 +140,8 @@ struct fwix_plan {
   int pslots = 0;             // depth iz lives in slot iz % pslots
   std::vector<int> pslot_iz;  // depth whose current factors a slot holds, -1 for none
   int pq_nx() const { return d.NX / 2 + 1; }
-  int pq_ny() const { return d.NY / 2 + 1; }
+  // ky extent of the phase table rounded up to even: 16-byte rows for the TMA tiles
+  int pq_ny() const { return (d.NY / 2 + 2) & ~1; }
   long long pdepth() const { return (long long)desc.nref * d.nw * pq_nx() * pq_ny(); }
   float coef[5] = {1.f, 1.f / 2.f, 3.f / 8.f, 5.f / 16.f, 35.f / 128.f};  // Scatter.h:526
 
@@ -202,6 +204,7 @@ struct fwix_plan {
     a.tstride = chunk * d.slice;
     a.tma = col_tma ? 1 : 0;
     a.err = err;
+    a.qtile = qtile;
     return a;
   }
 };
@@ -695,6 +698,7 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
     p->fused = p->d.NX == 256 && p->d.NY == 256 && env && env[0] == '1';
     const char* tma = getenv("FWIX_COL_TMA");
     p->col_tma = !(tma && tma[0] == '0');
+    if (const char* q = getenv("FWIX_QTILE")) p->qtile = atoi(q) & 3;
   }
   std::vector<float> w2(q.nw), w(q.nw);
   for (int i = 0; i < q.nw; ++i) {

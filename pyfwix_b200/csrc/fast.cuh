@@ -20,6 +20,7 @@
 // barrier.  Column passes (lines along y) stage a tile of LX columns x NY rows
 // through shared memory so that HBM is read and written in row segments.
 #pragma once
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -797,20 +798,50 @@ struct ColTma {
   static constexpr int NBOX = P::N <= 256 ? 1 : (P::N % 2 == 0 && P::N / 2 <= 256 ? 2 : 4);
   static constexpr int ROWS = P::N / NBOX;  // rows per box (<= 256)
   static_assert(ROWS * NBOX == P::N && ROWS <= 256, "a tile is a whole number of boxes of at most 256 rows");
-  // two tiles, the twiddles, two mbarriers, and room to align the tiles to 1024 bytes
-  static size_t smem() { return (size_t)2 * TILE * sizeof(float2) + tw_size<P>() * sizeof(float2) + 16 + 1024; }
+  // two tiles, the twiddles, two mbarriers, and room to align the tiles to 1024
+  // bytes; with the phase tiles (qt samples each: LX |kx| rows of the cached
+  // quarter spectrum) two of those after the term tiles
+  static size_t smem(size_t qt = 0) {
+    return (size_t)(2 * TILE + 2 * qt) * sizeof(float2) + tw_size<P>() * sizeof(float2) + 16 + 1024;
+  }
 };
 
-template <class P, int QM>
+// The CTA's columns x0 .. x0 + LX - 1 read the phase factors of |kx| = min(x, NX - x):
+// LX consecutive values from k0 (increasing for x0 < NX / 2, decreasing above; a
+// tile never straddles NX / 2 when NX / 2 is a multiple of LX).  Row of column x.
+template <class P>
+__device__ __forceinline__ int qtile_k0(const SpecArgs& a, int x0) {
+  constexpr int LX = ColGeo<P>::LX;
+  return x0 < a.d.NX / 2 ? x0 : a.d.NX - x0 - (LX - 1);
+}
+__device__ __forceinline__ int qtile_row(const SpecArgs& a, int x, int k0, int lx) {
+  return min(max(min(x, a.d.NX - x) - k0, 0), lx - 1);
+}
+// Whether the adjoint phase factor of reference t at frequency iw is conj(P)
+// (qcol's rule: the reference keeps P where its b > 0 branch applies).
+template <int QM>
+__device__ __forceinline__ bool qflip(const SpecArgs& a, int t, int iw) {
+  if (QM != Q_PS_ADJ) return false;
+  const float2 sr = a.sref[t * a.d.nw + iw];
+  return !(a.w2[iw] * (sr.y - a.eps * sr.x) > 0.f);
+}
+
+// kQT: the phase factors of each term come as a TMA tile with the term's column
+// tile (the cached table of the phase shift modes); else col_factors loads them
+// from global memory before the tile wait.
+template <class P, int QM, bool kQT>
 __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
     k_col_b_tma(const SpecArgs a, int nxt, const __grid_constant__ CUtensorMap tin,
-                const __grid_constant__ CUtensorMap tout) {
+                const __grid_constant__ CUtensorMap tout, const __grid_constant__ CUtensorMap tq) {
   using C = ColTma<P>;
   static_assert(C::LX == 16, "TMA column tiles are 16 columns (128 bytes) wide");
   extern __shared__ unsigned char smem_raw[];
   float2* base = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   float2* tiles[2] = {base, base + C::TILE};
-  float2* tw = base + 2 * C::TILE;
+  const int pny = a.ptab_ny;
+  const int qt = kQT ? C::LX * pny : 0;  // samples per phase tile (pny even: 128-byte multiples)
+  float2* qs[2] = {base + 2 * C::TILE, base + 2 * C::TILE + qt};
+  float2* tw = base + 2 * C::TILE + 2 * qt;
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + tw_size<P>());
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane / P::T, t = lane % P::T, col = warp * P::G + g;
@@ -820,6 +851,8 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
   const int x = x0 + col;
   const int xq = x < a.d.NX ? x : 0;
   const int zstride = (int)(a.tstride / a.d.slice);  // slices per term in t1
+  const int k0 = qtile_k0<P>(a, x0);
+  const int qrow = qtile_row(a, xq, k0, C::LX) * pny;
   if (threadIdx.x == 0) {
     tma::mbar_init(&bar[0], 1);
     tma::mbar_init(&bar[1], 1);
@@ -828,10 +861,11 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
   load_stage_tw<P>(tw, a.twy);
   __syncthreads();
   auto issue = [&](int term, int buf) {
-    tma::mbar_expect_tx(&bar[buf], (unsigned)(C::TILE * sizeof(float2)));
+    tma::mbar_expect_tx(&bar[buf], (unsigned)((C::TILE + qt) * sizeof(float2)));
 #pragma unroll
     for (int k = 0; k < C::NBOX; ++k)
       tma::load_3d(tiles[buf] + k * C::ROWS * C::LX, &tin, x0, k * C::ROWS, term * zstride + (int)b, &bar[buf]);
+    if constexpr (kQT) tma::load_3d(qs[buf], &tq, 0, k0, term * a.d.nw + iw, &bar[buf]);
   };
   if (threadIdx.x == 0) issue(0, 0);
   float2 acc[P::E];
@@ -840,8 +874,8 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
   for (int term = 0; term < a.nterm; ++term) {
     const int buf = term & 1;
     if (threadIdx.x == 0 && term + 1 < a.nterm) issue(term + 1, buf ^ 1);
-    float2 q[P::E];
-    col_factors<P, QM>(a, term, iw, xq, t, q);
+    float2 q[kQT ? 1 : P::E];
+    if constexpr (!kQT) col_factors<P, QM>(a, term, iw, xq, t, q);
     const bool ok = tma::mbar_wait(&bar[buf], (unsigned)(term >> 1) & 1u);
     if (!__syncthreads_and(ok)) {
       if (threadIdx.x == 0) {
@@ -855,9 +889,20 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
     for (int e = 0; e < P::E; ++e) v[e] = tiles[buf][tma::sw128(pos_first<P>(t, e), col)];
     __syncthreads();  // the tile is in registers: its buffer is free for the exchanges
     fft_fwd<P>(v, t, tw, tiles[buf] + col * P::N);
+    if constexpr (kQT) {
+      const float2* qr = qs[buf] + qrow;
+      const bool flip = qflip<QM>(a, term, iw);
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) acc[e] = cadd(acc[e], cmul(v[e], q[e]));
-    tma::fence_proxy_async();  // the exchanges precede the next load into this buffer
+      for (int e = 0; e < P::E; ++e) {
+        const int ky = pos_last<P>(t, e);
+        const float2 f = qr[min(ky, P::N - ky)];
+        acc[e] = cadd(acc[e], cmul(v[e], flip ? cconj(f) : f));
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) acc[e] = cadd(acc[e], cmul(v[e], q[e]));
+    }
+    tma::fence_proxy_async();  // the exchanges and phase reads precede the next loads into this buffer
     __syncthreads();
   }
   // no load is pending: buffer 0 holds the inverse transform's exchanges, buffer 1 the result
@@ -883,21 +928,39 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
 template <class P>
 struct ColTmaA {
   static constexpr int LX = ColTma<P>::LX, TILE = ColTma<P>::TILE, NBOX = ColTma<P>::NBOX, ROWS = ColTma<P>::ROWS;
-  // input tile (then the exchange lines), staging tile, twiddles, one mbarrier, alignment room
-  static size_t smem() { return (size_t)2 * TILE * sizeof(float2) + tw_size<P>() * sizeof(float2) + 16 + 1024; }
+  // input tile (then the exchange lines), staging tile, two phase tiles of qt
+  // samples (none without them), twiddles, three mbarriers, alignment room
+  static size_t smem(size_t qt = 0) {
+    return (size_t)(2 * TILE + 2 * qt) * sizeof(float2) + tw_size<P>() * sizeof(float2) + 24 + 1024;
+  }
 };
 
-template <class P, int QM>
-__global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocksA)
+// Resident CTAs the single-input TMA pass is held to: with the phase tiles its
+// shared memory (two tiles, two phase tiles) leaves room for fewer CTAs than the
+// register budget of ColGeo::kMinBlocksA would allow, and registers beyond that
+// budget only avoid spills.
+template <class P>
+constexpr int col_a_tma_min_blocks(bool qtile) {
+  constexpr int LX = ColGeo<P>::LX;
+  constexpr size_t per = (size_t)(2 * P::N * LX + 2 * LX * ((P::N / 2 + 2) & ~1) + tw_size<P>()) * 8 + 24 + 1024;
+  constexpr int fit = (int)((227 * 1024) / per) > 0 ? (int)((227 * 1024) / per) : 1;
+  return qtile && fit < ColGeo<P>::kMinBlocksA ? fit : ColGeo<P>::kMinBlocksA;
+}
+
+template <class P, int QM, bool kQT>
+__global__ void __launch_bounds__(kWarps * 32, col_a_tma_min_blocks<P>(kQT))
     k_col_a_tma(const SpecArgs a, int nxt, const __grid_constant__ CUtensorMap tin,
-                const __grid_constant__ CUtensorMap tout) {
+                const __grid_constant__ CUtensorMap tout, const __grid_constant__ CUtensorMap tq) {
   using C = ColTmaA<P>;
   static_assert(C::LX == 16, "TMA column tiles are 16 columns (128 bytes) wide");
   extern __shared__ unsigned char smem_raw[];
   float2* in = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   float2* stage = in + C::TILE;
-  float2* tw = stage + C::TILE;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + tw_size<P>());
+  const int pny = a.ptab_ny;
+  const int qt = kQT ? C::LX * pny : 0;
+  float2* const q0 = stage + C::TILE;  // phase slot k at q0 + k * qt
+  float2* tw = stage + C::TILE + 2 * qt;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + tw_size<P>());  // input, phase slot 0, phase slot 1
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane / P::T, t = lane % P::T, col = warp * P::G + g;
   const long long b = blockIdx.x / nxt;
@@ -906,20 +969,48 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocksA)
   const int x = x0 + col;
   const int xq = x < a.d.NX ? x : 0;
   const int zstride = (int)(a.tstride / a.d.slice);
+  const int k0 = qtile_k0<P>(a, x0);
+  const int qrow = qtile_row(a, xq, k0, C::LX) * pny;
+  const int nterm = a.nterm;
   if (threadIdx.x == 0) {
-    tma::mbar_init(bar, 1);
+    tma::mbar_init(&bar[0], 1);
+    tma::mbar_init(&bar[1], 1);
+    tma::mbar_init(&bar[2], 1);
     tma::fence_mbar_init();
   }
   load_stage_tw<P>(tw, a.twy);
   __syncthreads();
+  auto issue_q = [&](int term) {  // the phase tile of `term` into slot term & 1
+    uint64_t* qb = &bar[1 + (term & 1)];
+    tma::mbar_expect_tx(qb, (unsigned)(qt * sizeof(float2)));
+    tma::load_3d(q0 + (term & 1) * qt, &tq, 0, k0, term * a.d.nw + iw, qb);
+  };
   if (threadIdx.x == 0) {
-    tma::mbar_expect_tx(bar, (unsigned)(C::TILE * sizeof(float2)));
+    tma::mbar_expect_tx(&bar[0], (unsigned)(C::TILE * sizeof(float2)));
 #pragma unroll
-    for (int k = 0; k < C::NBOX; ++k) tma::load_3d(in + k * C::ROWS * C::LX, &tin, x0, k * C::ROWS, (int)b, bar);
+    for (int k = 0; k < C::NBOX; ++k) tma::load_3d(in + k * C::ROWS * C::LX, &tin, x0, k * C::ROWS, (int)b, &bar[0]);
+    if constexpr (kQT) {
+      if (nterm > 0) issue_q(0);
+      if (nterm > 1) issue_q(1);
+    }
   }
-  const bool ok = tma::mbar_wait(bar, 0u);
+  // Bounded-wait failure: count it, let the loads in flight land (bounded) and
+  // the committed stores read their source, then leave together.
+  auto bail = [&](int pending_q) {
+    if (threadIdx.x == 0) {
+      atomicAdd(a.err, 1u);
+      if (kQT && pending_q >= 0 && pending_q < nterm)
+        tma::mbar_wait(&bar[1 + (pending_q & 1)], (unsigned)(pending_q >> 1) & 1u);
+      tma::store_wait_read();
+    }
+  };
+  const bool ok = tma::mbar_wait(&bar[0], 0u);
   if (!__syncthreads_and(ok)) {
-    if (threadIdx.x == 0) atomicAdd(a.err, 1u);
+    if (threadIdx.x == 0 && kQT) {
+      // the phase loads of terms 0 and 1 may be in flight
+      for (int k = 0; k < 2 && k < nterm; ++k) tma::mbar_wait(&bar[1 + k], 0u);
+    }
+    bail(-1);
     return;
   }
   float2 psi[P::E];
@@ -952,17 +1043,35 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocksA)
   __syncthreads();  // every lane holds its column: the input tile becomes the exchange lines
   float2* line = in + col * P::N;
   fft_fwd<P>(psi, t, tw, line);
-  const int nterm = a.nterm;
   for (int term = first; term < nterm; ++term) {
     float2 v[P::E];
-    col_factors<P, QM>(a, term, iw, xq, t, v);
+    if constexpr (kQT) {
+      const bool qok = tma::mbar_wait(&bar[1 + (term & 1)], (unsigned)(term >> 1) & 1u);
+      if (!__syncthreads_and(qok)) {
+        bail(term + 1);
+        return;
+      }
+      const float2* qr = q0 + (term & 1) * qt + qrow;
+      const bool flip = qflip<QM>(a, term, iw);
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) v[e] = cmul(psi[e], v[e]);
+      for (int e = 0; e < P::E; ++e) {
+        const int ky = pos_last<P>(t, e);
+        const float2 f = qr[min(ky, P::N - ky)];
+        v[e] = cmul(psi[e], flip ? cconj(f) : f);
+      }
+    } else {
+      col_factors<P, QM>(a, term, iw, xq, t, v);
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) v[e] = cmul(psi[e], v[e]);
+    }
     fft_inv<P>(v, t, tw, line);
     stage_free();
 #pragma unroll
     for (int e = 0; e < P::E; ++e) stage[tma::sw128(pos_first<P>(t, e), col)] = v[e];
-    store(term);
+    store(term);  // also orders this term's phase reads before the slot's next load
+    if constexpr (kQT) {
+      if (threadIdx.x == 0 && term + 2 < nterm) issue_q(term + 2);
+    }
   }
   if (threadIdx.x == 0) tma::store_wait_read();
 }
@@ -1070,26 +1179,51 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+// Whether a TMA column pass of plan P takes its phase factors as TMA tiles: the
+// phase-shift modes with the cached table, asked for in a.qtile (bit 0 the
+// multi-input pass k_col_b, bit 1 the single-input k_col_a), rows of at most 256
+// even-length entries, and tiles that never straddle NX / 2 (so that a tile's |kx|
+// are consecutive).
+template <class P>
+bool use_qtile(const SpecArgs& a, int qmode, int bit) {
+  constexpr int LX = ColGeo<P>::LX;
+  return ((a.qtile >> bit) & 1) && (qmode == Q_PS_FWD || qmode == Q_PS_ADJ) && a.ptab && a.ptab_ny % 2 == 0 &&
+         a.ptab_ny <= 256 && (a.d.NX / 2) % LX == 0 && a.ptab_nx >= LX;
+}
+
 template <class P>
 cudaError_t col_type_a_tma(const SpecArgs& a, int qmode, cudaStream_t s) {
   using C = ColTmaA<P>;
   const int nxt = (a.d.NX + C::LX - 1) / C::LX;
   const unsigned grid = (unsigned)(a.nb * nxt);
-  const size_t sm = C::smem();
-  CUtensorMap tin, tout;
+  const bool qtile = use_qtile<P>(a, qmode, 1);
+  const size_t sm = C::smem(qtile ? (size_t)C::LX * a.ptab_ny : 0);
+  CUtensorMap tin, tout, tq;
+  std::memset(&tq, 0, sizeof(tq));
   cudaError_t e = tile_map(&tin, a.t1, a.d.NX, a.d.NY, a.nb, C::ROWS);
   if (e == cudaSuccess) e = tile_map(&tout, a.t2, a.d.NX, a.d.NY, (a.tstride / a.d.slice) * (a.term0 + a.nterm), C::ROWS);
+  if (e == cudaSuccess && qtile) e = qtab_map(&tq, a.ptab, a.ptab_ny, a.ptab_nx, (long long)a.nterm * a.d.nw, C::LX);
   if (e != cudaSuccess) return e;
-#define FWIX_FAST_CAT(Q)                                                                  \
-  case Q:                                                                                 \
-    e = opt_in_smem(k_col_a_tma<P, Q>, sm);                                               \
-    if (e == cudaSuccess) k_col_a_tma<P, Q><<<grid, kWarps * 32, sm, s>>>(a, nxt, tin, tout); \
-    break;
+#define FWIX_FAST_CAT(Q, QT)                                                                          \
+  e = opt_in_smem(k_col_a_tma<P, Q, QT>, sm);                                                         \
+  if (e == cudaSuccess) k_col_a_tma<P, Q, QT><<<grid, kWarps * 32, sm, s>>>(a, nxt, tin, tout, tq);
   switch (qmode) {
-    FWIX_FAST_CAT(Q_PS_FWD)
-    FWIX_FAST_CAT(Q_PS_ADJ)
-    FWIX_FAST_CAT(Q_KPOW)
-    FWIX_FAST_CAT(Q_ONE)
+    case Q_PS_FWD:
+      if (qtile) {
+        FWIX_FAST_CAT(Q_PS_FWD, true)
+      } else {
+        FWIX_FAST_CAT(Q_PS_FWD, false)
+      }
+      break;
+    case Q_PS_ADJ:
+      if (qtile) {
+        FWIX_FAST_CAT(Q_PS_ADJ, true)
+      } else {
+        FWIX_FAST_CAT(Q_PS_ADJ, false)
+      }
+      break;
+    case Q_KPOW: FWIX_FAST_CAT(Q_KPOW, false) break;
+    case Q_ONE: FWIX_FAST_CAT(Q_ONE, false) break;
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_FAST_CAT
@@ -1130,21 +1264,34 @@ cudaError_t col_type_b_tma(const SpecArgs& a, int qmode, cudaStream_t s) {
   using C = ColTma<P>;
   const int nxt = (a.d.NX + C::LX - 1) / C::LX;
   const unsigned grid = (unsigned)(a.nb * nxt);
-  const size_t sm = C::smem();
-  CUtensorMap tin, tout;
+  const bool qtile = use_qtile<P>(a, qmode, 0);
+  const size_t sm = C::smem(qtile ? (size_t)C::LX * a.ptab_ny : 0);
+  CUtensorMap tin, tout, tq;
+  std::memset(&tq, 0, sizeof(tq));
   cudaError_t e = tile_map(&tin, a.t1, a.d.NX, a.d.NY, (a.tstride / a.d.slice) * a.nterm, C::ROWS);
   if (e == cudaSuccess) e = tile_map(&tout, a.t2, a.d.NX, a.d.NY, a.nb, C::ROWS);
+  if (e == cudaSuccess && qtile) e = qtab_map(&tq, a.ptab, a.ptab_ny, a.ptab_nx, (long long)a.nterm * a.d.nw, C::LX);
   if (e != cudaSuccess) return e;
-#define FWIX_FAST_CBT(Q)                                                                  \
-  case Q:                                                                                 \
-    e = opt_in_smem(k_col_b_tma<P, Q>, sm);                                               \
-    if (e == cudaSuccess) k_col_b_tma<P, Q><<<grid, kWarps * 32, sm, s>>>(a, nxt, tin, tout); \
-    break;
+#define FWIX_FAST_CBT(Q, QT)                                                                          \
+  e = opt_in_smem(k_col_b_tma<P, Q, QT>, sm);                                                         \
+  if (e == cudaSuccess) k_col_b_tma<P, Q, QT><<<grid, kWarps * 32, sm, s>>>(a, nxt, tin, tout, tq);
   switch (qmode) {
-    FWIX_FAST_CBT(Q_PS_FWD)
-    FWIX_FAST_CBT(Q_PS_ADJ)
-    FWIX_FAST_CBT(Q_KPOW)
-    FWIX_FAST_CBT(Q_ONE)
+    case Q_PS_FWD:
+      if (qtile) {
+        FWIX_FAST_CBT(Q_PS_FWD, true)
+      } else {
+        FWIX_FAST_CBT(Q_PS_FWD, false)
+      }
+      break;
+    case Q_PS_ADJ:
+      if (qtile) {
+        FWIX_FAST_CBT(Q_PS_ADJ, true)
+      } else {
+        FWIX_FAST_CBT(Q_PS_ADJ, false)
+      }
+      break;
+    case Q_KPOW: FWIX_FAST_CBT(Q_KPOW, false) break;
+    case Q_ONE: FWIX_FAST_CBT(Q_ONE, false) break;
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_FAST_CBT

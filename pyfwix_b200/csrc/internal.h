@@ -81,7 +81,8 @@ struct SpecArgs {
   long long img_w;     // ny*nx, or 0 for one image shared by every frequency
   // cached forward phase factors of this depth (x norm), element (ref, iw, |kx|, |ky|)
   // at ptab[((ref*nw + iw)*ptab_nx + kxq)*ptab_ny + kyq], kxq = min(x, NX-x),
-  // kyq = min(y, NY-y); NULL means evaluate the factors in the kernel
+  // kyq = min(y, NY-y); ptab_nx = NX/2 + 1, ptab_ny = NY/2 + 1 rounded up to even
+  // (16-byte rows for TMA); NULL means evaluate the factors in the kernel
   const float2* ptab;
   int ptab_nx, ptab_ny;
   // smooth step: padded local slowness [NY][NX] and the sorted real reference
@@ -117,6 +118,10 @@ struct SpecArgs {
   // bounded wait that runs out adds one to *err (the plan's error word)
   int tma;
   unsigned* err;
+  // TMA column passes with the cached phase table: bit 0, the multi-input pass
+  // takes each term's phase factors as a TMA tile with the term's column tile;
+  // bit 1, the single-input pass likewise (else they are loaded per lane)
+  int qtile;
   // inverse row pass image epilogue (the lockstep migration): for every output
   // sample of the unpadded window, ic_img[y][x] += Re(conj(ic_bg[b][y][x]) out)
   // by float atomics (ic_img NULL: none)
@@ -150,7 +155,7 @@ cudaError_t launch_scat_table(const SpecArgs& a, float2* dst, cudaStream_t s);
 bool fused_step_available();
 cudaError_t fused_step(const SpecArgs& a, int kind, int dir, cudaStream_t s);
 
-// Phase-factor cache of one depth (spectral.cu): dst [nref][nw][NX/2+1][NY/2+1].
+// Phase-factor cache of one depth (spectral.cu): dst [nref][nw][ptab_nx][ptab_ny].
 cudaError_t launch_phase_table(const SpecArgs& a, float2* dst, cudaStream_t s);
 
 // Pointwise kernels (pointwise.cu).

@@ -63,4 +63,37 @@ cudaError_t tile_map(CUtensorMap* out, const void* base, int nx, int ny, long lo
   return cudaSuccess;
 }
 
+cudaError_t qtab_map(CUtensorMap* out, const void* base, int pny, int pnx, long long nslices, int box_cols) {
+  using Key = std::tuple<const void*, int, int, long long, int>;
+  static std::mutex mu;
+  static std::map<Key, CUtensorMap> cache;
+  const Key key{base, pny, pnx, nslices, box_cols};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      *out = it->second;
+      return cudaSuccess;
+    }
+  }
+  auto fn = encode_fn();
+  if (!fn || nslices < 1 || pnx < box_cols || pny < 2 || pny > 256 || (pny % 2) != 0 || box_cols < 1 ||
+      box_cols > 256 || ((uintptr_t)base & 15) != 0)
+    return cudaErrorInvalidValue;
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  const cuuint64_t dims[3] = {(cuuint64_t)pny, (cuuint64_t)pnx, (cuuint64_t)nslices};
+  const cuuint64_t strides[2] = {(cuuint64_t)pny * 8, (cuuint64_t)pny * (cuuint64_t)pnx * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)pny, (cuuint32_t)box_cols, 1};
+  const cuuint32_t elem[3] = {1, 1, 1};
+  const CUresult r = fn(&m, CU_TENSOR_MAP_DATA_TYPE_INT64, 3, const_cast<void*>(base), dims, strides, box, elem,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = m;
+  *out = m;
+  return cudaSuccess;
+}
+
 }  // namespace fwix

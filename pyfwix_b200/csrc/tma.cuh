@@ -89,4 +89,10 @@ __device__ __forceinline__ int sw128(int y, int c) { return y * 16 + ((((c >> 1)
 // or the encoding is refused).
 cudaError_t tile_map(CUtensorMap* out, const void* base, int nx, int ny, long long nz, int box_rows);
 
+// Host side: a 3-D tensor map over the quarter-spectrum phase table of one depth,
+// [nslices][pnx][pny] 8-byte factors (ky fastest, pny even so that rows are 16-byte
+// multiples), box {pny, box_cols, 1} (every ky of box_cols consecutive kx of one
+// (reference, frequency) slice), no swizzle.  Cached like tile_map.
+cudaError_t qtab_map(CUtensorMap* out, const void* base, int pny, int pnx, long long nslices, int box_cols);
+
 }  // namespace fwix

@@ -13,23 +13,27 @@ from tests.gpu_helpers import make_case, make_plan, oracle_labels, rel, to_dev, 
 pytestmark = pytest.mark.gpu
 
 
-def _plans(monkeypatch, step, **kw):
+def _plans(monkeypatch, step, qtile=3, **kw):
     g, rng, sref, labels, slow, den = make_case(**kw)
     monkeypatch.setenv("FWIX_COL_TMA", "0")
     p0 = make_plan(g, 1, sref, labels, slow, den, step=step)
     monkeypatch.setenv("FWIX_COL_TMA", "1")
+    monkeypatch.setenv("FWIX_QTILE", str(qtile))
     p1 = make_plan(g, 1, sref, labels, slow, den, step=step)
     monkeypatch.delenv("FWIX_COL_TMA")
+    monkeypatch.delenv("FWIX_QTILE")
     return g, rng, sref, labels, slow, den, p0, p1
 
 
-# plan lengths whose column passes take 16 columns per CTA (128 bytes per tile row)
+# plan lengths whose column passes take 16 columns per CTA (128 bytes per tile row);
+# qtile 3: the phase factors arrive as TMA tiles too (both column passes), 0: per lane
 @pytest.mark.parametrize("n,pad", [(124, 4), (192, 0), (256, 0), (316, 4)])
 @pytest.mark.parametrize("step", ["pspi", "nsps"])
-def test_tma_steps_equal_copy_steps(monkeypatch, n, pad, step):
+@pytest.mark.parametrize("qtile", [0, 3])
+def test_tma_steps_equal_copy_steps(monkeypatch, n, pad, step, qtile):
     from pyfwix_b200 import _lib as L
-    g, rng, sref, labels, slow, den, p0, p1 = _plans(monkeypatch, step, nx=n, ny=n, nw=6, nz=3, nref=4, padx=pad,
-                                                     pady=pad, eps=0.01, complex_refs=True)
+    g, rng, sref, labels, slow, den, p0, p1 = _plans(monkeypatch, step, qtile, nx=n, ny=n, nw=6, nz=3, nref=4,
+                                                     padx=pad, pady=pad, eps=0.01, complex_refs=True)
     lab = oracle_labels(labels, g)
     st = wem.Stepper(g, sref, lab, step)
     for d in (L.FWD, L.ADJ_ADD, L.ADJ_INPL):
