@@ -127,9 +127,6 @@ struct fwix_plan {
   bool fused = false;   // 256 x 256 slices: one-launch cluster step (fused256.cu), opt-in
   bool col_tma = true;  // column passes with TMA tiles where the plan allows (FWIX_COL_TMA=0: copies)
   int qtile = 3;        // SpecArgs::qtile bits (FWIX_QTILE): both column passes, measured fastest
-  // Born scattering with taylor = 1 as one row and one column pass on the
-  // register-resident lengths (FWIX_SCAT_SEPARABLE=0: the 2D three-pass route)
-  bool scat_separable = true;
   // depth steps in chunks alternating between the caller's stream and lane_s
   // (lanes = 2, set by fwix_plan_autotune), each lane with its own intermediates
   int lanes = 1;
@@ -425,15 +422,6 @@ fwix_status do_scatter(fwix_plan* p, int iz, int adjoint, const float2* in, floa
     FWIX_TRY(cu(fwix::launch_scat_table(a0, p->scat_tab, s), "scatter weights"));
     a0.scat_tab = p->scat_tab;
   }
-  if (p->scat_separable && p->desc.taylor == 1 && fwix::fast_length(p->d.NX) && fwix::fast_length(p->d.NY)) {
-    // (|k| / w)^2 = kx^2 / w^2 + ky^2 / w^2: one row and one column pass
-    a0.image = adjoint ? nullptr : image;
-    a0.img_w = img_w;
-    return for_chunks(p, a0, [&](const SpecArgs& a) {
-      FWIX_TRY(cu(fwix::row_lap(a, !adjoint, s), "separable scatter row pass"));
-      return cu(fwix::col_lap(a, !adjoint, s), "separable scatter column pass");
-    });
-  }
   if (adjoint && p->desc.taylor >= 1 && fwix::fast_length(p->d.NX) && fwix::fast_length(p->d.NY)) {
     // the zeroth term's filter is the identity: conj(W_0) d is added by the inverse
     // row pass, and only orders 1 .. taylor go through the transforms.  (The
@@ -711,8 +699,6 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
     const char* tma = getenv("FWIX_COL_TMA");
     p->col_tma = !(tma && tma[0] == '0');
     if (const char* q = getenv("FWIX_QTILE")) p->qtile = atoi(q) & 3;
-    const char* sep = getenv("FWIX_SCAT_SEPARABLE");
-    p->scat_separable = !(sep && sep[0] == '0');
   }
   std::vector<float> w2(q.nw), w(q.nw);
   for (int i = 0; i < q.nw; ++i) {

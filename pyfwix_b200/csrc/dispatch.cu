@@ -8,9 +8,7 @@
   cudaError_t col_type_a_##TAG(const SpecArgs& a, int q, cudaStream_t s);                              \
   cudaError_t col_type_b_##TAG(const SpecArgs& a, int q, cudaStream_t s);                              \
   cudaError_t col_fft_##TAG(const SpecArgs& a, int inv, const float2* in, float2* out, int add, float sc, \
-                            cudaStream_t s);                                                           \
-  cudaError_t row_lap_##TAG(const SpecArgs& a, int fwd, cudaStream_t s);                               \
-  cudaError_t col_lap_##TAG(const SpecArgs& a, int fwd, cudaStream_t s);
+                            cudaStream_t s);
 
 namespace fwix {
 namespace fast {
@@ -122,40 +120,6 @@ cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* ou
     case 512: return fast::col_fft_512(a, inverse, in, out, add, scale, s);
     case 640: return fast::col_fft_640(a, inverse, in, out, add, scale, s);
     default: return generic_col_fft(a, inverse, in, out, add, scale, s);
-  }
-}
-
-// Separable Born scattering (taylor = 1), register-resident lengths only: the
-// row pass dispatches on NX, the column pass on NY.
-cudaError_t row_lap(const SpecArgs& a, int fwd, cudaStream_t s) {
-  switch (a.d.NX) {
-    case 64: return fast::row_lap_64(a, fwd, s);
-    case 96: return fast::row_lap_96(a, fwd, s);
-    case 128: return fast::row_lap_128(a, fwd, s);
-    case 160: return fast::row_lap_160(a, fwd, s);
-    case 192: return fast::row_lap_192(a, fwd, s);
-    case 256: return fast::row_lap_256(a, fwd, s);
-    case 320: return fast::row_lap_320(a, fwd, s);
-    case 384: return fast::row_lap_384(a, fwd, s);
-    case 512: return fast::row_lap_512(a, fwd, s);
-    case 640: return fast::row_lap_640(a, fwd, s);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-cudaError_t col_lap(const SpecArgs& a, int fwd, cudaStream_t s) {
-  switch (a.d.NY) {
-    case 64: return fast::col_lap_64(a, fwd, s);
-    case 96: return fast::col_lap_96(a, fwd, s);
-    case 128: return fast::col_lap_128(a, fwd, s);
-    case 160: return fast::col_lap_160(a, fwd, s);
-    case 192: return fast::col_lap_192(a, fwd, s);
-    case 256: return fast::col_lap_256(a, fwd, s);
-    case 320: return fast::col_lap_320(a, fwd, s);
-    case 384: return fast::col_lap_384(a, fwd, s);
-    case 512: return fast::col_lap_512(a, fwd, s);
-    case 640: return fast::col_lap_640(a, fwd, s);
-    default: return cudaErrorInvalidValue;
   }
 }
 

@@ -1105,106 +1105,6 @@ __global__ void __launch_bounds__(kWarps * 32) k_col_fft(const SpecArgs a, int n
   tile_to_cols<P>(c.tile, out, a, c.b, c.x0, add, scale);
 }
 
-// ---------------------------------------------------------------- separable scattering
-// With one Taylor term besides the zeroth (taylor = 1) the Born scattering is
-//   forward  Scat u = W_0 u + W_1 L u,   adjoint  Scat^H y = conj(W_0) y + L (conj(W_1) y),
-// L = F^-1 (kx^2 + ky^2) / w^2 F (scatter.cu:49-55 with n = 1), and L splits by
-// axis: L = Lx + Ly, Lx = F_x^-1 kx^2 / w^2 F_x / NX along the rows, Ly the same
-// along the columns.  One row pass forms u (forward: the input, or bg * image;
-// adjoint: conj(W_1) y) into t1 and the partial sum (forward: W_0 u + W_1 Lx u;
-// adjoint: conj(W_0) y + Lx u) into t2; one column pass adds Ly u (forward:
-// times W_1) to the partial sum into out.  Two 1D transform pairs per cell instead
-// of the five 1D transforms of the 2D route, and two passes instead of three.
-
-// Row pass (row plan P): t1 = u, t2 = partial sum (launch-local slices).
-template <class P, bool kFwd>
-__global__ void __launch_bounds__(kWarps * 32, 2) k_row_lap(const SpecArgs a, int nchunk) {
-  extern __shared__ float2 smem[];
-  RowCtx<P> c(a, smem, nchunk);
-  load_stage_tw<P>(c.tw, a.twx);
-  __syncthreads();
-  const long long roff = (c.b * a.d.NY + (c.live ? c.y : 0)) * P::N;
-  const long long loff = (c.bl * a.d.NY + (c.live ? c.y : 0)) * P::N;
-  // The weights are read before the transform, so their latency hides behind it:
-  // the zeroth-order product into p0, u into v (and t1); the forward keeps W_1
-  // for the first-order product after the transform.
-  float2 p0[P::E], v[P::E], w1[kFwd ? P::E : 1];
-#pragma unroll
-  for (int e = 0; e < P::E; ++e) {
-    const int x = pos_first<P>(c.t, e);
-    float2 in = make_float2(0.f, 0.f);
-    if (c.live) {
-      in = a.in[roff + x];
-      if (kFwd && a.image) in = row_weight<W_IC>(a, 0, c.iw, c.y, x, in);
-    }
-    const float2 W0 = scat_weight(a, 0, c.iw, c.y, x), W1 = scat_weight(a, 1, c.iw, c.y, x);
-    if constexpr (kFwd) {
-      w1[e] = W1;
-      p0[e] = cmul(in, W0);
-      v[e] = in;
-    } else {
-      p0[e] = cmul_conj(in, W0);
-      v[e] = cmul_conj(in, W1);
-    }
-    if (c.live) a.t1[loff + x] = v[e];
-  }
-  fft_fwd<P>(v, c.t, c.tw, c.line);
-  const float sc = 1.f / (a.w2[c.iw] * (float)P::N);
-#pragma unroll
-  for (int e = 0; e < P::E; ++e) {
-    const float k = a.kx[pos_last<P>(c.t, e)];
-    v[e] = cscale(v[e], k * k * sc);
-  }
-  fft_inv<P>(v, c.t, c.tw, c.line);
-  if (!c.live) return;
-#pragma unroll
-  for (int e = 0; e < P::E; ++e) {
-    const float2 p = kFwd ? cadd(p0[e], cmul(v[e], w1[e])) : cadd(p0[e], v[e]);
-    a.t2[loff + pos_first<P>(c.t, e)] = p;
-  }
-}
-
-// Column pass (column plan P): out (+)= t2 + gamma Ly t1, gamma = W_1 (forward) or 1.
-template <class P, bool kFwd>
-__global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocksA) k_col_lap(const SpecArgs a, int nxt) {
-  extern __shared__ float2 smem[];
-  ColCtx<P> c(a, smem, nxt);
-  load_stage_tw<P>(c.tw, a.twy);
-  cols_to_tile<P>(c.tile, a.t1, a, c.b, c.x0);
-  __syncthreads();
-  float2 v[P::E];
-#pragma unroll
-  for (int e = 0; e < P::E; ++e) v[e] = c.line[swz(pos_first<P>(c.t, e))];
-  fft_fwd<P>(v, c.t, c.tw, c.line);
-  const float sc = 1.f / (a.w2[c.iw] * (float)P::N);
-#pragma unroll
-  for (int e = 0; e < P::E; ++e) {
-    const float k = a.ky[pos_last<P>(c.t, e)];
-    v[e] = cscale(v[e], k * k * sc);
-  }
-  fft_inv<P>(v, c.t, c.tw, c.line);
-  __syncwarp();
-#pragma unroll
-  for (int e = 0; e < P::E; ++e) c.line[swz(pos_first<P>(c.t, e))] = v[e];
-  __syncthreads();
-  // coalesced epilogue over the tile's rows
-  constexpr int LX = ColGeo<P>::LX, NT = kWarps * 32;
-  const int cc = threadIdx.x % LX, x = c.x0 + cc;
-  if (x >= a.d.NX) return;
-  const float2* part = a.t2 + c.b * a.d.slice + x;
-  float2* dst = a.out + (a.b0 + c.b) * a.d.slice + x;
-#pragma unroll 4
-  for (int k = 0; k < LX * P::N / NT; ++k) {
-    const int y = (int)(threadIdx.x + k * NT) / LX;
-    float2 w = c.tile[cc * ColGeo<P>::LINE + swz(y)];
-    if (kFwd) w = cmul(w, scat_weight(a, 1, c.iw, y, x));
-    w = cadd(w, part[(long long)y * a.d.NX]);
-    float2* q = dst + (long long)y * a.d.NX;
-    if (a.add) w = cadd(*q, w);
-    *q = w;
-  }
-}
-
 // ---------------------------------------------------------------- launch helpers
 
 // Sets the shared-memory carveout and, above 48 KB, the dynamic shared-memory limit
@@ -1275,40 +1175,6 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
     default: return cudaErrorInvalidValue;
   }
 #undef FWIX_FAST_RI
-  if (e == cudaSuccess) count_launch();
-  return e != cudaSuccess ? e : cudaGetLastError();
-}
-
-template <class P>
-cudaError_t row_lap(const SpecArgs& a, int fwd, cudaStream_t s) {
-  const int nchunk = (a.d.NY + RowGeo<P>::ROWS - 1) / RowGeo<P>::ROWS;
-  const unsigned grid = (unsigned)(a.nb * nchunk);
-  const size_t sm = RowGeo<P>::smem();
-  cudaError_t e;
-  if (fwd) {
-    e = opt_in_smem(k_row_lap<P, true>, sm);
-    if (e == cudaSuccess) k_row_lap<P, true><<<grid, kWarps * 32, sm, s>>>(a, nchunk);
-  } else {
-    e = opt_in_smem(k_row_lap<P, false>, sm);
-    if (e == cudaSuccess) k_row_lap<P, false><<<grid, kWarps * 32, sm, s>>>(a, nchunk);
-  }
-  if (e == cudaSuccess) count_launch();
-  return e != cudaSuccess ? e : cudaGetLastError();
-}
-
-template <class P>
-cudaError_t col_lap(const SpecArgs& a, int fwd, cudaStream_t s) {
-  const int nxt = (a.d.NX + ColGeo<P>::LX - 1) / ColGeo<P>::LX;
-  const unsigned grid = (unsigned)(a.nb * nxt);
-  const size_t sm = ColGeo<P>::smem();
-  cudaError_t e;
-  if (fwd) {
-    e = opt_in_smem(k_col_lap<P, true>, sm);
-    if (e == cudaSuccess) k_col_lap<P, true><<<grid, kWarps * 32, sm, s>>>(a, nxt);
-  } else {
-    e = opt_in_smem(k_col_lap<P, false>, sm);
-    if (e == cudaSuccess) k_col_lap<P, false><<<grid, kWarps * 32, sm, s>>>(a, nxt);
-  }
   if (e == cudaSuccess) count_launch();
   return e != cudaSuccess ? e : cudaGetLastError();
 }
@@ -1498,7 +1364,5 @@ cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* ou
                             cudaStream_t s) {                                                               \
     return col_fft<CPLAN>(a, inv, in, out, add, sc, s);                                                     \
   }                                                                                                         \
-  cudaError_t row_lap_##TAG(const SpecArgs& a, int fwd, cudaStream_t s) { return row_lap<PLAN>(a, fwd, s); }    \
-  cudaError_t col_lap_##TAG(const SpecArgs& a, int fwd, cudaStream_t s) { return col_lap<CPLAN>(a, fwd, s); }   \
   }                                                                                                         \
   }

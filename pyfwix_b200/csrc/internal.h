@@ -139,11 +139,6 @@ cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s);     // t1[
 cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s);     // t1[0..nterm) -> t2[0]
 cudaError_t col_fft(const SpecArgs& a, int inverse, const float2* in, float2* out, int add,
                     float scale, cudaStream_t s);
-// Separable Born scattering with taylor = 1 (fast.cuh k_row_lap / k_col_lap; both
-// lengths register-resident): row pass in -> t1 (u), t2 (partial sum); column pass
-// t1, t2 -> out.  fwd selects the forward or the adjoint weights.
-cudaError_t row_lap(const SpecArgs& a, int fwd, cudaStream_t s);
-cudaError_t col_lap(const SpecArgs& a, int fwd, cudaStream_t s);
 cudaError_t generic_row_forward(const SpecArgs& a, int pre, cudaStream_t s);
 cudaError_t generic_row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s);
 cudaError_t generic_col_type_a(const SpecArgs& a, int qmode, cudaStream_t s);

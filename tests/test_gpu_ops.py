@@ -290,30 +290,3 @@ def test_phase_cache_matches_inline(complex_refs, eps):
         if k[0]:
             assert rel(v, outs[(False,) + k[1:]]) < 1e-6, k
 
-
-@pytest.mark.parametrize("n,pad,broadcast", [(256, 0, True), (252, 4, False), (384, 0, True), (60, 4, False)])
-def test_separable_scatter_equals_2d_route(monkeypatch, n, pad, broadcast):
-    """With one Taylor term the Born scattering runs as one row and one column pass
-    ((kx^2 + ky^2) / w^2 split by axis); it equals the 2D three-pass route to FP32
-    rounding, forward and adjoint, in place and with add, for a per-frequency and a
-    frequency-broadcast model, and matches the FP64 oracle."""
-    g, rng, sref, labels, slow, den = make_case(nx=n, ny=n, nw=3, nz=2, padx=pad, pady=pad, taylor=1)
-    if broadcast:
-        slow, den = slow[:, :1].copy(), den[:, :1].copy()
-    monkeypatch.setenv("FWIX_SCAT_SEPARABLE", "0")
-    p2d = make_plan(g, 1, sref, labels, slow, den)
-    monkeypatch.delenv("FWIX_SCAT_SEPARABLE")
-    p = make_plan(g, 1, sref, labels, slow, den)
-    x = wavefield(rng, 1, g)
-    d0 = wavefield(rng, 1, g)
-    slow_o = np.repeat(slow, g.nw, axis=1) if broadcast else slow
-    for adjoint in (False, True):
-        a = to_host(p.scatter(1, to_dev(x), to_dev(d0), adjoint=adjoint, add=True))
-        b = to_host(p2d.scatter(1, to_dev(x), to_dev(d0), adjoint=adjoint, add=True))
-        assert rel(a, b) < 2e-6, (adjoint, rel(a, b))
-        ref = (wem.scatter_adjoint if adjoint else wem.scatter_forward)(g, slow_o[1], x, d0)
-        assert rel(a, ref) < TOL
-        xin = to_dev(x)
-        c = to_host(p.scatter(1, xin, xin, adjoint=adjoint))  # in place
-        ref = (wem.scatter_adjoint if adjoint else wem.scatter_forward)(g, slow_o[1], x)
-        assert rel(c, ref) < TOL
