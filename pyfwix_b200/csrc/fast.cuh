@@ -226,6 +226,11 @@ __device__ __forceinline__ void cp_async8(float2* dst, const float2* src, bool v
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0));
 }
+// Asynchronous 16-byte global -> shared copy through L2 (both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async16(float2* dst, const float2* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -250,6 +255,13 @@ struct RowGeo {
   static constexpr int ROWS = kWarps * P::G;                // rows per CTA
   // after the twiddles: the smooth step's references and inverse spans (kMaxHatRefs each)
   static size_t smem() { return ((size_t)kWarps * P::G * LINE + tw_size<P>() + kMaxHatRefs) * sizeof(float2); }
+  // Born-weight rows of the CTA staged after the above (16-byte aligned): nterm
+  // tables x ROWS rows x N samples, when they fit in 160 KB
+  __host__ __device__ static constexpr size_t scat_offset() {
+    return ((size_t)kWarps * P::G * LINE + tw_size<P>() + kMaxHatRefs + 1) & ~(size_t)1;
+  }
+  __host__ __device__ static bool scat_stage(int nterm) { return (size_t)nterm * ROWS * P::N * 8 <= 160 * 1024; }
+  static size_t smem_scat(int nterm) { return (scat_offset() + (size_t)nterm * ROWS * P::N) * sizeof(float2); }
 };
 
 // Smooth-step references of the row passes, staged in shared memory once per CTA:
@@ -441,6 +453,26 @@ template <class P, int POST>
 __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 || P::E == 12) ? FWIX_ROW_MULTI_MINB : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
+  // Born weights from the per-depth table: the CTA's rows of every term's table
+  // are copied into shared memory (cp.async, 16 bytes a thread and instruction)
+  // while the first term loads and transforms, and read from there after each
+  // transform instead of from L2 behind it.
+  constexpr bool kScat = POST == W_SCAT;
+  const int nterm = multi_term(POST) ? a.nterm : 1;
+  const bool scat_smem = kScat && a.scat_tab && RowGeo<P>::scat_stage(nterm);
+  float2* wt = smem + RowGeo<P>::scat_offset();
+  const int y0 = (int)(blockIdx.x - c.bl * nchunk) * RowGeo<P>::ROWS;
+  if (scat_smem) {
+    const int rows = min(RowGeo<P>::ROWS, a.d.NY - y0);
+    const int per = rows * (P::N / 2);  // 16-byte chunks of one term's rows
+    for (int i = threadIdx.x; i < nterm * per; i += blockDim.x) {
+      const int t = i / per, r = (i - t * per) / (P::N / 2), q = i - t * per - r * (P::N / 2);
+      cp_async16(wt + ((size_t)t * RowGeo<P>::ROWS + r) * P::N + 2 * q,
+                 a.scat_tab + ((long long)(t + a.term0) * a.d.NY + y0 + r) * P::N + 2 * q);
+    }
+    cp_async_commit();
+  }
+  bool wt_ready = false;
   load_stage_tw<P>(c.tw, a.twx);
   constexpr bool kPair = POST == W_SMOOTH_PAIR;
   constexpr bool kSmooth = POST == W_SMOOTH || POST == W_SMOOTH_DERIV || kPair;
@@ -449,7 +481,6 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   const float* hinv = href + kMaxHatRefs;
   if (hat_smem) stage_hat_refs<P>(a, const_cast<float*>(href), const_cast<float*>(hinv));
   __syncthreads();
-  const int nterm = multi_term(POST) ? a.nterm : 1;
   float g[kSmooth ? P::E : 1];
   float2 acc[P::E];
   float2 acc2[kPair ? P::E : 1];
@@ -534,6 +565,17 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
           acc[e] = cadd(acc[e], cmul(v[e], hat_ref_weight<POST>(h, wdz, C)));
         }
       }
+    } else if (kScat && scat_smem) {
+      if (!wt_ready) {  // every warp reaches this after its first transform (no term is skipped)
+        cp_async_wait<0>();
+        __syncthreads();
+        wt_ready = true;
+      }
+      const float f = 0.5f * a.w[c.iw] * a.dz * a.coef[term + a.term0];
+      const float2* wrow = wt + ((size_t)term * RowGeo<P>::ROWS + (c.y - y0)) * P::N;
+#pragma unroll
+      for (int e = 0; e < P::E; ++e)
+        if (c.live) acc[e] = cadd(acc[e], cmul(v[e], rot90<false>(cscale(wrow[pos_first<P>(c.t, e)], f))));
     } else {
 #pragma unroll
       for (int e = 0; e < P::E; ++e) {
@@ -1157,7 +1199,8 @@ template <class P>
 cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_t s) {
   const int nchunk = (a.d.NY + RowGeo<P>::ROWS - 1) / RowGeo<P>::ROWS;
   const unsigned grid = (unsigned)(a.nb * nchunk);
-  const size_t sm = RowGeo<P>::smem();
+  const size_t sm = post == W_SCAT && a.scat_tab && RowGeo<P>::scat_stage(a.nterm) ? RowGeo<P>::smem_scat(a.nterm)
+                                                                                   : RowGeo<P>::smem();
   cudaError_t e;
 #define FWIX_FAST_RI(W)                                                                          \
   case W:                                                                                        \
