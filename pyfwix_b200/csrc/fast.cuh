@@ -362,6 +362,24 @@ template <class P, int PRE>
 __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_row_fwd(const SpecArgs a, int nchunk) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
+  // Born weights (W_SCAT_CONJ) from the per-depth table: the CTA's rows of every
+  // transformed term's table copied into shared memory (cp.async) while the input
+  // rows load, instead of one L2 read per sample and term in each lane.
+  constexpr bool kScatC = PRE == W_SCAT_CONJ;
+  const int nterm_s = kScatC ? a.nterm : 0;
+  const bool scat_smem = kScatC && a.scat_tab && RowGeo<P>::scat_stage(nterm_s);
+  float2* wt = smem + RowGeo<P>::scat_offset();
+  const int y0 = (int)(blockIdx.x - c.bl * nchunk) * RowGeo<P>::ROWS;
+  if (scat_smem) {
+    const int rows = min(RowGeo<P>::ROWS, a.d.NY - y0);
+    const int per = rows * (P::N / 2);
+    for (int i = threadIdx.x; i < nterm_s * per; i += blockDim.x) {
+      const int t = i / per, r = (i - t * per) / (P::N / 2), q = i - t * per - r * (P::N / 2);
+      cp_async16(wt + ((size_t)t * RowGeo<P>::ROWS + r) * P::N + 2 * q,
+                 a.scat_tab + ((long long)(t + a.term0) * a.d.NY + y0 + r) * P::N + 2 * q);
+    }
+    cp_async_commit();
+  }
   load_stage_tw<P>(c.tw, a.twx);
   if (PRE == W_SMOOTH_CONJ && a.sm_n <= kMaxHatRefs)
     stage_hat_refs<P>(a, reinterpret_cast<float*>(c.tw + tw_size<P>()),
@@ -409,6 +427,10 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
     for (int o = 1; o < 32; o <<= 1) mine |= __shfl_xor_sync(0xffffffffu, mine, o);
     used = mine;
   }
+  if (scat_smem) {  // the weight rows have landed (the input rows are in registers)
+    cp_async_wait<0>();
+    __syncthreads();
+  }
   for (int term = 0; term < nterm; ++term) {
     float2 v[P::E];
     if (!((used >> (term & 31)) & 1u)) {
@@ -426,6 +448,12 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
       for (int e = 0; e < P::E; ++e)
         v[e] = c.live ? cmul(raw[e], hat_ref_weight<PRE>(hat_at(hinv, a.sm_n, term, g[e]), wdz, C))
                       : make_float2(0.f, 0.f);
+    } else if (kScatC && scat_smem) {
+      const float f = 0.5f * a.w[c.iw] * a.dz * a.coef[term + a.term0];
+      const float2* wrow = wt + ((size_t)term * RowGeo<P>::ROWS + (c.y - y0)) * P::N;
+#pragma unroll
+      for (int e = 0; e < P::E; ++e)
+        v[e] = c.live ? cmul_conj(raw[e], rot90<false>(cscale(wrow[pos_first<P>(c.t, e)], f))) : make_float2(0.f, 0.f);
     } else {
 #pragma unroll
       for (int e = 0; e < P::E; ++e) {
@@ -457,6 +485,9 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   // are copied into shared memory (cp.async, 16 bytes a thread and instruction)
   // while the first term loads and transforms, and read from there after each
   // transform instead of from L2 behind it.
+  // (Staging the scattering adjoint's zeroth term conj(W_0) d the same way,
+  // W_0 and d rows, measured slower: 34 -> 40 us per 64 slices at 256, its
+  // 64 KB of shared memory halving the resident CTAs of that light pass.)
   constexpr bool kScat = POST == W_SCAT;
   const int nterm = multi_term(POST) ? a.nterm : 1;
   const bool scat_smem = kScat && a.scat_tab && RowGeo<P>::scat_stage(nterm);
@@ -876,7 +907,7 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
     k_col_b_tma(const SpecArgs a, int nxt, const __grid_constant__ CUtensorMap tin,
                 const __grid_constant__ CUtensorMap tout, const __grid_constant__ CUtensorMap tq) {
   using C = ColTma<P>;
-  static_assert(C::LX == 16, "TMA column tiles are 16 columns (128 bytes) wide");
+  static_assert(C::LX == 16 || C::LX == 8, "TMA column tiles are 16 or 8 columns (128- or 64-byte rows)");
   extern __shared__ unsigned char smem_raw[];
   float2* base = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   float2* tiles[2] = {base, base + C::TILE};
@@ -928,7 +959,7 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
     }
     float2 v[P::E];
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) v[e] = tiles[buf][tma::sw128(pos_first<P>(t, e), col)];
+    for (int e = 0; e < P::E; ++e) v[e] = tiles[buf][tma::swz_tile<C::LX>(pos_first<P>(t, e), col)];
     __syncthreads();  // the tile is in registers: its buffer is free for the exchanges
     fft_fwd<P>(v, t, tw, tiles[buf] + col * P::N);
     if constexpr (kQT) {
@@ -950,7 +981,7 @@ __global__ void __launch_bounds__(kWarps * 32, ColGeo<P>::kMinBlocks)
   // no load is pending: buffer 0 holds the inverse transform's exchanges, buffer 1 the result
   fft_inv<P>(acc, t, tw, tiles[0] + col * P::N);
 #pragma unroll
-  for (int e = 0; e < P::E; ++e) tiles[1][tma::sw128(pos_first<P>(t, e), col)] = acc[e];
+  for (int e = 0; e < P::E; ++e) tiles[1][tma::swz_tile<C::LX>(pos_first<P>(t, e), col)] = acc[e];
   tma::fence_proxy_async();
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -994,7 +1025,7 @@ __global__ void __launch_bounds__(kWarps * 32, col_a_tma_min_blocks<P>(kQT))
     k_col_a_tma(const SpecArgs a, int nxt, const __grid_constant__ CUtensorMap tin,
                 const __grid_constant__ CUtensorMap tout, const __grid_constant__ CUtensorMap tq) {
   using C = ColTmaA<P>;
-  static_assert(C::LX == 16, "TMA column tiles are 16 columns (128 bytes) wide");
+  static_assert(C::LX == 16 || C::LX == 8, "TMA column tiles are 16 or 8 columns (128- or 64-byte rows)");
   extern __shared__ unsigned char smem_raw[];
   float2* in = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   float2* stage = in + C::TILE;
@@ -1057,7 +1088,7 @@ __global__ void __launch_bounds__(kWarps * 32, col_a_tma_min_blocks<P>(kQT))
   }
   float2 psi[P::E];
 #pragma unroll
-  for (int e = 0; e < P::E; ++e) psi[e] = in[tma::sw128(pos_first<P>(t, e), col)];
+  for (int e = 0; e < P::E; ++e) psi[e] = in[tma::swz_tile<C::LX>(pos_first<P>(t, e), col)];
   int first = 0;
   auto store = [&](int term) {  // staging tile -> t2[term]
     tma::fence_proxy_async();
@@ -1077,7 +1108,7 @@ __global__ void __launch_bounds__(kWarps * 32, col_a_tma_min_blocks<P>(kQT))
     if (a.term0 == 0 && a.nterm > 0) {
       const float sc = a.norm * (float)P::N;
 #pragma unroll
-      for (int e = 0; e < P::E; ++e) stage[tma::sw128(pos_first<P>(t, e), col)] = cscale(psi[e], sc);
+      for (int e = 0; e < P::E; ++e) stage[tma::swz_tile<C::LX>(pos_first<P>(t, e), col)] = cscale(psi[e], sc);
       store(0);
       first = 1;
     }
@@ -1109,7 +1140,7 @@ __global__ void __launch_bounds__(kWarps * 32, col_a_tma_min_blocks<P>(kQT))
     fft_inv<P>(v, t, tw, line);
     stage_free();
 #pragma unroll
-    for (int e = 0; e < P::E; ++e) stage[tma::sw128(pos_first<P>(t, e), col)] = v[e];
+    for (int e = 0; e < P::E; ++e) stage[tma::swz_tile<C::LX>(pos_first<P>(t, e), col)] = v[e];
     store(term);  // also orders this term's phase reads before the slot's next load
     if constexpr (kQT) {
       if (threadIdx.x == 0 && term + 2 < nterm) issue_q(term + 2);
@@ -1174,7 +1205,8 @@ template <class P>
 cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
   const int nchunk = (a.d.NY + RowGeo<P>::ROWS - 1) / RowGeo<P>::ROWS;
   const unsigned grid = (unsigned)(a.nb * nchunk);
-  const size_t sm = RowGeo<P>::smem();
+  const size_t sm = pre == W_SCAT_CONJ && a.scat_tab && RowGeo<P>::scat_stage(a.nterm) ? RowGeo<P>::smem_scat(a.nterm)
+                                                                                       : RowGeo<P>::smem();
   cudaError_t e;
 #define FWIX_FAST_RF(W)                                                              \
   case W:                                                                            \
@@ -1243,8 +1275,8 @@ cudaError_t col_type_a_tma(const SpecArgs& a, int qmode, cudaStream_t s) {
   const size_t sm = C::smem(qtile ? (size_t)C::LX * a.ptab_ny : 0);
   CUtensorMap tin, tout, tq;
   std::memset(&tq, 0, sizeof(tq));
-  cudaError_t e = tile_map(&tin, a.t1, a.d.NX, a.d.NY, a.nb, C::ROWS);
-  if (e == cudaSuccess) e = tile_map(&tout, a.t2, a.d.NX, a.d.NY, (a.tstride / a.d.slice) * (a.term0 + a.nterm), C::ROWS);
+  cudaError_t e = tile_map(&tin, a.t1, a.d.NX, a.d.NY, a.nb, C::ROWS, C::LX);
+  if (e == cudaSuccess) e = tile_map(&tout, a.t2, a.d.NX, a.d.NY, (a.tstride / a.d.slice) * (a.term0 + a.nterm), C::ROWS, C::LX);
   if (e == cudaSuccess && qtile) e = qtab_map(&tq, a.ptab, a.ptab_ny, a.ptab_nx, (long long)a.nterm * a.d.nw, C::LX);
   if (e != cudaSuccess) return e;
 #define FWIX_FAST_CAT(Q, QT)                                                                          \
@@ -1276,7 +1308,7 @@ cudaError_t col_type_a_tma(const SpecArgs& a, int qmode, cudaStream_t s) {
 
 template <class P>
 cudaError_t col_type_a(const SpecArgs& a, int qmode, cudaStream_t s) {
-  if constexpr (ColGeo<P>::LX == 16) {
+  if constexpr (ColGeo<P>::LX == 16 || ColGeo<P>::LX == 8) {
     if (a.tma && a.err && a.d.NX % 2 == 0) return col_type_a_tma<P>(a, qmode, s);
   }
   const int nxt = (a.d.NX + ColGeo<P>::LX - 1) / ColGeo<P>::LX;
@@ -1311,8 +1343,8 @@ cudaError_t col_type_b_tma(const SpecArgs& a, int qmode, cudaStream_t s) {
   const size_t sm = C::smem(qtile ? (size_t)C::LX * a.ptab_ny : 0);
   CUtensorMap tin, tout, tq;
   std::memset(&tq, 0, sizeof(tq));
-  cudaError_t e = tile_map(&tin, a.t1, a.d.NX, a.d.NY, (a.tstride / a.d.slice) * a.nterm, C::ROWS);
-  if (e == cudaSuccess) e = tile_map(&tout, a.t2, a.d.NX, a.d.NY, a.nb, C::ROWS);
+  cudaError_t e = tile_map(&tin, a.t1, a.d.NX, a.d.NY, (a.tstride / a.d.slice) * a.nterm, C::ROWS, C::LX);
+  if (e == cudaSuccess) e = tile_map(&tout, a.t2, a.d.NX, a.d.NY, a.nb, C::ROWS, C::LX);
   if (e == cudaSuccess && qtile) e = qtab_map(&tq, a.ptab, a.ptab_ny, a.ptab_nx, (long long)a.nterm * a.d.nw, C::LX);
   if (e != cudaSuccess) return e;
 #define FWIX_FAST_CBT(Q, QT)                                                                          \
@@ -1344,7 +1376,7 @@ cudaError_t col_type_b_tma(const SpecArgs& a, int qmode, cudaStream_t s) {
 
 template <class P>
 cudaError_t col_type_b(const SpecArgs& a, int qmode, cudaStream_t s) {
-  if constexpr (ColGeo<P>::LX == 16) {
+  if constexpr (ColGeo<P>::LX == 16 || ColGeo<P>::LX == 8) {
     if (a.tma && a.err && a.d.NX % 2 == 0) return col_type_b_tma<P>(a, qmode, s);
   }
   const int nxt = (a.d.NX + ColGeo<P>::LX - 1) / ColGeo<P>::LX;

@@ -79,15 +79,25 @@ __device__ __forceinline__ void store_wait_read() { asm volatile("cp.async.bulk.
 // the 128-byte swizzle: 16-byte chunk c / 2 of row y moves to chunk
 // (c / 2) ^ (y & 7).  The tile must start on a 1024-byte boundary.
 __device__ __forceinline__ int sw128(int y, int c) { return y * 16 + ((((c >> 1) ^ (y & 7)) << 1) | (c & 1)); }
+// The same for a tile of 8 columns (64-byte rows) with the 64-byte swizzle: 16-byte
+// chunk c / 2 of row y moves to chunk (c / 2) ^ ((y >> 1) & 3).  The tile must start
+// on a 512-byte boundary.
+__device__ __forceinline__ int sw64(int y, int c) { return y * 8 + ((((c >> 1) ^ ((y >> 1) & 3)) << 1) | (c & 1)); }
+// Tile index of sample (y, c) for LX-column tiles (16: sw128, 8: sw64).
+template <int LX>
+__device__ __forceinline__ int swz_tile(int y, int c) {
+  static_assert(LX == 16 || LX == 8, "TMA column tiles are 8 or 16 columns wide");
+  return LX == 16 ? sw128(y, c) : sw64(y, c);
+}
 
 }  // namespace tma
 
 // Host side: a 3-D tensor map over 8-byte samples [nz][ny][nx] at base (row
-// pitch nx samples, plane pitch ny * nx), box {16, box_rows, 1}, 128-byte
-// swizzle.  Maps are cached per (base, sizes, box).  Returns the CUDA error of
+// pitch nx samples, plane pitch ny * nx), box {box_cols, box_rows, 1} with the
+// 128-byte swizzle for 16 columns, the 64-byte swizzle for 8.  Maps are cached per (base, sizes, box).  Returns the CUDA error of
 // the driver call (cudaErrorInvalidValue when the driver entry point is missing
 // or the encoding is refused).
-cudaError_t tile_map(CUtensorMap* out, const void* base, int nx, int ny, long long nz, int box_rows);
+cudaError_t tile_map(CUtensorMap* out, const void* base, int nx, int ny, long long nz, int box_rows, int box_cols = 16);
 
 // Host side: a 3-D tensor map over the quarter-spectrum phase table of one depth,
 // [nslices][pnx][pny] 8-byte factors (ky fastest, pny even so that rows are 16-byte

@@ -25,9 +25,11 @@ def _plans(monkeypatch, step, qtile=3, **kw):
     return g, rng, sref, labels, slow, den, p0, p1
 
 
-# plan lengths whose column passes take 16 columns per CTA (128 bytes per tile row);
-# qtile 3: the phase factors arrive as TMA tiles too (both column passes), 0: per lane
-@pytest.mark.parametrize("n,pad", [(124, 4), (192, 0), (256, 0), (316, 4)])
+# plan lengths whose column passes take 16 columns per CTA (128 bytes per tile row,
+# 128-byte swizzle: 128 - 320) or 8 (64 bytes, 64-byte swizzle: 384 - 640); qtile 3:
+# the phase factors arrive as TMA tiles too (both column passes, lengths whose
+# quarter-spectrum rows fit one box: up to 510), 0: per lane
+@pytest.mark.parametrize("n,pad", [(124, 4), (192, 0), (256, 0), (316, 4), (380, 4), (512, 0), (640, 0)])
 @pytest.mark.parametrize("step", ["pspi", "nsps"])
 @pytest.mark.parametrize("qtile", [0, 3])
 def test_tma_steps_equal_copy_steps(monkeypatch, n, pad, step, qtile):
