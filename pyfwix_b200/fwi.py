@@ -42,11 +42,38 @@ backward against three for the checkpointed forward.
 """
 from __future__ import annotations
 
+import collections
+import weakref
+
 import numpy as np
 import torch
 
 from . import _lib as L
 from .plan import Plan
+
+# Plans of recent SmoothFWI sizes, reused by later problems of the same sizes (the
+# shots of one survey, the iterations of an inversion): a plan's tables, workspace
+# and phase-factor cache are built once, and each problem rebinds its slowness,
+# references and traces.  At most two are kept.
+_PLAN_CACHE: "collections.OrderedDict[tuple, Plan]" = collections.OrderedDict()
+_PLAN_CACHE_SIZE = 2
+
+
+def _cached_plan(key, make):
+    p = _PLAN_CACHE.get(key)
+    if p is None:
+        p = make()
+        _PLAN_CACHE[key] = p
+        while len(_PLAN_CACHE) > _PLAN_CACHE_SIZE:
+            _PLAN_CACHE.popitem(last=False)
+    else:
+        _PLAN_CACHE.move_to_end(key)
+    return p
+
+
+def clear_plan_cache():
+    """Releases the cached plans (their device memory) of earlier problems."""
+    _PLAN_CACHE.clear()
 
 
 def smooth_refs(s, nref, spread=1e-3):
@@ -110,12 +137,13 @@ class SmoothFWI:
         from .CudaWEM import _remap_ids
         s_ids, r_ids, ns = _remap_ids(geometry["s_ids"], geometry["r_ids"])
         self.padx, self.pady = int(_get(par, "padx", 0)), int(_get(par, "pady", 0))
-        self.plan = Plan(nx=nx, ny=ny, nw=nw, ns=ns, nz=nz, dx=_get(par, "dx", 1.0), dy=_get(par, "dy", 1.0),
-                         dz=_get(par, "dz", 1.0), ox=_get(par, "ox", 0.0), oy=_get(par, "oy", 0.0),
-                         oz=_get(par, "oz", 0.0), ow=_get(par, "ow", 1.0), dw=_get(par, "dw", 1.0),
-                         padx=self.padx, pady=self.pady, nref=int(_get(par, "nref", 2)),
-                         eps=float(_get(par, "eps", 0.0)), taperx=int(_get(par, "taperx", 0)),
-                         tapery=int(_get(par, "tapery", 0)), step="pspi", device=self.device)
+        kw = dict(nx=nx, ny=ny, nw=nw, ns=ns, nz=nz, dx=float(_get(par, "dx", 1.0)), dy=float(_get(par, "dy", 1.0)),
+                  dz=float(_get(par, "dz", 1.0)), ox=float(_get(par, "ox", 0.0)), oy=float(_get(par, "oy", 0.0)),
+                  oz=float(_get(par, "oz", 0.0)), ow=float(_get(par, "ow", 1.0)), dw=float(_get(par, "dw", 1.0)),
+                  padx=self.padx, pady=self.pady, nref=int(_get(par, "nref", 2)), eps=float(_get(par, "eps", 0.0)),
+                  taperx=int(_get(par, "taperx", 0)), tapery=int(_get(par, "tapery", 0)))
+        key = (str(self.device),) + tuple(sorted(kw.items()))
+        self.plan = _cached_plan(key, lambda: Plan(step="pspi", device=self.device, **kw))
         p = self.plan
         self.src = p.traces(geometry["sx"], geometry["sy"], geometry["sz"], s_ids)
         self.rec = p.traces(geometry["rx"], geometry["ry"], geometry["rz"], r_ids)
@@ -160,6 +188,7 @@ class SmoothFWI:
         p = self.plan
         s = torch.as_tensor(s).to(self.device, torch.float32).contiguous()
         self.s = s
+        p._fwi_owner = weakref.ref(self)  # whose slowness the (possibly shared) plan holds
         refs = self.refs_fixed if self.refs_fixed is not None else smooth_refs(s, p.nref)
         self.refs = torch.as_tensor(refs).to(self.device, torch.float32)
         p.set_smooth(pad_edge(s, self.padx, self.pady), self.refs)
@@ -291,6 +320,9 @@ class SmoothFWI:
     def gradient(self, res):
         """dJ/ds [nz][ny][nx] (float32) for the residual res = d - d_obs, after
         model(s, keep=True)."""
+        owner = getattr(self.plan, "_fwi_owner", None)
+        if owner is None or owner() is not self:
+            self.set_slowness(self.s)  # another problem rebound the shared plan since model()
         p, nz = self.plan, self.plan.nz
         res = torch.as_tensor(res).to(self.device, torch.complex64).contiguous()
         gpad = torch.zeros((nz, p.NY, p.NX), dtype=torch.float32, device=self.device)

@@ -116,6 +116,7 @@ class Plan:
         zst = labels.shape[1] * self.NY * self.NX
         L.check(self.lib.fwix_plan_set_refs(self._h, _p(sref), _p(labels), zst, wst))
         self._keep["sref"], self._keep["labels"] = sref, labels
+        self._keep.pop("sm_ref_bound", None)  # the smooth references no longer match the bound ones
         if phase_cache and "pcache" not in self._keep and not self.enable_phase_cache():
             # no room for every depth: a few depths in rotation still spare the
             # column passes the per-sample factors (a migration level reuses its table)
@@ -148,9 +149,14 @@ class Plan:
             raise ValueError("smooth inputs must be [nz][NY][NX] and [nz][nref]")
         if self.nref > 1 and not bool(torch.all(sr[:, 1:] > sr[:, :-1])):
             raise ValueError("reference slownesses must increase strictly within each depth")
-        sref2 = (sr.double() ** 2)[:, :, None].expand(self.nz, self.nref, self.nw).to(torch.complex64)
-        labels = torch.zeros((self.nz, 1, self.NY, self.NX), dtype=torch.uint8, device=self.device)
-        self.set_refs(sref2, labels)
+        prev = self._keep.get("sm_ref_bound")
+        if prev is None or prev.shape != sr.shape or not torch.equal(prev, sr):
+            # new references: their phase factors replace the cached ones; the same
+            # references as bound keep the cache (the shots of one inversion step)
+            sref2 = (sr.double() ** 2)[:, :, None].expand(self.nz, self.nref, self.nw).to(torch.complex64)
+            labels = torch.zeros((self.nz, 1, self.NY, self.NX), dtype=torch.uint8, device=self.device)
+            self.set_refs(sref2, labels)
+            self._keep["sm_ref_bound"] = sr.clone()
         L.check(self.lib.fwix_plan_set_smooth(self._h, _p(sp), _p(sr)))
         self._keep["sm_s"], self._keep["sm_ref"] = sp, sr
         return sp, sr

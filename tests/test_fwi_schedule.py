@@ -25,6 +25,13 @@ def _put(t, a):
     return t
 
 
+@pytest.fixture(autouse=True)
+def _no_shared_plans():
+    """Plans of these tests (counting stand-ins) stay out of later tests' reach."""
+    yield
+    fwi.clear_plan_cache()
+
+
 class OraclePlan:
     """The part of ``pyfwix_b200.plan.Plan`` that SmoothFWI calls, on the oracle."""
 
@@ -112,6 +119,7 @@ def _problem(nz=7):
 
 def _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, checkpoint):
     monkeypatch.setattr(fwi, "Plan", OraclePlan)
+    fwi.clear_plan_cache()  # a plan (and its step counters) of its own
     prob = fwi.SmoothFWI(s.shape, geom, torch.from_numpy(wav), dict(par, checkpoint=checkpoint), device="cpu")
     data = prob.model(torch.from_numpy(s), keep=True)
     res = data - torch.from_numpy(d_obs).to(torch.complex64)
@@ -157,6 +165,7 @@ def test_checkpointed_step_count(monkeypatch):
     the up derivatives as paired steps, the mu fields, and nu."""
     g, s, refs, geom, wav, par, acq, d_obs = _problem(nz=12)
     monkeypatch.setattr(fwi, "Plan", OraclePlan)
+    fwi.clear_plan_cache()
     prob = fwi.SmoothFWI(s.shape, geom, torch.from_numpy(wav), dict(par, checkpoint=4), device="cpu")
     data = prob.model(torch.from_numpy(s), keep=True)
     fwd = dict(prob.plan.calls)
