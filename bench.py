@@ -806,6 +806,9 @@ def main():
             sh["s"] = float(tt.item())
         sh["shots_per_s"] = ws / sh["s"]
         fwi["shots_across_ranks"] = sh
+        from pyfwix_b200.fwi import clear_plan_cache
+        clear_plan_cache()  # the FWI plan's phase cache is not needed by the timings below
+        torch.cuda.empty_cache()
     config1 = config1_timing(device, autotune=not a.no_autotune) if not a.no_config1 else None
     if ws == 1 and not a.no_batched:
         batched = batched_timing(device, nshots=a.batched_shots, nz=a.batched_nz, nstreams=a.batched_streams)
