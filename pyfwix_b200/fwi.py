@@ -166,6 +166,11 @@ class SmoothFWI:
         # memory torch's allocator holds but does not use (fields of an earlier shot)
         # is free for this shot's fields as well
         free += torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
+        # a reused plan's phase-factor cache belongs to the working set the budget
+        # is for (a new plan allocates it after this decision)
+        pc = p._keep.get("pcache") if hasattr(p, "_keep") else None
+        if pc is not None:
+            free += pc.numel() * pc.element_size()
         budget = 0.6 * free
         if 3 * p.nz * wb + 4 * wb <= budget:
             return None
