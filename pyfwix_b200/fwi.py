@@ -24,8 +24,10 @@ with D / U the down / up fields, R_iz = (s_iz - s_iz+1) / (s_iz + s_iz+1)
 slownesses of each depth held fixed.  Every operator is a kernel of
 libfwix_b200.so; this module only sequences them.
 
-Storage: the down and up fields of every depth and the mu field of every depth
-are kept in device memory (``checkpoint=None``), or, with ``checkpoint=k``,
+Storage: the down field, the up step's slowness derivative dS_iz(U_iz+1) (the
+only use the gradient makes of U; the modelling's up pass takes it with the
+paired step) and the mu field of every depth are kept in device memory
+(``checkpoint=None``), or, with ``checkpoint=k``,
 only every k-th down / up / mu field is kept and each k-level segment is
 recomputed from its checkpoint when the backward sweeps reach it;
 ``checkpoint="auto"`` (the default) stores everything when it fits in device
@@ -212,9 +214,14 @@ class SmoothFWI:
             store.copy_(D)
         p.smooth_step(iz, D, D)
 
-    def _up_step(self, iz, U, Dz, data):
+    def _up_step(self, iz, U, Dz, data, deriv=None):
+        """U_iz from U_iz+1 in place; with ``deriv`` the paired step also writes
+        dS_iz(U_iz+1) there (what the gradient takes of U)."""
         p = self.plan
-        p.smooth_step(iz, U, U)
+        if deriv is None:
+            p.smooth_step(iz, U, U)
+        else:
+            p.smooth_step_pair(iz, U, U, deriv)
         p.reflect(iz, Dz, U, add=True)
         p.inject(self.rec, iz, data, U, adjoint=True)
 
@@ -226,17 +233,24 @@ class SmoothFWI:
         data = torch.zeros((self.ntrace, p.nw), dtype=torch.complex64, device=self.device)
         D = self._field()
         if self.k is None:
-            self.Ds = [self._field() for _ in range(nz)]
+            # one block per stored family (not nz fields): the caching allocator
+            # hands the previous shot's block back whole, with no device allocation.
+            # The up pass reflects every down field, so they are kept either way.
+            self.Ds = list(self._block(nz))
             for iz in range(nz):
                 self._down_step(iz, D, data, self.Ds[iz])
+            # the gradient takes U only through dS_iz(U_iz+1): the up pass's paired
+            # step stores that instead of U (one derivative step fewer per level in
+            # the backward, the same memory)
             U = self._field()
-            self.Us = [None] * nz
+            self.dSU = [None] * nz
+            dblk = self._block(nz - 1) if keep and nz > 1 else None
             for iz in range(nz - 1, -1, -1):
-                self._up_step(iz, U, self.Ds[iz], data)
-                if keep:
-                    self.Us[iz] = U.clone()
+                d = dblk[iz] if dblk is not None and iz + 1 < nz else None
+                self._up_step(iz, U, self.Ds[iz], data, deriv=d)
+                self.dSU[iz] = d
             if not keep:
-                self.Ds = self.Us = None
+                self.Ds = self.dSU = None
             return data
         k = self.k
         self.Dck = {}
@@ -255,6 +269,10 @@ class SmoothFWI:
 
     def _empty(self):
         return torch.empty(self.plan.wshape, dtype=torch.complex64, device=self.device)
+
+    def _block(self, n):
+        """n uninitialised fields in one allocation, [n][ns][nw][NY][NX]."""
+        return torch.empty((n,) + tuple(self.plan.wshape), dtype=torch.complex64, device=self.device)
 
     def _segment_D(self, a, derivs=False):
         """Down fields D_a .. D_{a+k-1} (after injection) recomputed from the
@@ -335,12 +353,11 @@ class SmoothFWI:
         G = self._field()
         if self.k is None:
             Dget = lambda iz: self.Ds[iz]
-            Uget = lambda iz: self.Us[iz]
-            mus = [None] * nz
+            mus = self._block(nz)
             mu = self._field()
             for iz in range(nz):
-                self._mu_level(iz, mu, res, Dget(iz), Uget(iz + 1) if iz + 1 < nz else None, gpad, crefl, G)
-                mus[iz] = mu.clone()
+                self._mu_level(iz, mu, res, Dget(iz), self.dSU[iz], gpad, crefl)
+                mus[iz].copy_(mu)
             nu = self._field()
             for iz in range(nz - 1, -1, -1):
                 self._nu_level(iz, nu, res, Dget(iz), mus[iz], gpad, G)
@@ -384,14 +401,13 @@ class SmoothFWI:
             grefl[1:] += crefl[:-1] * (-2 * s0 / den)
         return fold_edge(gpad, p.ny, p.nx) + grefl
 
-    def _mu_level(self, iz, mu, res, Dz, Unext, gpad, crefl, G):
+    def _mu_level(self, iz, mu, res, Dz, dSU, gpad, crefl):
         p = self.plan
         if iz > 0:
             p.smooth_step(iz - 1, mu, mu, mode=L.SMOOTH_ADJ)
         p.inject(self.rec, iz, res, mu)
-        if Unext is not None:
-            p.smooth_step(iz, Unext, G, mode=L.SMOOTH_DERIV)
-            p.correlate(mu, G, gpad[iz], add=True, padded=True)
+        if dSU is not None:  # dS_iz(U_iz+1), from the modelling's up pass
+            p.correlate(mu, dSU, gpad[iz], add=True, padded=True)
             p.correlate(mu, Dz, crefl[iz], add=True, padded=False)
 
     def _nu_level(self, iz, nu, res, Dz, muz, gpad, G):

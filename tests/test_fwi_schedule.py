@@ -145,8 +145,9 @@ def test_every_depth_matches_oracle_gradient(monkeypatch):
 def test_checkpoints_match_every_depth(monkeypatch, k):
     """k = 3 leaves a short last segment (7 levels), k = 7 makes one segment and
     k = 16 is deeper than the grid.  With every depth stored the driver takes
-    6 nz - 3 steps (down and up modelling, mu and its derivative steps, nu and
-    its derivative steps); checkpoints add the recomputed segments."""
+    4 nz - 1 steps and nz - 1 paired steps (down modelling; up modelling paired
+    with the derivative of U; mu steps; nu and its derivative steps);
+    checkpoints add the recomputed segments."""
     g, s, refs, geom, wav, par, acq, d_obs = _problem()
     data0, grad0, full = _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, None)
     data, grad, prob = _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, k)
@@ -154,8 +155,8 @@ def test_checkpoints_match_every_depth(monkeypatch, k):
     assert _rel(data, data0) < 1e-6
     assert _rel(grad, grad0) < 1e-5
     nz = g.nz
-    assert full.plan.calls["step"] == 6 * nz - 3 and full.plan.calls["pair"] == 0
-    assert prob.plan.calls["step"] + prob.plan.calls["pair"] > full.plan.calls["step"]
+    assert full.plan.calls["step"] == 4 * nz - 1 and full.plan.calls["pair"] == nz - 1
+    assert prob.plan.calls["step"] + prob.plan.calls["pair"] > full.plan.calls["step"] + full.plan.calls["pair"]
 
 
 def test_checkpointed_step_count(monkeypatch):
