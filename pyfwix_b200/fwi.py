@@ -260,8 +260,9 @@ class SmoothFWI:
             self._down_step(iz, D, data, None)
         self.Uck = {nz: self._field()}
         U = self._field()
+        bufs = dict(D=self._block(k))
         for a in reversed(range(0, nz, k)):
-            seg = self._segment_D(a)
+            seg = self._segment_D(a, bufs)
             for iz in range(min(a + k, nz) - 1, a - 1, -1):
                 self._up_step(iz, U, seg[iz - a], data)
             self.Uck[a] = U.clone()
@@ -274,46 +275,56 @@ class SmoothFWI:
         """n uninitialised fields in one allocation, [n][ns][nw][NY][NX]."""
         return torch.empty((n,) + tuple(self.plan.wshape), dtype=torch.complex64, device=self.device)
 
-    def _segment_D(self, a, derivs=False):
+    def _seg_buffers(self):
+        """Fields of one checkpoint segment, allocated once per sweep and reused by
+        every segment: down fields, their derivatives, up derivatives, mu fields
+        (k each) and two up fields for the walk."""
+        k = self.k
+        return dict(D=self._block(k), dSD=self._block(k), dSU=self._block(k), mu=self._block(k), U=self._block(2))
+
+    def _segment_D(self, a, bufs, derivs=False):
         """Down fields D_a .. D_{a+k-1} (after injection) recomputed from the
         checkpoint at a, without recording; with ``derivs`` also dS_iz(D_iz) for
         every level of the segment above the bottom of the model.  Each step
-        writes the next level's field (no copies)."""
+        writes the next level's field (no copies); the fields live in ``bufs``."""
         p, nz = self.plan, self.plan.nz
         top = min(a + self.k, nz)
-        D = self.Dck[a].clone()
+        Db, dDb = bufs["D"], bufs.get("dSD")
+        D = Db[0]
+        D.copy_(self.Dck[a])
         out, der = [], []
         for iz in range(a, top):
             p.inject(self.src, iz, self.wavelet, D)
             out.append(D)
             last = iz + 1 == top
             if derivs and iz + 1 < nz:
-                d = self._empty()
+                d = dDb[iz - a]
                 if last:
                     p.smooth_step(iz, D, d, mode=L.SMOOTH_DERIV)
                 else:
-                    nxt = self._empty()
+                    nxt = Db[iz - a + 1]
                     p.smooth_step_pair(iz, D, nxt, d)
                     D = nxt
                 der.append(d)
             elif not last:
-                nxt = self._empty()
+                nxt = Db[iz - a + 1]
                 p.smooth_step(iz, D, nxt)
                 D = nxt
         return (out, der) if derivs else out
 
-    def _segment_U_derivs(self, a, Dseg):
+    def _segment_U_derivs(self, a, Dseg, bufs):
         """dS_iz(U_{iz+1}) for the levels iz of the segment above the bottom of the
         model, walking the up fields from the checkpoint U_{a+k} (which stays
         untouched) with the paired step; index iz - a."""
         p, nz = self.plan, self.plan.nz
         top = min(a + self.k, nz)
         der = [None] * (top - a)
+        Ub, dUb = bufs["U"], bufs["dSU"]
         U = self.Uck[top]
-        for iz in range(top - 1, a - 1, -1):
-            nxt = self._empty()
+        for j, iz in enumerate(range(top - 1, a - 1, -1)):
+            nxt = Ub[j & 1]
             if iz + 1 < nz:
-                d = self._empty()
+                d = dUb[iz - a]
                 p.smooth_step_pair(iz, U, nxt, d)
                 der[iz - a] = d
             else:
@@ -323,13 +334,14 @@ class SmoothFWI:
                 U = nxt
         return der
 
-    def _segment_mu(self, a):
+    def _segment_mu(self, a, bufs):
         """mu_a .. mu_{a+k-1} recomputed from mu_{a-1} (kept at a)."""
         p, nz = self.plan, self.plan.nz
         out = []
         m = self.Mck[a]
+        Mb = bufs["mu"]
         for iz in range(a, min(a + self.k, nz)):
-            nxt = self._empty()
+            nxt = Mb[iz - a]
             if iz > 0:
                 p.smooth_step(iz - 1, m, nxt, mode=L.SMOOTH_ADJ)
             else:
@@ -376,10 +388,11 @@ class SmoothFWI:
             del mu
             # nu recursion segment by segment from the bottom, with every gradient term
             nu = self._field()
+            bufs = self._seg_buffers()
             for a in reversed(range(0, nz, k)):
-                Dseg, dSD = self._segment_D(a, derivs=True)
-                dSU = self._segment_U_derivs(a, Dseg)
-                mseg = self._segment_mu(a)
+                Dseg, dSD = self._segment_D(a, bufs, derivs=True)
+                dSU = self._segment_U_derivs(a, Dseg, bufs)
+                mseg = self._segment_mu(a, bufs)
                 for iz in range(min(a + k, nz) - 1, a - 1, -1):
                     j = iz - a
                     if iz + 1 < nz:
