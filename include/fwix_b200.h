@@ -190,6 +190,29 @@ fwix_status fwix_smooth_step_pair(fwix_plan* plan, int iz, const void* in, void*
 fwix_status fwix_correlate(fwix_plan* plan, const void* a, const void* b, float* out, int add, int padded,
                            void* stream);
 
+/* Every-depth FWI sweeps of the smooth step (no reference counterpart: the
+ * reference's gradient is ExtendedBorn's adjoint, propagator/src/ExtendedBorn.cpp:
+ * 122-150, whose piecewise-constant reference selection has no slowness
+ * derivative).  The level loops of the FWI driver with every depth stored, each
+ * on one stream; fields are [ns][nw][NY][NX], field blocks [nz] (dSU [nz-1]) of
+ * them.  Needs fwix_plan_set_smooth / set_refs and a model (the reflections).
+ * Model sweep: data = recorded down + up fields of the source injection (zeroed
+ * first); Ds[iz] = the down field at iz after injection; dSU[iz] = dS_iz(U_iz+1),
+ * the slowness derivative of the up pass's step (dSU may be NULL); D, U
+ * working fields. */
+fwix_status fwix_smooth_model_sweep(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
+                                    const void* wavelet, void* data, void* D, void* U, void* Ds, void* dSU,
+                                    void* stream);
+/* Gradient sweep for the residual res [ntrace][nw]: gpad [nz][NY][NX] = the
+ * slowness-derivative correlations (the padded gradient before folding the pad),
+ * crefl [nz][ny][nx] = the correlations with the reflection coefficients, both
+ * overwritten; Ds and dSU as the model sweep left them (dSU may be NULL only
+ * when nz == 1); mus [nz] receives the mu field of every depth; mu, nu, G
+ * working fields. */
+fwix_status fwix_smooth_gradient_sweep(fwix_plan* plan, const fwix_traces* rec, const void* res, const void* Ds,
+                                       const void* dSU, void* mus, void* mu, void* nu, void* G, float* gpad,
+                                       float* crefl, void* stream);
+
 /* ---- acquisition ------------------------------------------------------------ */
 /* Host coordinate arrays; ids are dense shot indices in [0, ns).  ntrace may be 0
  * (the arrays may then be NULL); a [ntrace][nw] trace buffer of an empty trace set

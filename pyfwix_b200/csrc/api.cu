@@ -8,7 +8,6 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
-#include <map>
 #include <string>
 #include <vector>
 
@@ -134,6 +133,7 @@ struct fwix_plan {
   cudaEvent_t lane_fork = nullptr, lane_join = nullptr;
   unsigned* err = nullptr;  // device word: bounded waits of the TMA passes that ran out
   float2* scat_tab = nullptr;     // scatter weights of one depth, [taylor+1][NY][NX]
+  float2* rf_tab = nullptr;       // coefficients of the reflections fused into a step, [2][ny][nx]
   const float* sm_s = nullptr;    // smooth step: padded slowness [nz][NY][NX]
   const float* sm_ref = nullptr;  // smooth step: sorted real reference slownesses [nz][nref]
   float2* pcache = nullptr;   // phase-factor cache of pslots depths (fwix_plan_set_phase_cache)
@@ -312,14 +312,30 @@ fwix_status step_chunk(fwix_plan* p, int kind, int iz, int dir, SpecArgs a, cuda
   return FWIX_OK;
 }
 
+// Reflections taken into a depth step (SpecArgs::rf_at): at 1 the step's input is
+// in + tab[0] f1, at 2 its output gains tab[0] f1 + tab[1] f2.
+struct Refl {
+  int at;
+  const float2* tab;
+  const float2* f1;
+  const float2* f2;
+};
+
 fwix_status do_step(fwix_plan* p, int kind, int iz, int dir, const float2* in, float2* out, int add,
                     cudaStream_t s, const float2* in2 = nullptr, const float2* ic_bg = nullptr,
-                    float* ic_img = nullptr) {
+                    float* ic_img = nullptr, const Refl* rf = nullptr) {
   SpecArgs a0 = p->args(in, out, add);
   a0.in2 = in2;  // the step of in + in2 (linear: one step instead of two)
   // image epilogue of the last (inverse row) pass: ic_img += Re sum conj(ic_bg) out
   a0.ic_bg = ic_bg;
   a0.ic_img = ic_img;
+  if (rf) {
+    if (p->fused) return fail(FWIX_ERR_STATE, "reflections cannot be fused into the cluster step");
+    a0.rf_at = rf->at;
+    a0.rf_tab = rf->tab;
+    a0.rf_f1 = rf->f1;
+    a0.rf_f2 = rf->f2;
+  }
   FWIX_TRY(phase_factors(p, iz, a0, s));
   if (p->lanes < 2 || p->fused)
     return for_chunks(p, a0, [&](const SpecArgs& a) { return step_chunk(p, kind, iz, dir, a, s); });
@@ -533,6 +549,12 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
   // the four-sweep operators up to float rounding.
   float2* SC = p->wSC();
   const bool pspi = k == FWIX_STEP_PSPI;
+  // With a model and perturbation shared by every frequency the per-level
+  // reflections ride in the depth steps' row passes (a per-cell coefficient table
+  // instead of two read-modify-write passes over the field), and the adjoint's two
+  // frequency sums of a level share one pass.  The cluster step has no such
+  // epilogue: it keeps the separate passes.
+  const bool frf = p->m_w == 0 && mw == 0 && !p->fused;
   if (!adjoint) {
     if (!add && rec->ntrace > 0) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
     // down scattering (ExtendedBorn.cpp:152-178): store[iz] = dD_iz, the field
@@ -557,6 +579,21 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
         const float2* bu;
         FWIX_TRY(U.get(p, iz + 1, s, &bu));
         FWIX_TRY(do_scatter(p, iz, 0, bu, SC, 0, ds + (iz + 1) * M, mw, s));
+        if (frf) {
+          // both reflections of this level added by the step's inverse row pass:
+          // Z_iz = S_iz(Z_iz+1 + scat) + r dD_iz + dr bg_down_iz
+          const float2 *dz, *bd;
+          FWIX_TRY(Lv.get(iz, s, &dz));
+          FWIX_TRY(D.get(p, iz, s, &bd));
+          FWIX_TRY(cu(fwix::launch_refl_table(p->d, 0, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                              p->den + iz * p->m_z, p->den + z1 * p->m_z, ds + iz * M,
+                                              ds + z1 * M, dr + iz * M, dr + z1 * M, p->rf_tab, s),
+                      "reflection coefficients"));
+          const Refl rf{2, p->rf_tab, dz, bd};
+          FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s, SC, nullptr, nullptr, &rf));
+          FWIX_TRY(do_record(p, rec, iz, A, data, s));
+          continue;
+        }
         FWIX_TRY(do_step(p, k, iz, FWIX_FWD, A, A, 0, s, SC));
       }
       const float2* dz;
@@ -596,6 +633,7 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
   for (int iz = 0; iz < nz; ++iz) {
     const int z1 = lower_iz(p, iz);
     float2* cur = Lv.field(iz);
+    const float2* ic_bu = nullptr;  // imaging-condition pair summed by the reflection pass below
     if (iz > 0) {
       // (with the packed store the previous level and this one are the same
       // working field: the step reads it before the taper or the step writes it)
@@ -609,7 +647,10 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
       }
       const float2* bu;
       FWIX_TRY(U.get(p, iz, s, &bu));
-      FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bu, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
+      if (frf && z1 != iz)
+        ic_bu = bu;
+      else
+        FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bu, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
     }
     FWIX_TRY(do_inject(p, rec, iz, data, cur, s));
     if (z1 != iz) {  // nothing at the bottom level (see the forward)
@@ -617,7 +658,8 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
       FWIX_TRY(D.get(p, iz, s, &bd));
       FWIX_TRY(cu(fwix::launch_lin_reflect_ic(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
                                               p->den + iz * p->m_z, p->den + z1 * p->m_z, p->m_w, ds + iz * M,
-                                              ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, cur, 1, s),
+                                              ds + z1 * M, dr + iz * M, dr + z1 * M, mw, bd, cur, 1, s, ic_bu,
+                                              ic_bu ? SC : nullptr),
                   "linearised reflection adjoint"));
     }
     FWIX_TRY(Lv.keep(iz, s));
@@ -625,23 +667,42 @@ fwix_status born_body(fwix_plan* p, int adjoint, const fwix_traces* rec, BgSrc& 
   // upward: eta_iz = Rec_iz^H d + conj(R_iz) zeta_iz + S_iz^H eta_iz+1, the adjoint of
   // the down-scattering recursion (reflected :240-280 and direct :180-208)
   FWIX_CU(cudaMemsetAsync(A, 0, wb, s));
+  const float2* pend = nullptr;  // (fused) level field whose reflection the next step takes in
   for (int iz = nz - 1; iz >= 0; --iz) {
     if (iz < nz - 1) {
+      const Refl rf{1, p->rf_tab, pend, nullptr};
+      const Refl* rfp = pend ? &rf : nullptr;
       if (pspi) {
-        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, SC, 0, s));
+        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, SC, 0, s, nullptr, nullptr, nullptr, rfp));
         FWIX_TRY(taper_into(SC, A));
         FWIX_TRY(do_scatter(p, iz, 1, SC, SC, 0, nullptr, 0, s));
       } else {
-        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, A, 0, s));
+        FWIX_TRY(do_step(p, k, iz, FWIX_ADJ_ADD, A, A, 0, s, nullptr, nullptr, nullptr, rfp));
         FWIX_TRY(do_scatter(p, iz, 1, A, SC, 0, nullptr, 0, s));
       }
+      pend = nullptr;
       const float2* bd;
       FWIX_TRY(D.get(p, iz, s, &bd));
       FWIX_TRY(cu(fwix::launch_ic_adj(p->d, bd, SC, ds + iz * M, mw, 1, s), "imaging adjoint"));
     }
+    // eta_0 feeds nothing: the top level's reflection and injection are not formed
+    if (iz == 0) break;
     const float2* zz;
     FWIX_TRY(Lv.get(iz, s, &zz));
-    FWIX_TRY(do_reflect(p, iz, 1, zz, A, 1, s));
+    const int z1 = lower_iz(p, iz);
+    if (frf) {
+      // conj(R_iz) zeta_iz is only read by the next step: it enters as that step's
+      // input (the bottom level reflects against itself, r = 0, and adds nothing)
+      if (z1 != iz) {
+        FWIX_TRY(cu(fwix::launch_refl_table(p->d, 1, p->slow + iz * p->m_z, p->slow + z1 * p->m_z,
+                                            p->den + iz * p->m_z, p->den + z1 * p->m_z, nullptr, nullptr,
+                                            nullptr, nullptr, p->rf_tab, s),
+                    "reflection coefficients"));
+        pend = zz;
+      }
+    } else {
+      FWIX_TRY(do_reflect(p, iz, 1, zz, A, 1, s));
+    }
     FWIX_TRY(do_inject(p, rec, iz, data, A, s));
   }
   return FWIX_OK;
@@ -719,6 +780,7 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
   if (e == cudaSuccess) e = upload(&p->tapy, taper_table(p->d.NY, q.tapery));
   if (e == cudaSuccess)
     e = cudaMalloc((void**)&p->scat_tab, (size_t)(q.taylor + 1) * p->d.slice * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&p->rf_tab, (size_t)2 * p->d.nx * p->d.ny * sizeof(float2));
   if (e == cudaSuccess) e = cudaMalloc((void**)&p->err, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(p->err, 0, sizeof(unsigned));
   if (e != cudaSuccess) {
@@ -731,7 +793,7 @@ fwix_status fwix_plan_create(const fwix_desc* desc, fwix_plan** out) {
 
 fwix_status fwix_plan_destroy(fwix_plan* p) {
   if (!p) return FWIX_OK;
-  void* ptrs[] = {p->twx, p->twy, p->kx, p->ky, p->w2, p->w, p->tapx, p->tapy, p->scat_tab, p->err};
+  void* ptrs[] = {p->twx, p->twy, p->kx, p->ky, p->w2, p->w, p->tapx, p->tapy, p->scat_tab, p->rf_tab, p->err};
   for (void* v : ptrs)
     if (v) cudaFree(v);
   if (p->lane_fork) cudaEventDestroy(p->lane_fork);
@@ -914,6 +976,96 @@ fwix_status fwix_reflect(fwix_plan* p, int iz, int adjoint, const void* in, void
   return do_reflect(p, iz, adjoint, (const float2*)in, (float2*)out, add, (cudaStream_t)stream);
 }
 
+// Every-depth FWI sweeps of the smooth step: the level loops of the FWI driver
+// (pyfwix_b200/fwi.py, SmoothFWI with every depth stored) enqueued from here, so
+// that a sweep's ~10 launches per level leave the host once instead of through
+// one binding call each.  Steps whose results nothing reads are not taken: the
+// down field's step below the bottom, the up field's step of the zero field
+// below the model, and the last adjoint step of nu.
+fwix_status fwix_smooth_model_sweep(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec,
+                                    const void* wavelet, void* data, void* D, void* U, void* Ds, void* dSU,
+                                    void* stream) {
+  if (!p || !D || !U || !Ds || no_traces(src, wavelet) || no_traces(rec, data))
+    return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_smooth(p));
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nz = p->desc.nz;
+  const size_t wb = p->wbytes();
+  float2* d = (float2*)D;
+  float2* u = (float2*)U;
+  float2* ds = (float2*)Ds;
+  float2* dsu = (float2*)dSU;
+  if (rec->ntrace > 0) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
+  FWIX_CU(cudaMemsetAsync(d, 0, wb, s));
+  for (int iz = 0; iz < nz; ++iz) {
+    FWIX_TRY(do_inject(p, src, iz, (const float2*)wavelet, d, s));
+    FWIX_TRY(do_record(p, rec, iz, d, (float2*)data, s));
+    FWIX_CU(cudaMemcpyAsync(ds + (long long)iz * p->d.wfld, d, wb, cudaMemcpyDeviceToDevice, s));
+    if (iz + 1 < nz) FWIX_TRY(fwix_smooth_step(p, iz, FWIX_SMOOTH_FWD, d, d, 0, s));
+  }
+  FWIX_CU(cudaMemsetAsync(u, 0, wb, s));
+  for (int iz = nz - 1; iz >= 0; --iz) {
+    if (iz + 1 < nz) {
+      if (dsu)
+        FWIX_TRY(fwix_smooth_step_pair(p, iz, u, u, dsu + (long long)iz * p->d.wfld, 0, s));
+      else
+        FWIX_TRY(fwix_smooth_step(p, iz, FWIX_SMOOTH_FWD, u, u, 0, s));
+    }
+    FWIX_TRY(do_reflect(p, iz, 0, ds + (long long)iz * p->d.wfld, u, 1, s));
+    FWIX_TRY(do_record(p, rec, iz, u, (float2*)data, s));
+  }
+  return FWIX_OK;
+}
+
+fwix_status fwix_smooth_gradient_sweep(fwix_plan* p, const fwix_traces* rec, const void* res, const void* Ds,
+                                       const void* dSU, void* mus, void* mu, void* nu, void* G, float* gpad,
+                                       float* crefl, void* stream) {
+  if (!p || !Ds || !mus || !mu || !nu || !G || !gpad || !crefl || no_traces(rec, res) ||
+      (!dSU && p->desc.nz > 1))
+    return fail(FWIX_ERR_INVALID, "null argument");
+  FWIX_TRY(need_smooth(p));
+  FWIX_TRY(need_model(p));
+  FWIX_TRY(need_ws(p, FWIX_WS_STEP));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nz = p->desc.nz;
+  const size_t wb = p->wbytes();
+  const long long W = p->d.wfld, gp = (long long)p->d.NY * p->d.NX, gc = (long long)p->d.ny * p->d.nx;
+  const float2* ds = (const float2*)Ds;
+  const float2* dsu = (const float2*)dSU;
+  const float2* r = (const float2*)res;
+  float2* m = (float2*)mu;
+  float2* v = (float2*)nu;
+  float2* ms = (float2*)mus;
+  FWIX_CU(cudaMemsetAsync(gpad, 0, (size_t)nz * gp * sizeof(float), s));
+  FWIX_CU(cudaMemsetAsync(crefl, 0, (size_t)nz * gc * sizeof(float), s));
+  // mu_iz = Rec_iz^H res + S_iz-1^H mu_iz-1, and the terms it meets at iz
+  FWIX_CU(cudaMemsetAsync(m, 0, wb, s));
+  for (int iz = 0; iz < nz; ++iz) {
+    if (iz > 0) FWIX_TRY(fwix_smooth_step(p, iz - 1, FWIX_SMOOTH_ADJ, m, m, 0, s));
+    FWIX_TRY(do_inject(p, rec, iz, r, m, s));
+    if (iz + 1 < nz) {
+      FWIX_TRY(fwix_correlate(p, m, dsu + iz * W, gpad + iz * gp, 1, 1, s));
+      FWIX_TRY(fwix_correlate(p, m, ds + iz * W, crefl + iz * gc, 1, 0, s));
+    }
+    FWIX_CU(cudaMemcpyAsync(ms + iz * W, m, wb, cudaMemcpyDeviceToDevice, s));
+  }
+  // nu_iz = S_iz^H (nu_iz+1 + conj(R_iz) mu_iz + Rec_iz^H res), met by dS_iz(D_iz)
+  FWIX_CU(cudaMemsetAsync(v, 0, wb, s));
+  for (int iz = nz - 1; iz >= 0; --iz) {
+    if (iz + 1 < nz) {
+      FWIX_TRY(fwix_smooth_step(p, iz, FWIX_SMOOTH_DERIV, ds + iz * W, G, 0, s));
+      FWIX_TRY(fwix_correlate(p, v, G, gpad + iz * gp, 1, 1, s));
+    }
+    if (iz == 0) break;
+    FWIX_TRY(fwix_smooth_step(p, iz, FWIX_SMOOTH_ADJ, v, v, 0, s));
+    FWIX_TRY(do_reflect(p, iz, 1, ms + iz * W, v, 1, s));
+    FWIX_TRY(do_inject(p, rec, iz, r, v, s));
+  }
+  return FWIX_OK;
+}
+
 fwix_status fwix_imaging(fwix_plan* p, int adjoint, const void* bg, void* image, void* wfld, int add,
                          void* stream) {
   if (!p || !bg || !image || !wfld) return fail(FWIX_ERR_INVALID, "null argument");
@@ -951,8 +1103,13 @@ fwix_status fwix_traces_create(fwix_plan* p, int ntrace, const float* cx, const 
   const float OX = p->desc.ox, OY = p->desc.oy, DX = p->desc.dx, DY = p->desc.dy;
   const float oz = p->desc.oz, dz = p->desc.dz;
   const int nlevel = p->desc.nz;
-  // gather lists per level: cell -> (trace, weight)
-  std::vector<std::map<long long, std::vector<std::pair<int, float>>>> inj(nlevel);
+  // gather entries per level: (cell, trace, weight), grouped by cell below
+  struct Entry {
+    long long cell;
+    int trace;
+    float w;
+  };
+  std::vector<std::vector<Entry>> inj(nlevel);
   std::vector<std::vector<int>> rtr(nlevel), rcell(nlevel);
   std::vector<std::vector<float4>> rw(nlevel);
   for (int t = 0; t < ntrace; ++t) {
@@ -974,10 +1131,10 @@ fwix_status fwix_traces_create(fwix_plan* p, int ntrace, const float* cx, const 
       const float w0 = zz * lx * ly, w1 = zz * (1 - lx) * ly, w2 = zz * lx * (1 - ly),
                   w3 = zz * (1 - lx) * (1 - ly);
       const long long base = (long long)ids[t] * d.slice + (long long)iy * d.NX + ix;
-      inj[lev][base].push_back({t, w0});
-      inj[lev][base + 1].push_back({t, w1});
-      inj[lev][base + d.NX].push_back({t, w2});
-      inj[lev][base + d.NX + 1].push_back({t, w3});
+      inj[lev].push_back({base, t, w0});
+      inj[lev].push_back({base + 1, t, w1});
+      inj[lev].push_back({base + d.NX, t, w2});
+      inj[lev].push_back({base + d.NX + 1, t, w3});
       rtr[lev].push_back(t);
       rcell[lev].push_back((int)base);
       rw[lev].push_back(make_float4(w0, w1, w2, w3));
@@ -997,18 +1154,23 @@ fwix_status fwix_traces_create(fwix_plan* p, int ntrace, const float* cx, const 
     off_start[lev] = starts.size();
     off_tr[lev] = trs.size();
     off_r[lev] = rtrace.size();
-    for (auto& kv : inj[lev]) {
-      if (kv.first > 0x7fffffffLL) {
-        delete tr;
-        return fail(FWIX_ERR_UNSUPPORTED, "wavefield batch too large for 32-bit cell indices");
+    // cells ascending, each cell's traces in trace order (a stable sort of the
+    // entries, which were appended trace by trace)
+    std::vector<Entry>& en = inj[lev];
+    std::stable_sort(en.begin(), en.end(), [](const Entry& a, const Entry& b) { return a.cell < b.cell; });
+    for (size_t i = 0; i < en.size(); ++i) {
+      if (i == 0 || en[i].cell != en[i - 1].cell) {
+        if (en[i].cell > 0x7fffffffLL) {
+          delete tr;
+          return fail(FWIX_ERR_UNSUPPORTED, "wavefield batch too large for 32-bit cell indices");
+        }
+        cells.push_back((int)en[i].cell);
+        starts.push_back((int)(trs.size() - off_tr[lev]));
       }
-      cells.push_back((int)kv.first);
-      starts.push_back((int)(trs.size() - off_tr[lev]));
-      for (auto& tw : kv.second) {
-        trs.push_back(tw.first);
-        wts.push_back(tw.second);
-      }
+      trs.push_back(en[i].trace);
+      wts.push_back(en[i].w);
     }
+    std::vector<Entry>().swap(en);
     starts.push_back((int)(trs.size() - off_tr[lev]));
     for (size_t k = 0; k < rtr[lev].size(); ++k) {
       rtrace.push_back(rtr[lev][k]);

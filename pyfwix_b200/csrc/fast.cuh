@@ -357,8 +357,10 @@ constexpr int row_fwd_min_blocks() {
   return multi_term(PRE) && (P::E == 16 || P::E == 12) ? FWIX_ROW_MULTI_MINB : 0;
 }
 
-// t1[term] = F_x(pre_term * in) for each term.
-template <class P, int PRE>
+// t1[term] = F_x(pre_term * in) for each term.  RF: the input is in + the
+// reflection term of SpecArgs::rf_at 1 (separate instances, so that the passes
+// without it keep their registers).
+template <class P, int PRE, bool RF = false>
 __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_row_fwd(const SpecArgs a, int nchunk) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
@@ -394,6 +396,15 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
     const float2* src2 = a.in2 + roff;
 #pragma unroll
     for (int e = 0; e < P::E; ++e) raw[e] = cadd(raw[e], src2[pos_first<P>(c.t, e)]);
+  }
+  if constexpr (RF) {
+    if (c.live && c.y < a.d.ny) {
+#pragma unroll
+      for (int e = 0; e < P::E; ++e) {
+        const int x = pos_first<P>(c.t, e);
+        if (x < a.d.nx) raw[e] = cadd(raw[e], refl_term(a, roff, c.y, x));
+      }
+    }
   }
   const int nterm = multi_term(PRE) ? a.nterm : 1;
   Labels<P::E> lab;
@@ -476,8 +487,10 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
 // prefetched while the current one is transformed, and with labels the terms
 // that no sample of the warp's rows selects are skipped.  W_SMOOTH_PAIR sums each
 // transformed term twice, with the smooth weights into out and with their
-// slowness derivatives into out2.
-template <class P, int POST>
+// slowness derivatives into out2.  RF (W_ONE, W_MASK): the output gains the
+// reflection terms of SpecArgs::rf_at 2 (separate instances, as in the forward
+// row pass).
+template <class P, int POST, bool RF = false>
 __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 || P::E == 12) ? FWIX_ROW_MULTI_MINB : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
@@ -641,6 +654,11 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
     if constexpr (POST == W_ONE_DIRECT) v = cadd(v, scat_direct(a, c.b, c.iw, c.y, x));
     if (post_taper) v = cscale(v, a.tapx[x] * ty);
     if (a.add) v = cadd(dst[x], v);
+    // (Loading these terms before the transforms, as the start of the sum, held
+    // their registers through the transforms: 39 -> 60 us per 64 slices at 256.)
+    if constexpr (RF) {
+      if (c.y < a.d.ny && x < a.d.nx) v = cadd(v, refl_term(a, (c.b * a.d.NY + c.y) * P::N, c.y, x));
+    }
     dst[x] = v;
     if (a.ic_img && c.y < a.d.ny && x < a.d.nx) {
       // a warp's lanes hold consecutive x for each e: coalesced reductions
@@ -1213,6 +1231,18 @@ cudaError_t row_forward(const SpecArgs& a, int pre, cudaStream_t s) {
     e = opt_in_smem(k_row_fwd<P, W>, sm);                                            \
     if (e == cudaSuccess) k_row_fwd<P, W><<<grid, kWarps * 32, sm, s>>>(a, nchunk);  \
     break;
+  if (a.rf_at == 1 && pre != W_ONE && pre != W_MASK) return cudaErrorInvalidValue;
+  if (a.rf_at == 1) {
+    if (pre == W_ONE) {
+      e = opt_in_smem(k_row_fwd<P, W_ONE, true>, sm);
+      if (e == cudaSuccess) k_row_fwd<P, W_ONE, true><<<grid, kWarps * 32, sm, s>>>(a, nchunk);
+    } else {
+      e = opt_in_smem(k_row_fwd<P, W_MASK, true>, sm);
+      if (e == cudaSuccess) k_row_fwd<P, W_MASK, true><<<grid, kWarps * 32, sm, s>>>(a, nchunk);
+    }
+    if (e == cudaSuccess) count_launch();
+    return e != cudaSuccess ? e : cudaGetLastError();
+  }
   switch (pre) {
     FWIX_FAST_RF(W_ONE)
     FWIX_FAST_RF(W_TAPER)
@@ -1239,6 +1269,18 @@ cudaError_t row_inverse(const SpecArgs& a, int post, int post_taper, cudaStream_
     e = opt_in_smem(k_row_inv<P, W>, sm);                                                        \
     if (e == cudaSuccess) k_row_inv<P, W><<<grid, kWarps * 32, sm, s>>>(a, nchunk, post_taper);  \
     break;
+  if (a.rf_at == 2 && post != W_ONE && post != W_MASK) return cudaErrorInvalidValue;
+  if (a.rf_at == 2) {
+    if (post == W_ONE) {
+      e = opt_in_smem(k_row_inv<P, W_ONE, true>, sm);
+      if (e == cudaSuccess) k_row_inv<P, W_ONE, true><<<grid, kWarps * 32, sm, s>>>(a, nchunk, post_taper);
+    } else {
+      e = opt_in_smem(k_row_inv<P, W_MASK, true>, sm);
+      if (e == cudaSuccess) k_row_inv<P, W_MASK, true><<<grid, kWarps * 32, sm, s>>>(a, nchunk, post_taper);
+    }
+    if (e == cudaSuccess) count_launch();
+    return e != cudaSuccess ? e : cudaGetLastError();
+  }
   switch (post) {
     FWIX_FAST_RI(W_ONE)
     FWIX_FAST_RI(W_ONE_DIRECT)

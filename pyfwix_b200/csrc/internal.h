@@ -127,6 +127,15 @@ struct SpecArgs {
   // by float atomics (ic_img NULL: none)
   const float2* ic_bg;
   float* ic_img;
+  // reflections fused into a depth step (a model shared by every frequency):
+  // per-cell coefficients rf_tab [2][ny][nx] and fields laid out like `in`, over
+  // the unpadded window.  rf_at 1: the first (forward row) pass steps
+  // in + rf_tab[0] rf_f1; rf_at 2: the last (inverse row) pass adds
+  // rf_tab[0] rf_f1 (+ rf_tab[1] rf_f2 when rf_f2 != NULL) to its output; 0: none.
+  int rf_at;
+  const float2* rf_tab;
+  const float2* rf_f1;
+  const float2* rf_f2;
 };
 
 // Spectral passes (dispatch.cu: register-resident passes for lengths with a
@@ -178,11 +187,19 @@ cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, con
                                float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
                                int add, cudaStream_t s);
 // Linearised reflection fused with the imaging condition: forward wf (+)= bg * LR(dm)
-// on every shot; adjoint dm (+)= LR^H(sum_s conj(bg) wf).
+// on every shot; adjoint dm (+)= LR^H(sum_s conj(bg) wf).  With wf2 (adjoint, mw == 0
+// and dm_w == 0 only) the imaging-condition adjoint sum_{s,w} conj(bg2) wf2 is added
+// to dm0 in the same pass.
 cudaError_t launch_lin_reflect_ic(const Dims& d, int adjoint, const float2* s0, const float2* s1,
                                   const float2* r0, const float2* r1, long long mw, float2* dm0, float2* dm1,
                                   float2* dm2, float2* dm3, long long dm_w, const float2* bg, float2* wf, int add,
-                                  cudaStream_t s);
+                                  cudaStream_t s, const float2* bg2 = nullptr, const float2* wf2 = nullptr);
+// Per-cell coefficients of the reflections fused into a depth step (model shared
+// by every frequency): tab[0][y][x] = r (conj(r) for the adjoint), and with a
+// perturbation dm0..dm3 ([ny][nx] each) tab[1][y][x] = its linearised reflection.
+cudaError_t launch_refl_table(const Dims& d, int adjoint, const float2* s0, const float2* s1, const float2* r0,
+                              const float2* r1, const float2* dm0, const float2* dm1, const float2* dm2,
+                              const float2* dm3, float2* tab, cudaStream_t s);
 cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, float* img, int add,
                              cudaStream_t s);
 // img[y][x] (+)= Re sum_{s,w} conj(S) R over the padded NY x NX slice.

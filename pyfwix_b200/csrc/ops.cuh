@@ -5,6 +5,15 @@
 
 namespace fwix {
 
+// Reflection term fused into a row pass (SpecArgs::rf_at) at sample x of the row
+// that starts at roff (row y < ny of the unpadded window; the caller checks x < nx).
+__device__ __forceinline__ float2 refl_term(const SpecArgs& a, long long roff, int y, int x) {
+  const long long yx = (long long)y * a.d.nx + x;
+  float2 v = cmul(a.rf_tab[yx], a.rf_f1[roff + x]);
+  if (a.rf_f2) v = cadd(v, cmul(a.rf_tab[(long long)a.d.ny * a.d.nx + yx], a.rf_f2[roff + x]));
+  return v;
+}
+
 // Born weight W_n = (-i w dz / 2) c_n s~^(-1/2-n), s~ = Re s^2 + i (Im s^2 - eps Re s^2),
 // read from the unpadded slice with edge replication into the pad
 // (scatter.cu:61-106 slow_scale, :155-195 scale_by_iw, :240-277 pad_fwd).

@@ -71,6 +71,7 @@ __device__ __forceinline__ void reduce_groups(float2 (&v)[K]) {
 
 unsigned cell_blocks(const Dims& d) { return (unsigned)((d.ny * d.nx + kCells - 1) / kCells); }
 
+template <bool S1>
 __global__ void __launch_bounds__(kCells * kGroups)
     k_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
               const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw,
@@ -87,6 +88,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
   }
   if (!c.ok) return;
   float2 r = mw == 0 ? rs[threadIdx.x] : make_float2(0.f, 0.f);
+  const int ns = S1 ? 1 : d.ns;
 #pragma unroll 4
   for (int iw = threadIdx.y; iw < d.nw; iw += kGroups) {
     if (mw != 0) {
@@ -94,7 +96,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
       r = refl_coef(s0[m], s1[m], r0[m], r1[m]);
       if (adjoint) r = cconj(r);
     }
-    for (int s = 0; s < d.ns; ++s) {
+    for (int s = 0; s < ns; ++s) {
       const long long k = wf_index(d, s, iw, c);
       out[k] = cadd(out[k], cmul(in[k], r));
     }
@@ -118,15 +120,17 @@ __global__ void __launch_bounds__(kCells * kGroups)
 
 // image[w, y, x] (+)= sum_s conj(bg) wfld; with wsum the frequencies are summed as well
 // into image[y, x].
+template <bool S1>
 __global__ void __launch_bounds__(kCells * kGroups)
     k_ic_adj(Dims d, const float2* __restrict__ bg, const float2* __restrict__ wfld, float2* __restrict__ image,
              int add, int wsum) {
   const Cell c = this_cell(d);
   float2 acc[1] = {make_float2(0.f, 0.f)};
+  const int ns = S1 ? 1 : d.ns;
 #pragma unroll 4
   for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups) {
     float2 t = make_float2(0.f, 0.f);
-    for (int s = 0; s < d.ns; ++s) {
+    for (int s = 0; s < ns; ++s) {
       const long long k = wf_index(d, s, iw, c);
       t = cadd(t, cmul_conj(wfld[k], bg[k]));
     }
@@ -168,14 +172,19 @@ __device__ __forceinline__ LinCoef lin_coef(float2 s0, float2 s1, float2 r0, flo
 // With IC the reflectivity perturbation dr is not stored: the forward adds
 // bg * dr to the wavefield wf of every shot (the imaging-condition forward,
 // imaging_condition.cu:9-55) and the adjoint takes dr = sum_s conj(bg) wf (its
-// adjoint, :57-108), which saves writing and re-reading dr.
-template <bool IC>
+// adjoint, :57-108), which saves writing and re-reading dr.  IC2 (adjoint, model
+// and perturbation shared by every frequency): the same pass also sums the
+// imaging-condition adjoint of another pair, dm0 += sum conj(bg2) wf2, so that
+// one read of the four fields serves both frequency sums of a level.
+template <bool IC, bool S1, bool IC2>
 __global__ void __launch_bounds__(kCells * kGroups)
     k_lin_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
                   const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw, float2* dm0,
                   float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr, int add,
-                  const float2* __restrict__ bg, float2* __restrict__ wf) {
+                  const float2* __restrict__ bg, float2* __restrict__ wf, const float2* __restrict__ bg2,
+                  const float2* __restrict__ wf2) {
   const Cell c = this_cell(d);
+  const int ns = S1 ? 1 : d.ns;
   const long long plane = (long long)d.ny * d.nx;
   const int wsum = adjoint && dm_w == 0;
   LinCoef cf;
@@ -198,22 +207,28 @@ __global__ void __launch_bounds__(kCells * kGroups)
       v = cadd(v, csub(cmul(cf.ar, dm3[k]), cmul(cf.br, dm2[k])));
 #pragma unroll 4
       for (int iw = threadIdx.y; iw < d.nw; iw += kGroups)
-        for (int sh = 0; sh < d.ns; ++sh) {
+        for (int sh = 0; sh < ns; ++sh) {
           const long long q = wf_index(d, sh, iw, c);
           wf[q] = cadd(wf[q], cmul(bg[q], v));
         }
       return;
     }
-    float2 gi[1] = {make_float2(0.f, 0.f)};
+    constexpr int K = IC2 ? 2 : 1;
+    float2 gi[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) gi[j] = make_float2(0.f, 0.f);
 #pragma unroll 4
     for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups)
-      for (int sh = 0; sh < d.ns; ++sh) {
+      for (int sh = 0; sh < ns; ++sh) {
         const long long q = wf_index(d, sh, iw, c);
         gi[0] = cadd(gi[0], cmul_conj(wf[q], bg[q]));
+        if constexpr (IC2) gi[K - 1] = cadd(gi[K - 1], cmul_conj(wf2[q], bg2[q]));
       }
-    reduce_groups<1>(gi);  // every thread of the block
+    reduce_groups<K>(gi);  // every thread of the block
     if (threadIdx.y != 0 || !c.ok) return;
-    const float2 t0 = cmul_conj(gi[0], cf.as), t1 = cscale(cmul_conj(gi[0], cf.bs), -1.f);
+    float2 t0 = cmul_conj(gi[0], cf.as);
+    const float2 t1 = cscale(cmul_conj(gi[0], cf.bs), -1.f);
+    if constexpr (IC2) t0 = cadd(t0, gi[K - 1]);
     const float2 t3 = cmul_conj(gi[0], cf.ar), t2 = cscale(cmul_conj(gi[0], cf.br), -1.f);
     dm0[k] = add ? cadd(dm0[k], t0) : t0;
     dm1[k] = (add || dm1 == dm0) ? cadd(dm1[k], t1) : t1;
@@ -232,7 +247,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
       float2 v = csub(cmul(cf.as, dm0[k]), cmul(cf.bs, dm1[k]));
       v = cadd(v, csub(cmul(cf.ar, dm3[k]), cmul(cf.br, dm2[k])));
       if (IC) {
-        for (int sh = 0; sh < d.ns; ++sh) {
+        for (int sh = 0; sh < ns; ++sh) {
           const long long q = wf_index(d, sh, iw, c);
           wf[q] = cadd(wf[q], cmul(bg[q], v));
         }
@@ -244,7 +259,7 @@ __global__ void __launch_bounds__(kCells * kGroups)
     float2 gi;
     if (IC) {
       gi = make_float2(0.f, 0.f);
-      for (int sh = 0; sh < d.ns; ++sh) {
+      for (int sh = 0; sh < ns; ++sh) {
         const long long q = wf_index(d, sh, iw, c);
         gi = cadd(gi, cmul_conj(wf[q], bg[q]));
       }
@@ -276,14 +291,40 @@ __global__ void __launch_bounds__(kCells * kGroups)
   dm3[k] = (add || dm3 == dm2) ? cadd(dm3[k], g[3]) : g[3];
 }
 
+// Per-cell reflection coefficients of a model shared by every frequency, for the
+// reflections fused into a depth step (SpecArgs::rf_tab): tab[yx] = r (conj(r)
+// for the adjoint) and, given a perturbation (dm0 != NULL, one value per cell),
+// tab[ny nx + yx] = as dm0 - bs dm1 + ar dm3 - br dm2, the linearised reflection
+// that k_lin_reflect's forward forms.
+__global__ void __launch_bounds__(256)
+    k_refl_table(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
+                 const float2* __restrict__ r0, const float2* __restrict__ r1, const float2* __restrict__ dm0,
+                 const float2* __restrict__ dm1, const float2* __restrict__ dm2, const float2* __restrict__ dm3,
+                 float2* __restrict__ tab) {
+  const long long n = (long long)d.ny * d.nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float2 r = refl_coef(s0[i], s1[i], r0[i], r1[i]);
+    tab[i] = adjoint ? cconj(r) : r;
+    if (dm0) {
+      const LinCoef cf = lin_coef(s0[i], s1[i], r0[i], r1[i]);
+      float2 v = csub(cmul(cf.as, dm0[i]), cmul(cf.bs, dm1[i]));
+      v = cadd(v, csub(cmul(cf.ar, dm3[i]), cmul(cf.br, dm2[i])));
+      tab[n + i] = v;
+    }
+  }
+}
+
+template <bool S1>
 __global__ void __launch_bounds__(kCells * kGroups)
     k_image_acc(Dims d, const float2* __restrict__ S, const float2* __restrict__ R, float* __restrict__ img,
                 int add) {
   const Cell c = this_cell(d);
   float2 acc[1] = {make_float2(0.f, 0.f)};
+  const int ns = S1 ? 1 : d.ns;
 #pragma unroll 4
   for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups)
-    for (int s = 0; s < d.ns; ++s) {
+    for (int s = 0; s < ns; ++s) {
       const long long k = wf_index(d, s, iw, c);
       const float2 a = S[k], b = R[k];
       acc[0].x += a.x * b.x + a.y * b.y;  // Re(conj(S) R)
@@ -367,7 +408,10 @@ cudaError_t launch_reflect(const Dims& d, int adjoint, const float2* s0, const f
     cudaError_t e = cudaMemsetAsync(out, 0, d.wfld * sizeof(float2), s);
     if (e != cudaSuccess) return e;
   }
-  k_reflect<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, in, out);
+  if (d.ns == 1)
+    k_reflect<true><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, in, out);
+  else
+    k_reflect<false><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, in, out);
   count_launch();
   return cudaGetLastError();
 }
@@ -385,7 +429,10 @@ cudaError_t launch_ic_fwd(const Dims& d, const float2* bg, const float2* image, 
 
 cudaError_t launch_ic_adj(const Dims& d, const float2* bg, const float2* wfld, float2* image,
                           long long img_w, int add, cudaStream_t s) {
-  k_ic_adj<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, bg, wfld, image, add, img_w == 0);
+  if (d.ns == 1)
+    k_ic_adj<true><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, bg, wfld, image, add, img_w == 0);
+  else
+    k_ic_adj<false><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, bg, wfld, image, add, img_w == 0);
   count_launch();
   return cudaGetLastError();
 }
@@ -394,8 +441,8 @@ cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, con
                                const float2* r0, const float2* r1, long long mw, float2* dm0,
                                float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr,
                                int add, cudaStream_t s) {
-  k_lin_reflect<false><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1,
-                                                                       dm2, dm3, dm_w, dr, add, nullptr, nullptr);
+  k_lin_reflect<false, false, false><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(
+      d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3, dm_w, dr, add, nullptr, nullptr, nullptr, nullptr);
   count_launch();
   return cudaGetLastError();
 }
@@ -403,16 +450,41 @@ cudaError_t launch_lin_reflect(const Dims& d, int adjoint, const float2* s0, con
 cudaError_t launch_lin_reflect_ic(const Dims& d, int adjoint, const float2* s0, const float2* s1,
                                   const float2* r0, const float2* r1, long long mw, float2* dm0, float2* dm1,
                                   float2* dm2, float2* dm3, long long dm_w, const float2* bg, float2* wf, int add,
-                                  cudaStream_t s) {
-  k_lin_reflect<true><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1,
-                                                                      dm2, dm3, dm_w, nullptr, add, bg, wf);
+                                  cudaStream_t s, const float2* bg2, const float2* wf2) {
+  const dim3 grid(cell_blocks(d)), block(kCells, kGroups);
+  if (wf2) {
+    if (!adjoint || mw != 0 || dm_w != 0 || !bg2) return cudaErrorInvalidValue;
+    if (d.ns == 1)
+      k_lin_reflect<true, true, true><<<grid, block, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3,
+                                                             dm_w, nullptr, add, bg, wf, bg2, wf2);
+    else
+      k_lin_reflect<true, false, true><<<grid, block, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3,
+                                                              dm_w, nullptr, add, bg, wf, bg2, wf2);
+  } else if (d.ns == 1) {
+    k_lin_reflect<true, true, false><<<grid, block, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3,
+                                                            dm_w, nullptr, add, bg, wf, nullptr, nullptr);
+  } else {
+    k_lin_reflect<true, false, false><<<grid, block, 0, s>>>(d, adjoint, s0, s1, r0, r1, mw, dm0, dm1, dm2, dm3,
+                                                             dm_w, nullptr, add, bg, wf, nullptr, nullptr);
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refl_table(const Dims& d, int adjoint, const float2* s0, const float2* s1, const float2* r0,
+                              const float2* r1, const float2* dm0, const float2* dm1, const float2* dm2,
+                              const float2* dm3, float2* tab, cudaStream_t s) {
+  k_refl_table<<<grid1d((long long)d.ny * d.nx), 256, 0, s>>>(d, adjoint, s0, s1, r0, r1, dm0, dm1, dm2, dm3, tab);
   count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, float* img, int add,
                              cudaStream_t s) {
-  k_image_acc<<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, S, R, img, add);
+  if (d.ns == 1)
+    k_image_acc<true><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, S, R, img, add);
+  else
+    k_image_acc<false><<<cell_blocks(d), dim3(kCells, kGroups), 0, s>>>(d, S, R, img, add);
   count_launch();
   return cudaGetLastError();
 }
@@ -422,7 +494,10 @@ cudaError_t launch_correlate_padded(const Dims& d, const float2* S, const float2
   Dims full = d;  // iterate over the padded slice: the cell window is the whole NY x NX
   full.nx = d.NX;
   full.ny = d.NY;
-  k_image_acc<<<cell_blocks(full), dim3(kCells, kGroups), 0, s>>>(full, S, R, img, add);
+  if (d.ns == 1)
+    k_image_acc<true><<<cell_blocks(full), dim3(kCells, kGroups), 0, s>>>(full, S, R, img, add);
+  else
+    k_image_acc<false><<<cell_blocks(full), dim3(kCells, kGroups), 0, s>>>(full, S, R, img, add);
   count_launch();
   return cudaGetLastError();
 }

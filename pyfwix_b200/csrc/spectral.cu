@@ -57,7 +57,12 @@ __global__ void __launch_bounds__(256) k_row_forward(const SpecArgs a, int nchun
   for (int y = chunk * nwarp + warp; y < a.d.NY; y += nchunk * nwarp) {
     const long long roff = (b * a.d.NY + y) * NX;
     const long long loff = (bl * a.d.NY + y) * NX;
-    for (int x = lane; x < NX; x += 32) lineIn[x] = a.in2 ? cadd(a.in[roff + x], a.in2[roff + x]) : a.in[roff + x];
+    const bool rf = (PRE == W_ONE || PRE == W_MASK) && a.rf_at == 1 && y < a.d.ny;
+    for (int x = lane; x < NX; x += 32) {
+      float2 v = a.in2 ? cadd(a.in[roff + x], a.in2[roff + x]) : a.in[roff + x];
+      if (rf && x < a.d.nx) v = cadd(v, refl_term(a, roff, y, x));
+      lineIn[x] = v;
+    }
     __syncwarp();
     for (int t = 0; t < nterm; ++t) {
       for (int x = lane; x < NX; x += 32) lineA[x] = row_weight<PRE>(a, t, iw, y, x, lineIn[x]);
@@ -116,6 +121,8 @@ __global__ void __launch_bounds__(256) k_row_inverse(const SpecArgs a, int nchun
       float2 v = acc[x];
       if (post_taper) v = cscale(v, a.tapx[x] * ty);
       if (a.add) v = cadd(a.out[roff + x], v);
+      if ((POST == W_ONE || POST == W_MASK) && a.rf_at == 2 && y < a.d.ny && x < a.d.nx)
+        v = cadd(v, refl_term(a, roff, y, x));
       a.out[roff + x] = v;
       if (a.ic_img && y < a.d.ny && x < a.d.nx) {
         const float2 bg = a.ic_bg[roff + x];

@@ -45,6 +45,7 @@ backward against three for the checkpointed forward.
 from __future__ import annotations
 
 import collections
+import hashlib
 import weakref
 
 import numpy as np
@@ -76,6 +77,38 @@ def _cached_plan(key, make):
 def clear_plan_cache():
     """Releases the cached plans (their device memory) of earlier problems."""
     _PLAN_CACHE.clear()
+
+
+_TRACES_PER_PLAN = 16
+
+
+def _traces(plan, cx, cy, cz, ids):
+    """Gather lists of a trace set on ``plan``, kept while the plan lives (the
+    last 16 sets): an FWI run visits the same shots every iteration, and the
+    lists of a receiver on every surface node take a noticeable host time to
+    build."""
+    arrs = (np.ascontiguousarray(cx, np.float32), np.ascontiguousarray(cy, np.float32),
+            np.ascontiguousarray(cz, np.float32), np.ascontiguousarray(ids, np.int32))
+    h = hashlib.blake2b(digest_size=20)
+    for a in arrs:
+        h.update(np.int64(a.size).tobytes())
+        h.update(a.tobytes())
+    key = h.digest()
+    cache = plan.__dict__.setdefault("_traces_cache", collections.OrderedDict())
+    tr = cache.get(key)
+    if tr is None:
+        tr = plan.traces(*arrs)
+        cache[key] = tr
+        while len(cache) > _TRACES_PER_PLAN:
+            cache.popitem(last=False)
+    else:
+        cache.move_to_end(key)
+    return tr
+
+
+def _pool(plan):
+    """Stored-field blocks given back to a plan, keyed (family, fields)."""
+    return plan.__dict__.setdefault("_fwi_blocks", {})
 
 
 def smooth_refs(s, nref, spread=1e-3):
@@ -147,10 +180,15 @@ class SmoothFWI:
         key = (str(self.device),) + tuple(sorted(kw.items()))
         self.plan = _cached_plan(key, lambda: Plan(step="pspi", device=self.device, **kw))
         p = self.plan
-        self.src = p.traces(geometry["sx"], geometry["sy"], geometry["sz"], s_ids)
-        self.rec = p.traces(geometry["rx"], geometry["ry"], geometry["rz"], r_ids)
+        self.src = _traces(p, geometry["sx"], geometry["sy"], geometry["sz"], s_ids)
+        self.rec = _traces(p, geometry["rx"], geometry["ry"], geometry["rz"], r_ids)
         self.wavelet = wav.to(self.device, torch.complex64).contiguous()
         self.ntrace = len(np.asarray(geometry["rx"]))
+        # stored-field blocks in use; they go back to the plan's pool at the next
+        # model() or when this problem is released
+        self._held = {}
+        weakref.finalize(self, _pool(p).update, self._held)
+        self.Ds = self.dSU = self._blocks = None
         self.k = self._storage(_checkpoint_key(par))
         self.refs_fixed = _get(par, "refs", None)
         p.ensure_workspace(L.WS_STEP)
@@ -173,6 +211,9 @@ class SmoothFWI:
         pc = p._keep.get("pcache") if hasattr(p, "_keep") else None
         if pc is not None:
             free += pc.numel() * pc.element_size()
+        # and so are the stored-field blocks an earlier problem gave back to the plan
+        for b in _pool(p).values():
+            free += b.numel() * b.element_size()
         budget = 0.6 * free
         if 3 * p.nz * wb + 4 * wb <= budget:
             return None
@@ -206,22 +247,17 @@ class SmoothFWI:
         return torch.zeros(self.plan.wshape, dtype=torch.complex64, device=self.device)
 
     # ---------------------------------------------------------------- modelling
-    def _down_step(self, iz, D, data, store):
+    def _down_step(self, iz, D, data):
+        """The checkpointed modelling's down step at iz (injection, recording, step)."""
         p = self.plan
         p.inject(self.src, iz, self.wavelet, D)
         p.inject(self.rec, iz, data, D, adjoint=True)
-        if store is not None:
-            store.copy_(D)
         p.smooth_step(iz, D, D)
 
-    def _up_step(self, iz, U, Dz, data, deriv=None):
-        """U_iz from U_iz+1 in place; with ``deriv`` the paired step also writes
-        dS_iz(U_iz+1) there (what the gradient takes of U)."""
+    def _up_step(self, iz, U, Dz, data):
+        """U_iz from U_iz+1 in place, with its reflection and recording."""
         p = self.plan
-        if deriv is None:
-            p.smooth_step(iz, U, U)
-        else:
-            p.smooth_step_pair(iz, U, U, deriv)
+        p.smooth_step(iz, U, U)
         p.reflect(iz, Dz, U, add=True)
         p.inject(self.rec, iz, data, U, adjoint=True)
 
@@ -229,43 +265,46 @@ class SmoothFWI:
         """Data [ntrace][nw] for slowness s; with keep the fields the gradient
         needs are stored (all depths, or every k-th)."""
         self.set_slowness(s)
+        self._give_back()  # the fields of an earlier model() are dead
         p, nz = self.plan, self.plan.nz
         data = torch.zeros((self.ntrace, p.nw), dtype=torch.complex64, device=self.device)
         D = self._field()
         if self.k is None:
-            # one block per stored family (not nz fields): the caching allocator
-            # hands the previous shot's block back whole, with no device allocation.
+            # one block per stored family (not nz fields), taken from the plan's pool:
+            # the previous shot's block comes back whole, with no allocator traffic.
             # The up pass reflects every down field, so they are kept either way.
-            self.Ds = list(self._block(nz))
-            for iz in range(nz):
-                self._down_step(iz, D, data, self.Ds[iz])
-            # the gradient takes U only through dS_iz(U_iz+1): the up pass's paired
+            # The gradient takes U only through dS_iz(U_iz+1): the up pass's paired
             # step stores that instead of U (one derivative step fewer per level in
-            # the backward, the same memory)
-            U = self._field()
-            self.dSU = [None] * nz
-            dblk = self._block(nz - 1) if keep and nz > 1 else None
-            for iz in range(nz - 1, -1, -1):
-                d = dblk[iz] if dblk is not None and iz + 1 < nz else None
-                self._up_step(iz, U, self.Ds[iz], data, deriv=d)
-                self.dSU[iz] = d
+            # the backward, the same memory).  Both passes run as one library call.
+            dblk = self._take("D", nz)
+            ublk = self._take("dSU", nz - 1) if keep and nz > 1 else None
+            p.smooth_model_sweep(self.src, self.rec, self.wavelet, data, D, self._empty(), dblk, ublk)
+            self.Ds = list(dblk)
+            self.dSU = [ublk[iz] if ublk is not None and iz + 1 < nz else None for iz in range(nz)]
+            self._blocks = (dblk, ublk)
             if not keep:
-                self.Ds = self.dSU = None
+                self._give_back()
             return data
         k = self.k
+        nck = -(-nz // k)
+        dck, uck = self._take("Dck", nck), self._take("Uck", nck)
         self.Dck = {}
         for iz in range(nz):
             if iz % k == 0:
-                self.Dck[iz] = D.clone()   # the field before injection at iz
-            self._down_step(iz, D, data, None)
+                dck[iz // k].copy_(D)   # the field before injection at iz
+                self.Dck[iz] = dck[iz // k]
+            self._down_step(iz, D, data)
         self.Uck = {nz: self._field()}
         U = self._field()
-        bufs = dict(D=self._block(k))
+        bufs = dict(D=self._take("segD", k))
         for a in reversed(range(0, nz, k)):
             seg = self._segment_D(a, bufs)
             for iz in range(min(a + k, nz) - 1, a - 1, -1):
                 self._up_step(iz, U, seg[iz - a], data)
-            self.Uck[a] = U.clone()
+            uck[a // k].copy_(U)
+            self.Uck[a] = uck[a // k]
+        if not keep:
+            self._give_back()
         return data
 
     def _empty(self):
@@ -275,12 +314,37 @@ class SmoothFWI:
         """n uninitialised fields in one allocation, [n][ns][nw][NY][NX]."""
         return torch.empty((n,) + tuple(self.plan.wshape), dtype=torch.complex64, device=self.device)
 
+    def _take(self, name, n):
+        """The block of n fields of the stored family ``name``, held until
+        _give_back: the one the previous problem on this plan gave back (the same
+        device memory, so a family of tens of GB is never carved up by smaller
+        allocations or re-allocated behind a cache flush), else a new one."""
+        b = self._held.get((name, n))
+        if b is None:
+            b = _pool(self.plan).pop((name, n), None)
+        if b is None:
+            b = self._block(n)
+        self._held[(name, n)] = b
+        return b
+
+    def _give_back(self, families=None):
+        """Returns held blocks (all, or those of ``families``) to the plan's pool
+        once their fields are dead (later work on the same stream orders after the
+        reads already enqueued)."""
+        pool = _pool(self.plan)
+        for key in [q for q in self._held if families is None or q[0] in families]:
+            pool[key] = self._held.pop(key)
+        if families is None:
+            self.Ds = self.dSU = self._blocks = None
+            self.Dck = self.Uck = None
+
     def _seg_buffers(self):
-        """Fields of one checkpoint segment, allocated once per sweep and reused by
+        """Fields of one checkpoint segment, taken once per sweep and reused by
         every segment: down fields, their derivatives, up derivatives, mu fields
         (k each) and two up fields for the walk."""
         k = self.k
-        return dict(D=self._block(k), dSD=self._block(k), dSU=self._block(k), mu=self._block(k), U=self._block(2))
+        return dict(D=self._take("segD", k), dSD=self._take("segdSD", k), dSU=self._take("segdSU", k),
+                    mu=self._take("segmu", k), U=self._take("segU", 2))
 
     def _segment_D(self, a, bufs, derivs=False):
         """Down fields D_a .. D_{a+k-1} (after injection) recomputed from the
@@ -364,24 +428,22 @@ class SmoothFWI:
         crefl = torch.zeros((nz, p.ny, p.nx), dtype=torch.float32, device=self.device)
         G = self._field()
         if self.k is None:
-            Dget = lambda iz: self.Ds[iz]
-            mus = self._block(nz)
-            mu = self._field()
-            for iz in range(nz):
-                self._mu_level(iz, mu, res, Dget(iz), self.dSU[iz], gpad, crefl)
-                mus[iz].copy_(mu)
-            nu = self._field()
-            for iz in range(nz - 1, -1, -1):
-                self._nu_level(iz, nu, res, Dget(iz), mus[iz], gpad, G)
+            if self.Ds is None:
+                raise RuntimeError("gradient() needs model(s, keep=True) first")
+            dblk, ublk = self._blocks
+            mus = self._take("mu", nz)
+            p.smooth_gradient_sweep(self.rec, res, dblk, ublk, mus, self._empty(), self._empty(), G, gpad, crefl)
         else:
             k = self.k
             self._res = res
             # mu recursion alone, keeping mu_{a-1} at every segment start a
             mu = self._field()
+            mck = self._take("Mck", -(-nz // k))
             self.Mck = {}
             for iz in range(nz):
                 if iz % k == 0:
-                    self.Mck[iz] = mu.clone()
+                    mck[iz // k].copy_(mu)
+                    self.Mck[iz] = mck[iz // k]
                 if iz > 0:
                     p.smooth_step(iz - 1, mu, mu, mode=L.SMOOTH_ADJ)
                 p.inject(self.rec, iz, res, mu)
@@ -404,6 +466,9 @@ class SmoothFWI:
                     p.inject(self.rec, iz, res, nu)
                 del Dseg, dSD, dSU, mseg
             self._res = None
+            self.Mck = None
+        # the gradient's own blocks; the modelling's stay for another gradient call
+        self._give_back(("mu", "Mck", "segD", "segdSD", "segdSU", "segmu", "segU"))
         # reflection coefficients r_iz = (s_iz - s_iz+1) / (s_iz + s_iz+1)
         s = self.s
         grefl = torch.zeros_like(crefl)
@@ -413,24 +478,6 @@ class SmoothFWI:
             grefl[:-1] += crefl[:-1] * (2 * s1 / den)
             grefl[1:] += crefl[:-1] * (-2 * s0 / den)
         return fold_edge(gpad, p.ny, p.nx) + grefl
-
-    def _mu_level(self, iz, mu, res, Dz, dSU, gpad, crefl):
-        p = self.plan
-        if iz > 0:
-            p.smooth_step(iz - 1, mu, mu, mode=L.SMOOTH_ADJ)
-        p.inject(self.rec, iz, res, mu)
-        if dSU is not None:  # dS_iz(U_iz+1), from the modelling's up pass
-            p.correlate(mu, dSU, gpad[iz], add=True, padded=True)
-            p.correlate(mu, Dz, crefl[iz], add=True, padded=False)
-
-    def _nu_level(self, iz, nu, res, Dz, muz, gpad, G):
-        p = self.plan
-        if iz + 1 < p.nz:
-            p.smooth_step(iz, Dz, G, mode=L.SMOOTH_DERIV)
-            p.correlate(nu, G, gpad[iz], add=True, padded=True)
-        p.smooth_step(iz, nu, nu, mode=L.SMOOTH_ADJ)
-        p.reflect(iz, muz, nu, adjoint=True, add=True)
-        p.inject(self.rec, iz, res, nu)
 
 
 class FWIGradient(torch.autograd.Function):

@@ -86,6 +86,52 @@ class OraclePlan:
         f = wem.reflect_adjoint if adjoint else wem.reflect_forward
         return _put(out, f(self.g, self.s2, self.den, iz, _np(inp), _np(out)))
 
+    def smooth_model_sweep(self, src, rec, wavelet, data, D, U, Ds, dSU=None):
+        """The level loops of fwix_smooth_model_sweep on this stand-in's operators."""
+        nz = self.nz
+        data.zero_()
+        D.zero_()
+        for iz in range(nz):
+            self.inject(src, iz, wavelet, D)
+            self.inject(rec, iz, data, D, adjoint=True)
+            Ds[iz].copy_(D)
+            if iz + 1 < nz:
+                self.smooth_step(iz, D, D)
+        U.zero_()
+        for iz in range(nz - 1, -1, -1):
+            if iz + 1 < nz:
+                if dSU is not None:
+                    self.smooth_step_pair(iz, U, U, dSU[iz])
+                else:
+                    self.smooth_step(iz, U, U)
+            self.reflect(iz, Ds[iz], U, add=True)
+            self.inject(rec, iz, data, U, adjoint=True)
+
+    def smooth_gradient_sweep(self, rec, res, Ds, dSU, mus, mu, nu, G, gpad, crefl):
+        """The level loops of fwix_smooth_gradient_sweep on this stand-in's operators."""
+        nz = self.nz
+        gpad.zero_()
+        crefl.zero_()
+        mu.zero_()
+        for iz in range(nz):
+            if iz > 0:
+                self.smooth_step(iz - 1, mu, mu, mode=L.SMOOTH_ADJ)
+            self.inject(rec, iz, res, mu)
+            if iz + 1 < nz:
+                self.correlate(mu, dSU[iz], gpad[iz], add=True, padded=True)
+                self.correlate(mu, Ds[iz], crefl[iz], add=True, padded=False)
+            mus[iz].copy_(mu)
+        nu.zero_()
+        for iz in range(nz - 1, -1, -1):
+            if iz + 1 < nz:
+                self.smooth_step(iz, Ds[iz], G, mode=L.SMOOTH_DERIV)
+                self.correlate(nu, G, gpad[iz], add=True, padded=True)
+            if iz == 0:
+                break
+            self.smooth_step(iz, nu, nu, mode=L.SMOOTH_ADJ)
+            self.reflect(iz, mus[iz], nu, adjoint=True, add=True)
+            self.inject(rec, iz, res, nu)
+
     def correlate(self, a, b, out, add=False, padded=True):
         a, b = _np(a), _np(b)
         if not padded:
@@ -144,10 +190,10 @@ def test_every_depth_matches_oracle_gradient(monkeypatch):
 @pytest.mark.parametrize("k", [2, 3, 7, 16])
 def test_checkpoints_match_every_depth(monkeypatch, k):
     """k = 3 leaves a short last segment (7 levels), k = 7 makes one segment and
-    k = 16 is deeper than the grid.  With every depth stored the driver takes
-    4 nz - 1 steps and nz - 1 paired steps (down modelling; up modelling paired
-    with the derivative of U; mu steps; nu and its derivative steps);
-    checkpoints add the recomputed segments."""
+    k = 16 is deeper than the grid.  With every depth stored the sweeps take
+    4 (nz - 1) steps and nz - 1 paired steps (down modelling; up modelling paired
+    with the derivative of U; mu steps; nu and its derivative steps; no step whose
+    result nothing reads); checkpoints add the recomputed segments."""
     g, s, refs, geom, wav, par, acq, d_obs = _problem()
     data0, grad0, full = _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, None)
     data, grad, prob = _driver_gradient(monkeypatch, s, geom, wav, par, d_obs, k)
@@ -155,7 +201,7 @@ def test_checkpoints_match_every_depth(monkeypatch, k):
     assert _rel(data, data0) < 1e-6
     assert _rel(grad, grad0) < 1e-5
     nz = g.nz
-    assert full.plan.calls["step"] == 4 * nz - 1 and full.plan.calls["pair"] == nz - 1
+    assert full.plan.calls["step"] == 4 * (nz - 1) and full.plan.calls["pair"] == nz - 1
     assert prob.plan.calls["step"] + prob.plan.calls["pair"] > full.plan.calls["step"] + full.plan.calls["pair"]
 
 

@@ -111,6 +111,39 @@ def test_born(kind, taper, nx, ny, pad):
     assert rel(to_host(gr), gr_ref) < TOL
 
 
+@pytest.mark.parametrize("kind,taper,nx,ny,pad", [("pspi", 3, 32, 24, 4), ("nsps", 0, 32, 24, 4),
+                                                 ("pspi", 3, 64, 64, 0), ("nsps", 2, 64, 64, 0)])
+def test_born_broadcast_background(kind, taper, nx, ny, pad):
+    """Born forward / adjoint with a background model and a perturbation shared by
+    every frequency ([nz][1][ny][nx]): the case in which the per-level
+    reflections are added inside the depth steps' row passes (forward: the step's
+    output; adjoint: the next step's input) and the adjoint's two frequency sums
+    of a level share one pass.  Against the FP64 oracle on per-frequency copies."""
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind, taper=taper, nx=nx, ny=ny, pad=pad)
+    slow1, den1 = slow[:, :1].copy(), den[:, :1].copy()
+    slow_w, den_w = np.repeat(slow1, g.nw, 1), np.repeat(den1, g.nw, 1)
+    p.set_model(slow1, den1)
+    data, bgd, bgu = wem.propagate(g, st, acq, slow_w, den_w, wav)
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((len(acq.rec.ix), g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, to_dev(wav), d, bd, bu)
+    assert rel(to_host(d), data) < TOL
+    ms = crandn(rng, (g.nz, 1, g.ny, g.nx))
+    mr = crandn(rng, (g.nz, 1, g.ny, g.nx))
+    ref = wem.born_forward(g, st, acq, slow_w, den_w, bgd, bgu, np.repeat(ms, g.nw, 1), np.repeat(mr, g.nw, 1))
+    out = torch.empty_like(d)
+    p.born(rec, bd, bu, to_dev(ms), to_dev(mr), out)
+    assert rel(to_host(out), ref) < TOL
+    r = crandn(rng, d.shape)
+    gs_ref, gr_ref = wem.born_adjoint(g, st, acq, slow_w, den_w, bgd, bgu, r)
+    gs = torch.empty((g.nz, 1, g.ny, g.nx), dtype=torch.complex64, device="cuda")
+    gr = torch.empty_like(gs)
+    p.born(rec, bd, bu, gs, gr, to_dev(r), adjoint=True)
+    assert rel(to_host(gs), gs_ref.sum(1, keepdims=True)) < TOL
+    assert rel(to_host(gr), gr_ref.sum(1, keepdims=True)) < TOL
+
+
 def test_born_dot_product_device():
     """ExtendedBorn dot test (propagator/src/ExtendedBorn.h:61-128) entirely on the
     device, taper off as in born_unit_test.cpp:392-393."""
