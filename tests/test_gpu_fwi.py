@@ -103,6 +103,43 @@ def test_gradient_matches_oracle(checkpoint):
     assert rel(grad, grad_o) < 1e-3
 
 
+@pytest.mark.parametrize("checkpoint", [None, 2])
+def test_interleaved_problems_share_plan_and_blocks(checkpoint):
+    """Problems of the same sizes share one cached plan, its pool of stored-field
+    blocks and its trace lists: interleaved model / gradient calls of two
+    problems, and a second gradient call, give each problem's results alone."""
+    from pyfwix_b200 import fwi
+    g, rng, s, geom, wav, par = _case()
+    s = s.astype(np.float32)
+    sb = (s * 1.02).astype(np.float32)
+    fwi.clear_plan_cache()
+    prob = fwi.SmoothFWI(s.shape, geom, wav, dict(par, checkpoint=None))
+    d_obs = prob.model(torch.as_tensor(s * 1.01), keep=False)
+    par = dict(par, refs=prob.refs, checkpoint=checkpoint)
+    del prob
+
+    def alone(sv):
+        fwi.clear_plan_cache()
+        pr = fwi.SmoothFWI(s.shape, geom, wav, par)
+        d = pr.model(torch.as_tensor(sv), keep=True)
+        return to_host(d), to_host(pr.gradient(d - d_obs))
+
+    da, ga = alone(s)
+    db, gb = alone(sb)
+    fwi.clear_plan_cache()
+    A = fwi.SmoothFWI(s.shape, geom, wav, par)
+    B = fwi.SmoothFWI(s.shape, geom, wav, par)
+    assert A.plan is B.plan
+    dA = A.model(torch.as_tensor(s), keep=True)
+    dB = B.model(torch.as_tensor(sb), keep=True)
+    gA = A.gradient(dA - d_obs)
+    gB = B.gradient(dB - d_obs)
+    gA2 = A.gradient(dA - d_obs)
+    for got, ref in ((dA, da), (dB, db), (gA, ga), (gB, gb), (gA2, ga)):
+        assert rel(to_host(got), ref) < 1e-6
+    fwi.clear_plan_cache()
+
+
 def test_autograd_function():
     from pyfwix_b200.fwi import FWIGradient, SmoothFWI
     g, rng, s, geom, wav, par = _case(nz=4)
