@@ -75,7 +75,9 @@ def _cached_plan(key, make):
 
 
 def clear_plan_cache():
-    """Releases the cached plans (their device memory) of earlier problems."""
+    """Releases the cached plans of earlier problems with their device memory:
+    tables, workspace, phase-factor cache, the pooled stored-field blocks (tens
+    of GB for a large every-depth gradient) and the trace lists."""
     _PLAN_CACHE.clear()
 
 
