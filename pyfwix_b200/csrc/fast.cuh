@@ -232,6 +232,25 @@ __device__ __forceinline__ void cp_async16(float2* dst, const float2* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+// Hint that the 128-byte line at p is read soon: it moves into L2 without a
+// register waiting on it.
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
+// Prefetches into L2 the rows y0 .. y0 + rows - 1 (rows < ny of the unpadded
+// window, x < nx) of slice b of each field laid out like SpecArgs::in, one line
+// per thread and step, for the reflection terms a row pass reads (RF).
+template <class P>
+__device__ __forceinline__ void prefetch_refl_rows(const SpecArgs& a, long long b, int y0, int rows) {
+  const int nr = min(rows, a.d.ny - y0);
+  const int lines = (a.d.nx * 8 + 127) / 128;  // lines of one row's window
+  const float2* fs[2] = {a.rf_f1, a.rf_f2};
+  for (int f = 0; f < 2; ++f) {
+    if (!fs[f]) continue;
+    for (int i = threadIdx.x; i < nr * lines; i += blockDim.x) {
+      const int r = i / lines, l = i - r * lines;
+      prefetch_l2(fs[f] + (b * a.d.NY + y0 + r) * P::N + l * 16);
+    }
+  }
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
@@ -364,6 +383,7 @@ template <class P, int PRE, bool RF = false>
 __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_row_fwd(const SpecArgs a, int nchunk) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
+  if constexpr (RF) prefetch_refl_rows<P>(a, c.b, (int)(blockIdx.x - c.bl * nchunk) * RowGeo<P>::ROWS, RowGeo<P>::ROWS);
   // Born weights (W_SCAT_CONJ) from the per-depth table: the CTA's rows of every
   // transformed term's table copied into shared memory (cp.async) while the input
   // rows load, instead of one L2 read per sample and term in each lane.
@@ -491,9 +511,13 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
 // reflection terms of SpecArgs::rf_at 2 (separate instances, as in the forward
 // row pass).
 template <class P, int POST, bool RF = false>
-__global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 || P::E == 12) ? FWIX_ROW_MULTI_MINB : 0) k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
+__global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 || P::E == 12) ? FWIX_ROW_MULTI_MINB
+                                                                                              : (RF && POST == W_ONE ? 4 : 0))
+    k_row_inv(const SpecArgs a, int nchunk, int post_taper) {
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
+  // the reflection fields are read in the epilogue: their rows head for L2 now
+  if constexpr (RF) prefetch_refl_rows<P>(a, c.b, (int)(blockIdx.x - c.bl * nchunk) * RowGeo<P>::ROWS, RowGeo<P>::ROWS);
   // Born weights from the per-depth table: the CTA's rows of every term's table
   // are copied into shared memory (cp.async, 16 bytes a thread and instruction)
   // while the first term loads and transforms, and read from there after each
