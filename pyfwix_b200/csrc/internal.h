@@ -136,6 +136,10 @@ struct SpecArgs {
   const float2* rf_tab;
   const float2* rf_f1;
   const float2* rf_f2;
+  // register-resident row passes: each CTA hints into L2 the first input rows
+  // of the CTA pf_ctas launch positions later, the one that takes its place
+  // once every resident CTA has run (0: none)
+  int pf_ctas;
 };
 
 // Spectral passes (dispatch.cu: register-resident passes for lengths with a
