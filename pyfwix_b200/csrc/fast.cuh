@@ -372,9 +372,9 @@ struct RowCtx {
 // multi-term passes of 12- and 16-sample lanes at two (the scattering adjoint's,
 // with one term's weights and no labels, at three), the rest unhinted.
 // Compile-time occupancy knobs (defaults as measured best): resident CTAs of the
-// multi-term forward and inverse row passes and of the multi-input column pass
-// with 16-sample lanes, and whether the multi-term inverse row pass prefetches
-// the next term's row.
+// multi-term forward and inverse row passes and of the multi-input and the
+// single-input column pass with 16-sample lanes, and whether the multi-term
+// inverse row pass prefetches the next term's row.
 #ifndef FWIX_ROW_MULTI_MINB
 #define FWIX_ROW_MULTI_MINB 2
 #endif
@@ -383,6 +383,9 @@ struct RowCtx {
 #endif
 #ifndef FWIX_COLB_MINB16
 #define FWIX_COLB_MINB16 2
+#endif
+#ifndef FWIX_COLA_MINB16
+#define FWIX_COLA_MINB16 3
 #endif
 template <class P, int PRE>
 constexpr int row_fwd_min_blocks() {
@@ -730,7 +733,7 @@ struct ColGeo {
   static constexpr int kMinBlocks = P::E <= 8 ? 4 : P::E <= 16 ? FWIX_COLB_MINB16 : 1;
   // k_col_a holds one spectrum and one term in registers (k_col_b a running sum
   // as well): with 16 samples per lane it fits three CTAs per SM
-  static constexpr int kMinBlocksA = P::E <= 8 ? 4 : P::E <= 12 ? 2 : P::E <= 16 ? 3 : 1;
+  static constexpr int kMinBlocksA = P::E <= 8 ? 4 : P::E <= 12 ? 2 : P::E <= 16 ? FWIX_COLA_MINB16 : 1;
   static size_t smem2() { return ((size_t)2 * LX * LINE + tw_size<P>()) * sizeof(float2); }  // tile, tw, tile
 };
 

@@ -144,6 +144,37 @@ def test_born_broadcast_background(kind, taper, nx, ny, pad):
     assert rel(to_host(gr), gr_ref.sum(1, keepdims=True)) < TOL
 
 
+@pytest.mark.parametrize("kind", ["pspi", "nsps"])
+def test_born_broadcast_background_two_lanes(kind):
+    """The reflections inside the steps under the tuner's two-lane form (chunks of
+    slices alternating between two streams, each with its own intermediates):
+    Born forward and adjoint equal the one-launch plan's."""
+    g, rng, st, acq, p, src, rec, wav, slow, den = _acq_case(kind, taper=2, nx=64, ny=64, pad=0)
+    p.set_model(slow[:, :1].copy(), den[:, :1].copy())
+    bd = torch.empty((g.nz,) + p.wshape, dtype=torch.complex64, device="cuda")
+    bu = torch.empty_like(bd)
+    d = torch.empty((len(acq.rec.ix), g.nw), dtype=torch.complex64, device="cuda")
+    p.propagate(src, rec, to_dev(wav), d, bd, bu)
+    ms = to_dev(crandn(rng, (g.nz, 1, g.ny, g.nx)))
+    mr = to_dev(crandn(rng, (g.nz, 1, g.ny, g.nx)))
+    r = to_dev(crandn(rng, d.shape))
+
+    def run():
+        out = torch.empty_like(d)
+        p.born(rec, bd, bu, ms, mr, out)
+        gs = torch.empty_like(ms)
+        gr = torch.empty_like(ms)
+        p.born(rec, bd, bu, gs, gr, r, adjoint=True)
+        torch.cuda.synchronize()
+        return to_host(out), to_host(gs), to_host(gr)
+
+    one = run()
+    p.set_tuning(dict(col_tma=True, slices_per_launch=g.nw // 2, streams=2))
+    two = run()
+    for a, b in zip(two, one):
+        assert rel(a, b) < 1e-6
+
+
 def test_born_dot_product_device():
     """ExtendedBorn dot test (propagator/src/ExtendedBorn.h:61-128) entirely on the
     device, taper off as in born_unit_test.cpp:392-393."""
