@@ -140,6 +140,30 @@ def test_interleaved_problems_share_plan_and_blocks(checkpoint):
     fwi.clear_plan_cache()
 
 
+def test_sweeps_refuse_missing_fields():
+    """The every-depth sweeps of the C ABI refuse missing buffers (a gradient of
+    more than one level needs the up pass's derivatives) with FWIX_ERR_INVALID
+    and leave the plan usable."""
+    from pyfwix_b200 import _lib as L
+    from pyfwix_b200 import fwi
+    g, rng, s, geom, wav, par = _case(nz=3)
+    prob = fwi.SmoothFWI(s.shape, geom, wav, dict(par, checkpoint=None))
+    data = prob.model(torch.as_tensor(s.astype(np.float32)), keep=True)
+    p = prob.plan
+    dblk, ublk = prob._blocks
+    f = lambda: torch.empty(p.wshape, dtype=torch.complex64, device="cuda")
+    gpad = torch.empty((p.nz, p.NY, p.NX), dtype=torch.float32, device="cuda")
+    crefl = torch.empty((p.nz, p.ny, p.nx), dtype=torch.float32, device="cuda")
+    mus = torch.empty((p.nz,) + tuple(p.wshape), dtype=torch.complex64, device="cuda")
+    with pytest.raises(RuntimeError, match="INVALID|null"):
+        p.smooth_gradient_sweep(prob.rec, data, dblk, None, mus, f(), f(), f(), gpad, crefl)
+    with pytest.raises(RuntimeError, match="INVALID|null"):
+        p.smooth_model_sweep(prob.src, prob.rec, prob.wavelet, data, f(), f(), None)
+    grad = prob.gradient(data - data)  # zero residual: zero gradient, plan still usable
+    assert float(grad.abs().max()) == 0.0
+    fwi.clear_plan_cache()
+
+
 def test_autograd_function():
     from pyfwix_b200.fwi import FWIGradient, SmoothFWI
     g, rng, s, geom, wav, par = _case(nz=4)
