@@ -197,21 +197,20 @@ fwix_status fwix_correlate(fwix_plan* plan, const void* a, const void* b, float*
  * on one stream; fields are [ns][nw][NY][NX], field blocks [nz] (dSU [nz-1]) of
  * them.  Needs fwix_plan_set_smooth / set_refs and a model (the reflections).
  * Model sweep: data = recorded down + up fields of the source injection (zeroed
- * first); Ds[iz] = the down field at iz after injection; dSU[iz] = dS_iz(U_iz+1),
- * the slowness derivative of the up pass's step (dSU may be NULL); D, U
- * working fields. */
+ * first); Ds[iz] = the down field at iz after injection (the down recursion runs
+ * in Ds itself); dSU[iz] = dS_iz(U_iz+1), the slowness derivative of the up
+ * pass's step (dSU may be NULL); U a working field. */
 fwix_status fwix_smooth_model_sweep(fwix_plan* plan, const fwix_traces* src, const fwix_traces* rec,
-                                    const void* wavelet, void* data, void* D, void* U, void* Ds, void* dSU,
-                                    void* stream);
+                                    const void* wavelet, void* data, void* U, void* Ds, void* dSU, void* stream);
 /* Gradient sweep for the residual res [ntrace][nw]: gpad [nz][NY][NX] = the
  * slowness-derivative correlations (the padded gradient before folding the pad),
  * crefl [nz][ny][nx] = the correlations with the reflection coefficients, both
  * overwritten; Ds and dSU as the model sweep left them (dSU may be NULL only
- * when nz == 1); mus [nz] receives the mu field of every depth; mu, nu, G
- * working fields. */
+ * when nz == 1); mus [nz] receives the mu field of every depth (the mu
+ * recursion runs in it); nu, G working fields. */
 fwix_status fwix_smooth_gradient_sweep(fwix_plan* plan, const fwix_traces* rec, const void* res, const void* Ds,
-                                       const void* dSU, void* mus, void* mu, void* nu, void* G, float* gpad,
-                                       float* crefl, void* stream);
+                                       const void* dSU, void* mus, void* nu, void* G, float* gpad, float* crefl,
+                                       void* stream);
 
 /* ---- acquisition ------------------------------------------------------------ */
 /* Host coordinate arrays; ids are dense shot indices in [0, ns).  ntrace may be 0

@@ -79,8 +79,8 @@ SIGNATURES = {
     "fwix_smooth_step": [P, I, I, P, P, I, P],
     "fwix_smooth_step_pair": [P, I, P, P, P, I, P],
     "fwix_correlate": [P, P, P, P, I, I, P],
-    "fwix_smooth_model_sweep": [P, P, P, P, P, P, P, P, P, P],
-    "fwix_smooth_gradient_sweep": [P, P, P, P, P, P, P, P, P, P, P, P],
+    "fwix_smooth_model_sweep": [P, P, P, P, P, P, P, P, P],
+    "fwix_smooth_gradient_sweep": [P, P, P, P, P, P, P, P, P, P, P],
     "fwix_scatter": [P, I, I, P, P, I, P],
     "fwix_reflect": [P, I, I, P, P, I, P],
     "fwix_imaging": [P, I, P, P, P, I, P],

@@ -983,9 +983,8 @@ fwix_status fwix_reflect(fwix_plan* p, int iz, int adjoint, const void* in, void
 // down field's step below the bottom, the up field's step of the zero field
 // below the model, and the last adjoint step of nu.
 fwix_status fwix_smooth_model_sweep(fwix_plan* p, const fwix_traces* src, const fwix_traces* rec,
-                                    const void* wavelet, void* data, void* D, void* U, void* Ds, void* dSU,
-                                    void* stream) {
-  if (!p || !D || !U || !Ds || no_traces(src, wavelet) || no_traces(rec, data))
+                                    const void* wavelet, void* data, void* U, void* Ds, void* dSU, void* stream) {
+  if (!p || !U || !Ds || no_traces(src, wavelet) || no_traces(rec, data))
     return fail(FWIX_ERR_INVALID, "null argument");
   FWIX_TRY(need_smooth(p));
   FWIX_TRY(need_model(p));
@@ -993,37 +992,38 @@ fwix_status fwix_smooth_model_sweep(fwix_plan* p, const fwix_traces* src, const 
   cudaStream_t s = (cudaStream_t)stream;
   const int nz = p->desc.nz;
   const size_t wb = p->wbytes();
-  float2* d = (float2*)D;
+  const long long W = p->d.wfld;
   float2* u = (float2*)U;
   float2* ds = (float2*)Ds;
   float2* dsu = (float2*)dSU;
   if (rec->ntrace > 0) FWIX_CU(cudaMemsetAsync(data, 0, (size_t)rec->ntrace * p->d.nw * sizeof(float2), s));
-  FWIX_CU(cudaMemsetAsync(d, 0, wb, s));
+  // the down recursion runs through the stored fields themselves: level iz's
+  // step writes level iz + 1's slot (no working field, no copies)
+  FWIX_CU(cudaMemsetAsync(ds, 0, wb, s));
   for (int iz = 0; iz < nz; ++iz) {
+    float2* d = ds + iz * W;
     FWIX_TRY(do_inject(p, src, iz, (const float2*)wavelet, d, s));
     FWIX_TRY(do_record(p, rec, iz, d, (float2*)data, s));
-    FWIX_CU(cudaMemcpyAsync(ds + (long long)iz * p->d.wfld, d, wb, cudaMemcpyDeviceToDevice, s));
-    if (iz + 1 < nz) FWIX_TRY(fwix_smooth_step(p, iz, FWIX_SMOOTH_FWD, d, d, 0, s));
+    if (iz + 1 < nz) FWIX_TRY(fwix_smooth_step(p, iz, FWIX_SMOOTH_FWD, d, d + W, 0, s));
   }
   FWIX_CU(cudaMemsetAsync(u, 0, wb, s));
   for (int iz = nz - 1; iz >= 0; --iz) {
     if (iz + 1 < nz) {
       if (dsu)
-        FWIX_TRY(fwix_smooth_step_pair(p, iz, u, u, dsu + (long long)iz * p->d.wfld, 0, s));
+        FWIX_TRY(fwix_smooth_step_pair(p, iz, u, u, dsu + iz * W, 0, s));
       else
         FWIX_TRY(fwix_smooth_step(p, iz, FWIX_SMOOTH_FWD, u, u, 0, s));
     }
-    FWIX_TRY(do_reflect(p, iz, 0, ds + (long long)iz * p->d.wfld, u, 1, s));
+    FWIX_TRY(do_reflect(p, iz, 0, ds + iz * W, u, 1, s));
     FWIX_TRY(do_record(p, rec, iz, u, (float2*)data, s));
   }
   return FWIX_OK;
 }
 
 fwix_status fwix_smooth_gradient_sweep(fwix_plan* p, const fwix_traces* rec, const void* res, const void* Ds,
-                                       const void* dSU, void* mus, void* mu, void* nu, void* G, float* gpad,
-                                       float* crefl, void* stream) {
-  if (!p || !Ds || !mus || !mu || !nu || !G || !gpad || !crefl || no_traces(rec, res) ||
-      (!dSU && p->desc.nz > 1))
+                                       const void* dSU, void* mus, void* nu, void* G, float* gpad, float* crefl,
+                                       void* stream) {
+  if (!p || !Ds || !mus || !nu || !G || !gpad || !crefl || no_traces(rec, res) || (!dSU && p->desc.nz > 1))
     return fail(FWIX_ERR_INVALID, "null argument");
   FWIX_TRY(need_smooth(p));
   FWIX_TRY(need_model(p));
@@ -1035,21 +1035,21 @@ fwix_status fwix_smooth_gradient_sweep(fwix_plan* p, const fwix_traces* rec, con
   const float2* ds = (const float2*)Ds;
   const float2* dsu = (const float2*)dSU;
   const float2* r = (const float2*)res;
-  float2* m = (float2*)mu;
   float2* v = (float2*)nu;
   float2* ms = (float2*)mus;
   FWIX_CU(cudaMemsetAsync(gpad, 0, (size_t)nz * gp * sizeof(float), s));
   FWIX_CU(cudaMemsetAsync(crefl, 0, (size_t)nz * gc * sizeof(float), s));
-  // mu_iz = Rec_iz^H res + S_iz-1^H mu_iz-1, and the terms it meets at iz
-  FWIX_CU(cudaMemsetAsync(m, 0, wb, s));
+  // mu_iz = Rec_iz^H res + S_iz-1^H mu_iz-1 in its own slot of mus (each step
+  // writes the next level's slot), and the terms it meets at iz
+  FWIX_CU(cudaMemsetAsync(ms, 0, wb, s));
   for (int iz = 0; iz < nz; ++iz) {
-    if (iz > 0) FWIX_TRY(fwix_smooth_step(p, iz - 1, FWIX_SMOOTH_ADJ, m, m, 0, s));
+    float2* m = ms + iz * W;
+    if (iz > 0) FWIX_TRY(fwix_smooth_step(p, iz - 1, FWIX_SMOOTH_ADJ, m - W, m, 0, s));
     FWIX_TRY(do_inject(p, rec, iz, r, m, s));
     if (iz + 1 < nz) {
       FWIX_TRY(fwix_correlate(p, m, dsu + iz * W, gpad + iz * gp, 1, 1, s));
       FWIX_TRY(fwix_correlate(p, m, ds + iz * W, crefl + iz * gc, 1, 0, s));
     }
-    FWIX_CU(cudaMemcpyAsync(ms + iz * W, m, wb, cudaMemcpyDeviceToDevice, s));
   }
   // nu_iz = S_iz^H (nu_iz+1 + conj(R_iz) mu_iz + Rec_iz^H res), met by dS_iz(D_iz)
   FWIX_CU(cudaMemsetAsync(v, 0, wb, s));

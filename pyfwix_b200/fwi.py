@@ -270,7 +270,6 @@ class SmoothFWI:
         self._give_back()  # the fields of an earlier model() are dead
         p, nz = self.plan, self.plan.nz
         data = torch.zeros((self.ntrace, p.nw), dtype=torch.complex64, device=self.device)
-        D = self._field()
         if self.k is None:
             # one block per stored family (not nz fields), taken from the plan's pool:
             # the previous shot's block comes back whole, with no allocator traffic.
@@ -280,7 +279,7 @@ class SmoothFWI:
             # the backward, the same memory).  Both passes run as one library call.
             dblk = self._take("D", nz)
             ublk = self._take("dSU", nz - 1) if keep and nz > 1 else None
-            p.smooth_model_sweep(self.src, self.rec, self.wavelet, data, D, self._empty(), dblk, ublk)
+            p.smooth_model_sweep(self.src, self.rec, self.wavelet, data, self._empty(), dblk, ublk)
             self.Ds = list(dblk)
             self.dSU = [ublk[iz] if ublk is not None and iz + 1 < nz else None for iz in range(nz)]
             self._blocks = (dblk, ublk)
@@ -288,6 +287,7 @@ class SmoothFWI:
                 self._give_back()
             return data
         k = self.k
+        D = self._field()
         nck = -(-nz // k)
         dck, uck = self._take("Dck", nck), self._take("Uck", nck)
         self.Dck = {}
@@ -434,7 +434,7 @@ class SmoothFWI:
                 raise RuntimeError("gradient() needs model(s, keep=True) first")
             dblk, ublk = self._blocks
             mus = self._take("mu", nz)
-            p.smooth_gradient_sweep(self.rec, res, dblk, ublk, mus, self._empty(), self._empty(), G, gpad, crefl)
+            p.smooth_gradient_sweep(self.rec, res, dblk, ublk, mus, self._empty(), G, gpad, crefl)
         else:
             k = self.k
             self._res = res

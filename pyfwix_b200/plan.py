@@ -201,21 +201,22 @@ class Plan:
         L.check(self.lib.fwix_smooth_step_pair(self._h, iz, _p(inp), _p(out), _p(deriv), int(add), _stream()))
         return out, deriv
 
-    def smooth_model_sweep(self, src, rec, wavelet, data, D, U, Ds, dSU=None):
+    def smooth_model_sweep(self, src, rec, wavelet, data, U, Ds, dSU=None):
         """Every-depth modelling sweep of the smooth step (fwix_smooth_model_sweep):
-        data = recorded wavefield, Ds [nz] down fields, dSU [nz-1] (or None) the
-        up pass's step derivatives; D, U working fields."""
+        data = recorded wavefield, Ds [nz] down fields (the recursion runs in
+        them), dSU [nz-1] (or None) the up pass's step derivatives; U a working
+        field."""
         self.ensure_workspace(L.WS_STEP)
-        L.check(self.lib.fwix_smooth_model_sweep(self._h, src._h, rec._h, _p(wavelet), _p(data), _p(D), _p(U),
-                                                 _p(Ds), _p(dSU), _stream()))
+        L.check(self.lib.fwix_smooth_model_sweep(self._h, src._h, rec._h, _p(wavelet), _p(data), _p(U), _p(Ds),
+                                                 _p(dSU), _stream()))
 
-    def smooth_gradient_sweep(self, rec, res, Ds, dSU, mus, mu, nu, G, gpad, crefl):
+    def smooth_gradient_sweep(self, rec, res, Ds, dSU, mus, nu, G, gpad, crefl):
         """Every-depth gradient sweep (fwix_smooth_gradient_sweep): gpad [nz][NY][NX]
         and crefl [nz][ny][nx] (float) overwritten with the correlations; mus [nz]
-        receives the mu fields; mu, nu, G working fields."""
+        receives the mu fields (the recursion runs in them); nu, G working fields."""
         self.ensure_workspace(L.WS_STEP)
-        L.check(self.lib.fwix_smooth_gradient_sweep(self._h, rec._h, _p(res), _p(Ds), _p(dSU), _p(mus), _p(mu),
-                                                    _p(nu), _p(G), _p(gpad), _p(crefl), _stream()))
+        L.check(self.lib.fwix_smooth_gradient_sweep(self._h, rec._h, _p(res), _p(Ds), _p(dSU), _p(mus), _p(nu),
+                                                    _p(G), _p(gpad), _p(crefl), _stream()))
 
     def correlate(self, a, b, out, add=False, padded=True):
         """out (+)= Re sum_{shots, w} conj(a) b, [NY][NX] (padded) or [ny][nx]."""

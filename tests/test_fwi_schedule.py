@@ -86,17 +86,16 @@ class OraclePlan:
         f = wem.reflect_adjoint if adjoint else wem.reflect_forward
         return _put(out, f(self.g, self.s2, self.den, iz, _np(inp), _np(out)))
 
-    def smooth_model_sweep(self, src, rec, wavelet, data, D, U, Ds, dSU=None):
+    def smooth_model_sweep(self, src, rec, wavelet, data, U, Ds, dSU=None):
         """The level loops of fwix_smooth_model_sweep on this stand-in's operators."""
         nz = self.nz
         data.zero_()
-        D.zero_()
+        Ds[0].zero_()
         for iz in range(nz):
-            self.inject(src, iz, wavelet, D)
-            self.inject(rec, iz, data, D, adjoint=True)
-            Ds[iz].copy_(D)
+            self.inject(src, iz, wavelet, Ds[iz])
+            self.inject(rec, iz, data, Ds[iz], adjoint=True)
             if iz + 1 < nz:
-                self.smooth_step(iz, D, D)
+                self.smooth_step(iz, Ds[iz], Ds[iz + 1])
         U.zero_()
         for iz in range(nz - 1, -1, -1):
             if iz + 1 < nz:
@@ -107,20 +106,19 @@ class OraclePlan:
             self.reflect(iz, Ds[iz], U, add=True)
             self.inject(rec, iz, data, U, adjoint=True)
 
-    def smooth_gradient_sweep(self, rec, res, Ds, dSU, mus, mu, nu, G, gpad, crefl):
+    def smooth_gradient_sweep(self, rec, res, Ds, dSU, mus, nu, G, gpad, crefl):
         """The level loops of fwix_smooth_gradient_sweep on this stand-in's operators."""
         nz = self.nz
         gpad.zero_()
         crefl.zero_()
-        mu.zero_()
+        mus[0].zero_()
         for iz in range(nz):
             if iz > 0:
-                self.smooth_step(iz - 1, mu, mu, mode=L.SMOOTH_ADJ)
-            self.inject(rec, iz, res, mu)
+                self.smooth_step(iz - 1, mus[iz - 1], mus[iz], mode=L.SMOOTH_ADJ)
+            self.inject(rec, iz, res, mus[iz])
             if iz + 1 < nz:
-                self.correlate(mu, dSU[iz], gpad[iz], add=True, padded=True)
-                self.correlate(mu, Ds[iz], crefl[iz], add=True, padded=False)
-            mus[iz].copy_(mu)
+                self.correlate(mus[iz], dSU[iz], gpad[iz], add=True, padded=True)
+                self.correlate(mus[iz], Ds[iz], crefl[iz], add=True, padded=False)
         nu.zero_()
         for iz in range(nz - 1, -1, -1):
             if iz + 1 < nz:

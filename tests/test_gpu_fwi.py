@@ -156,9 +156,9 @@ def test_sweeps_refuse_missing_fields():
     crefl = torch.empty((p.nz, p.ny, p.nx), dtype=torch.float32, device="cuda")
     mus = torch.empty((p.nz,) + tuple(p.wshape), dtype=torch.complex64, device="cuda")
     with pytest.raises(RuntimeError, match="INVALID|null"):
-        p.smooth_gradient_sweep(prob.rec, data, dblk, None, mus, f(), f(), f(), gpad, crefl)
+        p.smooth_gradient_sweep(prob.rec, data, dblk, None, mus, f(), f(), gpad, crefl)
     with pytest.raises(RuntimeError, match="INVALID|null"):
-        p.smooth_model_sweep(prob.src, prob.rec, prob.wavelet, data, f(), f(), None)
+        p.smooth_model_sweep(prob.src, prob.rec, prob.wavelet, data, f(), None)
     grad = prob.gradient(data - data)  # zero residual: zero gradient, plan still usable
     assert float(grad.abs().max()) == 0.0
     fwi.clear_plan_cache()
