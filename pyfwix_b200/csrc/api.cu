@@ -1046,10 +1046,10 @@ fwix_status fwix_smooth_gradient_sweep(fwix_plan* p, const fwix_traces* rec, con
     float2* m = ms + iz * W;
     if (iz > 0) FWIX_TRY(fwix_smooth_step(p, iz - 1, FWIX_SMOOTH_ADJ, m - W, m, 0, s));
     FWIX_TRY(do_inject(p, rec, iz, r, m, s));
-    if (iz + 1 < nz) {
-      FWIX_TRY(fwix_correlate(p, m, dsu + iz * W, gpad + iz * gp, 1, 1, s));
-      FWIX_TRY(fwix_correlate(p, m, ds + iz * W, crefl + iz * gc, 1, 0, s));
-    }
+    if (iz + 1 < nz)  // mu meets dS_iz(U_iz+1) and D_iz in one pass over mu
+      FWIX_TRY(cu(fwix::launch_correlate2_padded(p->d, m, dsu + iz * W, ds + iz * W, gpad + iz * gp, crefl + iz * gc,
+                                                 1, s),
+                  "correlate"));
   }
   // nu_iz = S_iz^H (nu_iz+1 + conj(R_iz) mu_iz + Rec_iz^H res), met by dS_iz(D_iz)
   FWIX_CU(cudaMemsetAsync(v, 0, wb, s));

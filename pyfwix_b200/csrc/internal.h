@@ -209,6 +209,10 @@ cudaError_t launch_image_acc(const Dims& d, const float2* S, const float2* R, fl
 // img[y][x] (+)= Re sum_{s,w} conj(S) R over the padded NY x NX slice.
 cudaError_t launch_correlate_padded(const Dims& d, const float2* S, const float2* R, float* img, int add,
                                     cudaStream_t s);
+// Both at once for one field S: img1 [NY][NX] (+)= Re sum conj(S) R1 over the
+// padded slice, img2 [ny][nx] (+)= Re sum conj(S) R2 over the model window.
+cudaError_t launch_correlate2_padded(const Dims& d, const float2* S, const float2* R1, const float2* R2,
+                                     float* img1, float* img2, int add, cudaStream_t s);
 cudaError_t launch_axpy(long long n, const float2* x, float2* y, cudaStream_t s);
 // Fixed-rate lossy wavefield store (pack.cu): bytes of one packed array of nfloat
 // floats, and the packing / unpacking launches.

@@ -333,6 +333,37 @@ __global__ void __launch_bounds__(kCells * kGroups)
   if (threadIdx.y == 0 && c.ok) img[c.yx] = add ? img[c.yx] + acc[0].x : acc[0].x;
 }
 
+// Two correlations of one field S in one pass over the padded window (the
+// caller's Dims widened to NY x NX): img1[y][x] (+)= Re sum conj(S) R1 there, and
+// img2[y][x] (+)= Re sum conj(S) R2 over the model window ny2 x nx2.
+template <bool S1>
+__global__ void __launch_bounds__(kCells * kGroups)
+    k_image_acc2(Dims d, int ny2, int nx2, const float2* __restrict__ S, const float2* __restrict__ R1,
+                 const float2* __restrict__ R2, float* __restrict__ img1, float* __restrict__ img2, int add) {
+  const Cell c = this_cell(d);
+  float2 acc[1] = {make_float2(0.f, 0.f)};
+  const int ns = S1 ? 1 : d.ns;
+  const bool in2 = c.ok && c.y < ny2 && c.x < nx2;
+#pragma unroll 4
+  for (int iw = threadIdx.y; c.ok && iw < d.nw; iw += kGroups)
+    for (int s = 0; s < ns; ++s) {
+      const long long k = wf_index(d, s, iw, c);
+      const float2 a = S[k], b = R1[k];
+      acc[0].x += a.x * b.x + a.y * b.y;
+      if (in2) {
+        const float2 e = R2[k];
+        acc[0].y += a.x * e.x + a.y * e.y;
+      }
+    }
+  reduce_groups<1>(acc);
+  if (threadIdx.y != 0 || !c.ok) return;
+  img1[c.yx] = add ? img1[c.yx] + acc[0].x : acc[0].x;
+  if (in2) {
+    float* o = img2 + (long long)c.y * nx2 + c.x;
+    *o = add ? *o + acc[0].y : acc[0].y;
+  }
+}
+
 __global__ void k_axpy(long long n, const float2* __restrict__ x, float2* __restrict__ y) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -498,6 +529,21 @@ cudaError_t launch_correlate_padded(const Dims& d, const float2* S, const float2
     k_image_acc<true><<<cell_blocks(full), dim3(kCells, kGroups), 0, s>>>(full, S, R, img, add);
   else
     k_image_acc<false><<<cell_blocks(full), dim3(kCells, kGroups), 0, s>>>(full, S, R, img, add);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_correlate2_padded(const Dims& d, const float2* S, const float2* R1, const float2* R2,
+                                     float* img1, float* img2, int add, cudaStream_t s) {
+  Dims full = d;  // the padded slice; img2 covers the model window d.ny x d.nx
+  full.nx = d.NX;
+  full.ny = d.NY;
+  if (d.ns == 1)
+    k_image_acc2<true><<<cell_blocks(full), dim3(kCells, kGroups), 0, s>>>(full, d.ny, d.nx, S, R1, R2, img1, img2,
+                                                                           add);
+  else
+    k_image_acc2<false><<<cell_blocks(full), dim3(kCells, kGroups), 0, s>>>(full, d.ny, d.nx, S, R1, R2, img1,
+                                                                            img2, add);
   count_launch();
   return cudaGetLastError();
 }
