@@ -48,7 +48,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from . import refsampler
+from . import hostcopy, refsampler
 from .plan import Plan
 from .vectors import Axis, Hypercube, SuperVector, Vector
 
@@ -109,6 +109,9 @@ def _dev(x, device, shape=None, zero=False):
         return t
     if zero:
         return torch.zeros(tuple(np.shape(t)) if shape is None else shape, dtype=torch.complex64, device=device)
+    h = hostcopy.host_view(t)
+    if h is not None:
+        return hostcopy.to_device(h, device)
     t = torch.as_tensor(t)
     if not t.is_complex():
         t = t.to(torch.float32)
@@ -119,7 +122,10 @@ def _store(dst, t):
     """Copy a device result back into the caller's object when it is not the
     same memory."""
     raw = _raw(dst)
-    if isinstance(raw, torch.Tensor):
+    h = hostcopy.host_view(raw) if t.is_cuda else None
+    if h is not None and h.flags.writeable:
+        hostcopy.to_host(t, h)                 # staged through pinned buffers
+    elif isinstance(raw, torch.Tensor):
         if raw.data_ptr() != t.data_ptr() or raw.device != t.device:
             raw.copy_(t.reshape(raw.shape))
     elif isinstance(raw, np.ndarray):

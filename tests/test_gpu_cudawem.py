@@ -345,3 +345,41 @@ def test_compress_rate_packed_backgrounds():
     assert rel(g3[0].arr.numpy(), g1[0].arr.numpy()) < 1e-3
     with pytest.raises(ValueError):
         CudaWEM.Propagator(model, data_c, wav, _par(g, compress_rate=4), geom).forward(False, model, data_c)
+
+
+def test_staged_host_copies(monkeypatch):
+    """Large host operands cross the host link through pinned staging buffers
+    (pyfwix_b200.hostcopy: chunks, two buffers, host copies on a thread pool):
+    the round trip is exact for a length that is no multiple of the chunk, and a
+    Born forward + adjoint through the surface with every operand staged equals
+    the plain copies bit for bit."""
+    from pyfwix_b200 import hostcopy
+    monkeypatch.setattr(hostcopy, "CHUNK_BYTES", 4096 + 24)
+    monkeypatch.setattr(hostcopy, "THRESHOLD_BYTES", 1)
+    rng = np.random.default_rng(3)
+    n = 100003
+    a = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    t = hostcopy.to_device(a, torch.device("cuda"))
+    assert np.array_equal(t.cpu().numpy(), a)
+    b = np.empty_like(a)
+    hostcopy.to_host(t * 2, b)
+    assert np.array_equal(b, 2 * a)
+    assert hostcopy.host_view(torch.from_numpy(a)) is not None
+
+    def born_run():
+        g, rng2, s2, den, model, geom, wav, data, prop = _born_setup("nsps")
+        prop.forward(False, model, data)
+        dm = [crandn(rng2, s2.shape).astype(np.complex64) * 1e-3, crandn(rng2, s2.shape).astype(np.complex64) * 1e-2]
+        born = CudaWEM.ExtendedBorn(dm, data, model, prop)
+        d1 = np.zeros_like(data)
+        born.forward(False, dm, d1)
+        gs, gr = np.zeros_like(dm[0]), np.zeros_like(dm[1])
+        born.adjoint(False, [gs, gr], d1)
+        torch.cuda.synchronize()
+        return d1, gs, gr
+
+    staged = born_run()
+    monkeypatch.setattr(hostcopy, "THRESHOLD_BYTES", 1 << 62)
+    plain = born_run()
+    for x, y in zip(staged, plain):
+        assert np.array_equal(x, y)
