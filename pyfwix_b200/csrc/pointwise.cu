@@ -120,11 +120,8 @@ __global__ void __launch_bounds__(kCells * kGroups)
 
 // image[w, y, x] (+)= sum_s conj(bg) wfld; with wsum the frequencies are summed as well
 // into image[y, x].
-#ifndef FWIX_CELL_SUM_MINB
-#define FWIX_CELL_SUM_MINB 0
-#endif
 template <bool S1>
-__global__ void __launch_bounds__(kCells * kGroups, S1 ? FWIX_CELL_SUM_MINB : 0)
+__global__ void __launch_bounds__(kCells * kGroups)
     k_ic_adj(Dims d, const float2* __restrict__ bg, const float2* __restrict__ wfld, float2* __restrict__ image,
              int add, int wsum) {
   const Cell c = this_cell(d);
@@ -180,7 +177,7 @@ __device__ __forceinline__ LinCoef lin_coef(float2 s0, float2 s1, float2 r0, flo
 // imaging-condition adjoint of another pair, dm0 += sum conj(bg2) wf2, so that
 // one read of the four fields serves both frequency sums of a level.
 template <bool IC, bool S1, bool IC2>
-__global__ void __launch_bounds__(kCells * kGroups, S1 && IC2 ? FWIX_CELL_SUM_MINB : 0)
+__global__ void __launch_bounds__(kCells * kGroups)
     k_lin_reflect(Dims d, int adjoint, const float2* __restrict__ s0, const float2* __restrict__ s1,
                   const float2* __restrict__ r0, const float2* __restrict__ r1, long long mw, float2* dm0,
                   float2* dm1, float2* dm2, float2* dm3, long long dm_w, float2* dr, int add,
