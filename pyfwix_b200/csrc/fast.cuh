@@ -265,6 +265,15 @@ __device__ __forceinline__ void prefetch_refl_rows(const SpecArgs& a, long long 
     }
   }
 }
+// The same for the whole padded rows y0 .. y0 + rows - 1 (< NY) of slice b of
+// one field laid out like SpecArgs::in (the direct term of W_ONE_DIRECT).
+template <class P>
+__device__ __forceinline__ void prefetch_full_rows(const SpecArgs& a, const float2* f, long long b, int y0,
+                                                   int rows) {
+  const int nr = min(rows, a.d.NY - y0);
+  for (int i = threadIdx.x; i < nr * (P::N / 16); i += blockDim.x)
+    prefetch_l2(f + (b * a.d.NY + y0) * P::N + 16LL * i);
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
@@ -444,6 +453,20 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
       }
     }
   }
+  if constexpr (PRE == W_IC) {
+    // the image values load beside the background's samples (one wait for
+    // both) and weight them here; the term loop takes the products as they are
+    float2 im[P::E];
+    const bool rowin = c.live && c.y < a.d.ny;
+    const float2* irow = a.image + (long long)c.iw * a.img_w + (long long)(rowin ? c.y : 0) * a.d.nx;
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) {
+      const int x = pos_first<P>(c.t, e);
+      im[e] = rowin && x < a.d.nx ? irow[x] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int e = 0; e < P::E; ++e) raw[e] = cmul(raw[e], im[e]);
+  }
   const int nterm = multi_term(PRE) ? a.nterm : 1;
   Labels<P::E> lab;
   if (PRE == W_MASK) {
@@ -508,6 +531,8 @@ __global__ void __launch_bounds__(kWarps * 32, row_fwd_min_blocks<P, PRE>()) k_r
       for (int e = 0; e < P::E; ++e) {
         if (PRE == W_MASK)
           v[e] = lab.get(e) == term ? raw[e] : make_float2(0.f, 0.f);
+        else if (PRE == W_IC)
+          v[e] = c.live ? raw[e] : make_float2(0.f, 0.f);  // weighted at the load
         else
           v[e] = c.live ? row_weight<PRE>(a, term, c.iw, c.y, pos_first<P>(c.t, e), raw[e]) : make_float2(0.f, 0.f);
       }
@@ -535,8 +560,12 @@ __global__ void __launch_bounds__(kWarps * 32, multi_term(POST) && (P::E == 16 |
   extern __shared__ float2 smem[];
   RowCtx<P> c(a, smem, nchunk);
   prefetch_next_ctas<P::N, RowGeo<P>::ROWS>(a, a.t2, true, nchunk);  // the first term of a later CTA
-  // the reflection fields are read in the epilogue: their rows head for L2 now
+  // the reflection fields (the direct term's field) are read in the epilogue:
+  // their rows head for L2 now
   if constexpr (RF) prefetch_refl_rows<P>(a, c.b, (int)(blockIdx.x - c.bl * nchunk) * RowGeo<P>::ROWS, RowGeo<P>::ROWS);
+  if constexpr (POST == W_ONE_DIRECT)
+    if (a.direct)
+      prefetch_full_rows<P>(a, a.direct, c.b, (int)(blockIdx.x - c.bl * nchunk) * RowGeo<P>::ROWS, RowGeo<P>::ROWS);
   // Born weights from the per-depth table: the CTA's rows of every term's table
   // are copied into shared memory (cp.async, 16 bytes a thread and instruction)
   // while the first term loads and transforms, and read from there after each
